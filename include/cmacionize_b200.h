@@ -1,0 +1,228 @@
+/*
+ * cmacionize_b200.h -- C ABI of the B200 photon-packet transport and
+ * ionization-balance library (libcmacionize_b200.so).
+ *
+ * This is the drop-in boundary for the plain photoionization method of
+ * ParallelCMacIonize.  The reference has no plugin or FFI layer; its de-facto
+ * boundary is three C++ calls, each mapped here:
+ *
+ *   DensitySubGrid::interact(Photon&, int)          DensitySubGrid.hpp:1180
+ *       -> cmi_trace_packet (one packet, with its cell sequence)
+ *   do_photon_traversal(PhotonBuffer&, DensitySubGrid&, PhotonBuffer*, bool*)
+ *                                                  testDensitySubGrid_omp.cpp:607
+ *       -> cmi_traverse_buffer
+ *   DensitySubGrid::compute_neutral_fraction(double, unsigned int)
+ *                                                  DensitySubGrid.hpp:1628
+ *       -> cmi_compute_neutral_fraction
+ *
+ * plus the whole shoot-packets -> solve-balance iteration of the driver's
+ * main loop (testDensitySubGrid_omp.cpp:2213-2434) as cmi_run_iterations.
+ *
+ * Conventions: every entry point returns an int status (CMI_OK = 0); no
+ * exception crosses the ABI; cmi_last_error_string() describes the last
+ * failure of the calling thread.  A context owns all of its device memory and
+ * is used by one host thread at a time.  Field arrays are FP64, one value per
+ * cell, in one of two orders (cmi_layout).  All pointers are host pointers
+ * unless a function says otherwise.
+ */
+#ifndef CMACIONIZE_B200_H
+#define CMACIONIZE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMI_ABI_VERSION 1
+#define CMI_NUM_DIRECTIONS 27           /* TRAVELDIRECTION_NUMBER, TravelDirections.hpp:74 */
+#define CMI_NEIGHBOUR_OUTSIDE 0xffffffffu /* NEIGHBOUR_OUTSIDE, DensitySubGrid.hpp:53 */
+#define CMI_PHOTONBUFFER_SIZE 200       /* PHOTONBUFFER_SIZE, PhotonBuffer.hpp:42 */
+
+/* status codes */
+enum cmi_status {
+  CMI_OK = 0,
+  CMI_ERR_INVALID_ARGUMENT = 1,
+  CMI_ERR_CUDA = 2,
+  CMI_ERR_OUT_OF_MEMORY = 3,
+  CMI_ERR_CAPACITY = 4,       /* a device queue or buffer would overflow */
+  CMI_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up */
+  CMI_ERR_INVARIANT = 6,      /* a device-side invariant check failed */
+  CMI_ERR_NOT_SUPPORTED = 7
+};
+
+/* One photon packet.  Same 80-byte layout and field order as the reference
+ * Photon (Photon.hpp:49-68): position (m), unit direction, target optical
+ * depth, photoionization cross section (m^2), weight, packet type. */
+typedef struct {
+  double position[3];
+  double direction[3];
+  double target_optical_depth;
+  double photoionization_cross_section;
+  double weight;
+  int32_t type;
+  int32_t reserved;
+} cmi_photon;
+
+/* One grid instance: a box cut into num_subgrid[0..2] subgrids of equal size
+ * (testDensitySubGrid_omp.cpp:1801-1877).  ncell must be a multiple of
+ * num_subgrid on every axis. */
+typedef struct {
+  double box[6];              /* anchor x y z, side lengths x y z (m) */
+  int32_t ncell[3];           /* cells per axis, whole grid */
+  int32_t num_subgrid[3];     /* subgrids per axis */
+  double recombination_rate;  /* alpha_H (m^3/s); reference: 4e-19 (DensitySubGrid.hpp:1637) */
+  double cross_section;       /* sigma (m^2); reference: 6.3e-22 (testDensitySubGrid_omp.cpp:589) */
+} cmi_grid_desc;
+
+enum cmi_precision {
+  CMI_TRANSPORT_FP64 = 0, /* the reference's FP64 walk, operation for operation */
+  CMI_TRANSPORT_FP32 = 1  /* FP32 cell-unit walk, compensated FP32 tallies merged into FP64 */
+};
+enum cmi_balance_form {
+  CMI_BALANCE_REFERENCE = 0, /* x = 1 + a(1 - sqrt(2/a + 1)), DensitySubGrid.hpp:1650 */
+  CMI_BALANCE_STABLE = 1     /* x = 1 / (1 + a + sqrt(a(a + 2))), same value, no cancellation */
+};
+enum cmi_rng {
+  CMI_RNG_PHILOX = 0, /* counter-based Philox4x32-10 per packet */
+  CMI_RNG_RANLUX = 1  /* the reference's ranlxd, one stream per 200-packet buffer */
+};
+enum cmi_layout {
+  CMI_LAYOUT_BLOCKED = 0, /* subgrid after subgrid, each in DensitySubGrid order (reference output order) */
+  CMI_LAYOUT_CUBE = 1     /* whole grid, index (ix * ny + iy) * nz + iz */
+};
+enum cmi_memory {
+  CMI_MEMORY_HOST = 0,
+  CMI_MEMORY_DEVICE = 1
+};
+
+typedef struct {
+  int32_t transport_precision; /* cmi_precision */
+  int32_t balance_form;        /* cmi_balance_form */
+  int32_t rng;                 /* cmi_rng */
+  int32_t device;              /* CUDA device ordinal */
+  int32_t threads_per_cta;     /* 0 = library default (256) */
+  int32_t ctas_per_sm;         /* 0 = as many as fit */
+  int32_t packets_per_chunk;   /* 0 = library default (4096) */
+  int32_t compensated_tally;   /* FP32 mode: 1 = hi/lo compensated smem tallies (default), 0 = plain */
+  int32_t use_graph;           /* 1 = capture each iteration as a CUDA graph (default) */
+  int32_t reserved[7];
+} cmi_options;
+
+/* Per-instance counters of one iteration. */
+typedef struct {
+  uint64_t packets_emitted;
+  uint64_t packets_absorbed;
+  uint64_t packets_escaped;
+  uint64_t cell_crossings;   /* iterations of the interact loop, DensitySubGrid.hpp:1221 */
+  uint64_t subgrid_transits; /* calls of interact */
+  double mean_abs_dx;        /* mean |x_new - x_old| over the cells of the instance */
+  uint32_t error_flags;      /* CMI_FLAG_* bits raised on the device */
+  uint32_t rounds;           /* wavefront rounds that carried packets */
+} cmi_stats;
+
+#define CMI_FLAG_ARENA_OVERFLOW 1u
+#define CMI_FLAG_STAGE_TIMEOUT 2u
+#define CMI_FLAG_WALK_LIMIT 4u     /* a transit exceeded its step bound (NaN direction, ...) */
+#define CMI_FLAG_LEFTOVER 8u       /* packets left after the last round */
+#define CMI_FLAG_BAD_INPUT 16u
+
+typedef struct cmi_context cmi_context;
+
+void cmi_default_options(cmi_options *options);
+const char *cmi_last_error_string(void);
+int cmi_abi_version(void);
+
+/* Create a context holding num_instances independent grids (a batch of one
+ * is the plain method).  Fields start as n_H = 1e8 m^-3 and x_H = 1e-6, the
+ * reference's initial state (DensitySubGrid.hpp:544-551). */
+int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_options *options,
+               cmi_context **context);
+int cmi_destroy(cmi_context *context);
+
+/* Copy n_H (m^-3) and/or x_H into an instance; either pointer may be NULL. */
+int cmi_set_fields(cmi_context *context, int32_t instance, int32_t layout, int32_t memory,
+                   const double *number_density, const double *neutral_fraction);
+/* Read x_H and/or the intensity integral J (m^3); either pointer may be NULL. */
+int cmi_get_fields(cmi_context *context, int32_t instance, int32_t layout, int32_t memory,
+                   double *neutral_fraction, double *intensity_integral);
+/* Overwrite the intensity integrals (e.g. to merge tallies of other processes). */
+int cmi_set_intensity(cmi_context *context, int32_t instance, int32_t layout, int32_t memory,
+                      const double *intensity_integral);
+
+/* Point sources of an instance (Source.hpp:34-109): positions (3 per source,
+ * m) and ionizing luminosities (s^-1). */
+int cmi_set_sources(cmi_context *context, int32_t instance, const double *positions,
+                    const double *luminosities, int32_t num_sources);
+/* Packets emitted per iteration by an instance (num_photon). */
+int cmi_set_packet_budget(cmi_context *context, int32_t instance, uint64_t num_photon);
+
+/* Run whole iterations of the plain method on every instance: emit the
+ * packets, trace them to absorption or escape, solve the ionization balance
+ * (testDensitySubGrid_omp.cpp:2213-2434).  stats receives num_iterations x
+ * num_instances records (iteration-major) and may be NULL. */
+int cmi_run_iterations(cmi_context *context, int32_t num_iterations, uint64_t seed,
+                       cmi_stats *stats);
+/* Transport phase only (no balance); J keeps accumulating. */
+int cmi_shoot_packets(cmi_context *context, uint64_t seed, uint32_t iteration, cmi_stats *stats);
+
+/* Trace caller-supplied packets through an instance until absorption or
+ * escape (the driver's task loop for a given packet list).  start_subgrid[i]
+ * is the subgrid that contains packet i; every packet starts INSIDE it. */
+int cmi_transport_packets(cmi_context *context, int32_t instance, const cmi_photon *packets,
+                          const uint32_t *start_subgrid, uint64_t num_packets, cmi_stats *stats);
+
+/* do_photon_traversal (testDensitySubGrid_omp.cpp:607-666): walk every photon
+ * of one buffer through one subgrid, entering from input_direction, and sort
+ * the results into the 27 TravelDirection output buffers.  out receives the
+ * updated photons grouped by output direction (direction-major, input order
+ * inside a group), out_count[d] the size of group d.  Groups whose
+ * output_enabled[d] is 0 are dropped and counted in *num_done (NULL enables
+ * all 27).  The walk tallies into the subgrid's J. */
+int cmi_traverse_buffer(cmi_context *context, int32_t instance, uint32_t subgrid,
+                        int32_t input_direction, const cmi_photon *in, uint32_t num_photons,
+                        const uint8_t *output_enabled, cmi_photon *out,
+                        uint32_t out_count[CMI_NUM_DIRECTIONS], uint32_t *num_done);
+
+/* DensitySubGrid::interact (DensitySubGrid.hpp:1180-1323) for one packet,
+ * with its cell sequence: cells[k] is the subgrid-local cell index of loop
+ * iteration k and lengths[k] its path length lmin (m).  *num_steps receives
+ * the full count even when it exceeds max_steps.  *photon is updated and
+ * *output_direction receives the exit TravelDirection. */
+int cmi_trace_packet(cmi_context *context, int32_t instance, uint32_t subgrid,
+                     int32_t input_direction, cmi_photon *photon, int32_t max_steps,
+                     int32_t *cells, double *lengths, int32_t *num_steps,
+                     int32_t *output_direction);
+
+/* compute_neutral_fraction (DensitySubGrid.hpp:1628-1658) on every cell of
+ * an instance with the given total luminosity and packet count; resets J. */
+int cmi_compute_neutral_fraction(cmi_context *context, int32_t instance, double luminosity,
+                                 uint64_t num_photon, double *mean_abs_dx);
+
+/* Device-side access for interop (zero-copy views, NCCL reductions): the
+ * instance's J (which = 0), x_H (1) or n_H (2) array in BLOCKED layout, and
+ * the CUDA stream every kernel of the context runs on. */
+int cmi_device_field(cmi_context *context, int32_t instance, int32_t which, double **device_ptr,
+                     uint64_t *count);
+int cmi_get_stream(cmi_context *context, void **cuda_stream);
+int cmi_synchronize(cmi_context *context);
+
+/* Kernel launches issued by the most recent cmi_run_iterations /
+ * cmi_shoot_packets call (graph replays count their kernel nodes). */
+int cmi_last_launch_count(cmi_context *context, uint64_t *launches);
+
+/* Per-kernel timing with CUDA events on the context's stream.  While enabled,
+ * iterations are launched kernel by kernel (no graph) with an event pair
+ * around every launch; cmi_kernel_timing returns the summed device time (ms)
+ * and launch count of each kernel class since the last call:
+ * [0] walk, [1] plan + scatter, [2] emission, [3] balance. */
+#define CMI_KERNEL_CLASSES 4
+int cmi_set_kernel_timing(cmi_context *context, int32_t enable);
+int cmi_kernel_timing(cmi_context *context, double milliseconds[CMI_KERNEL_CLASSES],
+                      uint64_t launches[CMI_KERNEL_CLASSES]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CMACIONIZE_B200_H */

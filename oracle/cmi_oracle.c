@@ -1,0 +1,800 @@
+/*
+ * CPU oracle: plain-C restatement of the reference photon transport and
+ * ionization balance (bwvdnbro/ParallelCMacIonize).  TEST INFRASTRUCTURE:
+ * only tests/, the smoke check and bench.py's CPU-baseline leg load this.
+ *
+ * Build: oracle/Makefile  (-O2 -ffp-contract=off, no -ffast-math, so every
+ * FP64 operation happens in the order written and is rounded once).
+ *
+ * Each function cites the reference file:line whose behaviour it restates.
+ */
+#include "cmi_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* TravelDirections (TravelDirections.hpp:46-403).                           */
+/* Every direction is a triple of axis signs: +1 = upper (P) face of that    */
+/* axis, -1 = lower (N) face, 0 = axis not involved.                         */
+/* ------------------------------------------------------------------------ */
+static const signed char kSigns[CMIO_NUM_DIRECTIONS][3] = {
+    {0, 0, 0},                                                  /* INSIDE */
+    {1, 1, 1},   {1, 1, -1},  {1, -1, 1},  {1, -1, -1},         /* CORNER_P.. */
+    {-1, 1, 1},  {-1, 1, -1}, {-1, -1, 1}, {-1, -1, -1},        /* CORNER_N.. */
+    {0, 1, 1},   {0, 1, -1},  {0, -1, 1},  {0, -1, -1},         /* EDGE_X_yz */
+    {1, 0, 1},   {1, 0, -1},  {-1, 0, 1},  {-1, 0, -1},         /* EDGE_Y_xz */
+    {1, 1, 0},   {1, -1, 0},  {-1, 1, 0},  {-1, -1, 0},         /* EDGE_Z_xy */
+    {1, 0, 0},   {-1, 0, 0},  {0, 1, 0},   {0, -1, 0},          /* FACE_X/Y */
+    {0, 0, 1},   {0, 0, -1}};                                   /* FACE_Z */
+
+static int direction_from_signs(int sx, int sy, int sz) {
+  for (int d = 0; d < CMIO_NUM_DIRECTIONS; ++d) {
+    if (kSigns[d][0] == sx && kSigns[d][1] == sy && kSigns[d][2] == sz) {
+      return d;
+    }
+  }
+  return -1;
+}
+
+/* TravelDirections.hpp:89-152: swap every P for N. */
+int cmio_output_to_input_direction(int output_direction) {
+  if (output_direction < 0 || output_direction >= CMIO_NUM_DIRECTIONS) {
+    return -1;
+  }
+  const signed char *s = kSigns[output_direction];
+  return direction_from_signs(-s[0], -s[1], -s[2]);
+}
+
+/* TravelDirections.hpp:315-403: bits (x_high,x_low,y_high,y_low,z_high,z_low). */
+int cmio_direction_from_mask(int mask) {
+  if (mask < 0 || mask > 63) {
+    return -1;
+  }
+  int s[3];
+  for (int a = 0; a < 3; ++a) {
+    const int high = (mask >> (5 - 2 * a)) & 1;
+    const int low = (mask >> (4 - 2 * a)) & 1;
+    if (high && low) {
+      return -1;
+    }
+    s[a] = high ? 1 : (low ? -1 : 0);
+  }
+  return direction_from_signs(s[0], s[1], s[2]);
+}
+
+/* TravelDirections.hpp:163-224 (leaving moves along the face's sign). */
+int cmio_is_compatible_output_direction(const double *direction, int output_direction) {
+  if (output_direction < 0 || output_direction >= CMIO_NUM_DIRECTIONS) {
+    return 0;
+  }
+  for (int a = 0; a < 3; ++a) {
+    const int s = kSigns[output_direction][a];
+    if ((s > 0 && !(direction[a] > 0.)) || (s < 0 && !(direction[a] < 0.))) {
+      return 0;
+    }
+  }
+  return 1;
+}
+
+/* TravelDirections.hpp:235-298 (entering moves against the face's sign). */
+int cmio_is_compatible_input_direction(const double *direction, int input_direction) {
+  if (input_direction < 0 || input_direction >= CMIO_NUM_DIRECTIONS) {
+    return 0;
+  }
+  for (int a = 0; a < 3; ++a) {
+    const int s = kSigns[input_direction][a];
+    if ((s > 0 && !(direction[a] < 0.)) || (s < 0 && !(direction[a] > 0.))) {
+      return 0;
+    }
+  }
+  return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* DensitySubGrid geometry.                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* DensitySubGrid.hpp:516-527 (constructor initialiser list). */
+void cmio_subgrid_init(cmio_subgrid *sg, const double box[6], const int32_t ncell[3]) {
+  for (int a = 0; a < 3; ++a) {
+    sg->anchor[a] = box[a];
+    sg->cell_size[a] = box[3 + a] / ncell[a];
+    sg->inv_cell_size[a] = ncell[a] / box[3 + a];
+    sg->ncell[a] = ncell[a];
+  }
+  sg->ncell[3] = ncell[1] * ncell[2];
+}
+
+/* DensitySubGrid.hpp:247-414: the entry axes are clamped to the face the
+ * packet enters through, the other axes are computed by truncation. */
+static int axis_start_index(const cmio_subgrid *sg, double x, int axis, int input_direction) {
+  const int s = kSigns[input_direction][axis];
+  if (s == 0) {
+    return (int)(x * sg->inv_cell_size[axis]);
+  }
+  return (s < 0) ? 0 : sg->ncell[axis] - 1;
+}
+
+/* DensitySubGrid.hpp:428-469. */
+int cmio_get_start_index(const cmio_subgrid *sg, const double position[3],
+                         int input_direction, int32_t three_index[3]) {
+  for (int a = 0; a < 3; ++a) {
+    three_index[a] = axis_start_index(sg, position[a], a, input_direction);
+  }
+  return three_index[0] * sg->ncell[3] + three_index[1] * sg->ncell[2] + three_index[2];
+}
+
+/* DensitySubGrid.hpp:483-506. */
+int cmio_get_output_direction(const cmio_subgrid *sg, const int32_t three_index[3]) {
+  int mask = 0;
+  for (int a = 0; a < 3; ++a) {
+    const int low = three_index[a] < 0;
+    const int high = (three_index[a] / sg->ncell[a]) > 0;
+    mask |= (high << (5 - 2 * a)) | (low << (4 - 2 * a));
+  }
+  return cmio_direction_from_mask(mask);
+}
+
+static inline int is_inside3(const int32_t idx[3], const int32_t n[3]) {
+  return idx[0] < n[0] && idx[0] >= 0 && idx[1] < n[1] && idx[1] >= 0 && idx[2] < n[2] &&
+         idx[2] >= 0;
+}
+
+/* std::min semantics: min(a, b) = (b < a) ? b : a. */
+static inline double min_d(double a, double b) { return (b < a) ? b : a; }
+static inline float min_f(float a, float b) { return (b < a) ? b : a; }
+
+/* DensitySubGrid::interact, DensitySubGrid.hpp:1180-1323. */
+int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, double *J,
+                  cmio_photon *photon, int input_direction, int32_t *trace_cells,
+                  double *trace_lengths, int32_t max_steps, int32_t *nsteps) {
+  const double *d = photon->direction;
+  const double inv[3] = {1. / d[0], 1. / d[1], 1. / d[2]};
+  double pos[3] = {photon->position[0] - sg->anchor[0], photon->position[1] - sg->anchor[1],
+                   photon->position[2] - sg->anchor[2]};
+  double tau_done = 0.;
+  const double tau_target = photon->target_optical_depth;
+  const double sigma = photon->cross_section;
+  const double weight = photon->weight;
+  int32_t idx[3];
+  int cell = cmio_get_start_index(sg, pos, input_direction, idx);
+  int32_t steps = 0;
+  while (tau_done < tau_target && is_inside3(idx, sg->ncell)) {
+    const double lo[3] = {idx[0] * sg->cell_size[0], idx[1] * sg->cell_size[1],
+                          idx[2] * sg->cell_size[2]};
+    const double hi[3] = {(idx[0] + 1.) * sg->cell_size[0], (idx[1] + 1.) * sg->cell_size[1],
+                          (idx[2] + 1.) * sg->cell_size[2]};
+    double l[3];
+    for (int a = 0; a < 3; ++a) {
+      if (d[a] > 0.) {
+        l[a] = (hi[a] - pos[a]) * inv[a];
+      } else if (d[a] < 0.) {
+        l[a] = (lo[a] - pos[a]) * inv[a];
+      } else {
+        l[a] = DBL_MAX;
+      }
+    }
+    double lmin = min_d(l[0], min_d(l[1], l[2]));
+    double lminsigma = lmin * sigma;
+    const double tau = lminsigma * nH[cell] * xH[cell];
+    tau_done += tau;
+    if (tau_done >= tau_target) {
+      const double correction = (tau_done - tau_target) / tau;
+      lmin *= (1. - correction);
+      lminsigma = lmin * sigma;
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        if (l[a] == lmin) {
+          idx[a] += (d[a] > 0.) ? 1 : -1;
+        }
+      }
+    }
+    J[cell] += lminsigma * weight;
+    if (trace_cells != NULL && steps < max_steps) {
+      trace_cells[steps] = cell;
+      trace_lengths[steps] = lmin;
+    }
+    ++steps;
+    for (int a = 0; a < 3; ++a) {
+      pos[a] = (l[a] == lmin) ? ((d[a] > 0.) ? hi[a] : lo[a]) : pos[a] + lmin * d[a];
+    }
+    cell = idx[0] * sg->ncell[3] + idx[1] * sg->ncell[2] + idx[2];
+  }
+  photon->target_optical_depth = tau_target - tau_done;
+  for (int a = 0; a < 3; ++a) {
+    photon->position[a] = pos[a] + sg->anchor[a];
+  }
+  if (nsteps != NULL) {
+    *nsteps = steps;
+  }
+  if (tau_done >= tau_target) {
+    return CMIO_INSIDE;
+  }
+  return cmio_get_output_direction(sg, idx);
+}
+
+/* FP32 cell-unit walk.  Same loop as interact above, with positions in cell
+ * units relative to the subgrid (cell faces are exact small integers) and
+ * path lengths in metres: l = (face - p) * (cell_size / d).  On exit the
+ * position is re-expressed relative to the neighbour across the exit face
+ * (exact: the exit coordinate is 0 or n). */
+int cmio_interact32(const int32_t ncell[3], const float cell_size[3], const float *kappa,
+                    double *tally, cmio_packet32 *packet, int32_t *trace_cells,
+                    float *trace_lengths, int32_t max_steps, int32_t *nsteps) {
+  const int in_dir = (int)(packet->meta & 31u);
+  const float *d = packet->dir;
+  float p[3] = {packet->pos[0], packet->pos[1], packet->pos[2]};
+  float inv[3], dcs[3];
+  int32_t idx[3];
+  for (int a = 0; a < 3; ++a) {
+    dcs[a] = d[a] / cell_size[a];
+    inv[a] = cell_size[a] / d[a];
+    const int s = kSigns[in_dir][a];
+    idx[a] = (s == 0) ? (int32_t)p[a] : ((s < 0) ? 0 : ncell[a] - 1);
+  }
+  const int32_t nyz = ncell[1] * ncell[2];
+  int32_t cell = idx[0] * nyz + idx[1] * ncell[2] + idx[2];
+  float tau_done = 0.f;
+  const float tau_target = packet->tau_left;
+  int32_t steps = 0;
+  while (tau_done < tau_target && is_inside3(idx, ncell)) {
+    float lo[3], hi[3], l[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = (float)idx[a];
+      hi[a] = (float)(idx[a] + 1);
+      if (d[a] > 0.f) {
+        l[a] = (hi[a] - p[a]) * inv[a];
+      } else if (d[a] < 0.f) {
+        l[a] = (lo[a] - p[a]) * inv[a];
+      } else {
+        l[a] = FLT_MAX;
+      }
+    }
+    float lmin = min_f(l[0], min_f(l[1], l[2]));
+    const float tau = lmin * kappa[cell];
+    tau_done += tau;
+    if (tau_done >= tau_target) {
+      const float correction = (tau_done - tau_target) / tau;
+      lmin *= (1.f - correction);
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        if (l[a] == lmin) {
+          idx[a] += (d[a] > 0.f) ? 1 : -1;
+        }
+      }
+    }
+    if (tally != NULL) {
+      tally[cell] += (double)lmin;
+    }
+    if (trace_cells != NULL && steps < max_steps) {
+      trace_cells[steps] = cell;
+      trace_lengths[steps] = lmin;
+    }
+    ++steps;
+    for (int a = 0; a < 3; ++a) {
+      p[a] = (l[a] == lmin) ? ((d[a] > 0.f) ? hi[a] : lo[a]) : fmaf(lmin, dcs[a], p[a]);
+    }
+    cell = idx[0] * nyz + idx[1] * ncell[2] + idx[2];
+  }
+  packet->tau_left = tau_target - tau_done;
+  if (nsteps != NULL) {
+    *nsteps = steps;
+  }
+  int out = CMIO_INSIDE;
+  if (!(tau_done >= tau_target)) {
+    int mask = 0;
+    for (int a = 0; a < 3; ++a) {
+      const int low = idx[a] < 0;
+      const int high = (idx[a] / ncell[a]) > 0;
+      mask |= (high << (5 - 2 * a)) | (low << (4 - 2 * a));
+      if (high) {
+        p[a] -= (float)ncell[a];
+      } else if (low) {
+        p[a] += (float)ncell[a];
+      }
+    }
+    out = cmio_direction_from_mask(mask);
+  }
+  packet->pos[0] = p[0];
+  packet->pos[1] = p[1];
+  packet->pos[2] = p[2];
+  return out;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ionization balance, DensitySubGrid.hpp:1628-1658.                         */
+/* ------------------------------------------------------------------------ */
+double cmio_jfac(double luminosity, double num_photon, const double inv_cell_size[3]) {
+  return luminosity / num_photon * inv_cell_size[0] * inv_cell_size[1] * inv_cell_size[2];
+}
+
+void cmio_compute_neutral_fraction(int64_t ncell, const double *nH, double *xH, double *J,
+                                   double jfac, double alpha_H, int form) {
+  for (int64_t i = 0; i < ncell; ++i) {
+    const double jH = jfac * J[i];
+    if (jH > 0.) {
+      const double ntot = nH[i];
+      const double aa = 0.5 * jH / (ntot * alpha_H);
+      if (form == 0) {
+        const double bb = 2. / aa;
+        const double cc = sqrt(bb + 1.);
+        xH[i] = 1. + aa * (1. - cc);
+      } else {
+        xH[i] = 1. / (1. + aa + sqrt(aa * (aa + 2.)));
+      }
+    } else {
+      xH[i] = 1.;
+    }
+    J[i] = 0.;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* ranlxd generator, RandomGenerator.hpp:36-232 (restating GSL ranlxd with   */
+/* luxury 397; the sequence must match bit for bit).                         */
+/* ------------------------------------------------------------------------ */
+#define RL_ONE_BIT (1.0 / 281474976710656.0) /* 2^-48 */
+
+/* One subtract-with-borrow step at slot ir with partner slot jr. */
+static inline void rl_step(double *x, double *carry, uint32_t ir, uint32_t jr) {
+  double y = x[jr] - x[ir];
+  y = y - *carry;
+  if (y < 0) {
+    *carry = RL_ONE_BIT;
+    y += 1;
+  } else {
+    *carry = 0;
+  }
+  x[ir] = y;
+}
+
+/* RandomGenerator.hpp:80-150.  Leading single steps until ir wraps to 0,
+ * then 12-step blocks whose partner slot is (i+7) mod 12, then trailing
+ * single steps up to pr. */
+static void rl_increment(cmio_ranlux *r) {
+  double *x = r->x;
+  double carry = r->carry;
+  uint32_t ir = r->ir;
+  uint32_t jr = r->jr;
+  int32_t k = 0;
+  for (; ir > 0; ++k) {
+    rl_step(x, &carry, ir, jr);
+    ir = (ir + 1) % 12;
+    jr = (jr + 1) % 12;
+  }
+  const int32_t kblock = (int32_t)r->pr - 12;
+  for (; k <= kblock; k += 12) {
+    for (uint32_t i = 0; i < 12; ++i) {
+      rl_step(x, &carry, i, (i + 7) % 12);
+    }
+  }
+  for (; k < (int32_t)r->pr; ++k) {
+    rl_step(x, &carry, ir, jr);
+    ir = (ir + 1) % 12;
+    jr = (jr + 1) % 12;
+  }
+  r->ir = ir;
+  r->ir_old = ir;
+  r->jr = jr;
+  r->carry = carry;
+}
+
+/* RandomGenerator.hpp:158-197. */
+void cmio_ranlux_seed(cmio_ranlux *r, int32_t seed) {
+  if (seed == 0) {
+    seed = 1;
+  }
+  int32_t bits[31];
+  int32_t v = seed & 0x7FFFFFFF;
+  for (int k = 0; k < 31; ++k) {
+    bits[k] = v % 2;
+    v /= 2;
+  }
+  int ib = 0, jb = 18;
+  for (int k = 0; k < 12; ++k) {
+    double acc = 0;
+    for (int m = 1; m <= 48; ++m) {
+      const double y = (double)((bits[ib] + 1) % 2);
+      acc += acc + y;
+      bits[ib] = (bits[ib] + bits[jb]) % 2;
+      ib = (ib + 1) % 31;
+      jb = (jb + 1) % 31;
+    }
+    r->x[k] = RL_ONE_BIT * acc;
+  }
+  r->carry = 0;
+  r->ir = 11;
+  r->jr = 7;
+  r->ir_old = 0;
+  r->pr = 397;
+}
+
+/* RandomGenerator.hpp:214-222. */
+double cmio_ranlux_uniform(cmio_ranlux *r) {
+  r->ir = (r->ir + 1) % 12;
+  if (r->ir == r->ir_old) {
+    rl_increment(r);
+  }
+  return r->x[r->ir];
+}
+
+/* ------------------------------------------------------------------------ */
+/* Emission, testDensitySubGrid_omp.cpp:529-597.                             */
+/* ------------------------------------------------------------------------ */
+void cmio_random_direction(cmio_ranlux *rng, double direction[3]) {
+  const double cost = 2. * cmio_ranlux_uniform(rng) - 1.;
+  const double phi = 2. * M_PI * cmio_ranlux_uniform(rng);
+  const double s2 = 1. - cost * cost;
+  const double sint = sqrt((s2 < 0.) ? 0. : s2);
+  const double cosp = cos(phi);
+  const double sinp = sin(phi);
+  direction[0] = sint * cosp;
+  direction[1] = sint * sinp;
+  direction[2] = cost;
+}
+
+void cmio_fill_packets(cmio_ranlux *rng, const double source_position[3], cmio_photon *out,
+                       int32_t n, double cross_section) {
+  for (int32_t i = 0; i < n; ++i) {
+    cmio_photon *p = &out[i];
+    memset(p, 0, sizeof(*p));
+    p->position[0] = source_position[0];
+    p->position[1] = source_position[1];
+    p->position[2] = source_position[2];
+    cmio_random_direction(rng, p->direction);
+    p->weight = 1.;
+    p->target_optical_depth = -log(cmio_ranlux_uniform(rng));
+    p->cross_section = cross_section;
+  }
+}
+
+void cmio_fill_buffer_stream(int32_t seed, const double source_position[3], cmio_photon *out,
+                             int32_t n, double cross_section) {
+  cmio_ranlux rng;
+  cmio_ranlux_seed(&rng, seed);
+  (void)cmio_ranlux_uniform(&rng); /* Source::get_subgrid_index draw */
+  cmio_fill_packets(&rng, source_position, out, n, cross_section);
+}
+
+/* testDensitySubGrid_omp.cpp:2199-2208: packets proportional to luminosity. */
+void cmio_source_numbers(int32_t nsrc, const double *luminosity, uint32_t num_photon,
+                         uint32_t *numbers) {
+  double total = 0.;
+  for (int32_t i = 0; i < nsrc; ++i) {
+    total += luminosity[i];
+  }
+  for (int32_t i = 0; i < nsrc; ++i) {
+    numbers[i] = (uint32_t)(luminosity[i] / total * num_photon);
+  }
+}
+
+/* testDensitySubGrid_omp.cpp:1650-1677: the distribute_number smallest of
+ * total_number uniform draws receive one extra packet. */
+typedef struct {
+  double v;
+  int32_t i;
+} rl_pair;
+static int cmp_pair(const void *a, const void *b) {
+  const rl_pair *x = (const rl_pair *)a, *y = (const rl_pair *)b;
+  if (x->v < y->v) return -1;
+  if (y->v < x->v) return 1;
+  return (x->i < y->i) ? -1 : (x->i > y->i);
+}
+void cmio_distribute(int32_t total_number, int32_t distribute_number, cmio_ranlux *rng,
+                     uint32_t *result) {
+  rl_pair *p = (rl_pair *)malloc(sizeof(rl_pair) * (size_t)(total_number > 0 ? total_number : 1));
+  for (int32_t i = 0; i < total_number; ++i) {
+    p[i].v = cmio_ranlux_uniform(rng);
+    p[i].i = i;
+    result[i] = 0;
+  }
+  qsort(p, (size_t)total_number, sizeof(rl_pair), cmp_pair);
+  for (int32_t i = 0; i < distribute_number && i < total_number; ++i) {
+    result[p[i].i] = 1;
+  }
+  free(p);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).                        */
+/* ------------------------------------------------------------------------ */
+void cmio_philox4x32(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c0 = counter[0], c1 = counter[1], c2 = counter[2], c3 = counter[3];
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    const uint32_t n1 = (uint32_t)p1;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    const uint32_t n3 = (uint32_t)p0;
+    c0 = n0;
+    c1 = n1;
+    c2 = n2;
+    c3 = n3;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+void cmio_philox_packet(uint64_t seed, uint32_t stream, uint64_t packet, double direction[3],
+                        double *tau) {
+  const uint32_t ctr[4] = {(uint32_t)packet, (uint32_t)(packet >> 32), stream, 0x434D4901u};
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t w[4];
+  cmio_philox4x32(ctr, key, w);
+  const double u0 = ((double)w[0] + 0.5) * (1.0 / 4294967296.0);
+  const double u1 = ((double)w[1] + 0.5) * (1.0 / 4294967296.0);
+  const uint64_t k53 = ((uint64_t)w[2] << 21) ^ (uint64_t)(w[3] >> 11);
+  const double u2 = ((double)k53 + 0.5) * (1.0 / 9007199254740992.0);
+  const double cost = 2. * u0 - 1.;
+  const double phi = 2. * M_PI * u1;
+  const double s2 = 1. - cost * cost;
+  const double sint = sqrt((s2 < 0.) ? 0. : s2);
+  direction[0] = sint * cos(phi);
+  direction[1] = sint * sin(phi);
+  direction[2] = cost;
+  *tau = -log(u2);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Lattice of subgrids (testDensitySubGrid_omp.cpp:1801-1877).               */
+/* ------------------------------------------------------------------------ */
+int cmio_lattice_init(cmio_lattice *lat, const double box[6], const int32_t ncell[3],
+                      const int32_t num_subgrid[3]) {
+  memset(lat, 0, sizeof(*lat));
+  for (int a = 0; a < 3; ++a) {
+    if (num_subgrid[a] <= 0 || ncell[a] % num_subgrid[a] != 0) {
+      return -1;
+    }
+    lat->num_subgrid[a] = num_subgrid[a];
+    lat->sub_ncell[a] = ncell[a] / num_subgrid[a];
+  }
+  lat->cells_per_subgrid = (int64_t)lat->sub_ncell[0] * lat->sub_ncell[1] * lat->sub_ncell[2];
+  lat->nsub = (int64_t)num_subgrid[0] * num_subgrid[1] * num_subgrid[2];
+  lat->sub = (cmio_subgrid *)calloc((size_t)lat->nsub, sizeof(cmio_subgrid));
+  lat->ngb = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)lat->nsub * CMIO_NUM_DIRECTIONS);
+  const double side[3] = {box[3] / num_subgrid[0], box[4] / num_subgrid[1],
+                          box[5] / num_subgrid[2]};
+  const int32_t ns1 = num_subgrid[1], ns2 = num_subgrid[2];
+  for (int64_t s = 0; s < lat->nsub; ++s) {
+    const int32_t ix = (int32_t)(s / (ns1 * ns2));
+    const int32_t iy = (int32_t)((s - (int64_t)ix * ns1 * ns2) / ns2);
+    const int32_t iz = (int32_t)(s - (int64_t)ix * ns1 * ns2 - (int64_t)iy * ns2);
+    const double sbox[6] = {box[0] + ix * side[0], box[1] + iy * side[1], box[2] + iz * side[2],
+                            side[0], side[1], side[2]};
+    cmio_subgrid_init(&lat->sub[s], sbox, lat->sub_ncell);
+    uint32_t *ngb = &lat->ngb[s * CMIO_NUM_DIRECTIONS];
+    for (int d = 0; d < CMIO_NUM_DIRECTIONS; ++d) {
+      ngb[d] = CMIO_NEIGHBOUR_OUTSIDE;
+    }
+    for (int nx = -1; nx < 2; ++nx) {
+      for (int ny = -1; ny < 2; ++ny) {
+        for (int nz = -1; nz < 2; ++nz) {
+          const int cx = ix + nx, cy = iy + ny, cz = iz + nz;
+          if (cx >= 0 && cx < num_subgrid[0] && cy >= 0 && cy < ns1 && cz >= 0 && cz < ns2) {
+            ngb[direction_from_signs(nx, ny, nz)] = (uint32_t)((cx * ns1 + cy) * ns2 + cz);
+          }
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+void cmio_lattice_free(cmio_lattice *lat) {
+  free(lat->sub);
+  free(lat->ngb);
+  memset(lat, 0, sizeof(*lat));
+}
+
+uint32_t cmio_lattice_locate(const cmio_lattice *lat, const double box[6],
+                             const double position[3]) {
+  uint32_t i3[3];
+  for (int a = 0; a < 3; ++a) {
+    int64_t v = (int64_t)((position[a] - box[a]) / box[3 + a] * lat->num_subgrid[a]);
+    if (v < 0) v = 0;
+    if (v >= lat->num_subgrid[a]) v = lat->num_subgrid[a] - 1;
+    i3[a] = (uint32_t)v;
+  }
+  return (i3[0] * lat->num_subgrid[1] + i3[1]) * lat->num_subgrid[2] + i3[2];
+}
+
+/* do_photon_traversal + routing (testDensitySubGrid_omp.cpp:607-666,
+ * 1178-1191) applied to one packet at a time until absorption (INSIDE with
+ * reemission off) or escape (neighbour NEIGHBOUR_OUTSIDE). */
+void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH, double *J,
+                    cmio_photon *packets, const uint32_t *start_subgrid, int64_t n,
+                    cmio_counts *counts) {
+  const int64_t C = lat->cells_per_subgrid;
+  for (int64_t i = 0; i < n; ++i) {
+    uint32_t s = start_subgrid[i];
+    int in_dir = CMIO_INSIDE;
+    for (;;) {
+      int32_t steps = 0;
+      const int out = cmio_interact(&lat->sub[s], nH + s * C, xH + s * C, J + s * C, &packets[i],
+                                    in_dir, NULL, NULL, 0, &steps);
+      counts->crossings += (uint64_t)steps;
+      counts->transits += 1;
+      if (out == CMIO_INSIDE) {
+        counts->absorbed += 1;
+        break;
+      }
+      const uint32_t ngb = lat->ngb[s * CMIO_NUM_DIRECTIONS + out];
+      if (ngb == CMIO_NEIGHBOUR_OUTSIDE) {
+        counts->escaped += 1;
+        break;
+      }
+      s = ngb;
+      in_dir = cmio_output_to_input_direction(out);
+    }
+  }
+}
+
+void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally,
+                      cmio_packet32 *packets, const uint32_t *start_subgrid, int64_t n,
+                      cmio_counts *counts) {
+  const int64_t C = lat->cells_per_subgrid;
+  for (int64_t i = 0; i < n; ++i) {
+    uint32_t s = start_subgrid[i];
+    for (;;) {
+      const cmio_subgrid *sg = &lat->sub[s];
+      const float cs[3] = {(float)sg->cell_size[0], (float)sg->cell_size[1],
+                           (float)sg->cell_size[2]};
+      int32_t steps = 0;
+      const int out = cmio_interact32(lat->sub_ncell, cs, kappa + s * C,
+                                      tally ? tally + s * C : NULL, &packets[i], NULL, NULL, 0,
+                                      &steps);
+      counts->crossings += (uint64_t)steps;
+      counts->transits += 1;
+      if (out == CMIO_INSIDE) {
+        counts->absorbed += 1;
+        break;
+      }
+      const uint32_t ngb = lat->ngb[s * CMIO_NUM_DIRECTIONS + out];
+      if (ngb == CMIO_NEIGHBOUR_OUTSIDE) {
+        counts->escaped += 1;
+        break;
+      }
+      s = ngb;
+      packets[i].meta = (packets[i].meta & ~31u) | (uint32_t)cmio_output_to_input_direction(out);
+    }
+  }
+}
+
+void cmio_kappa32(int64_t ncell, const double *nH, const double *xH, double sigma,
+                  float *kappa) {
+  for (int64_t i = 0; i < ncell; ++i) {
+    kappa[i] = (float)(sigma * nH[i] * xH[i]);
+  }
+}
+
+void cmio_split_packets(int32_t nsrc, const double *luminosity, uint64_t num_photon,
+                        uint64_t seed, uint32_t iteration, uint64_t *numbers) {
+  double total = 0.;
+  for (int32_t i = 0; i < nsrc; ++i) {
+    total += luminosity[i];
+  }
+  uint64_t assigned = 0;
+  for (int32_t i = 0; i < nsrc; ++i) {
+    numbers[i] = (uint64_t)(luminosity[i] / total * (double)num_photon);
+    assigned += numbers[i];
+  }
+  uint64_t rem = (num_photon > assigned) ? num_photon - assigned : 0;
+  /* rank sources by a Philox draw; the rem smallest get one packet each */
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t *draw = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(nsrc > 0 ? nsrc : 1));
+  for (int32_t i = 0; i < nsrc; ++i) {
+    const uint32_t ctr[4] = {(uint32_t)i, 0u, iteration, 0x434D4902u};
+    uint32_t w[4];
+    cmio_philox4x32(ctr, key, w);
+    draw[i] = w[0];
+  }
+  while (rem > 0) {
+    int32_t best = -1;
+    for (int32_t i = 0; i < nsrc; ++i) {
+      if (draw[i] != 0xFFFFFFFFu || best < 0) {
+        if (best < 0 || draw[i] < draw[best] || (draw[i] == draw[best] && i < best)) {
+          best = i;
+        }
+      }
+    }
+    numbers[best] += 1;
+    draw[best] = 0xFFFFFFFFu;
+    --rem;
+  }
+  free(draw);
+}
+
+void cmio_iteration_omp(const cmio_lattice *lat, const double box[6], const double *nH,
+                        double *xH, double *J, int32_t nsrc, const double *src_pos,
+                        const double *src_lum, uint64_t num_photon, uint64_t seed,
+                        uint32_t iteration, double alpha_H, double cross_section,
+                        int balance_form, int threads, cmio_counts *counts) {
+  const int64_t C = lat->cells_per_subgrid;
+  const int64_t ncell = C * lat->nsub;
+  uint64_t *numbers = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)nsrc);
+  uint64_t *first = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(nsrc + 1));
+  uint32_t *src_sub = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)nsrc);
+  cmio_split_packets(nsrc, src_lum, num_photon, seed, iteration, numbers);
+  first[0] = 0;
+  double total_lum = 0.;
+  for (int32_t i = 0; i < nsrc; ++i) {
+    first[i + 1] = first[i] + numbers[i];
+    src_sub[i] = cmio_lattice_locate(lat, box, &src_pos[3 * i]);
+    total_lum += src_lum[i];
+  }
+  if (threads <= 0) {
+#ifdef _OPENMP
+    threads = omp_get_max_threads();
+#else
+    threads = 1;
+#endif
+  }
+  double *priv = (double *)calloc((size_t)threads * (size_t)ncell, sizeof(double));
+  uint64_t c_abs = 0, c_esc = 0, c_cross = 0, c_tr = 0;
+#pragma omp parallel num_threads(threads) reduction(+ : c_abs, c_esc, c_cross, c_tr)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double *Jt = priv + (size_t)tid * (size_t)ncell;
+    cmio_counts local = {0, 0, 0, 0};
+#pragma omp for schedule(dynamic, 4096)
+    for (int64_t p = 0; p < (int64_t)num_photon; ++p) {
+      int32_t src = 0;
+      while (src + 1 < nsrc && (uint64_t)p >= first[src + 1]) {
+        ++src;
+      }
+      cmio_photon ph;
+      memset(&ph, 0, sizeof(ph));
+      ph.position[0] = src_pos[3 * src];
+      ph.position[1] = src_pos[3 * src + 1];
+      ph.position[2] = src_pos[3 * src + 2];
+      cmio_philox_packet(seed, iteration, (uint64_t)p, ph.direction, &ph.target_optical_depth);
+      ph.cross_section = cross_section;
+      ph.weight = 1.;
+      const uint32_t s0 = src_sub[src];
+      cmio_transport(lat, nH, xH, Jt, &ph, &s0, 1, &local);
+    }
+    c_abs += local.absorbed;
+    c_esc += local.escaped;
+    c_cross += local.crossings;
+    c_tr += local.transits;
+  }
+#pragma omp parallel for num_threads(threads) schedule(static)
+  for (int64_t i = 0; i < ncell; ++i) {
+    double acc = J[i];
+    for (int t = 0; t < threads; ++t) {
+      acc += priv[(size_t)t * (size_t)ncell + (size_t)i];
+    }
+    J[i] = acc;
+  }
+  const double jfac = cmio_jfac(total_lum, (double)num_photon, lat->sub[0].inv_cell_size);
+#pragma omp parallel for num_threads(threads) schedule(static)
+  for (int64_t s = 0; s < lat->nsub; ++s) {
+    cmio_compute_neutral_fraction(C, nH + s * C, xH + s * C, J + s * C, jfac, alpha_H,
+                                  balance_form);
+  }
+  counts->absorbed += c_abs;
+  counts->escaped += c_esc;
+  counts->crossings += c_cross;
+  counts->transits += c_tr;
+  free(priv);
+  free(numbers);
+  free(first);
+  free(src_sub);
+}

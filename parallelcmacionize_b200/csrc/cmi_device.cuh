@@ -1,0 +1,308 @@
+// Device-side data layout and helpers of the B200 transport engine.
+//
+// Internal header of cmi_engine.cu (single translation unit): structures in
+// HBM, TravelDirection tables, the counter-based and the reference random
+// generators.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cmi {
+
+constexpr int kNumDirections = 27;
+constexpr uint32_t kOutside = 0xffffffffu;
+constexpr int kInside = 0;
+
+// ---------------------------------------------------------------------------
+// TravelDirections (TravelDirections.hpp:46-403) as axis-sign triples.
+// Packed code of a direction: bits [2a, 2a+1] hold sign(axis a) + 1.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int dir_from_signs(int sx, int sy, int sz) {
+  // INSIDE 0, CORNER 1-8, EDGE_X 9-12, EDGE_Y 13-16, EDGE_Z 17-20, FACE 21-26
+  return (sx == 0 && sy == 0 && sz == 0) ? 0
+         : (sx != 0 && sy != 0 && sz != 0)
+             ? 1 + (sx < 0) * 4 + (sy < 0) * 2 + (sz < 0)
+         : (sx == 0 && sy != 0 && sz != 0) ? 9 + (sy < 0) * 2 + (sz < 0)
+         : (sy == 0 && sx != 0 && sz != 0) ? 13 + (sx < 0) * 2 + (sz < 0)
+         : (sz == 0 && sx != 0 && sy != 0) ? 17 + (sx < 0) * 2 + (sy < 0)
+         : (sx != 0)                       ? 21 + (sx < 0)
+         : (sy != 0)                       ? 23 + (sy < 0)
+                                           : 25 + (sz < 0);
+}
+
+struct DirectionTables {
+  uint8_t sign_code[32];  // per direction
+  uint8_t mirror[32];     // output_to_input_direction
+  uint8_t mask_dir[64];   // 6-bit out-of-range mask -> direction (255: invalid)
+};
+
+inline DirectionTables make_direction_tables() {
+  DirectionTables t{};
+  for (int sx = -1; sx <= 1; ++sx)
+    for (int sy = -1; sy <= 1; ++sy)
+      for (int sz = -1; sz <= 1; ++sz) {
+        const int d = dir_from_signs(sx, sy, sz);
+        t.sign_code[d] = (uint8_t)((sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4));
+        t.mirror[d] = (uint8_t)dir_from_signs(-sx, -sy, -sz);
+      }
+  for (int m = 0; m < 64; ++m) {
+    int s[3];
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+      const int hi = (m >> (5 - 2 * a)) & 1, lo = (m >> (4 - 2 * a)) & 1;
+      ok = ok && !(hi && lo);
+      s[a] = hi ? 1 : (lo ? -1 : 0);
+    }
+    t.mask_dir[m] = ok ? (uint8_t)dir_from_signs(s[0], s[1], s[2]) : (uint8_t)255;
+  }
+  return t;
+}
+
+__device__ __forceinline__ int sign_of(uint8_t code, int axis) {
+  return (int)((code >> (2 * axis)) & 3u) - 1;
+}
+
+// ---------------------------------------------------------------------------
+// Structures resident in HBM.
+// ---------------------------------------------------------------------------
+struct alignas(16) DevSubgrid {
+  double anchor[3];
+  double cell_size[3];
+  double inv_cell_size[3];
+  float cell_size_f[3];
+  int32_t ncell[3];
+  int32_t ncells;         // nx * ny * nz
+  int32_t padded_cells;   // ncells rounded up to a multiple of 4 (16 B in FP32)
+  int64_t field_offset;   // first cell in the flat field arrays (multiple of 4)
+  uint32_t instance;
+  uint32_t ngb[kNumDirections];
+};
+
+struct alignas(16) DevInstance {
+  double jfac;            // L_tot / N / V_cell (DensitySubGrid.hpp:1633)
+  double alpha;
+  double sigma;
+  double total_luminosity;
+  uint64_t num_photon;
+  uint32_t first_subgrid, num_subgrids;
+  uint32_t first_source, num_sources;
+  int64_t num_cells;
+};
+
+struct alignas(16) DevSource {
+  double position[3];
+  double luminosity;
+  float pos_cell[3];      // position in cell units relative to its subgrid
+  uint32_t subgrid;       // global subgrid index
+  uint32_t instance;
+  uint32_t local_index;   // index among the instance's sources
+};
+
+// Work unit of a wavefront round: packets [begin, begin+count) of the sorted
+// arena, all waiting to enter `subgrid`.
+struct alignas(16) Chunk {
+  uint32_t subgrid;
+  uint32_t count;
+  uint32_t begin;
+  uint32_t pad;
+};
+
+// Per-iteration counters of one instance (device side of cmi_stats).
+struct alignas(16) DevStats {
+  unsigned long long emitted, absorbed, escaped, crossings, transits;
+  double dx_sum;
+  uint32_t flags, rounds;
+};
+
+// Control block of the wavefront.
+struct alignas(16) RoundState {
+  uint32_t chunk_next;     // chunks claimed in this round
+  uint32_t num_chunks;     // chunks of this round
+  uint32_t arena_count;    // packets appended by this round
+  uint32_t total_in;       // packets in the sorted arena
+  uint32_t emit_total;     // packets emitted this iteration
+  uint32_t iteration;      // Philox stream of the current iteration
+  uint64_t seed;
+  uint32_t flags;          // CMI_FLAG_* of the whole context
+  uint32_t rounds_active;
+  uint32_t capacity;       // arena capacity (packets)
+  uint32_t pad[3];
+};
+
+// FP64 packet: the reference Photon layout (80 B); `meta` (the reserved
+// slot) carries the input TravelDirection.
+struct alignas(16) Packet64 {
+  double pos[3];
+  double dir[3];
+  double tau;
+  double sigma;
+  double weight;
+  int32_t type;
+  uint32_t meta;
+};
+static_assert(sizeof(Packet64) == 80, "Packet64 must match cmi_photon");
+
+// FP32 packet (32 B, one sector): position in cell units relative to the
+// subgrid it is about to enter, direction, remaining target optical depth.
+struct alignas(16) Packet32 {
+  float pos[3];
+  float dir[3];
+  float tau;
+  uint32_t meta;  // low 5 bits: input TravelDirection
+};
+static_assert(sizeof(Packet32) == 32, "Packet32 is one 32-byte sector");
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy
+// as 1, 2, 3", SC'11).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi,
+                                                   uint32_t &lo) {
+#ifdef __CUDA_ARCH__
+  lo = a * b;
+  hi = __umulhi(a, b);
+#else
+  const uint64_t p = (uint64_t)a * b;
+  lo = (uint32_t)p;
+  hi = (uint32_t)(p >> 32);
+#endif
+}
+
+__host__ __device__ __forceinline__ void philox4x32_10(const uint32_t in[4], uint32_t k0,
+                                                       uint32_t k1, uint32_t out[4]) {
+  uint32_t c0 = in[0], c1 = in[1], c2 = in[2], c3 = in[3];
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo32(0xD2511F53u, c0, hi0, lo0);
+    mulhilo32(0xCD9E8D57u, c2, hi1, lo1);
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+constexpr uint32_t kPhiloxPacketTag = 0x434D4901u;
+constexpr uint32_t kPhiloxSplitTag = 0x434D4902u;
+
+// Isotropic direction and exponential optical depth of one packet
+// (testDensitySubGrid_omp.cpp:529-545, 585-586, drawn from Philox).
+__device__ __forceinline__ void philox_packet(uint64_t seed, uint32_t instance,
+                                              uint32_t iteration, uint64_t packet,
+                                              double dir[3], double &tau) {
+  const uint32_t ctr[4] = {(uint32_t)packet, (uint32_t)(packet >> 32), iteration,
+                           kPhiloxPacketTag};
+  uint32_t w[4];
+  philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32) + instance, w);
+  const double u0 = ((double)w[0] + 0.5) * (1.0 / 4294967296.0);
+  const double u1 = ((double)w[1] + 0.5) * (1.0 / 4294967296.0);
+  const uint64_t k53 = ((uint64_t)w[2] << 21) ^ (uint64_t)(w[3] >> 11);
+  const double u2 = ((double)k53 + 0.5) * (1.0 / 9007199254740992.0);
+  const double cost = 2. * u0 - 1.;
+  const double phi = 2. * 3.14159265358979323846 * u1;
+  const double s2 = 1. - cost * cost;
+  const double sint = sqrt((s2 < 0.) ? 0. : s2);
+  double sp, cp;
+  sincos(phi, &sp, &cp);
+  dir[0] = sint * cp;
+  dir[1] = sint * sp;
+  dir[2] = cost;
+  tau = -log(u2);
+}
+
+// ---------------------------------------------------------------------------
+// ranlxd (RandomGenerator.hpp:36-232), the reference's generator, for
+// replaying the reference's per-buffer streams on the device.
+// ---------------------------------------------------------------------------
+struct Ranlux {
+  double x[12];
+  double carry;
+  uint32_t ir, jr, ir_old, pr;
+
+  static constexpr double kOneBit = 1.0 / 281474976710656.0;  // 2^-48
+
+  __host__ __device__ void step(uint32_t i, uint32_t j) {
+    double y = x[j] - x[i];
+    y = y - carry;
+    if (y < 0) {
+      carry = kOneBit;
+      y += 1;
+    } else {
+      carry = 0;
+    }
+    x[i] = y;
+  }
+
+  // RandomGenerator.hpp:80-150
+  __host__ __device__ void increment() {
+    uint32_t i = ir, j = jr;
+    int32_t k = 0;
+    for (; i > 0; ++k) {
+      step(i, j);
+      i = (i + 1) % 12;
+      j = (j + 1) % 12;
+    }
+    for (; k <= (int32_t)pr - 12; k += 12) {
+      for (uint32_t q = 0; q < 12; ++q) step(q, (q + 7) % 12);
+    }
+    for (; k < (int32_t)pr; ++k) {
+      step(i, j);
+      i = (i + 1) % 12;
+      j = (j + 1) % 12;
+    }
+    ir = i;
+    ir_old = i;
+    jr = j;
+  }
+
+  // RandomGenerator.hpp:158-197
+  __host__ __device__ void seed(int32_t s) {
+    if (s == 0) s = 1;
+    int32_t bits[31];
+    int32_t v = s & 0x7FFFFFFF;
+    for (int k = 0; k < 31; ++k) {
+      bits[k] = v % 2;
+      v /= 2;
+    }
+    int ib = 0, jb = 18;
+    for (int k = 0; k < 12; ++k) {
+      double acc = 0;
+      for (int m = 1; m <= 48; ++m) {
+        const double y = (double)((bits[ib] + 1) % 2);
+        acc += acc + y;
+        bits[ib] = (bits[ib] + bits[jb]) % 2;
+        ib = (ib + 1) % 31;
+        jb = (jb + 1) % 31;
+      }
+      x[k] = kOneBit * acc;
+    }
+    carry = 0;
+    ir = 11;
+    jr = 7;
+    ir_old = 0;
+    pr = 397;
+  }
+
+  // RandomGenerator.hpp:214-222
+  __host__ __device__ double uniform() {
+    ir = (ir + 1) % 12;
+    if (ir == ir_old) increment();
+    return x[ir];
+  }
+};
+
+}  // namespace cmi

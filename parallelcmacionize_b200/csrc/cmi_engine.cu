@@ -1,0 +1,1207 @@
+// Host side of the B200 transport engine: context, device memory, launch
+// sequence of one iteration, CUDA-graph capture and the extern "C" ABI of
+// include/cmacionize_b200.h.
+#include "cmacionize_b200.h"
+
+#include "cmi_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace cmi;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CMI_CUDA(call)                                                                     \
+  do {                                                                                     \
+    const cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? CMI_ERR_OUT_OF_MEMORY : CMI_ERR_CUDA, \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,       \
+                  __LINE__);                                                               \
+    }                                                                                      \
+  } while (0)
+
+#define CMI_TRY(expr)           \
+  do {                          \
+    const int rc_ = (expr);     \
+    if (rc_ != CMI_OK) return rc_; \
+  } while (0)
+
+constexpr int kWalkThreads = 256;
+
+struct HostInstance {
+  cmi_grid_desc desc;
+  int32_t sub_ncell[3];
+  int32_t cells_per_sub;
+  int32_t padded_per_sub;
+  uint32_t first_sub, nsub;
+  int64_t first_cell;  // padded offset of the first subgrid
+  int64_t ncells;
+  std::vector<double> src_pos, src_lum;
+  uint64_t num_photon = 0;
+};
+
+template <class T>
+int dev_alloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  CMI_CUDA(cudaMalloc((void **)p, sizeof(T) * count));
+  return CMI_OK;
+}
+
+template <class T>
+void dev_free(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+}  // namespace
+
+struct cmi_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cmi_options opt{};
+  int num_sms = 0;
+  std::vector<HostInstance> inst;
+  std::vector<DevSubgrid> h_sub;
+  uint32_t S = 0;
+  int64_t total_padded = 0;
+  int32_t max_padded = 0;
+  int rounds = 1;
+  DirectionTables tables{};
+
+  DevSubgrid *d_sub = nullptr;
+  DevInstance *d_inst = nullptr;
+  DevSource *d_src = nullptr;
+  int nsrc_total = 0;
+  double *d_nH = nullptr, *d_xH = nullptr, *d_J = nullptr;
+  float *d_kappa = nullptr;
+  uint64_t *d_src_count = nullptr, *d_src_first = nullptr, *d_buf_first = nullptr;
+  RoundState *d_state = nullptr;
+  DevStats *d_stats = nullptr;
+  uint32_t *d_hist = nullptr, *d_bucket_off = nullptr;
+  uint32_t *d_tile_pk = nullptr, *d_tile_ch = nullptr, *d_tile_pk_off = nullptr,
+           *d_tile_ch_off = nullptr;
+  uint32_t ntiles = 0;
+  Chunk *d_chunks = nullptr;
+  uint64_t chunk_capacity = 0;
+  void *d_arena_in = nullptr, *d_arena_out = nullptr;
+  uint32_t *d_keys = nullptr, *d_ranks = nullptr;
+  uint64_t capacity = 0;  // packets
+  double *d_stage = nullptr;
+  size_t stage_bytes = 0;
+
+  // walk launch configuration
+  int walk_grid = 0;
+  size_t walk_smem = 0;
+  uint32_t chunk = 4096;
+
+  // graph of one iteration
+  cudaGraphExec_t graph_exec = nullptr;
+  bool graph_dirty = true;
+  uint64_t graph_kernels = 0;
+  uint64_t last_launches = 0;
+  uint64_t enqueued = 0;  // kernel launches of the current enqueue
+  DevStats *h_stats = nullptr;  // pinned
+  size_t h_stats_count = 0;
+
+  // optional per-kernel event timing
+  bool timing = false;
+  struct Timed {
+    int cls;
+    cudaEvent_t start, stop;
+  };
+  std::vector<Timed> timed;
+  std::vector<cudaEvent_t> event_pool;
+
+  bool fp32() const { return opt.transport_precision == CMI_TRANSPORT_FP32; }
+  size_t packet_bytes() const { return fp32() ? sizeof(Packet32) : sizeof(Packet64); }
+};
+
+namespace {
+
+int check_ctx(cmi_context *c) {
+  if (!c) return fail(CMI_ERR_INVALID_ARGUMENT, "null context");
+  CMI_CUDA(cudaSetDevice(c->device));
+  return CMI_OK;
+}
+
+int check_instance(cmi_context *c, int32_t i) {
+  if (i < 0 || i >= (int32_t)c->inst.size())
+    return fail(CMI_ERR_INVALID_ARGUMENT, "instance %d out of range [0, %zu)", i, c->inst.size());
+  return CMI_OK;
+}
+
+void free_graph(cmi_context *c) {
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  c->graph_exec = nullptr;
+  c->graph_dirty = true;
+}
+
+cudaEvent_t pool_event(cmi_context *c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Event pair around the launches issued by `launch` (timing mode only).
+template <class F>
+int timed_launch(cmi_context *c, int cls, F &&launch) {
+  if (!c->timing) return launch();
+  cmi_context::Timed t{cls, pool_event(c), pool_event(c)};
+  cudaEventRecord(t.start, c->stream);
+  const int rc = launch();
+  cudaEventRecord(t.stop, c->stream);
+  c->timed.push_back(t);
+  return rc;
+}
+
+// Arena for `packets` packets in flight.
+int ensure_capacity(cmi_context *c, uint64_t packets) {
+  if (packets <= c->capacity && c->d_arena_in) return CMI_OK;
+  if (packets > 0xF0000000ull)
+    return fail(CMI_ERR_CAPACITY, "%llu packets exceed the 32-bit arena index",
+                (unsigned long long)packets);
+  const uint64_t cap = std::max<uint64_t>(packets, 1024);
+  free_graph(c);
+  dev_free(c->d_arena_in);
+  dev_free(c->d_arena_out);
+  dev_free(c->d_keys);
+  dev_free(c->d_ranks);
+  dev_free(c->d_chunks);
+  const size_t pb = c->packet_bytes();
+  CMI_CUDA(cudaMalloc(&c->d_arena_in, pb * cap));
+  CMI_CUDA(cudaMalloc(&c->d_arena_out, pb * cap));
+  CMI_TRY(dev_alloc(&c->d_keys, cap));
+  CMI_TRY(dev_alloc(&c->d_ranks, cap));
+  c->chunk_capacity = (uint64_t)c->S + cap / c->chunk + 16;
+  CMI_TRY(dev_alloc(&c->d_chunks, c->chunk_capacity));
+  c->capacity = cap;
+  const uint32_t cap32 = (uint32_t)cap;
+  CMI_CUDA(cudaMemcpyAsync(&c->d_state->capacity, &cap32, sizeof(cap32), cudaMemcpyHostToDevice,
+                           c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return CMI_OK;
+}
+
+int ensure_stage(cmi_context *c, size_t bytes) {
+  if (bytes <= c->stage_bytes) return CMI_OK;
+  dev_free(c->d_stage);
+  CMI_CUDA(cudaMalloc(&c->d_stage, bytes));
+  c->stage_bytes = bytes;
+  return CMI_OK;
+}
+
+uint64_t total_budget(const cmi_context *c) {
+  uint64_t n = 0;
+  for (const auto &I : c->inst) n += I.num_photon;
+  return n;
+}
+
+// Upload instance + source tables (after sources or budgets change).
+int upload_tables(cmi_context *c) {
+  std::vector<DevInstance> di(c->inst.size());
+  std::vector<DevSource> ds;
+  for (size_t i = 0; i < c->inst.size(); ++i) {
+    HostInstance &I = c->inst[i];
+    DevInstance &D = di[i];
+    double L = 0.;
+    for (double l : I.src_lum) L += l;
+    const double inv[3] = {I.sub_ncell[0] / (I.desc.box[3] / I.desc.num_subgrid[0]),
+                           I.sub_ncell[1] / (I.desc.box[4] / I.desc.num_subgrid[1]),
+                           I.sub_ncell[2] / (I.desc.box[5] / I.desc.num_subgrid[2])};
+    // DensitySubGrid.hpp:1633: luminosity / num_photon * inv_cell_size^3
+    D.jfac = (I.num_photon > 0) ? L / (double)I.num_photon * inv[0] * inv[1] * inv[2] : 0.;
+    D.alpha = I.desc.recombination_rate;
+    D.sigma = I.desc.cross_section;
+    D.total_luminosity = L;
+    D.num_photon = I.num_photon;
+    D.first_subgrid = I.first_sub;
+    D.num_subgrids = I.nsub;
+    D.first_source = (uint32_t)ds.size();
+    D.num_sources = (uint32_t)I.src_lum.size();
+    D.num_cells = I.ncells;
+    const int32_t *ns = I.desc.num_subgrid;
+    for (size_t k = 0; k < I.src_lum.size(); ++k) {
+      DevSource s{};
+      uint32_t si[3];
+      for (int a = 0; a < 3; ++a) {
+        s.position[a] = I.src_pos[3 * k + a];
+        // testDensitySubGrid_omp.cpp:1983-1990, clamped to the box
+        long v = (long)((s.position[a] - I.desc.box[a]) / I.desc.box[3 + a] * ns[a]);
+        v = std::min<long>(std::max<long>(v, 0), ns[a] - 1);
+        si[a] = (uint32_t)v;
+      }
+      const uint32_t local = (si[0] * ns[1] + si[1]) * ns[2] + si[2];
+      s.subgrid = I.first_sub + local;
+      const DevSubgrid &S = c->h_sub[s.subgrid];
+      for (int a = 0; a < 3; ++a) {
+        s.pos_cell[a] = (float)((s.position[a] - S.anchor[a]) * S.inv_cell_size[a]);
+      }
+      s.luminosity = I.src_lum[k];
+      s.instance = (uint32_t)i;
+      s.local_index = (uint32_t)k;
+      ds.push_back(s);
+    }
+  }
+  dev_free(c->d_src);
+  dev_free(c->d_src_count);
+  dev_free(c->d_src_first);
+  dev_free(c->d_buf_first);
+  c->nsrc_total = (int)ds.size();
+  CMI_TRY(dev_alloc(&c->d_src, ds.size()));
+  CMI_TRY(dev_alloc(&c->d_src_count, ds.size() + 1));
+  CMI_TRY(dev_alloc(&c->d_src_first, ds.size() + 1));
+  CMI_TRY(dev_alloc(&c->d_buf_first, ds.size() + 1));
+  if (!ds.empty())
+    CMI_CUDA(cudaMemcpyAsync(c->d_src, ds.data(), sizeof(DevSource) * ds.size(),
+                             cudaMemcpyHostToDevice, c->stream));
+  CMI_CUDA(cudaMemcpyAsync(c->d_inst, di.data(), sizeof(DevInstance) * di.size(),
+                           cudaMemcpyHostToDevice, c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  free_graph(c);
+  return CMI_OK;
+}
+
+int refresh_kappa(cmi_context *c, int32_t i) {
+  if (!c->fp32()) return CMI_OK;
+  const HostInstance &I = c->inst[i];
+  k_kappa<<<I.nsub, 256, 0, c->stream>>>(c->d_sub, c->d_inst, I.first_sub, c->d_nH, c->d_xH,
+                                         c->d_kappa);
+  CMI_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers (each counts its kernel)
+// ---------------------------------------------------------------------------
+int launch_plan(cmi_context *c) {
+  k_plan_count<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
+                                                          c->d_tile_pk, c->d_tile_ch);
+  k_plan_offsets<<<1, kPlanThreads, 0, c->stream>>>(c->ntiles, c->d_tile_pk, c->d_tile_ch,
+                                                     c->d_tile_pk_off, c->d_tile_ch_off,
+                                                     c->d_state);
+  k_plan_write<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
+                                                          c->d_tile_pk_off, c->d_tile_ch_off,
+                                                          c->d_bucket_off, c->d_chunks);
+  const int grid = c->num_sms * 8;
+  if (c->fp32()) {
+    k_scatter<Packet32><<<grid, 256, 0, c->stream>>>(
+        (const Packet32 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
+        (Packet32 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
+  } else {
+    k_scatter<Packet64><<<grid, 256, 0, c->stream>>>(
+        (const Packet64 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
+        (Packet64 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
+  }
+  c->enqueued += 4;
+  CMI_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+
+WalkParams walk_params(cmi_context *c) {
+  WalkParams p{};
+  p.subs = c->d_sub;
+  p.inst = c->d_inst;
+  p.chunks = c->d_chunks;
+  p.st = c->d_state;
+  p.stats = c->d_stats;
+  p.arena_in = c->d_arena_in;
+  p.arena_out = c->d_arena_out;
+  p.keys = c->d_keys;
+  p.ranks = c->d_ranks;
+  p.hist = c->d_hist;
+  p.capacity = (uint32_t)c->capacity;
+  p.max_padded = c->max_padded;
+  p.kappa = c->d_kappa;
+  p.nH = c->d_nH;
+  p.xH = c->d_xH;
+  p.J = c->d_J;
+  p.tables = c->tables;
+  return p;
+}
+
+template <bool kF32, bool kComp>
+void launch_walk_t(cmi_context *c, const WalkParams &p) {
+  k_walk<kF32, kComp, kWalkThreads><<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+}
+
+int launch_walk(cmi_context *c) {
+  const WalkParams p = walk_params(c);
+  if (c->fp32()) {
+    if (c->opt.compensated_tally) launch_walk_t<true, true>(c, p);
+    else launch_walk_t<true, false>(c, p);
+  } else {
+    launch_walk_t<false, false>(c, p);
+  }
+  c->enqueued += 1;
+  CMI_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+
+template <bool kF32, bool kComp>
+int config_walk_t(cmi_context *c) {
+  auto fn = k_walk<kF32, kComp, kWalkThreads>;
+  CMI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)c->walk_smem));
+  int per_sm = 0;
+  CMI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWalkThreads,
+                                                         c->walk_smem));
+  if (per_sm <= 0)
+    return fail(CMI_ERR_NOT_SUPPORTED, "walk kernel does not fit on an SM (smem %zu B)",
+                c->walk_smem);
+  if (c->opt.ctas_per_sm > 0) per_sm = std::min(per_sm, (int)c->opt.ctas_per_sm);
+  c->walk_grid = c->num_sms * per_sm;
+  return CMI_OK;
+}
+
+int config_walk(cmi_context *c) {
+  const size_t head = (sizeof(WalkShared) + 15) & ~(size_t)15;
+  const size_t per_cell = c->fp32() ? (c->opt.compensated_tally ? 12 : 8) : 24;
+  c->walk_smem = head + per_cell * (size_t)c->max_padded;
+  if (c->fp32()) {
+    if (c->opt.compensated_tally) return config_walk_t<true, true>(c);
+    return config_walk_t<true, false>(c);
+  }
+  return config_walk_t<false, false>(c);
+}
+
+EmitParams emit_params(cmi_context *c) {
+  EmitParams e{};
+  e.inst = c->d_inst;
+  e.src = c->d_src;
+  e.nsrc_total = c->nsrc_total;
+  e.src_count = c->d_src_count;
+  e.src_first = c->d_src_first;
+  e.buf_first = c->d_buf_first;
+  e.st = c->d_state;
+  e.arena = c->d_arena_out;
+  e.keys = c->d_keys;
+  e.ranks = c->d_ranks;
+  e.hist = c->d_hist;
+  e.capacity = (uint32_t)c->capacity;
+  return e;
+}
+
+// Wavefront rounds after packets were appended to the arena.
+int enqueue_rounds(cmi_context *c) {
+  for (int r = 0; r < c->rounds; ++r) {
+    CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c); }));
+    CMI_TRY(timed_launch(c, 0, [&] { return launch_walk(c); }));
+  }
+  // final plan: counts what the last round left over (must be zero)
+  CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c); }));
+  return CMI_OK;
+}
+
+int enqueue_iteration(cmi_context *c, bool balance) {
+  const int ninst = (int)c->inst.size();
+  k_begin_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst);
+  k_emission_plan<<<1, 128, 0, c->stream>>>(c->d_inst, ninst, c->d_src, c->nsrc_total,
+                                            c->d_state, c->d_src_count, c->d_src_first,
+                                            c->d_buf_first, c->d_stats);
+  c->enqueued += 2;
+  const EmitParams e = emit_params(c);
+  const int egrid = c->num_sms * 8;
+  CMI_TRY(timed_launch(c, 2, [&] {
+    if (c->opt.rng == CMI_RNG_RANLUX) {
+      if (c->fp32()) k_emit_ranlux<true><<<egrid, 128, 0, c->stream>>>(e);
+      else k_emit_ranlux<false><<<egrid, 128, 0, c->stream>>>(e);
+    } else {
+      if (c->fp32()) k_emit_philox<true><<<egrid, 256, 0, c->stream>>>(e);
+      else k_emit_philox<false><<<egrid, 256, 0, c->stream>>>(e);
+    }
+    return CMI_OK;
+  }));
+  c->enqueued += 1;
+  CMI_CUDA(cudaGetLastError());
+  CMI_TRY(enqueue_rounds(c));
+  if (balance) {
+    BalanceParams b{};
+    b.subs = c->d_sub;
+    b.inst = c->d_inst;
+    b.nH = c->d_nH;
+    b.xH = c->d_xH;
+    b.J = c->d_J;
+    b.kappa = c->fp32() ? c->d_kappa : nullptr;
+    b.stats = c->d_stats;
+    b.first_sub = 0;
+    b.num_subs = c->S;
+    b.jfac_override = -1.;
+    CMI_TRY(timed_launch(c, 3, [&] {
+      if (c->opt.balance_form == CMI_BALANCE_REFERENCE)
+        k_balance<0><<<c->S, 256, 0, c->stream>>>(b);
+      else
+        k_balance<1><<<c->S, 256, 0, c->stream>>>(b);
+      return CMI_OK;
+    }));
+    c->enqueued += 1;
+  }
+  k_end_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst, 1);
+  c->enqueued += 1;
+  CMI_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+
+int validate_ready(cmi_context *c) {
+  for (size_t i = 0; i < c->inst.size(); ++i) {
+    if (c->inst[i].num_photon > 0 && c->inst[i].src_lum.empty())
+      return fail(CMI_ERR_INVALID_ARGUMENT, "instance %zu has a packet budget but no sources", i);
+  }
+  return ensure_capacity(c, total_budget(c));
+}
+
+void to_stats(const DevStats &d, const HostInstance &I, cmi_stats &s) {
+  s.packets_emitted = d.emitted;
+  s.packets_absorbed = d.absorbed;
+  s.packets_escaped = d.escaped;
+  s.cell_crossings = d.crossings;
+  s.subgrid_transits = d.transits;
+  s.mean_abs_dx = (I.ncells > 0) ? d.dx_sum / (double)I.ncells : 0.;
+  s.error_flags = d.flags;
+  s.rounds = d.rounds;
+}
+
+int ensure_host_stats(cmi_context *c, size_t n) {
+  if (n <= c->h_stats_count) return CMI_OK;
+  if (c->h_stats) cudaFreeHost(c->h_stats);
+  c->h_stats = nullptr;
+  CMI_CUDA(cudaMallocHost((void **)&c->h_stats, sizeof(DevStats) * n));
+  c->h_stats_count = n;
+  return CMI_OK;
+}
+
+int run(cmi_context *c, int32_t iterations, uint64_t seed, uint32_t first_iteration,
+        bool balance, cmi_stats *stats) {
+  CMI_TRY(validate_ready(c));
+  const int ninst = (int)c->inst.size();
+  CMI_TRY(ensure_host_stats(c, (size_t)iterations * ninst));
+  const uint64_t hs[2] = {seed, 0};
+  CMI_CUDA(cudaMemcpyAsync(&c->d_state->seed, hs, sizeof(uint64_t), cudaMemcpyHostToDevice,
+                           c->stream));
+  CMI_CUDA(cudaMemcpyAsync(&c->d_state->iteration, &first_iteration, sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, c->stream));
+  c->last_launches = 0;
+  const bool use_graph = c->opt.use_graph != 0 && balance && !c->timing;
+  if (use_graph && (c->graph_dirty || !c->graph_exec)) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+    cudaGraph_t g = nullptr;
+    CMI_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    c->enqueued = 0;
+    const int rc = enqueue_iteration(c, true);
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    if (rc != CMI_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ec != cudaSuccess) return fail(CMI_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess)
+      return fail(CMI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+    c->graph_kernels = c->enqueued;
+    c->graph_dirty = false;
+  }
+  for (int32_t it = 0; it < iterations; ++it) {
+    if (use_graph) {
+      CMI_CUDA(cudaGraphLaunch(c->graph_exec, c->stream));
+      c->last_launches += c->graph_kernels;
+    } else {
+      c->enqueued = 0;
+      CMI_TRY(enqueue_iteration(c, balance));
+      c->last_launches += c->enqueued;
+    }
+    CMI_CUDA(cudaMemcpyAsync(c->h_stats + (size_t)it * ninst, c->d_stats,
+                             sizeof(DevStats) * ninst, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  uint32_t flags_any = 0;
+  for (int32_t it = 0; it < iterations; ++it)
+    for (int i = 0; i < ninst; ++i) {
+      const DevStats &d = c->h_stats[(size_t)it * ninst + i];
+      flags_any |= d.flags;
+      if (stats) to_stats(d, c->inst[i], stats[(size_t)it * ninst + i]);
+    }
+  if (flags_any & (kFlagArenaOverflow | kFlagLeftover))
+    return fail(CMI_ERR_CAPACITY, "device queue overflow or packets left over (flags 0x%x)",
+                flags_any);
+  if (flags_any & kFlagStageTimeout)
+    return fail(CMI_ERR_DEVICE_TIMEOUT, "shared-memory staging wait timed out (flags 0x%x)",
+                flags_any);
+  if (flags_any & (kFlagWalkLimit | kFlagBadInput))
+    return fail(CMI_ERR_INVARIANT, "device invariant violated (flags 0x%x)", flags_any);
+  return CMI_OK;
+}
+
+int clear_flags(cmi_context *c) {
+  const uint32_t z = 0;
+  CMI_CUDA(cudaMemcpyAsync(&c->d_state->flags, &z, sizeof(z), cudaMemcpyHostToDevice, c->stream));
+  return CMI_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// extern "C" ABI
+// ===========================================================================
+extern "C" {
+
+int cmi_abi_version(void) { return CMI_ABI_VERSION; }
+
+const char *cmi_last_error_string(void) { return g_last_error.c_str(); }
+
+void cmi_default_options(cmi_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->transport_precision = CMI_TRANSPORT_FP32;
+  o->balance_form = CMI_BALANCE_STABLE;
+  o->rng = CMI_RNG_PHILOX;
+  o->device = 0;
+  o->threads_per_cta = 0;
+  o->ctas_per_sm = 0;
+  o->packets_per_chunk = 0;
+  o->compensated_tally = 1;
+  o->use_graph = 1;
+}
+
+int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_options *options,
+               cmi_context **out) {
+  if (!out) return fail(CMI_ERR_INVALID_ARGUMENT, "null output pointer");
+  *out = nullptr;
+  if (!grids || num_instances <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "no grid given");
+  cmi_options opt;
+  if (options) opt = *options; else cmi_default_options(&opt);
+  if (opt.transport_precision != CMI_TRANSPORT_FP32 && opt.transport_precision != CMI_TRANSPORT_FP64)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "unknown transport precision %d", opt.transport_precision);
+  if (opt.balance_form != CMI_BALANCE_REFERENCE && opt.balance_form != CMI_BALANCE_STABLE)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "unknown balance form %d", opt.balance_form);
+  if (opt.rng != CMI_RNG_PHILOX && opt.rng != CMI_RNG_RANLUX)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "unknown rng %d", opt.rng);
+  if (opt.threads_per_cta != 0 && opt.threads_per_cta != kWalkThreads)
+    return fail(CMI_ERR_NOT_SUPPORTED, "threads_per_cta must be 0 or %d", kWalkThreads);
+  if (opt.packets_per_chunk < 0) return fail(CMI_ERR_INVALID_ARGUMENT, "negative chunk size");
+
+  cmi_context *c = new (std::nothrow) cmi_context();
+  if (!c) return fail(CMI_ERR_OUT_OF_MEMORY, "host allocation failed");
+  c->opt = opt;
+  c->device = opt.device;
+  c->tables = make_direction_tables();
+  c->chunk = opt.packets_per_chunk > 0 ? (uint32_t)opt.packets_per_chunk : 4096u;
+  auto bail = [&](int rc) {
+    cmi_destroy(c);
+    return rc;
+  };
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    delete c;
+    return fail(CMI_ERR_CUDA, "no CUDA device available");
+  }
+  if (c->device < 0 || c->device >= ndev) {
+    const int dev = c->device;
+    delete c;
+    return fail(CMI_ERR_INVALID_ARGUMENT, "device %d out of range", dev);
+  }
+  if (cudaSetDevice(c->device) != cudaSuccess) {
+    delete c;
+    return fail(CMI_ERR_CUDA, "cudaSetDevice failed");
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(CMI_ERR_CUDA, "stream creation failed");
+  }
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+
+  // ---- instances and the global subgrid table ----
+  int64_t cell_off = 0;
+  for (int32_t i = 0; i < num_instances; ++i) {
+    const cmi_grid_desc &g = grids[i];
+    HostInstance I;
+    I.desc = g;
+    for (int a = 0; a < 3; ++a) {
+      if (g.ncell[a] <= 0 || g.num_subgrid[a] <= 0 || g.ncell[a] % g.num_subgrid[a] != 0)
+        return bail(fail(CMI_ERR_INVALID_ARGUMENT,
+                         "instance %d: ncell must be a positive multiple of num_subgrid", i));
+      if (!(g.box[3 + a] > 0.))
+        return bail(fail(CMI_ERR_INVALID_ARGUMENT, "instance %d: box sides must be > 0", i));
+      I.sub_ncell[a] = g.ncell[a] / g.num_subgrid[a];
+    }
+    if (!(g.recombination_rate > 0.) || !(g.cross_section > 0.))
+      return bail(fail(CMI_ERR_INVALID_ARGUMENT,
+                       "instance %d: recombination rate and cross section must be > 0", i));
+    I.cells_per_sub = I.sub_ncell[0] * I.sub_ncell[1] * I.sub_ncell[2];
+    I.padded_per_sub = (I.cells_per_sub + 3) & ~3;
+    if (I.padded_per_sub > 8192 || (opt.transport_precision == CMI_TRANSPORT_FP64 && I.padded_per_sub > 4096))
+      return bail(fail(CMI_ERR_NOT_SUPPORTED,
+                       "instance %d: %d cells per subgrid exceed the shared-memory limit "
+                       "(4096 in FP64, 8192 in FP32)",
+                       i, I.cells_per_sub));
+    I.first_sub = (uint32_t)c->h_sub.size();
+    I.nsub = (uint32_t)g.num_subgrid[0] * g.num_subgrid[1] * g.num_subgrid[2];
+    I.first_cell = cell_off;
+    I.ncells = (int64_t)g.ncell[0] * g.ncell[1] * g.ncell[2];
+    const double side[3] = {g.box[3] / g.num_subgrid[0], g.box[4] / g.num_subgrid[1],
+                            g.box[5] / g.num_subgrid[2]};
+    const int32_t *ns = g.num_subgrid;
+    for (uint32_t s = 0; s < I.nsub; ++s) {
+      const int ix = s / (ns[1] * ns[2]);
+      const int iy = (s - ix * ns[1] * ns[2]) / ns[2];
+      const int iz = s - ix * ns[1] * ns[2] - iy * ns[2];
+      DevSubgrid S{};
+      const int idx3[3] = {ix, iy, iz};
+      for (int a = 0; a < 3; ++a) {
+        // DensitySubGrid(box, ncell), testDensitySubGrid_omp.cpp:1822-1828
+        S.anchor[a] = g.box[a] + idx3[a] * side[a];
+        S.cell_size[a] = side[a] / I.sub_ncell[a];
+        S.inv_cell_size[a] = I.sub_ncell[a] / side[a];
+        S.cell_size_f[a] = (float)S.cell_size[a];
+        S.ncell[a] = I.sub_ncell[a];
+      }
+      S.ncells = I.cells_per_sub;
+      S.padded_cells = I.padded_per_sub;
+      S.field_offset = cell_off;
+      cell_off += I.padded_per_sub;
+      S.instance = (uint32_t)i;
+      for (int d = 0; d < kNumDirections; ++d) S.ngb[d] = kOutside;
+      for (int nx = -1; nx < 2; ++nx)
+        for (int ny = -1; ny < 2; ++ny)
+          for (int nz = -1; nz < 2; ++nz) {
+            const int cx = ix + nx, cy = iy + ny, cz = iz + nz;
+            if (cx >= 0 && cx < ns[0] && cy >= 0 && cy < ns[1] && cz >= 0 && cz < ns[2])
+              S.ngb[dir_from_signs(nx, ny, nz)] = I.first_sub + (uint32_t)((cx * ns[1] + cy) * ns[2] + cz);
+          }
+      c->h_sub.push_back(S);
+    }
+    c->max_padded = std::max(c->max_padded, I.padded_per_sub);
+    c->rounds = std::max(c->rounds, ns[0] + ns[1] + ns[2] - 2);
+    c->inst.push_back(I);
+  }
+  c->S = (uint32_t)c->h_sub.size();
+  c->total_padded = cell_off;
+  c->ntiles = (c->S + kPlanTile - 1) / kPlanTile;
+
+  int rc = CMI_OK;
+  if ((rc = dev_alloc(&c->d_sub, c->S)) || (rc = dev_alloc(&c->d_inst, c->inst.size())) ||
+      (rc = dev_alloc(&c->d_nH, c->total_padded)) || (rc = dev_alloc(&c->d_xH, c->total_padded)) ||
+      (rc = dev_alloc(&c->d_J, c->total_padded)) ||
+      (rc = dev_alloc(&c->d_kappa, c->fp32() ? c->total_padded : 1)) ||
+      (rc = dev_alloc(&c->d_state, 1)) || (rc = dev_alloc(&c->d_stats, c->inst.size())) ||
+      (rc = dev_alloc(&c->d_hist, c->S)) || (rc = dev_alloc(&c->d_bucket_off, c->S)) ||
+      (rc = dev_alloc(&c->d_tile_pk, c->ntiles)) || (rc = dev_alloc(&c->d_tile_ch, c->ntiles)) ||
+      (rc = dev_alloc(&c->d_tile_pk_off, c->ntiles)) ||
+      (rc = dev_alloc(&c->d_tile_ch_off, c->ntiles)))
+    return bail(rc);
+  if (cudaMemcpyAsync(c->d_sub, c->h_sub.data(), sizeof(DevSubgrid) * c->S,
+                      cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_state, 0, sizeof(RoundState), c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_hist, 0, sizeof(uint32_t) * c->S, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_J, 0, sizeof(double) * c->total_padded, c->stream) != cudaSuccess)
+    return bail(fail(CMI_ERR_CUDA, "initial upload failed"));
+  // reference initial state, DensitySubGrid.hpp:544-551
+  k_fill<<<c->num_sms * 4, 256, 0, c->stream>>>(c->d_nH, 1.e8, c->total_padded);
+  k_fill<<<c->num_sms * 4, 256, 0, c->stream>>>(c->d_xH, 1.e-6, c->total_padded);
+  if (cudaGetLastError() != cudaSuccess) return bail(fail(CMI_ERR_CUDA, "initial fill failed"));
+  if ((rc = upload_tables(c))) return bail(rc);
+  for (int32_t i = 0; i < num_instances; ++i)
+    if ((rc = refresh_kappa(c, i))) return bail(rc);
+  if ((rc = config_walk(c))) return bail(rc);
+  int64_t max_cells = 0;
+  for (const auto &I : c->inst) max_cells = std::max(max_cells, I.ncells);
+  if ((rc = ensure_stage(c, sizeof(double) * (size_t)max_cells))) return bail(rc);
+  if ((rc = ensure_capacity(c, 1024))) return bail(rc);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return bail(fail(CMI_ERR_CUDA, "context set-up failed: %s",
+                     cudaGetErrorString(cudaGetLastError())));
+  *out = c;
+  return CMI_OK;
+}
+
+int cmi_destroy(cmi_context *c) {
+  if (!c) return CMI_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_graph(c);
+  dev_free(c->d_sub);
+  dev_free(c->d_inst);
+  dev_free(c->d_src);
+  dev_free(c->d_nH);
+  dev_free(c->d_xH);
+  dev_free(c->d_J);
+  dev_free(c->d_kappa);
+  dev_free(c->d_src_count);
+  dev_free(c->d_src_first);
+  dev_free(c->d_buf_first);
+  dev_free(c->d_state);
+  dev_free(c->d_stats);
+  dev_free(c->d_hist);
+  dev_free(c->d_bucket_off);
+  dev_free(c->d_tile_pk);
+  dev_free(c->d_tile_ch);
+  dev_free(c->d_tile_pk_off);
+  dev_free(c->d_tile_ch_off);
+  dev_free(c->d_chunks);
+  dev_free(c->d_arena_in);
+  dev_free(c->d_arena_out);
+  dev_free(c->d_keys);
+  dev_free(c->d_ranks);
+  dev_free(c->d_stage);
+  if (c->h_stats) cudaFreeHost(c->h_stats);
+  for (auto &t : c->timed) {
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return CMI_OK;
+}
+
+static int copy_field_in(cmi_context *c, int32_t instance, int32_t layout, int32_t memory,
+                         const double *src, double *dst) {
+  const HostInstance &I = c->inst[instance];
+  const double *dsrc = src;
+  if (memory == CMI_MEMORY_HOST) {
+    CMI_CUDA(cudaMemcpyAsync(c->d_stage, src, sizeof(double) * I.ncells, cudaMemcpyHostToDevice,
+                             c->stream));
+    dsrc = c->d_stage;
+  }
+  LayoutParams lp{};
+  lp.subs = c->d_sub;
+  lp.first_sub = I.first_sub;
+  for (int a = 0; a < 3; ++a) {
+    lp.ns[a] = I.desc.num_subgrid[a];
+    lp.ncell[a] = I.desc.ncell[a];
+  }
+  lp.layout = layout;
+  k_fields_in<<<I.nsub, 256, 0, c->stream>>>(lp, dsrc, dst);
+  CMI_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+
+static int copy_field_out(cmi_context *c, int32_t instance, int32_t layout, int32_t memory,
+                          const double *src, double *dst) {
+  const HostInstance &I = c->inst[instance];
+  double *ddst = (memory == CMI_MEMORY_HOST) ? c->d_stage : dst;
+  LayoutParams lp{};
+  lp.subs = c->d_sub;
+  lp.first_sub = I.first_sub;
+  for (int a = 0; a < 3; ++a) {
+    lp.ns[a] = I.desc.num_subgrid[a];
+    lp.ncell[a] = I.desc.ncell[a];
+  }
+  lp.layout = layout;
+  k_fields_out<<<I.nsub, 256, 0, c->stream>>>(lp, src, ddst);
+  CMI_CUDA(cudaGetLastError());
+  if (memory == CMI_MEMORY_HOST) {
+    CMI_CUDA(cudaMemcpyAsync(dst, c->d_stage, sizeof(double) * I.ncells, cudaMemcpyDeviceToHost,
+                             c->stream));
+    CMI_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return CMI_OK;
+}
+
+static int check_layout(int32_t layout, int32_t memory) {
+  if (layout != CMI_LAYOUT_BLOCKED && layout != CMI_LAYOUT_CUBE)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "unknown layout %d", layout);
+  if (memory != CMI_MEMORY_HOST && memory != CMI_MEMORY_DEVICE)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "unknown memory kind %d", memory);
+  return CMI_OK;
+}
+
+int cmi_set_fields(cmi_context *c, int32_t instance, int32_t layout, int32_t memory,
+                   const double *nH, const double *xH) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  CMI_TRY(check_layout(layout, memory));
+  if (nH) CMI_TRY(copy_field_in(c, instance, layout, memory, nH, c->d_nH));
+  if (xH) CMI_TRY(copy_field_in(c, instance, layout, memory, xH, c->d_xH));
+  CMI_TRY(refresh_kappa(c, instance));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return CMI_OK;
+}
+
+int cmi_get_fields(cmi_context *c, int32_t instance, int32_t layout, int32_t memory, double *xH,
+                   double *J) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  CMI_TRY(check_layout(layout, memory));
+  if (xH) CMI_TRY(copy_field_out(c, instance, layout, memory, c->d_xH, xH));
+  if (J) CMI_TRY(copy_field_out(c, instance, layout, memory, c->d_J, J));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return CMI_OK;
+}
+
+int cmi_set_intensity(cmi_context *c, int32_t instance, int32_t layout, int32_t memory,
+                      const double *J) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  CMI_TRY(check_layout(layout, memory));
+  if (!J) return fail(CMI_ERR_INVALID_ARGUMENT, "null intensity array");
+  CMI_TRY(copy_field_in(c, instance, layout, memory, J, c->d_J));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return CMI_OK;
+}
+
+int cmi_set_sources(cmi_context *c, int32_t instance, const double *positions,
+                    const double *luminosities, int32_t n) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  if (n < 0 || n > 64) return fail(CMI_ERR_INVALID_ARGUMENT, "0..64 sources per instance, got %d", n);
+  if (n > 0 && (!positions || !luminosities))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "null source arrays");
+  HostInstance &I = c->inst[instance];
+  for (int32_t k = 0; k < n; ++k) {
+    if (!(luminosities[k] > 0.) || !std::isfinite(luminosities[k]))
+      return fail(CMI_ERR_INVALID_ARGUMENT, "source %d: luminosity must be finite and > 0", k);
+    for (int a = 0; a < 3; ++a) {
+      const double p = positions[3 * k + a];
+      if (!(p >= I.desc.box[a] && p <= I.desc.box[a] + I.desc.box[3 + a]))
+        return fail(CMI_ERR_INVALID_ARGUMENT, "source %d lies outside the box", k);
+    }
+  }
+  I.src_pos.assign(positions, positions + 3 * n);
+  I.src_lum.assign(luminosities, luminosities + n);
+  return upload_tables(c);
+}
+
+int cmi_set_packet_budget(cmi_context *c, int32_t instance, uint64_t num_photon) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  c->inst[instance].num_photon = num_photon;
+  CMI_TRY(upload_tables(c));
+  return ensure_capacity(c, total_budget(c));
+}
+
+int cmi_run_iterations(cmi_context *c, int32_t iterations, uint64_t seed, cmi_stats *stats) {
+  CMI_TRY(check_ctx(c));
+  if (iterations <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "iterations must be > 0");
+  CMI_TRY(clear_flags(c));
+  // the first iteration index of this call continues from the previous call
+  uint32_t it0 = 0;
+  CMI_CUDA(cudaMemcpyAsync(&it0, &c->d_state->iteration, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return run(c, iterations, seed, it0, true, stats);
+}
+
+int cmi_shoot_packets(cmi_context *c, uint64_t seed, uint32_t iteration, cmi_stats *stats) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(clear_flags(c));
+  return run(c, 1, seed, iteration, false, stats);
+}
+
+int cmi_transport_packets(cmi_context *c, int32_t instance, const cmi_photon *packets,
+                          const uint32_t *start_subgrid, uint64_t n, cmi_stats *stats) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  if (n > 0 && (!packets || !start_subgrid))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "null packet arrays");
+  CMI_TRY(clear_flags(c));
+  CMI_TRY(ensure_capacity(c, std::max<uint64_t>(n, total_budget(c))));
+  const size_t bytes = sizeof(Packet64) * n + sizeof(uint32_t) * n + 64;
+  CMI_TRY(ensure_stage(c, bytes));
+  Packet64 *d_ph = reinterpret_cast<Packet64 *>(c->d_stage);
+  uint32_t *d_start = reinterpret_cast<uint32_t *>(
+      reinterpret_cast<char *>(c->d_stage) + ((sizeof(Packet64) * n + 15) & ~(size_t)15));
+  if (n > 0) {
+    CMI_CUDA(cudaMemcpyAsync(d_ph, packets, sizeof(Packet64) * n, cudaMemcpyHostToDevice,
+                             c->stream));
+    CMI_CUDA(cudaMemcpyAsync(d_start, start_subgrid, sizeof(uint32_t) * n,
+                             cudaMemcpyHostToDevice, c->stream));
+  }
+  const int ninst = (int)c->inst.size();
+  k_begin_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst);
+  const HostInstance &I = c->inst[instance];
+  UploadParams u{};
+  u.photons = d_ph;
+  u.start = d_start;
+  u.n = n;
+  u.subs = c->d_sub;
+  u.first_sub = I.first_sub;
+  u.nsub = I.nsub;
+  u.st = c->d_state;
+  u.arena = c->d_arena_out;
+  u.keys = c->d_keys;
+  u.ranks = c->d_ranks;
+  u.hist = c->d_hist;
+  u.capacity = (uint32_t)c->capacity;
+  const int grid = c->num_sms * 8;
+  if (c->fp32()) k_upload<true><<<grid, 256, 0, c->stream>>>(u);
+  else k_upload<false><<<grid, 256, 0, c->stream>>>(u);
+  CMI_CUDA(cudaGetLastError());
+  c->enqueued = 0;
+  CMI_TRY(enqueue_rounds(c));
+  k_end_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst, 0);
+  CMI_CUDA(cudaGetLastError());
+  c->last_launches = c->enqueued + 3;
+  CMI_TRY(ensure_host_stats(c, ninst));
+  CMI_CUDA(cudaMemcpyAsync(c->h_stats, c->d_stats, sizeof(DevStats) * ninst,
+                           cudaMemcpyDeviceToHost, c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  DevStats d = c->h_stats[instance];
+  d.emitted = n;
+  if (stats) to_stats(d, I, *stats);
+  if (d.flags & (kFlagArenaOverflow | kFlagLeftover))
+    return fail(CMI_ERR_CAPACITY, "device queue overflow or packets left over (flags 0x%x)",
+                d.flags);
+  if (d.flags & kFlagBadInput) return fail(CMI_ERR_INVALID_ARGUMENT, "start subgrid out of range");
+  if (d.flags & kFlagStageTimeout) return fail(CMI_ERR_DEVICE_TIMEOUT, "staging wait timed out");
+  if (d.flags & kFlagWalkLimit) return fail(CMI_ERR_INVARIANT, "walk step bound exceeded");
+  return CMI_OK;
+}
+
+static int traverse(cmi_context *c, int32_t instance, uint32_t subgrid, int32_t input_direction,
+                    const cmi_photon *in, uint32_t n, cmi_photon *out_grouped,
+                    int32_t *out_dir_host, const uint8_t *enabled, uint32_t *out_count,
+                    uint32_t *num_done, int32_t max_steps, int32_t *cells, double *lengths,
+                    int32_t *num_steps) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  const HostInstance &I = c->inst[instance];
+  if (subgrid >= I.nsub)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "subgrid %u out of range [0, %u)", subgrid, I.nsub);
+  if (input_direction < 0 || input_direction >= kNumDirections)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "input direction %d out of range", input_direction);
+  if (n > 0 && !in) return fail(CMI_ERR_INVALID_ARGUMENT, "null input buffer");
+  CMI_TRY(clear_flags(c));
+  const size_t a16 = (sizeof(Packet64) * (size_t)n + 15) & ~(size_t)15;
+  const size_t bytes = 2 * a16 + 16 * (size_t)n + 27 * 4 + 256 + 16 * (size_t)std::max(max_steps, 0);
+  CMI_TRY(ensure_stage(c, bytes));
+  char *base = reinterpret_cast<char *>(c->d_stage);
+  Packet64 *d_in = reinterpret_cast<Packet64 *>(base);
+  Packet64 *d_out = reinterpret_cast<Packet64 *>(base + a16);
+  int32_t *d_dir = reinterpret_cast<int32_t *>(base + 2 * a16);
+  char *tail = base + 2 * a16 + (((size_t)n * 4 + 15) & ~(size_t)15);
+  uint32_t *d_counts = reinterpret_cast<uint32_t *>(tail);
+  uint32_t *d_done = d_counts + 28;
+  uint8_t *d_enabled = reinterpret_cast<uint8_t *>(d_counts + 32);
+  int32_t *d_steps = reinterpret_cast<int32_t *>(d_counts + 48);
+  int32_t *d_cells = reinterpret_cast<int32_t *>(d_counts + 64);
+  double *d_len = reinterpret_cast<double *>(
+      (reinterpret_cast<uintptr_t>(d_cells + std::max(max_steps, 1)) + 15) & ~(uintptr_t)15);
+  if (n > 0)
+    CMI_CUDA(cudaMemcpyAsync(d_in, in, sizeof(Packet64) * n, cudaMemcpyHostToDevice, c->stream));
+  if (enabled)
+    CMI_CUDA(cudaMemcpyAsync(d_enabled, enabled, 27, cudaMemcpyHostToDevice, c->stream));
+  TraverseParams t{};
+  t.subs = c->d_sub;
+  t.inst = c->d_inst;
+  t.sub = I.first_sub + subgrid;
+  t.input_direction = input_direction;
+  t.in = d_in;
+  t.n = n;
+  t.out = d_out;
+  t.out_dir = d_dir;
+  t.kappa = c->d_kappa;
+  t.nH = c->d_nH;
+  t.xH = c->d_xH;
+  t.J = c->d_J;
+  t.max_padded = c->max_padded;
+  t.trace_cells = d_cells;
+  t.trace_len = d_len;
+  t.max_steps = max_steps;
+  t.trace_steps = num_steps ? d_steps : nullptr;
+  t.st = c->d_state;
+  t.tables = c->tables;
+  const size_t smem = (c->fp32() ? 12 : 24) * (size_t)c->max_padded;
+  if (n > 0) {
+    const int grid = (int)((n + 255) / 256);
+    if (c->fp32()) {
+      CMI_CUDA(cudaFuncSetAttribute(k_traverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+      k_traverse<true><<<grid, 256, smem, c->stream>>>(t);
+    } else {
+      CMI_CUDA(cudaFuncSetAttribute(k_traverse<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_traverse<false><<<grid, 256, smem, c->stream>>>(t);
+    }
+    CMI_CUDA(cudaGetLastError());
+  }
+  if (out_grouped) {
+    k_partition<<<1, 256, 0, c->stream>>>(d_out, d_dir, n, enabled ? d_enabled : nullptr,
+                                          reinterpret_cast<Packet64 *>(d_in), d_counts, d_done);
+    CMI_CUDA(cudaGetLastError());
+  }
+  uint32_t flags = 0;
+  CMI_CUDA(cudaMemcpyAsync(&flags, &c->d_state->flags, sizeof(flags), cudaMemcpyDeviceToHost,
+                           c->stream));
+  uint32_t counts[28] = {0};
+  if (out_grouped) {
+    CMI_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof(uint32_t) * 28, cudaMemcpyDeviceToHost,
+                             c->stream));
+  }
+  if (out_dir_host && n > 0)
+    CMI_CUDA(cudaMemcpyAsync(out_dir_host, d_dir, sizeof(int32_t) * n, cudaMemcpyDeviceToHost,
+                             c->stream));
+  int32_t steps = 0;
+  if (num_steps)
+    CMI_CUDA(cudaMemcpyAsync(&steps, d_steps, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  if (out_grouped) {
+    uint32_t kept = 0;
+    for (int d = 0; d < kNumDirections; ++d) {
+      out_count[d] = counts[d];
+      kept += counts[d];
+    }
+    uint32_t done = 0;
+    CMI_CUDA(cudaMemcpy(&done, d_done, sizeof(done), cudaMemcpyDeviceToHost));
+    if (num_done) *num_done = done;
+    if (kept > 0)
+      CMI_CUDA(cudaMemcpy(out_grouped, d_in, sizeof(Packet64) * kept, cudaMemcpyDeviceToHost));
+  } else if (n > 0 && out_dir_host) {
+    // single packet trace: photon comes back in place of the input
+    CMI_CUDA(cudaMemcpy(const_cast<cmi_photon *>(in), d_out, sizeof(Packet64) * n,
+                        cudaMemcpyDeviceToHost));
+  }
+  if (num_steps) {
+    *num_steps = steps;
+    const int32_t k = std::min(steps, max_steps);
+    if (k > 0) {
+      CMI_CUDA(cudaMemcpy(cells, d_cells, sizeof(int32_t) * k, cudaMemcpyDeviceToHost));
+      CMI_CUDA(cudaMemcpy(lengths, d_len, sizeof(double) * k, cudaMemcpyDeviceToHost));
+    }
+  }
+  if (flags & kFlagWalkLimit) return fail(CMI_ERR_INVARIANT, "walk step bound exceeded");
+  return CMI_OK;
+}
+
+int cmi_traverse_buffer(cmi_context *c, int32_t instance, uint32_t subgrid,
+                        int32_t input_direction, const cmi_photon *in, uint32_t n,
+                        const uint8_t *enabled, cmi_photon *out, uint32_t out_count[27],
+                        uint32_t *num_done) {
+  if (!out || !out_count) return fail(CMI_ERR_INVALID_ARGUMENT, "null output buffers");
+  return traverse(c, instance, subgrid, input_direction, in, n, out, nullptr, enabled,
+                  out_count, num_done, 0, nullptr, nullptr, nullptr);
+}
+
+int cmi_trace_packet(cmi_context *c, int32_t instance, uint32_t subgrid, int32_t input_direction,
+                     cmi_photon *photon, int32_t max_steps, int32_t *cells, double *lengths,
+                     int32_t *num_steps, int32_t *output_direction) {
+  if (!photon || !num_steps || !output_direction)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "null photon or outputs");
+  if (max_steps < 0 || (max_steps > 0 && (!cells || !lengths)))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "bad trace arrays");
+  return traverse(c, instance, subgrid, input_direction, photon, 1, nullptr, output_direction,
+                  nullptr, nullptr, nullptr, max_steps, cells, lengths, num_steps);
+}
+
+int cmi_compute_neutral_fraction(cmi_context *c, int32_t instance, double luminosity,
+                                 uint64_t num_photon, double *mean_abs_dx) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  if (num_photon == 0) return fail(CMI_ERR_INVALID_ARGUMENT, "num_photon must be > 0");
+  const HostInstance &I = c->inst[instance];
+  const double inv[3] = {I.sub_ncell[0] / (I.desc.box[3] / I.desc.num_subgrid[0]),
+                         I.sub_ncell[1] / (I.desc.box[4] / I.desc.num_subgrid[1]),
+                         I.sub_ncell[2] / (I.desc.box[5] / I.desc.num_subgrid[2])};
+  // DensitySubGrid.hpp:1633 (num_photon is an unsigned int there)
+  const double jfac = luminosity / (double)num_photon * inv[0] * inv[1] * inv[2];
+  const int ninst = (int)c->inst.size();
+  k_begin_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst);
+  BalanceParams b{};
+  b.subs = c->d_sub;
+  b.inst = c->d_inst;
+  b.nH = c->d_nH;
+  b.xH = c->d_xH;
+  b.J = c->d_J;
+  b.kappa = c->fp32() ? c->d_kappa : nullptr;
+  b.stats = c->d_stats;
+  b.first_sub = I.first_sub;
+  b.num_subs = I.nsub;
+  b.jfac_override = jfac;
+  if (c->opt.balance_form == CMI_BALANCE_REFERENCE)
+    k_balance<0><<<I.nsub, 256, 0, c->stream>>>(b);
+  else
+    k_balance<1><<<I.nsub, 256, 0, c->stream>>>(b);
+  CMI_CUDA(cudaGetLastError());
+  DevStats d{};
+  CMI_CUDA(cudaMemcpyAsync(&d, c->d_stats + instance, sizeof(DevStats), cudaMemcpyDeviceToHost,
+                           c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  if (mean_abs_dx) *mean_abs_dx = d.dx_sum / (double)I.ncells;
+  return CMI_OK;
+}
+
+int cmi_device_field(cmi_context *c, int32_t instance, int32_t which, double **ptr,
+                     uint64_t *count) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  if (!ptr || !count) return fail(CMI_ERR_INVALID_ARGUMENT, "null output");
+  const HostInstance &I = c->inst[instance];
+  double *base = (which == 0) ? c->d_J : (which == 1) ? c->d_xH : (which == 2) ? c->d_nH : nullptr;
+  if (!base) return fail(CMI_ERR_INVALID_ARGUMENT, "which must be 0 (J), 1 (x_H) or 2 (n_H)");
+  *ptr = base + I.first_cell;
+  *count = (uint64_t)I.nsub * (uint64_t)I.padded_per_sub;
+  return CMI_OK;
+}
+
+int cmi_get_stream(cmi_context *c, void **s) {
+  if (!c || !s) return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  *s = (void *)c->stream;
+  return CMI_OK;
+}
+
+int cmi_synchronize(cmi_context *c) {
+  CMI_TRY(check_ctx(c));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return CMI_OK;
+}
+
+int cmi_set_kernel_timing(cmi_context *c, int32_t enable) {
+  CMI_TRY(check_ctx(c));
+  c->timing = enable != 0;
+  return CMI_OK;
+}
+
+int cmi_kernel_timing(cmi_context *c, double ms[CMI_KERNEL_CLASSES],
+                      uint64_t launches[CMI_KERNEL_CLASSES]) {
+  CMI_TRY(check_ctx(c));
+  if (!ms || !launches) return fail(CMI_ERR_INVALID_ARGUMENT, "null output");
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < CMI_KERNEL_CLASSES; ++k) {
+    ms[k] = 0.;
+    launches[k] = 0;
+  }
+  for (auto &t : c->timed) {
+    float v = 0.f;
+    CMI_CUDA(cudaEventElapsedTime(&v, t.start, t.stop));
+    ms[t.cls] += v;
+    launches[t.cls] += (t.cls == 1) ? 4 : 1;
+    c->event_pool.push_back(t.start);
+    c->event_pool.push_back(t.stop);
+  }
+  c->timed.clear();
+  return CMI_OK;
+}
+
+int cmi_last_launch_count(cmi_context *c, uint64_t *launches) {
+  if (!c || !launches) return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  *launches = c->last_launches;
+  return CMI_OK;
+}
+
+}  // extern "C"

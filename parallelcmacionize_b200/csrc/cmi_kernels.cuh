@@ -1,0 +1,1165 @@
+// Kernels of the B200 transport engine.
+//
+// One iteration of the plain method (testDensitySubGrid_omp.cpp:2213-2434)
+// runs as a wavefront over all instances of a context:
+//
+//   emission plan -> emit -> [plan -> scatter -> walk] x R -> balance
+//
+// * emit / walk append packets to an unsorted arena, warp-aggregated: one
+//   atomic per warp for the arena slot and one per group of lanes heading to
+//   the same subgrid for the rank inside that subgrid's bucket (the 27
+//   TravelDirection output buffers of a subgrid, do_photon_traversal's
+//   output_buffers, land in the buckets of its 26 neighbours);
+// * plan turns the per-subgrid counts into bucket offsets and chunks of at
+//   most `chunk` packets; scatter moves every packet to its bucket;
+// * walk: persistent CTAs claim chunks; a CTA owns the chunk's subgrid, whose
+//   fields are staged in shared memory by a TMA bulk copy; warps trace their
+//   packets one crossing per loop trip, refilling idle lanes; path lengths
+//   are tallied in shared-memory atomics and flushed to the FP64 J array in
+//   HBM once per subgrid residency.
+// R = max over instances of (sum of subgrids per axis - 2), the most subgrid
+// transits a straight ray can make, so no packet is left over.
+#pragma once
+
+#include "cmi_device.cuh"
+#include "cmi_walk.cuh"
+
+namespace cmi {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr int kDrop = 3;
+constexpr uint32_t kFlagArenaOverflow = 1u;
+constexpr uint32_t kFlagStageTimeout = 2u;
+constexpr uint32_t kFlagWalkLimit = 4u;
+constexpr uint32_t kFlagLeftover = 8u;
+constexpr uint32_t kFlagBadInput = 16u;
+constexpr int kPlanThreads = 1024;
+constexpr int kPlanPerThread = 4;
+constexpr int kPlanTile = kPlanThreads * kPlanPerThread;
+constexpr unsigned long long kStageWaitNs = 1000000000ull;  // 1 s
+
+// ---------------------------------------------------------------------------
+// packet load/store as 16-byte vectors
+// ---------------------------------------------------------------------------
+template <class P>
+__device__ __forceinline__ P load_packet(const P *src) {
+  static_assert(sizeof(P) % 16 == 0, "packet size");
+  P out;
+  const uint4 *s = reinterpret_cast<const uint4 *>(src);
+  uint4 *d = reinterpret_cast<uint4 *>(&out);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(P) / 16); ++i) d[i] = __ldg(s + i);
+  return out;
+}
+
+template <class P>
+__device__ __forceinline__ void store_packet(P *dst, const P &v) {
+  const uint4 *s = reinterpret_cast<const uint4 *>(&v);
+  uint4 *d = reinterpret_cast<uint4 *>(dst);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(P) / 16); ++i) d[i] = s[i];
+}
+
+// ---------------------------------------------------------------------------
+// Warp-aggregated append of the lanes with `append` set to the arena.  Must
+// be called by all 32 lanes.  key = destination subgrid (global index).
+// ---------------------------------------------------------------------------
+template <class P>
+__device__ __forceinline__ void warp_append(bool append, uint32_t key, const P &rec, P *arena,
+                                            uint32_t *keys, uint32_t *ranks, uint32_t *hist,
+                                            RoundState *st, uint32_t capacity) {
+  const unsigned am = __ballot_sync(kFull, append);
+  if (am == 0u) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int leader = __ffs(am) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&st->arena_count, (uint32_t)__popc(am));
+  base = __shfl_sync(kFull, base, leader);
+  if (append) {
+    const unsigned peers = __match_any_sync(am, key);
+    const int pl = __ffs(peers) - 1;
+    uint32_t kb = 0;
+    if (lane == pl) kb = atomicAdd(&hist[key], (uint32_t)__popc(peers));
+    kb = __shfl_sync(peers, kb, pl);
+    const uint32_t slot = base + (uint32_t)__popc(am & lt);
+    if (slot < capacity) {
+      store_packet(arena + slot, rec);
+      keys[slot] = key;
+      ranks[slot] = kb + (uint32_t)__popc(peers & lt);
+    } else {
+      atomicOr(&st->flags, kFlagArenaOverflow);
+    }
+  }
+}
+
+// block-wide exclusive scan of one uint32 per thread (blockDim multiple of 32)
+template <int kThreads>
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *warp_sums,
+                                                         uint32_t &total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = (lane < kThreads / 32) ? warp_sums[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kThreads / 32) warp_sums[lane] = w;
+  }
+  __syncthreads();
+  total = warp_sums[kThreads / 32 - 1];
+  const uint32_t before = (warp > 0) ? warp_sums[warp - 1] : 0u;
+  __syncthreads();
+  return before + x - v;
+}
+
+// ---------------------------------------------------------------------------
+// iteration bookkeeping
+// ---------------------------------------------------------------------------
+__global__ void k_begin_iteration(RoundState *st, DevStats *stats, int ninst) {
+  for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
+    DevStats z = {};
+    stats[i] = z;
+  }
+  if (threadIdx.x == 0) {
+    st->rounds_active = 0;
+    st->arena_count = 0;
+    st->num_chunks = 0;
+    st->chunk_next = 0;
+    st->total_in = 0;
+  }
+}
+
+__global__ void k_end_iteration(RoundState *st, DevStats *stats, int ninst, int advance) {
+  const uint32_t leftover = st->total_in ? kFlagLeftover : 0u;
+  for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
+    stats[i].flags |= st->flags | leftover;
+    stats[i].rounds = st->rounds_active;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st->flags |= leftover;
+    if (advance) st->iteration += 1;
+  }
+}
+
+// Packets per source of every instance for this iteration: the reference split
+// (testDensitySubGrid_omp.cpp:2199-2208) with the remainder given to the
+// sources holding the smallest Philox draws (stand-in for distribute(),
+// :1650-1677).  One block.
+__global__ void k_emission_plan(const DevInstance *inst, int ninst, const DevSource *src,
+                                int nsrc_total, RoundState *st, uint64_t *src_count,
+                                uint64_t *src_first, uint64_t *buf_first, DevStats *stats) {
+  const uint64_t seed = st->seed;
+  const uint32_t it = st->iteration;
+  for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
+    const DevInstance I = inst[i];
+    double total = 0.;
+    for (uint32_t k = 0; k < I.num_sources; ++k) total += src[I.first_source + k].luminosity;
+    uint64_t assigned = 0;
+    for (uint32_t k = 0; k < I.num_sources; ++k) {
+      const uint64_t n =
+          (uint64_t)(src[I.first_source + k].luminosity / total * (double)I.num_photon);
+      src_count[I.first_source + k] = n;
+      assigned += n;
+    }
+    uint64_t rem = (I.num_photon > assigned) ? I.num_photon - assigned : 0;
+    // rem < num_sources: pick the rem smallest draws, lower index on ties
+    uint32_t taken_lo = 0, taken_hi = 0;  // bitmask over <= 64 sources
+    while (rem > 0 && I.num_sources > 0) {
+      int best = -1;
+      uint32_t best_w = 0;
+      for (uint32_t k = 0; k < I.num_sources && k < 64; ++k) {
+        const bool taken = (k < 32) ? ((taken_lo >> k) & 1u) : ((taken_hi >> (k - 32)) & 1u);
+        if (taken) continue;
+        const uint32_t ctr[4] = {k, 0u, it, kPhiloxSplitTag};
+        uint32_t w[4];
+        philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32) + (uint32_t)i, w);
+        if (best < 0 || w[0] < best_w) {
+          best = (int)k;
+          best_w = w[0];
+        }
+      }
+      if (best < 0) break;
+      src_count[I.first_source + best] += 1;
+      if (best < 32) taken_lo |= 1u << best; else taken_hi |= 1u << (best - 32);
+      --rem;
+    }
+    stats[i].emitted = I.num_photon;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t acc = 0, bacc = 0;
+    for (int s = 0; s < nsrc_total; ++s) {
+      src_first[s] = acc;
+      buf_first[s] = bacc;
+      acc += src_count[s];
+      bacc += (src_count[s] + 199) / 200;
+    }
+    src_first[nsrc_total] = acc;
+    buf_first[nsrc_total] = bacc;
+    st->emit_total = (uint32_t)acc;
+    st->arena_count = 0;
+  }
+}
+
+// index s with first[s] <= g < first[s + 1] (first has n + 1 entries)
+__device__ __forceinline__ int find_bin(const uint64_t *first, int n, uint64_t g) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct EmitParams {
+  const DevInstance *inst;
+  const DevSource *src;
+  int nsrc_total;
+  const uint64_t *src_count, *src_first, *buf_first;
+  RoundState *st;
+  void *arena;
+  uint32_t *keys, *ranks, *hist;
+  uint32_t capacity;
+};
+
+template <bool kF32>
+__device__ __forceinline__ void make_emitted(const DevSource &S, const DevInstance &I,
+                                             const double dir[3], double tau, Packet32 &p32,
+                                             Packet64 &p64) {
+  if (kF32) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      p32.pos[a] = S.pos_cell[a];
+      p32.dir[a] = (float)dir[a];
+    }
+    p32.tau = (float)tau;
+    p32.meta = (uint32_t)kInside;
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      p64.pos[a] = S.position[a];
+      p64.dir[a] = dir[a];
+    }
+    p64.tau = tau;
+    p64.sigma = I.sigma;
+    p64.weight = 1.;
+    p64.type = 0;
+    p64.meta = (uint32_t)kInside;
+  }
+}
+
+// Emission with Philox: packet g of the batch belongs to source s; its id in
+// the instance is g - first packet of the instance.
+template <bool kF32>
+__global__ void __launch_bounds__(256) k_emit_philox(EmitParams prm) {
+  const RoundState *st = prm.st;
+  const uint64_t N = st->emit_total;
+  const uint64_t seed = st->seed;
+  const uint32_t it = st->iteration;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < N; base += stride) {
+    const uint64_t g = base + threadIdx.x;
+    const bool valid = g < N;
+    Packet32 p32{};
+    Packet64 p64{};
+    uint32_t key = 0;
+    if (valid) {
+      const int s = find_bin(prm.src_first, prm.nsrc_total + 1, g);
+      const DevSource S = prm.src[s];
+      const DevInstance I = prm.inst[S.instance];
+      const uint64_t id = g - prm.src_first[I.first_source];
+      double dir[3], tau;
+      philox_packet(seed, S.instance, it, id, dir, tau);
+      make_emitted<kF32>(S, I, dir, tau, p32, p64);
+      key = S.subgrid;
+    }
+    if (kF32) {
+      warp_append(valid, key, p32, (Packet32 *)prm.arena, prm.keys, prm.ranks, prm.hist,
+                  prm.st, prm.capacity);
+    } else {
+      warp_append(valid, key, p64, (Packet64 *)prm.arena, prm.keys, prm.ranks, prm.hist,
+                  prm.st, prm.capacity);
+    }
+  }
+}
+
+// Emission replaying the reference generator: buffer b of 200 packets (global
+// order over sources) draws from ranlxd(seed + b + iteration * buffers), one
+// draw for the subgrid-copy pick (Source.hpp:94-99), then per packet cos(theta),
+// phi and the optical depth (testDensitySubGrid_omp.cpp:529-597).
+template <bool kF32>
+__global__ void __launch_bounds__(128) k_emit_ranlux(EmitParams prm) {
+  const RoundState *st = prm.st;
+  const uint64_t nbuf = prm.buf_first[prm.nsrc_total];
+  const uint64_t seed = st->seed;
+  const uint32_t it = st->iteration;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < nbuf; base += stride) {
+    const uint64_t b = base + threadIdx.x;
+    const bool valid = b < nbuf;
+    Ranlux rng;
+    int s = 0;
+    uint32_t n_b = 0;
+    if (valid) {
+      s = find_bin(prm.buf_first, prm.nsrc_total + 1, b);
+      const uint64_t k0 = (b - prm.buf_first[s]) * 200u;
+      const uint64_t cnt = prm.src_count[s];
+      n_b = (uint32_t)min((uint64_t)200u, cnt - k0);
+      rng.seed((int32_t)(int64_t)(seed + b + (uint64_t)it * nbuf));
+      (void)rng.uniform();
+    }
+    const DevSource S = prm.src[valid ? s : 0];
+    const DevInstance I = prm.inst[S.instance];
+    for (uint32_t k = 0; k < 200u; ++k) {
+      const bool live = valid && k < n_b;
+      Packet32 p32{};
+      Packet64 p64{};
+      if (live) {
+        const double cost = 2. * rng.uniform() - 1.;
+        const double phi = 2. * 3.14159265358979323846 * rng.uniform();
+        const double s2 = 1. - cost * cost;
+        const double sint = sqrt((s2 < 0.) ? 0. : s2);
+        const double dir[3] = {sint * cos(phi), sint * sin(phi), cost};
+        const double tau = -log(rng.uniform());
+        make_emitted<kF32>(S, I, dir, tau, p32, p64);
+      }
+      if (!__any_sync(kFull, live)) break;
+      if (kF32) {
+        warp_append(live, S.subgrid, p32, (Packet32 *)prm.arena, prm.keys, prm.ranks, prm.hist,
+                    prm.st, prm.capacity);
+      } else {
+        warp_append(live, S.subgrid, p64, (Packet64 *)prm.arena, prm.keys, prm.ranks, prm.hist,
+                    prm.st, prm.capacity);
+      }
+    }
+  }
+}
+
+// Caller-supplied packets (cmi_transport_packets): FP64 photon records with
+// their start subgrid, converted to the transport precision and appended.
+struct UploadParams {
+  const Packet64 *photons;
+  const uint32_t *start;  // subgrid index inside the instance
+  uint64_t n;
+  const DevSubgrid *subs;
+  uint32_t first_sub, nsub;
+  RoundState *st;
+  void *arena;
+  uint32_t *keys, *ranks, *hist;
+  uint32_t capacity;
+};
+
+template <bool kF32>
+__global__ void __launch_bounds__(256) k_upload(UploadParams prm) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < prm.n; base += stride) {
+    const uint64_t g = base + threadIdx.x;
+    bool valid = g < prm.n;
+    uint32_t key = 0;
+    Packet32 p32{};
+    Packet64 p64{};
+    if (valid) {
+      const uint32_t ls = prm.start[g];
+      if (ls >= prm.nsub) {
+        atomicOr(&prm.st->flags, kFlagBadInput);
+        valid = false;
+      } else {
+        key = prm.first_sub + ls;
+        p64 = prm.photons[g];
+        p64.meta = (uint32_t)kInside;
+        if (kF32) {
+          const DevSubgrid &S = prm.subs[key];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            p32.pos[a] = (float)((p64.pos[a] - S.anchor[a]) * S.inv_cell_size[a]);
+            p32.dir[a] = (float)p64.dir[a];
+          }
+          p32.tau = (float)p64.tau;
+          p32.meta = (uint32_t)kInside;
+        }
+      }
+    }
+    if (kF32) {
+      warp_append(valid, key, p32, (Packet32 *)prm.arena, prm.keys, prm.ranks, prm.hist,
+                  prm.st, prm.capacity);
+    } else {
+      warp_append(valid, key, p64, (Packet64 *)prm.arena, prm.keys, prm.ranks, prm.hist,
+                  prm.st, prm.capacity);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// plan: per-subgrid counts -> bucket offsets + chunk list
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kPlanThreads) k_plan_count(const uint32_t *hist, uint32_t S,
+                                                             uint32_t chunk,
+                                                             uint32_t *tile_pk,
+                                                             uint32_t *tile_ch) {
+  __shared__ uint32_t ws[32];
+  const uint32_t s0 = blockIdx.x * kPlanTile + threadIdx.x * kPlanPerThread;
+  uint32_t pk = 0, ch = 0;
+#pragma unroll
+  for (int k = 0; k < kPlanPerThread; ++k) {
+    const uint32_t s = s0 + k;
+    const uint32_t c = (s < S) ? hist[s] : 0u;
+    pk += c;
+    ch += (c + chunk - 1) / chunk;
+  }
+  uint32_t tpk, tch;
+  (void)block_exclusive_scan<kPlanThreads>(pk, ws, tpk);
+  (void)block_exclusive_scan<kPlanThreads>(ch, ws, tch);
+  if (threadIdx.x == 0) {
+    tile_pk[blockIdx.x] = tpk;
+    tile_ch[blockIdx.x] = tch;
+  }
+}
+
+__global__ void __launch_bounds__(kPlanThreads) k_plan_offsets(uint32_t ntiles,
+                                                               const uint32_t *tile_pk,
+                                                               const uint32_t *tile_ch,
+                                                               uint32_t *tile_pk_off,
+                                                               uint32_t *tile_ch_off,
+                                                               RoundState *st) {
+  __shared__ uint32_t ws[32];
+  uint32_t carry_pk = 0, carry_ch = 0;
+  for (uint32_t b = 0; b < ntiles; b += kPlanThreads) {
+    const uint32_t t = b + threadIdx.x;
+    const uint32_t pk = (t < ntiles) ? tile_pk[t] : 0u;
+    const uint32_t ch = (t < ntiles) ? tile_ch[t] : 0u;
+    uint32_t tot_pk, tot_ch;
+    const uint32_t opk = block_exclusive_scan<kPlanThreads>(pk, ws, tot_pk);
+    const uint32_t och = block_exclusive_scan<kPlanThreads>(ch, ws, tot_ch);
+    if (t < ntiles) {
+      tile_pk_off[t] = carry_pk + opk;
+      tile_ch_off[t] = carry_ch + och;
+    }
+    carry_pk += tot_pk;
+    carry_ch += tot_ch;
+  }
+  if (threadIdx.x == 0) {
+    st->total_in = carry_pk;
+    st->num_chunks = carry_ch;
+    st->chunk_next = 0;
+    st->arena_count = 0;
+    if (carry_pk > 0) st->rounds_active += 1;
+  }
+}
+
+__global__ void __launch_bounds__(kPlanThreads) k_plan_write(uint32_t *hist, uint32_t S,
+                                                             uint32_t chunk,
+                                                             const uint32_t *tile_pk_off,
+                                                             const uint32_t *tile_ch_off,
+                                                             uint32_t *bucket_off,
+                                                             Chunk *chunks) {
+  __shared__ uint32_t ws[32];
+  const uint32_t s0 = blockIdx.x * kPlanTile + threadIdx.x * kPlanPerThread;
+  uint32_t c[kPlanPerThread];
+  uint32_t pk = 0, ch = 0;
+#pragma unroll
+  for (int k = 0; k < kPlanPerThread; ++k) {
+    const uint32_t s = s0 + k;
+    c[k] = (s < S) ? hist[s] : 0u;
+    pk += c[k];
+    ch += (c[k] + chunk - 1) / chunk;
+  }
+  uint32_t tpk, tch;
+  uint32_t opk = block_exclusive_scan<kPlanThreads>(pk, ws, tpk) + tile_pk_off[blockIdx.x];
+  uint32_t och = block_exclusive_scan<kPlanThreads>(ch, ws, tch) + tile_ch_off[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kPlanPerThread; ++k) {
+    const uint32_t s = s0 + k;
+    if (s >= S) break;
+    bucket_off[s] = opk;
+    for (uint32_t q = 0; q * chunk < c[k]; ++q) {
+      Chunk cc;
+      cc.subgrid = s;
+      cc.begin = opk + q * chunk;
+      cc.count = min(chunk, c[k] - q * chunk);
+      cc.pad = 0;
+      chunks[och++] = cc;
+    }
+    opk += c[k];
+    hist[s] = 0u;
+  }
+}
+
+template <class P>
+__global__ void __launch_bounds__(256) k_scatter(const P *out, const uint32_t *keys,
+                                                 const uint32_t *ranks,
+                                                 const uint32_t *bucket_off, P *in,
+                                                 const RoundState *st, uint32_t capacity) {
+  const uint32_t n = min(st->total_in, capacity);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t dst = bucket_off[keys[i]] + ranks[i];
+    if (dst < capacity) store_packet(in + dst, load_packet(out + i));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// walk: one wavefront round
+// ---------------------------------------------------------------------------
+struct WalkParams {
+  const DevSubgrid *subs;
+  const DevInstance *inst;
+  const Chunk *chunks;
+  RoundState *st;
+  DevStats *stats;
+  const void *arena_in;
+  void *arena_out;
+  uint32_t *keys, *ranks, *hist;
+  uint32_t capacity;
+  int32_t max_padded;     // largest padded cell count of any subgrid
+  const float *kappa;     // FP32 mode
+  const double *nH, *xH;  // FP64 mode
+  double *J;
+  DirectionTables tables;
+};
+
+struct WalkShared {
+  DirectionTables tab;
+  uint32_t ngb[kNumDirections];
+  int32_t n[3];
+  int32_t nyz;
+  int32_t ncells;
+  int32_t padded;
+  float cs_f[3];
+  double anchor[3], cs[3], inv_cs[3];
+  int64_t field_offset;
+  double sigma;
+  uint32_t instance;
+  int32_t chunk_id;
+  uint32_t chunk_sub, chunk_begin, chunk_count;
+  uint32_t claim;
+  alignas(8) unsigned long long mbar;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count)
+               : "memory");
+  // make the initialised barrier visible to the async (TMA) proxy
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// TMA bulk copy global -> this CTA's shared memory (no multicast); completion
+// is signalled on mbar.  dst, src and bytes are multiples of 16.
+__device__ __forceinline__ void tma_load_1d(void *dst, const void *src, uint32_t bytes,
+                                            unsigned long long *mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *mbar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(mbar)), "r"(phase)
+      : "memory");
+  return ok != 0u;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait (1 s) for a staging copy.  On timeout the flag is raised and a
+// second bounded wait (1 s) lets the copy land before the CTA reuses or
+// releases the buffer.
+__device__ __forceinline__ void mbar_wait_bounded(unsigned long long *mbar, uint32_t phase,
+                                                  uint32_t *flags) {
+  if (mbar_try_wait(mbar, phase)) return;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(mbar, phase)) {
+    if (global_ns() - t0 > kStageWaitNs) {
+      if (threadIdx.x == 0) atomicOr(flags, kFlagStageTimeout);
+      const unsigned long long t1 = global_ns();
+      while (!mbar_try_wait(mbar, phase) && global_ns() - t1 < kStageWaitNs) {
+      }
+      return;
+    }
+  }
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <bool kF32, bool kComp, int kThreads>
+__global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WalkShared &sh = *reinterpret_cast<WalkShared *>(smem_raw);
+  const size_t head = (sizeof(WalkShared) + 15) & ~(size_t)15;
+  const int P = prm.max_padded;
+  // FP32: kappa | hi | lo      FP64: nH | xH | J
+  float *s_kappa = reinterpret_cast<float *>(smem_raw + head);
+  float *s_hi = s_kappa + P;
+  float *s_lo = s_hi + P;
+  double *s_n = reinterpret_cast<double *>(smem_raw + head);
+  double *s_x = s_n + P;
+  double *s_J = s_x + P;
+
+  RoundState *st = prm.st;
+  const uint32_t nchunks = st->num_chunks;
+  if (nchunks == 0u) return;
+  const int tid = threadIdx.x;
+  if (tid < (int)sizeof(DirectionTables) / 4) {
+    reinterpret_cast<uint32_t *>(&sh.tab)[tid] =
+        reinterpret_cast<const uint32_t *>(&prm.tables)[tid];
+  }
+  if (tid == 0) mbar_init(&sh.mbar, 1);
+  if (kF32) {
+    for (int c = tid; c < P; c += kThreads) {
+      s_hi[c] = 0.f;
+      if (kComp) s_lo[c] = 0.f;
+    }
+  } else {
+    for (int c = tid; c < P; c += kThreads) s_J[c] = 0.;
+  }
+  __syncthreads();
+
+  const int lane = tid & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  uint32_t phase = 0;
+  uint32_t staged = kNone;
+  uint32_t c_cross = 0, c_trans = 0, c_abs = 0, c_esc = 0;
+
+  auto flush = [&]() {
+    // tallies -> J (FP64, HBM), counters -> instance stats
+    const int64_t off = sh.field_offset;
+    const int nc = sh.ncells;
+    if (kF32) {
+      const double sw = sh.sigma;  // sigma * weight; packets of the iteration have weight 1
+      for (int c = tid; c < nc; c += kThreads) {
+        const float h = s_hi[c];
+        const float l = kComp ? s_lo[c] : 0.f;
+        if (h != 0.f || l != 0.f) atomicAdd(&prm.J[off + c], ((double)h + (double)l) * sw);
+        s_hi[c] = 0.f;
+        if (kComp) s_lo[c] = 0.f;
+      }
+    } else {
+      for (int c = tid; c < nc; c += kThreads) {
+        const double v = s_J[c];
+        if (v != 0.) atomicAdd(&prm.J[off + c], v);
+        s_J[c] = 0.;
+      }
+    }
+    const uint32_t wc = __reduce_add_sync(kFull, c_cross);
+    const uint32_t wt = __reduce_add_sync(kFull, c_trans);
+    const uint32_t wa = __reduce_add_sync(kFull, c_abs);
+    const uint32_t we = __reduce_add_sync(kFull, c_esc);
+    if (lane == 0) {
+      DevStats &S = prm.stats[sh.instance];
+      if (wc) atomicAdd(&S.crossings, (unsigned long long)wc);
+      if (wt) atomicAdd(&S.transits, (unsigned long long)wt);
+      if (wa) atomicAdd(&S.absorbed, (unsigned long long)wa);
+      if (we) atomicAdd(&S.escaped, (unsigned long long)we);
+    }
+    c_cross = c_trans = c_abs = c_esc = 0;
+  };
+
+  for (;;) {
+    if (tid == 0) {
+      const uint32_t c = atomicAdd(&st->chunk_next, 1u);
+      if (c < nchunks) {
+        const Chunk ch = prm.chunks[c];
+        sh.chunk_id = (int32_t)c;
+        sh.chunk_sub = ch.subgrid;
+        sh.chunk_begin = ch.begin;
+        sh.chunk_count = ch.count;
+      } else {
+        sh.chunk_id = -1;
+      }
+      sh.claim = 0;
+    }
+    __syncthreads();
+    if (sh.chunk_id < 0) break;
+    const uint32_t sub = sh.chunk_sub;
+    if (sub != staged) {
+      if (staged != kNone) flush();
+      __syncthreads();
+      if (tid == 0) {
+        const DevSubgrid &S = prm.subs[sub];
+        for (int d = 0; d < kNumDirections; ++d) sh.ngb[d] = S.ngb[d];
+        for (int a = 0; a < 3; ++a) {
+          sh.n[a] = S.ncell[a];
+          sh.cs_f[a] = S.cell_size_f[a];
+          sh.anchor[a] = S.anchor[a];
+          sh.cs[a] = S.cell_size[a];
+          sh.inv_cs[a] = S.inv_cell_size[a];
+        }
+        sh.nyz = S.ncell[1] * S.ncell[2];
+        sh.ncells = S.ncells;
+        sh.padded = S.padded_cells;
+        sh.field_offset = S.field_offset;
+        sh.instance = S.instance;
+        sh.sigma = prm.inst[S.instance].sigma;
+        fence_proxy_async();
+        if (kF32) {
+          const uint32_t bytes = (uint32_t)S.padded_cells * 4u;
+          mbar_expect_tx(&sh.mbar, bytes);
+          tma_load_1d(s_kappa, prm.kappa + S.field_offset, bytes, &sh.mbar);
+        } else {
+          const uint32_t bytes = (uint32_t)S.padded_cells * 8u;
+          mbar_expect_tx(&sh.mbar, 2u * bytes);
+          tma_load_1d(s_n, prm.nH + S.field_offset, bytes, &sh.mbar);
+          tma_load_1d(s_x, prm.xH + S.field_offset, bytes, &sh.mbar);
+        }
+      }
+      mbar_wait_bounded(&sh.mbar, phase, &st->flags);
+      phase ^= 1u;
+      staged = sub;
+      __syncthreads();
+    }
+
+    // ---- trace the chunk's packets, one crossing per loop trip ----
+    const uint32_t count = sh.chunk_count, begin = sh.chunk_begin;
+    const int limit = sh.n[0] + sh.n[1] + sh.n[2] + 3;
+    View32 v32;
+    View64 v64;
+    if (kF32) {
+      v32.kappa = s_kappa;
+      v32.tally_hi = s_hi;
+      v32.tally_lo = s_lo;
+      v32.n[0] = sh.n[0];
+      v32.n[1] = sh.n[1];
+      v32.n[2] = sh.n[2];
+      v32.nyz = sh.nyz;
+      v32.cs[0] = sh.cs_f[0];
+      v32.cs[1] = sh.cs_f[1];
+      v32.cs[2] = sh.cs_f[2];
+    } else {
+      v64.nH = s_n;
+      v64.xH = s_x;
+      v64.J = s_J;
+      for (int a = 0; a < 3; ++a) {
+        v64.n[a] = sh.n[a];
+        v64.anchor[a] = sh.anchor[a];
+        v64.cs[a] = sh.cs[a];
+        v64.inv_cs[a] = sh.inv_cs[a];
+      }
+      v64.nyz = sh.nyz;
+    }
+    Walk32<kComp> w32;
+    Walk64 w64;
+    uint32_t wq_b = 0, wq_e = 0;
+    bool exhausted = false, have = false, fresh = false;
+    int entry = kRun;
+    for (;;) {
+      const unsigned idle = __ballot_sync(kFull, !have);
+      if (idle != 0u && !exhausted) {
+        if (wq_b >= wq_e) {
+          uint32_t base = 0;
+          if (lane == 0) base = atomicAdd(&sh.claim, 32u);
+          base = __shfl_sync(kFull, base, 0);
+          if (base >= count) {
+            exhausted = true;
+          } else {
+            wq_b = base;
+            wq_e = min(base + 32u, count);
+          }
+        }
+        if (wq_b < wq_e) {
+          const uint32_t take = min((uint32_t)__popc(idle), wq_e - wq_b);
+          const uint32_t r = (uint32_t)__popc(idle & lt);
+          if (!have && r < take) {
+            const uint32_t slot = begin + wq_b + r;
+            if (kF32) {
+              const Packet32 pk = load_packet(((const Packet32 *)prm.arena_in) + slot);
+              entry = w32.begin(pk, v32, sh.tab.sign_code);
+            } else {
+              const Packet64 pk = load_packet(((const Packet64 *)prm.arena_in) + slot);
+              entry = w64.begin(pk, v64, sh.tab.sign_code);
+            }
+            have = true;
+            fresh = true;
+          }
+          wq_b += take;
+        }
+      }
+      if (!__any_sync(kFull, have)) {
+        if (exhausted) break;
+        continue;
+      }
+      int status = kRun;
+      if (have) {
+        if (fresh) {
+          status = entry;
+          fresh = false;
+        }
+        if (status == kRun) {
+          status = kF32 ? w32.step(v32) : w64.step(v64);
+          ++c_cross;
+          if (status == kRun && (kF32 ? w32.steps : w64.steps) > limit) status = kDrop;
+        }
+      }
+      const bool fin = have && status != kRun;
+      if (__any_sync(kFull, fin)) {
+        uint32_t key = kOutside, meta = 0;
+        bool append = false;
+        if (fin) {
+          ++c_trans;
+          if (status == kExited) {
+            const int mask = kF32 ? w32.exit_mask(v32) : w64.exit_mask(v64);
+            const int od = sh.tab.mask_dir[mask];
+            if (od >= kNumDirections) {
+              atomicOr(&st->flags, kFlagWalkLimit);
+            } else {
+              key = sh.ngb[od];
+              meta = sh.tab.mirror[od];
+              if (key == kOutside) ++c_esc; else append = true;
+            }
+          } else if (status == kAbsorbed) {
+            ++c_abs;
+          } else {
+            atomicOr(&st->flags, kFlagWalkLimit);
+          }
+        }
+        if (kF32) {
+          Packet32 rec{};
+          if (append) rec = w32.packet(meta);
+          warp_append(append, key, rec, (Packet32 *)prm.arena_out, prm.keys, prm.ranks,
+                      prm.hist, st, prm.capacity);
+        } else {
+          Packet64 rec{};
+          if (append) rec = w64.packet(v64, meta);
+          warp_append(append, key, rec, (Packet64 *)prm.arena_out, prm.keys, prm.ranks,
+                      prm.hist, st, prm.capacity);
+        }
+        if (fin) have = false;
+      }
+    }
+    __syncthreads();
+  }
+  if (staged != kNone) flush();
+}
+
+// ---------------------------------------------------------------------------
+// ionization balance (DensitySubGrid.hpp:1628-1658), one block per subgrid
+// ---------------------------------------------------------------------------
+struct BalanceParams {
+  const DevSubgrid *subs;
+  const DevInstance *inst;
+  const double *nH;
+  double *xH, *J;
+  float *kappa;  // refreshed for the FP32 walk (may be null)
+  DevStats *stats;
+  uint32_t first_sub, num_subs;
+  double jfac_override;  // >= 0: use instead of the instance's jfac
+};
+
+template <int kForm>
+__global__ void __launch_bounds__(256) k_balance(BalanceParams prm) {
+  __shared__ double red[8];
+  const uint32_t s = prm.first_sub + blockIdx.x;
+  const DevSubgrid &S = prm.subs[s];
+  const DevInstance &I = prm.inst[S.instance];
+  const double jfac = (prm.jfac_override >= 0.) ? prm.jfac_override : I.jfac;
+  const double alpha = I.alpha;
+  const double sigma = I.sigma;
+  double dx = 0.;
+  for (int c = threadIdx.x; c < S.ncells; c += blockDim.x) {
+    const int64_t i = S.field_offset + c;
+    const double jH = jfac * prm.J[i];
+    const double x_old = prm.xH[i];
+    double x;
+    if (jH > 0.) {
+      const double ntot = prm.nH[i];
+      const double aa = 0.5 * jH / (ntot * alpha);
+      if (kForm == 0) {
+        const double bb = 2. / aa;
+        const double cc = sqrt(bb + 1.);
+        x = 1. + aa * (1. - cc);
+      } else {
+        x = 1. / (1. + aa + sqrt(aa * (aa + 2.)));
+      }
+    } else {
+      x = 1.;
+    }
+    prm.xH[i] = x;
+    prm.J[i] = 0.;
+    if (prm.kappa) prm.kappa[i] = (float)(sigma * prm.nH[i] * x);
+    dx += fabs(x - x_old);
+  }
+  for (int o = 16; o > 0; o >>= 1) dx += __shfl_down_sync(kFull, dx, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    if (prm.stats) atomicAdd(&prm.stats[S.instance].dx_sum, t);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fields: layout conversion between caller arrays and the padded device order
+// ---------------------------------------------------------------------------
+// src index of cell c of (instance-local) subgrid ls
+__device__ __forceinline__ int64_t layout_index(const DevSubgrid &S, uint32_t ls, int c,
+                                                int layout, const int32_t ns[3],
+                                                const int32_t ncell_tot[3]) {
+  if (layout == 0) return (int64_t)ls * S.ncells + c;
+  const int ix = c / (S.ncell[1] * S.ncell[2]);
+  const int iy = (c / S.ncell[2]) % S.ncell[1];
+  const int iz = c % S.ncell[2];
+  const int sx = ls / (ns[1] * ns[2]);
+  const int sy = (ls / ns[2]) % ns[1];
+  const int sz = ls % ns[2];
+  const int64_t gx = (int64_t)sx * S.ncell[0] + ix, gy = (int64_t)sy * S.ncell[1] + iy,
+                gz = (int64_t)sz * S.ncell[2] + iz;
+  return (gx * ncell_tot[1] + gy) * ncell_tot[2] + gz;
+}
+
+struct LayoutParams {
+  const DevSubgrid *subs;
+  uint32_t first_sub;
+  int32_t ns[3], ncell[3];
+  int layout;
+};
+
+__global__ void k_fields_in(LayoutParams lp, const double *src, double *dst) {
+  const uint32_t ls = blockIdx.x;
+  const DevSubgrid &S = lp.subs[lp.first_sub + ls];
+  for (int c = threadIdx.x; c < S.ncells; c += blockDim.x) {
+    dst[S.field_offset + c] = src[layout_index(S, ls, c, lp.layout, lp.ns, lp.ncell)];
+  }
+}
+
+__global__ void k_fields_out(LayoutParams lp, const double *src, double *dst) {
+  const uint32_t ls = blockIdx.x;
+  const DevSubgrid &S = lp.subs[lp.first_sub + ls];
+  for (int c = threadIdx.x; c < S.ncells; c += blockDim.x) {
+    dst[layout_index(S, ls, c, lp.layout, lp.ns, lp.ncell)] = src[S.field_offset + c];
+  }
+}
+
+__global__ void k_kappa(const DevSubgrid *subs, const DevInstance *inst, uint32_t first_sub,
+                        const double *nH, const double *xH, float *kappa) {
+  const DevSubgrid &S = subs[first_sub + blockIdx.x];
+  const double sigma = inst[S.instance].sigma;
+  for (int c = threadIdx.x; c < S.padded_cells; c += blockDim.x) {
+    const int64_t i = S.field_offset + c;
+    kappa[i] = (c < S.ncells) ? (float)(sigma * nH[i] * xH[i]) : 0.f;
+  }
+}
+
+__global__ void k_fill(double *a, double v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// one buffer through one subgrid (do_photon_traversal), optional trace
+// ---------------------------------------------------------------------------
+struct TraverseParams {
+  const DevSubgrid *subs;
+  const DevInstance *inst;
+  uint32_t sub;
+  int32_t input_direction;
+  const Packet64 *in;
+  uint32_t n;
+  Packet64 *out;
+  int32_t *out_dir;
+  const float *kappa;
+  const double *nH, *xH;
+  double *J;
+  int32_t max_padded;
+  int32_t *trace_cells;  // packet 0 only
+  double *trace_len;
+  int32_t max_steps;
+  int32_t *trace_steps;
+  RoundState *st;
+  DirectionTables tables;
+};
+
+template <bool kF32>
+__global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ DirectionTables tab;
+  const DevSubgrid &S = prm.subs[prm.sub];
+  const int P = prm.max_padded;
+  float *s_kappa = reinterpret_cast<float *>(smem_raw);
+  float *s_hi = s_kappa + P;
+  float *s_lo = s_hi + P;
+  double *s_n = reinterpret_cast<double *>(smem_raw);
+  double *s_x = s_n + P;
+  double *s_J = s_x + P;
+  if (threadIdx.x < sizeof(DirectionTables) / 4) {
+    reinterpret_cast<uint32_t *>(&tab)[threadIdx.x] =
+        reinterpret_cast<const uint32_t *>(&prm.tables)[threadIdx.x];
+  }
+  for (int c = threadIdx.x; c < S.ncells; c += blockDim.x) {
+    if (kF32) {
+      s_kappa[c] = prm.kappa[S.field_offset + c];
+      s_hi[c] = 0.f;
+      s_lo[c] = 0.f;
+    } else {
+      s_n[c] = prm.nH[S.field_offset + c];
+      s_x[c] = prm.xH[S.field_offset + c];
+      s_J[c] = 0.;
+    }
+  }
+  __syncthreads();
+  View32 v32;
+  View64 v64;
+  for (int a = 0; a < 3; ++a) {
+    v32.n[a] = v64.n[a] = S.ncell[a];
+    v32.cs[a] = S.cell_size_f[a];
+    v64.anchor[a] = S.anchor[a];
+    v64.cs[a] = S.cell_size[a];
+    v64.inv_cs[a] = S.inv_cell_size[a];
+  }
+  v32.nyz = v64.nyz = S.ncell[1] * S.ncell[2];
+  v32.kappa = s_kappa;
+  v32.tally_hi = s_hi;
+  v32.tally_lo = s_lo;
+  v64.nH = s_n;
+  v64.xH = s_x;
+  v64.J = s_J;
+  const int limit = S.ncell[0] + S.ncell[1] + S.ncell[2] + 3;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < prm.n) {
+    Packet64 ph = prm.in[i];
+    ph.meta = (uint32_t)prm.input_direction;
+    const bool tracing = (i == 0 && prm.trace_steps != nullptr);
+    int status, nsteps = 0;
+    int result = kInside;
+    if (kF32) {
+      Packet32 pk;
+      for (int a = 0; a < 3; ++a) {
+        pk.pos[a] = (float)((ph.pos[a] - S.anchor[a]) * S.inv_cell_size[a]);
+        pk.dir[a] = (float)ph.dir[a];
+      }
+      pk.tau = (float)ph.tau;
+      pk.meta = ph.meta;
+      Walk32<true> w;
+      status = w.begin(pk, v32, tab.sign_code);
+      while (status == kRun) {
+        const int cell = w.cell;
+        float len;
+        status = w.step(v32, &len);
+        if (tracing && nsteps < prm.max_steps) {
+          prm.trace_cells[nsteps] = cell;
+          prm.trace_len[nsteps] = (double)len;
+        }
+        ++nsteps;
+        if (status == kRun && w.steps > limit) status = kDrop;
+      }
+      for (int a = 0; a < 3; ++a) ph.pos[a] = S.anchor[a] + (double)w.p[a] * S.cell_size[a];
+      ph.tau = (double)__fsub_rn(w.tau_target, w.tau_done);
+      if (status == kExited) result = tab.mask_dir[w.exit_mask(v32)];
+    } else {
+      Walk64 w;
+      status = w.begin(ph, v64, tab.sign_code);
+      while (status == kRun) {
+        const int cell = w.cell;
+        double len;
+        status = w.step(v64, &len);
+        if (tracing && nsteps < prm.max_steps) {
+          prm.trace_cells[nsteps] = cell;
+          prm.trace_len[nsteps] = len;
+        }
+        ++nsteps;
+        if (status == kRun && w.steps > limit) status = kDrop;
+      }
+      ph = w.packet(v64, 0u);
+      if (status == kExited) result = tab.mask_dir[w.exit_mask(v64)];
+    }
+    if (status == kDrop || result >= kNumDirections) {
+      atomicOr(&prm.st->flags, kFlagWalkLimit);
+      result = kInside;
+    }
+    ph.meta = 0u;
+    prm.out[i] = ph;
+    prm.out_dir[i] = result;
+    if (tracing) *prm.trace_steps = nsteps;
+  }
+  __syncthreads();
+  const double sw = prm.inst[S.instance].sigma;
+  for (int c = threadIdx.x; c < S.ncells; c += blockDim.x) {
+    if (kF32) {
+      const double v = ((double)s_hi[c] + (double)s_lo[c]) * sw;
+      if (v != 0.) atomicAdd(&prm.J[S.field_offset + c], v);
+    } else {
+      if (s_J[c] != 0.) atomicAdd(&prm.J[S.field_offset + c], s_J[c]);
+    }
+  }
+}
+
+// Stable grouping of the traversed photons by output direction (the 27
+// output buffers of do_photon_traversal, in input order).  One block.
+__global__ void __launch_bounds__(256) k_partition(const Packet64 *photons,
+                                                   const int32_t *dirs, uint32_t n,
+                                                   const uint8_t *enabled, Packet64 *out,
+                                                   uint32_t *counts, uint32_t *done) {
+  __shared__ uint32_t cnt[256][kNumDirections + 1];
+  __shared__ uint32_t base[kNumDirections + 1];
+  const uint32_t per = (n + 255) / 256;
+  const uint32_t b = threadIdx.x * per, e = min(n, b + per);
+  for (int d = 0; d < kNumDirections; ++d) cnt[threadIdx.x][d] = 0;
+  for (uint32_t i = b; i < e; ++i) cnt[threadIdx.x][dirs[i]] += 1;
+  __syncthreads();
+  if (threadIdx.x < kNumDirections) {
+    const int d = threadIdx.x;
+    uint32_t acc = 0;
+    for (int t = 0; t < 256; ++t) {
+      const uint32_t c = cnt[t][d];
+      cnt[t][d] = acc;
+      acc += c;
+    }
+    base[d] = acc;  // total of direction d for now
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0, dropped = 0;
+    for (int d = 0; d < kNumDirections; ++d) {
+      const uint32_t tot = base[d];
+      const bool on = enabled == nullptr || enabled[d] != 0;
+      counts[d] = on ? tot : 0u;
+      base[d] = on ? acc : kNone;
+      if (on) acc += tot; else dropped += tot;
+    }
+    *done = dropped;
+  }
+  __syncthreads();
+  for (uint32_t i = b; i < e; ++i) {
+    const int d = dirs[i];
+    if (base[d] != kNone) {
+      out[base[d] + cnt[threadIdx.x][d]] = photons[i];
+    }
+    cnt[threadIdx.x][d] += 1;
+  }
+}
+
+}  // namespace cmi

@@ -1,0 +1,273 @@
+// Cell walk of one packet through one subgrid: DensitySubGrid::interact
+// (DensitySubGrid.hpp:1180-1323) split into entry + one-crossing steps, so a
+// warp can advance 32 packets one crossing at a time.
+//
+// Two precisions:
+//  * Walk64 -- the reference's FP64 arithmetic, operation for operation.  The
+//    translation unit is compiled with --fmad=false, so no multiply-add is
+//    contracted and every result rounds exactly as on the host.
+//  * Walk32 -- FP32 in cell units: the position is kept relative to the
+//    subgrid in units of cells, so cell faces are exact small integers; path
+//    lengths stay in metres, l = (face - p) * (cell_size / d).  Tallies of
+//    path length go to compensated FP32 shared-memory accumulators.
+#pragma once
+
+#include "cmi_device.cuh"
+
+namespace cmi {
+
+enum WalkStatus : int { kRun = 0, kAbsorbed = 1, kExited = 2 };
+
+template <class T>
+__device__ __forceinline__ T min_ref(T a, T b) {  // std::min semantics
+  return (b < a) ? b : a;
+}
+
+// View of the staged subgrid in shared memory (FP32 mode).
+struct View32 {
+  const float *kappa;  // sigma * n * x per cell (1/m)
+  float *tally_hi;     // path length sums (m)
+  float *tally_lo;     // their rounding errors (compensated mode)
+  int n[3];
+  int nyz;
+  float cs[3];
+};
+
+// View of the staged subgrid in shared memory (FP64 mode).
+struct View64 {
+  const double *nH;
+  const double *xH;
+  double *J;
+  int n[3];
+  int nyz;
+  double anchor[3];
+  double cs[3];
+  double inv_cs[3];
+};
+
+// ----------------------------------------------------------------------------
+// FP32 cell-unit walk
+// ----------------------------------------------------------------------------
+template <bool kCompensated>
+struct Walk32 {
+  float p[3], d[3], inv[3], dcs[3];
+  float tau_done, tau_target;
+  int idx[3];
+  int cell;
+  int steps;
+
+  // Entry: DensitySubGrid.hpp:1186-1219 (start index per get_start_index).
+  __device__ __forceinline__ int begin(const Packet32 &pk, const View32 &v,
+                                      const uint8_t *sign_code) {
+    const uint8_t code = sign_code[pk.meta & 31u];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      p[a] = pk.pos[a];
+      d[a] = pk.dir[a];
+      dcs[a] = __fdiv_rn(d[a], v.cs[a]);
+      inv[a] = __fdiv_rn(v.cs[a], d[a]);
+      const int s = sign_of(code, a);
+      idx[a] = (s == 0) ? __float2int_rz(p[a]) : ((s < 0) ? 0 : v.n[a] - 1);
+    }
+    cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
+    tau_done = 0.f;
+    tau_target = pk.tau;
+    steps = 0;
+    if (!(tau_done < tau_target)) return kAbsorbed;
+    return inside(v) ? kRun : kExited;
+  }
+
+  __device__ __forceinline__ bool inside(const View32 &v) const {
+    return idx[0] < v.n[0] && idx[0] >= 0 && idx[1] < v.n[1] && idx[1] >= 0 &&
+           idx[2] < v.n[2] && idx[2] >= 0;
+  }
+
+  __device__ __forceinline__ void tally(const View32 &v, float len) const {
+    if (kCompensated) {
+      // TwoSum of the atomic's own addition: old + len = nw + err exactly.
+      const float old = atomicAdd(&v.tally_hi[cell], len);
+      const float nw = __fadd_rn(old, len);
+      const float bv = __fsub_rn(nw, old);
+      const float err = __fadd_rn(__fsub_rn(old, __fsub_rn(nw, bv)), __fsub_rn(len, bv));
+      if (err != 0.f) atomicAdd(&v.tally_lo[cell], err);
+    } else {
+      atomicAdd(&v.tally_hi[cell], len);
+    }
+  }
+
+  // One iteration of the loop at DensitySubGrid.hpp:1221-1305.
+  __device__ __forceinline__ int step(const View32 &v, float *trace_len = nullptr) {
+    float lo[3], hi[3], l[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = __int2float_rn(idx[a]);
+      hi[a] = __int2float_rn(idx[a] + 1);
+      l[a] = (d[a] > 0.f)   ? __fmul_rn(__fsub_rn(hi[a], p[a]), inv[a])
+             : (d[a] < 0.f) ? __fmul_rn(__fsub_rn(lo[a], p[a]), inv[a])
+                            : FLT_MAX;
+    }
+    float lmin = min_ref(l[0], min_ref(l[1], l[2]));
+    const float tau = __fmul_rn(lmin, v.kappa[cell]);
+    tau_done = __fadd_rn(tau_done, tau);
+    const bool absorbed = tau_done >= tau_target;
+    if (absorbed) {
+      const float corr = __fdiv_rn(__fsub_rn(tau_done, tau_target), tau);
+      lmin = __fmul_rn(lmin, __fsub_rn(1.f, corr));
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (l[a] == lmin) idx[a] += (d[a] > 0.f) ? 1 : -1;
+      }
+    }
+    if (trace_len) *trace_len = lmin;
+    tally(v, lmin);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      p[a] = (l[a] == lmin) ? ((d[a] > 0.f) ? hi[a] : lo[a]) : __fmaf_rn(lmin, dcs[a], p[a]);
+    }
+    ++steps;
+    if (absorbed) return kAbsorbed;
+    if (!inside(v)) return kExited;
+    cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
+    return kRun;
+  }
+
+  // Exit: 6-bit mask (DensitySubGrid.hpp:483-506) and the position moved into
+  // the neighbour's cell frame (exact: the exit coordinate is 0 or n).
+  __device__ __forceinline__ int exit_mask(const View32 &v) {
+    int mask = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int low = idx[a] < 0;
+      const int high = (idx[a] / v.n[a]) > 0;
+      mask |= (high << (5 - 2 * a)) | (low << (4 - 2 * a));
+      if (high) {
+        p[a] = __fsub_rn(p[a], __int2float_rn(v.n[a]));
+      } else if (low) {
+        p[a] = __fadd_rn(p[a], __int2float_rn(v.n[a]));
+      }
+    }
+    return mask;
+  }
+
+  __device__ __forceinline__ Packet32 packet(uint32_t meta) const {
+    Packet32 pk;
+    pk.pos[0] = p[0];
+    pk.pos[1] = p[1];
+    pk.pos[2] = p[2];
+    pk.dir[0] = d[0];
+    pk.dir[1] = d[1];
+    pk.dir[2] = d[2];
+    pk.tau = __fsub_rn(tau_target, tau_done);
+    pk.meta = meta;
+    return pk;
+  }
+};
+
+// ----------------------------------------------------------------------------
+// FP64 reference walk
+// ----------------------------------------------------------------------------
+struct Walk64 {
+  double pos[3], d[3], inv[3];
+  double tau_done, tau_target, sigma, weight;
+  int idx[3];
+  int cell;
+  int steps;
+  int type;
+
+  // DensitySubGrid.hpp:1186-1219 and get_start_index (:428-469).
+  __device__ __forceinline__ int begin(const Packet64 &pk, const View64 &v,
+                                      const uint8_t *sign_code) {
+    const uint8_t code = sign_code[pk.meta & 31u];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      d[a] = pk.dir[a];
+      inv[a] = 1. / d[a];
+      pos[a] = pk.pos[a] - v.anchor[a];
+      const int s = sign_of(code, a);
+      idx[a] = (s == 0) ? __double2int_rz(pos[a] * v.inv_cs[a]) : ((s < 0) ? 0 : v.n[a] - 1);
+    }
+    cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
+    tau_done = 0.;
+    tau_target = pk.tau;
+    sigma = pk.sigma;
+    weight = pk.weight;
+    type = pk.type;
+    steps = 0;
+    if (!(tau_done < tau_target)) return kAbsorbed;
+    return inside(v) ? kRun : kExited;
+  }
+
+  __device__ __forceinline__ bool inside(const View64 &v) const {
+    return idx[0] < v.n[0] && idx[0] >= 0 && idx[1] < v.n[1] && idx[1] >= 0 &&
+           idx[2] < v.n[2] && idx[2] >= 0;
+  }
+
+  // DensitySubGrid.hpp:1221-1305, one iteration.
+  __device__ __forceinline__ int step(const View64 &v, double *trace_len = nullptr) {
+    double lo[3], hi[3], l[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = idx[a] * v.cs[a];
+      hi[a] = (idx[a] + 1.) * v.cs[a];
+      l[a] = (d[a] > 0.)   ? (hi[a] - pos[a]) * inv[a]
+             : (d[a] < 0.) ? (lo[a] - pos[a]) * inv[a]
+                           : DBL_MAX;
+    }
+    double lmin = min_ref(l[0], min_ref(l[1], l[2]));
+    double lminsigma = lmin * sigma;
+    const double tau = lminsigma * v.nH[cell] * v.xH[cell];
+    tau_done += tau;
+    const bool absorbed = tau_done >= tau_target;
+    if (absorbed) {
+      const double correction = (tau_done - tau_target) / tau;
+      lmin *= (1. - correction);
+      lminsigma = lmin * sigma;
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (l[a] == lmin) idx[a] += (d[a] > 0.) ? 1 : -1;
+      }
+    }
+    if (trace_len) *trace_len = lmin;
+    atomicAdd(&v.J[cell], lminsigma * weight);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      pos[a] = (l[a] == lmin) ? ((d[a] > 0.) ? hi[a] : lo[a]) : pos[a] + lmin * d[a];
+    }
+    ++steps;
+    if (absorbed) return kAbsorbed;
+    if (!inside(v)) return kExited;
+    cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
+    return kRun;
+  }
+
+  __device__ __forceinline__ int exit_mask(const View64 &v) const {
+    int mask = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int low = idx[a] < 0;
+      const int high = (idx[a] / v.n[a]) > 0;
+      mask |= (high << (5 - 2 * a)) | (low << (4 - 2 * a));
+    }
+    return mask;
+  }
+
+  // The photon as the reference leaves it (DensitySubGrid.hpp:1307-1309).
+  __device__ __forceinline__ Packet64 packet(const View64 &v, uint32_t meta) const {
+    Packet64 pk;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      pk.pos[a] = pos[a] + v.anchor[a];
+      pk.dir[a] = d[a];
+    }
+    pk.tau = tau_target - tau_done;
+    pk.sigma = sigma;
+    pk.weight = weight;
+    pk.type = type;
+    pk.meta = meta;
+    return pk;
+  }
+};
+
+}  // namespace cmi

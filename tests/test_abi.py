@@ -1,0 +1,53 @@
+"""The C-ABI library: loads on any machine and exports what the header declares."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+from parallelcmacionize_b200 import _lib
+
+HEADER = os.path.join(ROOT, "include", "cmacionize_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char \*)\s*(cmi_\w+)\s*\(", text,
+                                 re.MULTILINE)))
+
+
+def test_header_declares_the_binding_list():
+    assert declared_functions() == sorted(_lib.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.load()
+    for name in declared_functions():
+        assert hasattr(L, name), name
+    assert L.cmi_abi_version() == 1
+
+
+def test_default_options():
+    o = _lib.default_options()
+    assert o.transport_precision == _lib.TRANSPORT_FP32
+    assert o.balance_form == _lib.BALANCE_STABLE
+    assert o.compensated_tally == 1 and o.use_graph == 1
+    with pytest.raises(TypeError):
+        _lib.default_options(no_such_option=1)
+
+
+def test_struct_layouts_match_header():
+    assert C.sizeof(_lib.GridDesc) == 6 * 8 + 6 * 4 + 2 * 8
+    assert C.sizeof(_lib.Options) == 16 * 4
+    assert C.sizeof(_lib.Stats) == 6 * 8 + 2 * 4
+    assert _lib.PHOTON_DTYPE.itemsize == 80
+
+
+def test_null_arguments_fail_cleanly():
+    L = _lib.load()
+    assert L.cmi_create(None, 1, None, None) == _lib.ERR_INVALID_ARGUMENT
+    assert L.cmi_synchronize(None) == _lib.ERR_INVALID_ARGUMENT
+    assert b"null" in L.cmi_last_error_string()
+    assert L.cmi_destroy(None) == _lib.OK

@@ -1,0 +1,256 @@
+"""The CPU oracle pinned against the reference (CPU only).
+
+Every check compares the C restatement (oracle/cmi_oracle.c) with outputs of
+the reference's own code (tests/golden/, made by make_golden.py from the
+reference headers) or with the known answers of
+testDensitySubGridDirections.cpp:105-167.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+import oracle as O
+
+D = O.DIRECTION
+
+
+# ---------------------------------------------------------------------------
+# testDensitySubGridDirections.cpp: the reference's own unit test, 54 answers
+# ---------------------------------------------------------------------------
+OUTPUT_CASES = [  # testDensitySubGridDirections.cpp:105-132
+    ((4, 5, 3), "INSIDE"),
+    ((-1, 5, 3), "FACE_X_N"), ((10, 5, 3), "FACE_X_P"), ((4, -1, 3), "FACE_Y_N"),
+    ((4, 10, 3), "FACE_Y_P"), ((4, 5, -1), "FACE_Z_N"), ((4, 5, 10), "FACE_Z_P"),
+    ((-1, -1, 3), "EDGE_Z_NN"), ((-1, 10, 3), "EDGE_Z_NP"), ((10, -1, 3), "EDGE_Z_PN"),
+    ((10, 10, 3), "EDGE_Z_PP"), ((-1, 5, -1), "EDGE_Y_NN"), ((-1, 5, 10), "EDGE_Y_NP"),
+    ((10, 5, -1), "EDGE_Y_PN"), ((10, 5, 10), "EDGE_Y_PP"), ((4, -1, -1), "EDGE_X_NN"),
+    ((4, -1, 10), "EDGE_X_NP"), ((4, 10, -1), "EDGE_X_PN"), ((4, 10, 10), "EDGE_X_PP"),
+    ((-1, -1, -1), "CORNER_NNN"), ((-1, -1, 10), "CORNER_NNP"), ((-1, 10, -1), "CORNER_NPN"),
+    ((-1, 10, 10), "CORNER_NPP"), ((10, -1, -1), "CORNER_PNN"), ((10, -1, 10), "CORNER_PNP"),
+    ((10, 10, -1), "CORNER_PPN"), ((10, 10, 10), "CORNER_PPP"),
+]
+START_CASES = [  # testDensitySubGridDirections.cpp:138-167
+    ("INSIDE", (0.5, 0.5, 0.5), (5, 5, 5)),
+    ("FACE_X_N", (0., 0.5, 0.5), (0, 5, 5)), ("FACE_X_P", (1., 0.5, 0.5), (9, 5, 5)),
+    ("FACE_Y_N", (0.5, 0., 0.5), (5, 0, 5)), ("FACE_Y_P", (0.5, 1., 0.5), (5, 9, 5)),
+    ("FACE_Z_N", (0.5, 0.5, 0.), (5, 5, 0)), ("FACE_Z_P", (0.5, 0.5, 1.), (5, 5, 9)),
+    ("EDGE_X_NN", (0.5, 0., 0.), (5, 0, 0)), ("EDGE_X_NP", (0.5, 0., 1.), (5, 0, 9)),
+    ("EDGE_X_PN", (0.5, 1., 0.), (5, 9, 0)), ("EDGE_X_PP", (0.5, 1., 1.), (5, 9, 9)),
+    ("EDGE_Y_NN", (0., 0.5, 0.), (0, 5, 0)), ("EDGE_Y_NP", (0., 0.5, 1.), (0, 5, 9)),
+    ("EDGE_Y_PN", (1., 0.5, 0.), (9, 5, 0)), ("EDGE_Y_PP", (1., 0.5, 1.), (9, 5, 9)),
+    ("EDGE_Z_NN", (0., 0., 0.5), (0, 0, 5)), ("EDGE_Z_NP", (0., 1., 0.5), (0, 9, 5)),
+    ("EDGE_Z_PN", (1., 0., 0.5), (9, 0, 5)), ("EDGE_Z_PP", (1., 1., 0.5), (9, 9, 5)),
+    ("CORNER_NNN", (0., 0., 0.), (0, 0, 0)), ("CORNER_NNP", (0., 0., 1.), (0, 0, 9)),
+    ("CORNER_NPN", (0., 1., 0.), (0, 9, 0)), ("CORNER_NPP", (0., 1., 1.), (0, 9, 9)),
+    ("CORNER_PNN", (1., 0., 0.), (9, 0, 0)), ("CORNER_PNP", (1., 0., 1.), (9, 0, 9)),
+    ("CORNER_PPN", (1., 1., 0.), (9, 9, 0)), ("CORNER_PPP", (1., 1., 1.), (9, 9, 9)),
+]
+
+
+def test_reference_known_answers_output_direction(oracle_mod):
+    sg = O.subgrid([0, 0, 0, 1, 1, 1], [10, 10, 10])
+    assert len(OUTPUT_CASES) == 27
+    for three, name in OUTPUT_CASES:
+        assert O.get_output_direction(sg, three) == D[name], (three, name)
+
+
+def test_reference_known_answers_start_index(oracle_mod):
+    sg = O.subgrid([0, 0, 0, 1, 1, 1], [10, 10, 10])
+    assert len(START_CASES) == 27
+    for name, pos, ref in START_CASES:
+        assert O.get_start_index(sg, pos, D[name]) == ref, (name, pos)
+
+
+def test_directions_sweep_matches_reference(oracle_mod):
+    g = golden("directions.npz")
+    sg = O.subgrid([0, 0, 0, 1, 1, 1], [10, 10, 10])
+    for ix, iy, iz, ref in g["output"]:
+        assert O.get_output_direction(sg, (ix, iy, iz)) == ref
+    for row in g["start"]:
+        d, pos, ref = int(row[0]), row[1:4], tuple(int(v) for v in row[4:7])
+        assert O.get_start_index(sg, pos, d) == ref, (d, pos)
+    for d, m in g["mirror"]:
+        assert O.output_to_input_direction(int(d)) == m
+    for row in g["compat"]:
+        d, vec, cin, cout = int(row[0]), row[1:4], int(row[4]), int(row[5])
+        assert O.is_compatible_input_direction(vec, d) == bool(cin)
+        assert O.is_compatible_output_direction(vec, d) == bool(cout)
+
+
+def test_mask_table_is_total_and_involutive(oracle_mod):
+    valid = [m for m in range(64) if O.direction_from_mask(m) >= 0]
+    assert len(valid) == 27  # every other mask has both bits of one axis set
+    for d in range(27):
+        assert O.output_to_input_direction(O.output_to_input_direction(d)) == d
+
+
+# ---------------------------------------------------------------------------
+# RandomGenerator (ranlxd) and emission
+# ---------------------------------------------------------------------------
+def test_ranlux_streams_bit_exact(oracle_mod):
+    g = golden("rng.npz")
+    for seed, ref in zip(g["seeds"], g["streams"]):
+        gen = O.RanluxGenerator(int(seed))
+        assert np.array_equal(gen.uniform(ref.size), ref), seed
+
+
+def test_emission_streams_bit_exact(oracle_mod):
+    g = golden("emission.npz")
+    off = 0
+    for seed, n, src in zip(g["seeds"], g["counts"], g["sources"]):
+        ours = O.fill_buffer_stream(int(seed), src, int(n))
+        ref = g["photons"][off: off + n]
+        assert ours.tobytes() == ref.tobytes()
+        off += n
+
+
+# ---------------------------------------------------------------------------
+# DensitySubGrid::interact
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", ["interior16", "entries8", "edges16", "noncubic"])
+def test_interact_bit_exact(oracle_mod, case):
+    g = golden(f"walk_{case}.npz")
+    sg = O.subgrid(g["box"], g["ncell"])
+    nH, xH = g["nH"].copy(), g["xH"].copy()
+    J = np.zeros_like(nH)
+    for i in range(g["photons"].size):
+        p = g["photons"][i: i + 1].copy()
+        res, cells, lengths, n = O.interact(sg, nH, xH, J, p, int(g["in_dirs"][i]),
+                                            max_steps=4096)
+        assert res == g["result"][i]
+        assert p.tobytes() == g["out"][i: i + 1].tobytes()
+        # the cells the reference tallied for this packet alone: the nonzero
+        # lmin*sigma*w of the trace (a straight ray visits a cell once)
+        b, e = g["offsets"][i], g["offsets"][i + 1]
+        vals = lengths * p["sigma"][0] * p["weight"][0]
+        nz = vals != 0
+        order = np.argsort(cells[nz], kind="stable")
+        assert np.array_equal(cells[nz][order], g["cells"][b:e])
+        assert np.array_equal(vals[nz][order], g["values"][b:e])
+    assert np.array_equal(J, g["J"])  # same accumulation order -> same bits
+
+
+def test_interact_invariants(oracle_mod):
+    """DensitySubGrid.hpp:1230-1265 asserts: lmin >= 0 and cells stay inside."""
+    g = golden("walk_interior16.npz")
+    sg = O.subgrid(g["box"], g["ncell"])
+    J = np.zeros_like(g["nH"])
+    for i in range(g["photons"].size):
+        p = g["photons"][i: i + 1].copy()
+        res, cells, lengths, n = O.interact(sg, g["nH"], g["xH"], J, p, 0, max_steps=4096)
+        assert n == len(cells)
+        assert np.all(lengths >= 0)
+        assert np.all((cells >= 0) & (cells < g["nH"].size))
+        assert O.is_compatible_output_direction(p["direction"][0], res)
+
+
+# ---------------------------------------------------------------------------
+# compute_neutral_fraction
+# ---------------------------------------------------------------------------
+def test_balance_bit_exact(oracle_mod):
+    g = golden("balance.npz")
+    sg = O.subgrid(g["box"], g["ncell"])
+    nH, J = g["nH"].copy(), g["J"].copy()
+    x = np.zeros_like(nH)
+    jf = O.jfac(float(g["L"]), float(g["N"]), np.array(sg.inv_cell_size))
+    O.compute_neutral_fraction(nH, x, J, jf, 4e-19, form=0)
+    assert np.array_equal(x, g["xH"])
+    assert np.array_equal(J, g["J_after"])
+
+
+def test_balance_stable_form_agrees(oracle_mod):
+    """1/(1+a+sqrt(a(a+2))) == 1 + a(1 - sqrt(1 + 2/a)) up to the latter's cancellation."""
+    g = golden("balance.npz")
+    sg = O.subgrid(g["box"], g["ncell"])
+    nH = g["nH"].copy()
+    jf = O.jfac(float(g["L"]), float(g["N"]), np.array(sg.inv_cell_size))
+    xs = np.zeros_like(nH)
+    O.compute_neutral_fraction(nH, xs, g["J"].copy(), jf, 4e-19, form=1)
+    xr = g["xH"]
+    a = 0.5 * jf * g["J"] / (nH * 4e-19)
+    # 1 + a - a*sqrt(1 + 2/a) subtracts terms of size a: its absolute error is
+    # ~eps * a, which near full ionization (x ~ 1/(2a)) exceeds x itself and
+    # even makes the reference return negative neutral fractions
+    tol = 8 * 2.2e-16 * (1.0 + a)
+    assert np.all(np.abs(xs - xr) <= tol)
+    assert np.any(xr < 0) and np.all(xs > 0)
+    # and the stable form is exact to a few ulp against extended precision
+    aa = a.astype(np.longdouble)
+    exact = 1.0 / (1.0 + aa + np.sqrt(aa * (aa + 2.0)))
+    exact = np.where(g["J"] > 0, exact, 1.0)
+    assert np.all(np.abs(xs - exact.astype(np.float64)) <= 4e-16 * np.abs(xs))
+
+
+# ---------------------------------------------------------------------------
+# lattice routing (do_photon_traversal + neighbours)
+# ---------------------------------------------------------------------------
+def test_lattice_transport_bit_exact(oracle_mod):
+    g = golden("transport.npz")
+    lat = O.LatticeGrid(g["box"], g["ncell"], g["num_subgrid"])
+    J = np.zeros_like(g["nH"])
+    ph = g["photons"].copy()
+    counts = lat.transport(g["nH"], g["xH"], J, ph, g["start"])
+    assert ph.tobytes() == g["final"].tobytes()
+    assert np.array_equal(J, g["J"])
+    assert counts["absorbed"] == int(np.sum(g["fate"] == 0))
+    assert counts["escaped"] == int(np.sum(g["fate"] == 1))
+    assert counts["transits"] == int(g["transits"].sum())
+
+
+def test_neighbour_table(oracle_mod):
+    lat = O.LatticeGrid([0, 0, 0, 1, 1, 1], [8, 8, 8], [2, 2, 2])
+    ngb = lat.neighbours()
+    for s in range(8):
+        assert ngb[s, 0] == s  # INSIDE -> itself (testDensitySubGrid_omp.cpp:1855)
+    # subgrid 0 = (0,0,0): its P neighbours exist, N ones are outside
+    assert ngb[0, D["FACE_X_P"]] == 4 and ngb[0, D["FACE_X_N"]] == O.NEIGHBOUR_OUTSIDE
+    assert ngb[0, D["CORNER_PPP"]] == 7 and ngb[7, D["CORNER_NNN"]] == 0
+
+
+def test_fp32_walk_tracks_fp64(oracle_mod):
+    """The FP32 cell-unit walk (the GPU single-precision spec) follows the FP64 walk."""
+    g = golden("walk_interior16.npz")
+    sg = O.subgrid(g["box"], g["ncell"])
+    kappa = O.kappa32(g["nH"], g["xH"])
+    cs = np.array(sg.cell_size, dtype=np.float32)
+    same_seq = 0
+    for i in range(g["photons"].size):
+        p = g["photons"][i: i + 1].copy()
+        _, cells64, len64, _ = O.interact(sg, g["nH"], g["xH"], np.zeros_like(g["nH"]), p, 0,
+                                          max_steps=4096)
+        q = np.zeros(1, O.PACKET32_DTYPE)
+        q["pos"] = ((g["photons"]["position"][i] - g["box"][:3]) * np.array(sg.inv_cell_size))
+        q["dir"] = g["photons"]["direction"][i]
+        q["tau"] = g["photons"]["tau"][i]
+        _, cells32, len32, _ = O.interact32(g["ncell"], cs, kappa, None, q, max_steps=4096)
+        if np.array_equal(cells32, cells64):
+            same_seq += 1
+            # FP32 positions in cell units of a 16-cell subgrid: absolute error
+            # ~ 16 * 2^-24 cells, so the bound is on |dl| / cell size.  The
+            # last segment of an absorbed packet also carries the FP32 error of
+            # the accumulated optical depth, (tau_done - tau_target) / tau.
+            cs0 = float(sg.cell_size[0])
+            err = np.abs(len32.astype(np.float64) - len64) / cs0
+            assert np.all(err[:-1] <= 2e-5)
+            assert err[-1] <= 1e-3
+    assert same_seq >= 0.97 * g["photons"].size
+
+
+def test_philox_known_answer(oracle_mod):
+    # Random123 known-answer vectors for philox4x32-10
+    out = O.philox4x32([0, 0, 0, 0], [0, 0])
+    assert list(out) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    out = O.philox4x32([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)
+    assert list(out) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    out = O.philox4x32([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344],
+                       [0xA4093822, 0x299F31D0])
+    assert list(out) == [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def test_split_packets(oracle_mod):
+    L = np.array([4.26e48, 1.0e48, 3.3e48, 7.7e47])
+    n = O.split_packets(L, 10_000_001, seed=42, iteration=3)
+    assert int(n.sum()) == 10_000_001
+    base = (L / L.sum() * 10_000_001).astype(np.uint64)
+    assert np.all(n - base <= 1)
