@@ -232,7 +232,10 @@ def gen_transport():
 
 
 def gen_ensemble(seeds=8, packets=1_000_000, iterations=10):
-    """64^3 Stromgren sphere with the reference code (all host threads)."""
+    """64^3 Stromgren sphere with the reference code (all host threads).
+
+    Member k draws buffer b of iteration i from ranlxd(seed_k + b + i * 5000):
+    seeds 10^7 apart keep the members' streams disjoint."""
     box = np.array([-5 * PC, -5 * PC, -5 * PC, 10 * PC, 10 * PC, 10 * PC])
     ncell, nsub = (64, 64, 64), (8, 8, 8)
     cells = 64 ** 3
@@ -247,7 +250,7 @@ def gen_ensemble(seeds=8, packets=1_000_000, iterations=10):
     profiles, radii = [], []
     for k in range(seeds):
         x, its = O.ref_iterations(box, ncell, nsub, nH, xH0, [0.0, 0.0, 0.0], [4.26e49],
-                                  packets, iterations, seed=1000 + 97 * k,
+                                  packets, iterations, seed=1000 + 10_000_000 * k,
                                   binary="ref_harness_exact")
         cube = blocked_to_cube(x, ncell, nsub).reshape(-1)
         prof = np.array([cube[which == b].mean() for b in range(len(edges) - 1)])
