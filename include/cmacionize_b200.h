@@ -77,11 +77,17 @@ typedef struct {
 
 enum cmi_precision {
   CMI_TRANSPORT_FP64 = 0, /* the reference's FP64 walk, operation for operation */
-  CMI_TRANSPORT_FP32 = 1  /* FP32 cell-unit walk, compensated FP32 tallies merged into FP64 */
+  CMI_TRANSPORT_FP32 = 1  /* FP32 cell-unit walk, shared-memory tallies (cmi_tally) merged into FP64 */
 };
 enum cmi_balance_form {
   CMI_BALANCE_REFERENCE = 0, /* x = 1 + a(1 - sqrt(2/a + 1)), DensitySubGrid.hpp:1650 */
   CMI_BALANCE_STABLE = 1     /* x = 1 / (1 + a + sqrt(a(a + 2))), same value, no cancellation */
+};
+enum cmi_tally {
+  CMI_TALLY_FP32 = 0,              /* FP32 shared-memory atomics */
+  CMI_TALLY_FP32_COMPENSATED = 1,  /* FP32 atomics + TwoSum rounding error in a second FP32 word */
+  CMI_TALLY_FIXED64 = 2,           /* 64-bit fixed point (lref/2^24 units), 32-bit integer atomics + carry */
+  CMI_TALLY_FIXED64_ATOMIC64 = 3   /* 64-bit fixed point, 64-bit integer atomics */
 };
 enum cmi_rng {
   CMI_RNG_PHILOX = 0, /* counter-based Philox4x32-10 per packet */
@@ -103,8 +109,8 @@ typedef struct {
   int32_t device;              /* CUDA device ordinal */
   int32_t threads_per_cta;     /* 0 = library default (256) */
   int32_t ctas_per_sm;         /* 0 = as many as fit */
-  int32_t packets_per_chunk;   /* 0 = library default (4096) */
-  int32_t compensated_tally;   /* FP32 mode: 1 = hi/lo compensated smem tallies (default), 0 = plain */
+  int32_t packets_per_chunk;   /* 0 = library default (512); power of two in [32, 4096] */
+  int32_t tally_mode;          /* FP32 transport: cmi_tally (default CMI_TALLY_FIXED64) */
   int32_t use_graph;           /* 1 = capture each iteration as a CUDA graph (default) */
   int32_t reserved[7];
 } cmi_options;
@@ -198,6 +204,13 @@ int cmi_trace_packet(cmi_context *context, int32_t instance, uint32_t subgrid,
  * an instance with the given total luminosity and packet count; resets J. */
 int cmi_compute_neutral_fraction(cmi_context *context, int32_t instance, double luminosity,
                                  uint64_t num_photon, double *mean_abs_dx);
+
+/* The same for the subgrids [first_subgrid, first_subgrid + count) of an
+ * instance only: DensitySubGrid::compute_neutral_fraction called per subgrid. */
+int cmi_compute_neutral_fraction_subgrids(cmi_context *context, int32_t instance,
+                                          uint32_t first_subgrid, uint32_t count,
+                                          double luminosity, uint64_t num_photon,
+                                          double *mean_abs_dx);
 
 /* Device-side access for interop (zero-copy views, NCCL reductions): the
  * instance's J (which = 0), x_H (1) or n_H (2) array in BLOCKED layout, and

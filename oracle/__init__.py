@@ -122,7 +122,10 @@ def lib():
         L.cmio_get_output_direction.argtypes = [C.POINTER(Subgrid), pi32]
         L.cmio_interact.argtypes = [C.POINTER(Subgrid), pd, pd, pd, C.c_void_p, C.c_int,
                                     pi32, pd, i32, pi32]
-        L.cmio_interact32.argtypes = [pi32, pf, pf, pd, C.c_void_p, pi32, pf, i32, pi32]
+        L.cmio_interact32.argtypes = [pi32, pf, pf, pf, pd, C.POINTER(u64), C.c_float,
+                                      C.c_void_p, pi32, pf, i32, pi32]
+        L.cmio_fixed_scale.argtypes = [C.POINTER(Subgrid)]
+        L.cmio_fixed_scale.restype = C.c_float
         L.cmio_jfac.argtypes = [d, d, pd]
         L.cmio_jfac.restype = d
         L.cmio_compute_neutral_fraction.argtypes = [i64, pd, pd, pd, d, d, C.c_int]
@@ -140,8 +143,8 @@ def lib():
         L.cmio_lattice_locate.restype = u32
         L.cmio_transport.argtypes = [C.POINTER(Lattice), pd, pd, pd, C.c_void_p, pu32, i64,
                                      C.POINTER(Counts)]
-        L.cmio_transport32.argtypes = [C.POINTER(Lattice), pf, pd, C.c_void_p, pu32, i64,
-                                       C.POINTER(Counts)]
+        L.cmio_transport32.argtypes = [C.POINTER(Lattice), pf, pd, C.POINTER(u64), C.c_void_p,
+                                       pu32, i64, C.POINTER(Counts)]
         L.cmio_split_packets.argtypes = [i32, pd, u64, u64, u32, C.POINTER(u64)]
         L.cmio_kappa32.argtypes = [i64, pd, pd, d, pf]
         L.cmio_iteration_omp.argtypes = [C.POINTER(Lattice), pd, pd, pd, pd, i32, pd, pd, u64,
@@ -208,15 +211,20 @@ def interact(sg: Subgrid, nH, xH, J, photon, input_direction: int, max_steps: in
     return res, cells[:n].copy(), lengths[:n].copy(), nsteps.value
 
 
-def interact32(ncell, cell_size, kappa, tally, packet, max_steps: int = 0):
+def interact32(ncell, cell_size, kappa, tally, packet, max_steps: int = 0,
+               inv_cell_size=None):
+    """FP32 cell-unit walk; inv_cell_size defaults to float(1 / cell_size)."""
     n3 = np.ascontiguousarray(ncell, dtype=np.int32)
     cs = np.ascontiguousarray(cell_size, dtype=np.float32)
+    if inv_cell_size is None:
+        inv_cell_size = 1.0 / np.asarray(cell_size, dtype=np.float64)
+    ics = np.ascontiguousarray(inv_cell_size, dtype=np.float32)
     cells = np.zeros(max(max_steps, 1), dtype=np.int32)
     lengths = np.zeros(max(max_steps, 1), dtype=np.float32)
     nsteps = C.c_int32(0)
     res = lib().cmio_interact32(
-        _ptr(n3, C.c_int32), _ptr(cs, C.c_float), _ptr(kappa, C.c_float),
-        _ptr(tally, C.c_double) if tally is not None else None, packet.ctypes.data,
+        _ptr(n3, C.c_int32), _ptr(cs, C.c_float), _ptr(ics, C.c_float), _ptr(kappa, C.c_float),
+        _ptr(tally, C.c_double) if tally is not None else None, None, 1.0, packet.ctypes.data,
         _ptr(cells, C.c_int32) if max_steps else None,
         _ptr(lengths, C.c_float) if max_steps else None, max_steps, C.byref(nsteps))
     n = min(nsteps.value, max_steps)
@@ -330,14 +338,20 @@ class LatticeGrid:
                              packets.size, C.byref(counts))
         return counts.as_dict()
 
-    def transport32(self, kappa, tally, packets, start_subgrid):
+    def transport32(self, kappa, tally, packets, start_subgrid, fixed=None):
+        """FP32 transport; tally: double sums of lmin, fixed: uint64 fixed-point sums."""
         counts = Counts()
         s = np.ascontiguousarray(start_subgrid, dtype=np.uint32)
         lib().cmio_transport32(C.byref(self.lat), _ptr(kappa, C.c_float),
                                _ptr(tally, C.c_double) if tally is not None else None,
+                               _ptr(fixed, C.c_uint64) if fixed is not None else None,
                                packets.ctypes.data, _ptr(s, C.c_uint32), packets.size,
                                C.byref(counts))
         return counts.as_dict()
+
+    def fixed_unit(self, s=0):
+        """Metres per fixed-point tally unit of subgrid s (lref / 2^22)."""
+        return float(max(np.float32(v) for v in self.lat.sub[s].cell_size)) / 4194304.0
 
     def iteration_omp(self, nH, xH, J, src_pos, src_lum, num_photon, seed, iteration,
                       alpha_H=4e-19, cross_section=6.3e-22, balance_form=1, threads=0):

@@ -224,8 +224,18 @@ int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, do
  * path lengths in metres: l = (face - p) * (cell_size / d).  On exit the
  * position is re-expressed relative to the neighbour across the exit face
  * (exact: the exit coordinate is 0 or n). */
-int cmio_interact32(const int32_t ncell[3], const float cell_size[3], const float *kappa,
-                    double *tally, cmio_packet32 *packet, int32_t *trace_cells,
+float cmio_fixed_scale(const cmio_subgrid *sg) {
+  float lref = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    const float cs = (float)sg->cell_size[a];
+    lref = (cs > lref) ? cs : lref;
+  }
+  return 4194304.f / lref;
+}
+
+int cmio_interact32(const int32_t ncell[3], const float cell_size[3],
+                    const float inv_cell_size[3], const float *kappa, double *tally,
+                    uint64_t *fixed, float scale, cmio_packet32 *packet, int32_t *trace_cells,
                     float *trace_lengths, int32_t max_steps, int32_t *nsteps) {
   const int in_dir = (int)(packet->meta & 31u);
   const float *d = packet->dir;
@@ -233,8 +243,9 @@ int cmio_interact32(const int32_t ncell[3], const float cell_size[3], const floa
   float inv[3], dcs[3];
   int32_t idx[3];
   for (int a = 0; a < 3; ++a) {
-    dcs[a] = d[a] / cell_size[a];
-    inv[a] = cell_size[a] / d[a];
+    /* correctly rounded reciprocal and products (no divisions) */
+    dcs[a] = d[a] * inv_cell_size[a];
+    inv[a] = cell_size[a] * (1.f / d[a]);
     const int s = kSigns[in_dir][a];
     idx[a] = (s == 0) ? (int32_t)p[a] : ((s < 0) ? 0 : ncell[a] - 1);
   }
@@ -247,7 +258,7 @@ int cmio_interact32(const int32_t ncell[3], const float cell_size[3], const floa
     float lo[3], hi[3], l[3];
     for (int a = 0; a < 3; ++a) {
       lo[a] = (float)idx[a];
-      hi[a] = (float)(idx[a] + 1);
+      hi[a] = lo[a] + 1.f;
       if (d[a] > 0.f) {
         l[a] = (hi[a] - p[a]) * inv[a];
       } else if (d[a] < 0.f) {
@@ -271,6 +282,11 @@ int cmio_interact32(const int32_t ncell[3], const float cell_size[3], const floa
     }
     if (tally != NULL) {
       tally[cell] += (double)lmin;
+    }
+    if (fixed != NULL) {
+      /* round half to even of lmin * scale (< 2^23), clamped at 0 */
+      const float q = lmin * scale;
+      fixed[cell] += (q > 0.f) ? (uint64_t)nearbyintf(q) : 0u;
     }
     if (trace_cells != NULL && steps < max_steps) {
       trace_cells[steps] = cell;
@@ -644,8 +660,8 @@ void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH,
 }
 
 void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally,
-                      cmio_packet32 *packets, const uint32_t *start_subgrid, int64_t n,
-                      cmio_counts *counts) {
+                      uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
+                      int64_t n, cmio_counts *counts) {
   const int64_t C = lat->cells_per_subgrid;
   for (int64_t i = 0; i < n; ++i) {
     uint32_t s = start_subgrid[i];
@@ -653,10 +669,12 @@ void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally
       const cmio_subgrid *sg = &lat->sub[s];
       const float cs[3] = {(float)sg->cell_size[0], (float)sg->cell_size[1],
                            (float)sg->cell_size[2]};
+      const float ics[3] = {(float)sg->inv_cell_size[0], (float)sg->inv_cell_size[1],
+                            (float)sg->inv_cell_size[2]};
       int32_t steps = 0;
-      const int out = cmio_interact32(lat->sub_ncell, cs, kappa + s * C,
-                                      tally ? tally + s * C : NULL, &packets[i], NULL, NULL, 0,
-                                      &steps);
+      const int out = cmio_interact32(lat->sub_ncell, cs, ics, kappa + s * C,
+                                      tally ? tally + s * C : NULL, fixed ? fixed + s * C : NULL,
+                                      cmio_fixed_scale(sg), &packets[i], NULL, NULL, 0, &steps);
       counts->crossings += (uint64_t)steps;
       counts->transits += 1;
       if (out == CMIO_INSIDE) {

@@ -85,8 +85,12 @@ typedef struct {
   uint32_t meta; /* low 5 bits: input TravelDirection */
 } cmio_packet32;
 
+/* tally (may be NULL): double sum of the FP32 path lengths.  fixed (may be
+ * NULL): the fixed-point tally of the GPU kernels, sum of
+ * round_half_even(lmin * scale) clamped at 0, with scale = 2^22 / lref. */
 int cmio_interact32(const int32_t ncell[3], const float cell_size[3],
-                    const float *kappa, double *tally, cmio_packet32 *packet,
+                    const float inv_cell_size[3], const float *kappa, double *tally,
+                    uint64_t *fixed, float scale, cmio_packet32 *packet,
                     int32_t *trace_cells, float *trace_lengths, int32_t max_steps,
                     int32_t *nsteps);
 
@@ -156,8 +160,10 @@ void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH,
 
 /* FP32 counterpart of cmio_transport (same routing, cell-unit walk). */
 void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally,
-                      cmio_packet32 *packets, const uint32_t *start_subgrid,
+                      uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
                       int64_t n, cmio_counts *counts);
+/* scale of the fixed-point tally of a subgrid: 2^24 / max float cell size */
+float cmio_fixed_scale(const cmio_subgrid *sg);
 
 /* Packets per source for one iteration: the reference split
  * (uint)(L_i/L_tot*N), with the remainder going to the sources holding the

@@ -27,6 +27,10 @@ TRANSPORT_FP64 = 0
 TRANSPORT_FP32 = 1
 BALANCE_REFERENCE = 0
 BALANCE_STABLE = 1
+TALLY_FP32 = 0
+TALLY_FP32_COMPENSATED = 1
+TALLY_FIXED64 = 2
+TALLY_FIXED64_ATOMIC64 = 3
 RNG_PHILOX = 0
 RNG_RANLUX = 1
 LAYOUT_BLOCKED = 0
@@ -45,6 +49,7 @@ EXPORTED = [
     "cmi_transport_packets", "cmi_traverse_buffer", "cmi_trace_packet",
     "cmi_compute_neutral_fraction", "cmi_device_field", "cmi_get_stream", "cmi_synchronize",
     "cmi_last_launch_count", "cmi_set_kernel_timing", "cmi_kernel_timing",
+    "cmi_compute_neutral_fraction_subgrids",
 ]
 
 PHOTON_DTYPE = np.dtype(
@@ -80,7 +85,7 @@ class Options(C.Structure):
         ("threads_per_cta", C.c_int32),
         ("ctas_per_sm", C.c_int32),
         ("packets_per_chunk", C.c_int32),
-        ("compensated_tally", C.c_int32),
+        ("tally_mode", C.c_int32),
         ("use_graph", C.c_int32),
         ("reserved", C.c_int32 * 7),
     ]
@@ -143,6 +148,7 @@ def load():
     L.cmi_traverse_buffer.argtypes = [ctx, i32, u32, i32, vp, u32, vp, vp, vp, vp]
     L.cmi_trace_packet.argtypes = [ctx, i32, u32, i32, vp, i32, vp, vp, vp, vp]
     L.cmi_compute_neutral_fraction.argtypes = [ctx, i32, d, u64, vp]
+    L.cmi_compute_neutral_fraction_subgrids.argtypes = [ctx, i32, u32, u32, d, u64, vp]
     L.cmi_device_field.argtypes = [ctx, i32, i32, C.POINTER(C.POINTER(C.c_double)),
                                    C.POINTER(u64)]
     L.cmi_get_stream.argtypes = [ctx, C.POINTER(vp)]

@@ -9,6 +9,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "cmacionize/ranlxd.h"
+
 namespace cmi {
 
 constexpr int kNumDirections = 27;
@@ -106,7 +108,7 @@ struct alignas(16) Chunk {
   uint32_t subgrid;
   uint32_t count;
   uint32_t begin;
-  uint32_t pad;
+  uint32_t rem;  // chunks of this subgrid from this one to its last, inclusive
 };
 
 // Per-iteration counters of one instance (device side of cmi_stats).
@@ -224,85 +226,7 @@ __device__ __forceinline__ void philox_packet(uint64_t seed, uint32_t instance,
   tau = -log(u2);
 }
 
-// ---------------------------------------------------------------------------
-// ranlxd (RandomGenerator.hpp:36-232), the reference's generator, for
-// replaying the reference's per-buffer streams on the device.
-// ---------------------------------------------------------------------------
-struct Ranlux {
-  double x[12];
-  double carry;
-  uint32_t ir, jr, ir_old, pr;
-
-  static constexpr double kOneBit = 1.0 / 281474976710656.0;  // 2^-48
-
-  __host__ __device__ void step(uint32_t i, uint32_t j) {
-    double y = x[j] - x[i];
-    y = y - carry;
-    if (y < 0) {
-      carry = kOneBit;
-      y += 1;
-    } else {
-      carry = 0;
-    }
-    x[i] = y;
-  }
-
-  // RandomGenerator.hpp:80-150
-  __host__ __device__ void increment() {
-    uint32_t i = ir, j = jr;
-    int32_t k = 0;
-    for (; i > 0; ++k) {
-      step(i, j);
-      i = (i + 1) % 12;
-      j = (j + 1) % 12;
-    }
-    for (; k <= (int32_t)pr - 12; k += 12) {
-      for (uint32_t q = 0; q < 12; ++q) step(q, (q + 7) % 12);
-    }
-    for (; k < (int32_t)pr; ++k) {
-      step(i, j);
-      i = (i + 1) % 12;
-      j = (j + 1) % 12;
-    }
-    ir = i;
-    ir_old = i;
-    jr = j;
-  }
-
-  // RandomGenerator.hpp:158-197
-  __host__ __device__ void seed(int32_t s) {
-    if (s == 0) s = 1;
-    int32_t bits[31];
-    int32_t v = s & 0x7FFFFFFF;
-    for (int k = 0; k < 31; ++k) {
-      bits[k] = v % 2;
-      v /= 2;
-    }
-    int ib = 0, jb = 18;
-    for (int k = 0; k < 12; ++k) {
-      double acc = 0;
-      for (int m = 1; m <= 48; ++m) {
-        const double y = (double)((bits[ib] + 1) % 2);
-        acc += acc + y;
-        bits[ib] = (bits[ib] + bits[jb]) % 2;
-        ib = (ib + 1) % 31;
-        jb = (jb + 1) % 31;
-      }
-      x[k] = kOneBit * acc;
-    }
-    carry = 0;
-    ir = 11;
-    jr = 7;
-    ir_old = 0;
-    pr = 397;
-  }
-
-  // RandomGenerator.hpp:214-222
-  __host__ __device__ double uniform() {
-    ir = (ir + 1) % 12;
-    if (ir == ir_old) increment();
-    return x[ir];
-  }
-};
+// ranlxd, the reference's generator (shared with the host C++ surface)
+using Ranlux = cmi_ranlxd::Ranlxd;
 
 }  // namespace cmi

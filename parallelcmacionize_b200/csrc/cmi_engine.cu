@@ -300,14 +300,21 @@ int refresh_kappa(cmi_context *c, int32_t i) {
 // launch helpers (each counts its kernel)
 // ---------------------------------------------------------------------------
 int launch_plan(cmi_context *c) {
-  k_plan_count<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
-                                                          c->d_tile_pk, c->d_tile_ch);
-  k_plan_offsets<<<1, kPlanThreads, 0, c->stream>>>(c->ntiles, c->d_tile_pk, c->d_tile_ch,
-                                                     c->d_tile_pk_off, c->d_tile_ch_off,
-                                                     c->d_state);
-  k_plan_write<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
-                                                          c->d_tile_pk_off, c->d_tile_ch_off,
-                                                          c->d_bucket_off, c->d_chunks);
+  if (c->ntiles == 1) {
+    k_plan_fused<<<1, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk, c->d_bucket_off,
+                                                    c->d_chunks, c->d_state);
+    c->enqueued += 1;
+  } else {
+    k_plan_count<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
+                                                            c->d_tile_pk, c->d_tile_ch);
+    k_plan_offsets<<<1, kPlanThreads, 0, c->stream>>>(c->ntiles, c->d_tile_pk, c->d_tile_ch,
+                                                       c->d_tile_pk_off, c->d_tile_ch_off,
+                                                       c->d_state);
+    k_plan_write<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
+                                                            c->d_tile_pk_off, c->d_tile_ch_off,
+                                                            c->d_bucket_off, c->d_chunks);
+    c->enqueued += 3;
+  }
   const int grid = c->num_sms * 8;
   if (c->fp32()) {
     k_scatter<Packet32><<<grid, 256, 0, c->stream>>>(
@@ -318,13 +325,14 @@ int launch_plan(cmi_context *c) {
         (const Packet64 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
         (Packet64 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
   }
-  c->enqueued += 4;
+  c->enqueued += 1;
   CMI_CUDA(cudaGetLastError());
   return CMI_OK;
 }
 
 WalkParams walk_params(cmi_context *c) {
   WalkParams p{};
+  p.chunk = c->chunk;
   p.subs = c->d_sub;
   p.inst = c->d_inst;
   p.chunks = c->d_chunks;
@@ -345,27 +353,30 @@ WalkParams walk_params(cmi_context *c) {
   return p;
 }
 
-template <bool kF32, bool kComp>
-void launch_walk_t(cmi_context *c, const WalkParams &p) {
-  k_walk<kF32, kComp, kWalkThreads><<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+template <int kTally>
+void launch_walk32_t(cmi_context *c, const WalkParams &p) {
+  k_walk32<kWalkThreads, kTally><<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
 }
 
 int launch_walk(cmi_context *c) {
   const WalkParams p = walk_params(c);
   if (c->fp32()) {
-    if (c->opt.compensated_tally) launch_walk_t<true, true>(c, p);
-    else launch_walk_t<true, false>(c, p);
+    switch (c->opt.tally_mode) {
+      case 0: launch_walk32_t<0>(c, p); break;
+      case 1: launch_walk32_t<1>(c, p); break;
+      case 2: launch_walk32_t<2>(c, p); break;
+      default: launch_walk32_t<3>(c, p); break;
+    }
   } else {
-    launch_walk_t<false, false>(c, p);
+    k_walk64<kWalkThreads><<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
   }
   c->enqueued += 1;
   CMI_CUDA(cudaGetLastError());
   return CMI_OK;
 }
 
-template <bool kF32, bool kComp>
-int config_walk_t(cmi_context *c) {
-  auto fn = k_walk<kF32, kComp, kWalkThreads>;
+template <class F>
+int config_kernel(cmi_context *c, F fn) {
   CMI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)c->walk_smem));
   int per_sm = 0;
@@ -380,14 +391,23 @@ int config_walk_t(cmi_context *c) {
 }
 
 int config_walk(cmi_context *c) {
-  const size_t head = (sizeof(WalkShared) + 15) & ~(size_t)15;
-  const size_t per_cell = c->fp32() ? (c->opt.compensated_tally ? 12 : 8) : 24;
-  c->walk_smem = head + per_cell * (size_t)c->max_padded;
   if (c->fp32()) {
-    if (c->opt.compensated_tally) return config_walk_t<true, true>(c);
-    return config_walk_t<true, false>(c);
+    const size_t head = (sizeof(Walk32Shared) + 15) & ~(size_t)15;
+    const int tm = c->opt.tally_mode;
+    const size_t tally_bytes = (tm == 0 ? 4 : 8) * (size_t)c->max_padded + 16;
+    c->walk_smem = head + 4 * (size_t)c->max_padded + tally_bytes +
+                   sizeof(Packet32) * 2 * (size_t)c->chunk +
+                   (sizeof(Packet32) + 4) * (kWalkThreads / 32) * kStage;
+    switch (tm) {
+      case 0: return config_kernel(c, k_walk32<kWalkThreads, 0>);
+      case 1: return config_kernel(c, k_walk32<kWalkThreads, 1>);
+      case 2: return config_kernel(c, k_walk32<kWalkThreads, 2>);
+      default: return config_kernel(c, k_walk32<kWalkThreads, 3>);
+    }
   }
-  return config_walk_t<false, false>(c);
+  const size_t head = (sizeof(WalkShared) + 15) & ~(size_t)15;
+  c->walk_smem = head + 24 * (size_t)c->max_padded;
+  return config_kernel(c, k_walk64<kWalkThreads>);
 }
 
 EmitParams emit_params(cmi_context *c) {
@@ -585,7 +605,7 @@ void cmi_default_options(cmi_options *o) {
   o->threads_per_cta = 0;
   o->ctas_per_sm = 0;
   o->packets_per_chunk = 0;
-  o->compensated_tally = 1;
+  o->tally_mode = CMI_TALLY_FIXED64;
   o->use_graph = 1;
 }
 
@@ -604,14 +624,20 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
     return fail(CMI_ERR_INVALID_ARGUMENT, "unknown rng %d", opt.rng);
   if (opt.threads_per_cta != 0 && opt.threads_per_cta != kWalkThreads)
     return fail(CMI_ERR_NOT_SUPPORTED, "threads_per_cta must be 0 or %d", kWalkThreads);
-  if (opt.packets_per_chunk < 0) return fail(CMI_ERR_INVALID_ARGUMENT, "negative chunk size");
+  if (opt.packets_per_chunk < 0 || opt.packets_per_chunk > 4096 ||
+      (opt.packets_per_chunk > 0 &&
+       (opt.packets_per_chunk < 32 || (opt.packets_per_chunk & (opt.packets_per_chunk - 1)))))
+    return fail(CMI_ERR_INVALID_ARGUMENT,
+                "packets_per_chunk must be 0 or a power of two in [32, 4096]");
+  if (opt.tally_mode < CMI_TALLY_FP32 || opt.tally_mode > CMI_TALLY_FIXED64_ATOMIC64)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "unknown tally mode %d", opt.tally_mode);
 
   cmi_context *c = new (std::nothrow) cmi_context();
   if (!c) return fail(CMI_ERR_OUT_OF_MEMORY, "host allocation failed");
   c->opt = opt;
   c->device = opt.device;
   c->tables = make_direction_tables();
-  c->chunk = opt.packets_per_chunk > 0 ? (uint32_t)opt.packets_per_chunk : 4096u;
+  c->chunk = opt.packets_per_chunk > 0 ? (uint32_t)opt.packets_per_chunk : 512u;
   auto bail = [&](int rc) {
     cmi_destroy(c);
     return rc;
@@ -733,6 +759,8 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
   for (const auto &I : c->inst) max_cells = std::max(max_cells, I.ncells);
   if ((rc = ensure_stage(c, sizeof(double) * (size_t)max_cells))) return bail(rc);
   if ((rc = ensure_capacity(c, 1024))) return bail(rc);
+  // pinned per-iteration statistics: allocated here, not inside a timed run
+  if ((rc = ensure_host_stats(c, 256 * c->inst.size()))) return bail(rc);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess)
     return bail(fail(CMI_ERR_CUDA, "context set-up failed: %s",
                      cudaGetErrorString(cudaGetLastError())));
@@ -1109,12 +1137,17 @@ int cmi_trace_packet(cmi_context *c, int32_t instance, uint32_t subgrid, int32_t
                   nullptr, nullptr, nullptr, max_steps, cells, lengths, num_steps);
 }
 
-int cmi_compute_neutral_fraction(cmi_context *c, int32_t instance, double luminosity,
-                                 uint64_t num_photon, double *mean_abs_dx) {
+int cmi_compute_neutral_fraction_subgrids(cmi_context *c, int32_t instance,
+                                          uint32_t first_subgrid, uint32_t count,
+                                          double luminosity, uint64_t num_photon,
+                                          double *mean_abs_dx) {
   CMI_TRY(check_ctx(c));
   CMI_TRY(check_instance(c, instance));
   if (num_photon == 0) return fail(CMI_ERR_INVALID_ARGUMENT, "num_photon must be > 0");
   const HostInstance &I = c->inst[instance];
+  if (count == 0 || first_subgrid >= I.nsub || count > I.nsub - first_subgrid)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "subgrid range [%u, %u + %u) outside [0, %u)",
+                first_subgrid, first_subgrid, count, I.nsub);
   const double inv[3] = {I.sub_ncell[0] / (I.desc.box[3] / I.desc.num_subgrid[0]),
                          I.sub_ncell[1] / (I.desc.box[4] / I.desc.num_subgrid[1]),
                          I.sub_ncell[2] / (I.desc.box[5] / I.desc.num_subgrid[2])};
@@ -1130,20 +1163,28 @@ int cmi_compute_neutral_fraction(cmi_context *c, int32_t instance, double lumino
   b.J = c->d_J;
   b.kappa = c->fp32() ? c->d_kappa : nullptr;
   b.stats = c->d_stats;
-  b.first_sub = I.first_sub;
-  b.num_subs = I.nsub;
+  b.first_sub = I.first_sub + first_subgrid;
+  b.num_subs = count;
   b.jfac_override = jfac;
   if (c->opt.balance_form == CMI_BALANCE_REFERENCE)
-    k_balance<0><<<I.nsub, 256, 0, c->stream>>>(b);
+    k_balance<0><<<count, 256, 0, c->stream>>>(b);
   else
-    k_balance<1><<<I.nsub, 256, 0, c->stream>>>(b);
+    k_balance<1><<<count, 256, 0, c->stream>>>(b);
   CMI_CUDA(cudaGetLastError());
   DevStats d{};
   CMI_CUDA(cudaMemcpyAsync(&d, c->d_stats + instance, sizeof(DevStats), cudaMemcpyDeviceToHost,
                            c->stream));
   CMI_CUDA(cudaStreamSynchronize(c->stream));
-  if (mean_abs_dx) *mean_abs_dx = d.dx_sum / (double)I.ncells;
+  if (mean_abs_dx) *mean_abs_dx = d.dx_sum / ((double)count * (double)I.cells_per_sub);
   return CMI_OK;
+}
+
+int cmi_compute_neutral_fraction(cmi_context *c, int32_t instance, double luminosity,
+                                 uint64_t num_photon, double *mean_abs_dx) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  return cmi_compute_neutral_fraction_subgrids(c, instance, 0, c->inst[instance].nsub,
+                                               luminosity, num_photon, mean_abs_dx);
 }
 
 int cmi_device_field(cmi_context *c, int32_t instance, int32_t which, double **ptr,
@@ -1190,7 +1231,7 @@ int cmi_kernel_timing(cmi_context *c, double ms[CMI_KERNEL_CLASSES],
     float v = 0.f;
     CMI_CUDA(cudaEventElapsedTime(&v, t.start, t.stop));
     ms[t.cls] += v;
-    launches[t.cls] += (t.cls == 1) ? 4 : 1;
+    launches[t.cls] += (t.cls == 1) ? ((c->ntiles == 1) ? 2 : 4) : 1;
     c->event_pool.push_back(t.start);
     c->event_pool.push_back(t.stop);
   }

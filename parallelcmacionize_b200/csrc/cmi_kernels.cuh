@@ -483,16 +483,80 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan_write(uint32_t *hist, uin
     const uint32_t s = s0 + k;
     if (s >= S) break;
     bucket_off[s] = opk;
-    for (uint32_t q = 0; q * chunk < c[k]; ++q) {
+    const uint32_t nch = (c[k] + chunk - 1) / chunk;
+    for (uint32_t q = 0; q < nch; ++q) {
       Chunk cc;
       cc.subgrid = s;
       cc.begin = opk + q * chunk;
       cc.count = min(chunk, c[k] - q * chunk);
-      cc.pad = 0;
+      cc.rem = nch - q;
       chunks[och++] = cc;
     }
     opk += c[k];
     hist[s] = 0u;
+  }
+}
+
+// Whole plan in one block when every subgrid fits one tile (S <= 4096):
+// counts -> bucket offsets -> chunk list, and the round-state update.
+__global__ void __launch_bounds__(kPlanThreads) k_plan_fused(uint32_t *hist, uint32_t S,
+                                                             uint32_t chunk,
+                                                             uint32_t *bucket_off,
+                                                             Chunk *chunks, RoundState *st) {
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t s_choff[kPlanTile + 1];  // first chunk of each subgrid
+  __shared__ uint32_t s_pkoff[kPlanTile + 1];  // first packet of each subgrid
+  const uint32_t s0 = threadIdx.x * kPlanPerThread;
+  uint32_t c[kPlanPerThread];
+  uint32_t pk = 0, ch = 0;
+#pragma unroll
+  for (int k = 0; k < kPlanPerThread; ++k) {
+    const uint32_t s = s0 + k;
+    c[k] = (s < S) ? hist[s] : 0u;
+    pk += c[k];
+    ch += (c[k] + chunk - 1) / chunk;
+  }
+  uint32_t tpk, tch;
+  uint32_t opk = block_exclusive_scan<kPlanThreads>(pk, ws, tpk);
+  uint32_t och = block_exclusive_scan<kPlanThreads>(ch, ws, tch);
+#pragma unroll
+  for (int k = 0; k < kPlanPerThread; ++k) {
+    const uint32_t s = s0 + k;
+    s_choff[s] = och;
+    s_pkoff[s] = opk;
+    if (s < S) {
+      bucket_off[s] = opk;
+      hist[s] = 0u;
+    }
+    opk += c[k];
+    och += (c[k] + chunk - 1) / chunk;
+  }
+  if (threadIdx.x == 0) {
+    s_choff[kPlanTile] = tch;
+    s_pkoff[kPlanTile] = tpk;
+  }
+  __syncthreads();
+  // every thread writes chunks; the subgrid of chunk q by binary search
+  for (uint32_t q = threadIdx.x; q < tch; q += kPlanThreads) {
+    int lo = 0, hi = kPlanTile - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_choff[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t j = q - s_choff[lo];
+    Chunk cc;
+    cc.subgrid = (uint32_t)lo;
+    cc.begin = s_pkoff[lo] + j * chunk;
+    cc.count = min(chunk, (s_pkoff[lo + 1] - s_pkoff[lo]) - j * chunk);
+    cc.rem = (s_choff[lo + 1] - s_choff[lo]) - j;
+    chunks[q] = cc;
+  }
+  if (threadIdx.x == 0) {
+    st->total_in = tpk;
+    st->num_chunks = tch;
+    st->chunk_next = 0;
+    st->arena_count = 0;
+    if (tpk > 0) st->rounds_active += 1;
   }
 }
 
@@ -513,6 +577,7 @@ __global__ void __launch_bounds__(256) k_scatter(const P *out, const uint32_t *k
 // walk: one wavefront round
 // ---------------------------------------------------------------------------
 struct WalkParams {
+  uint32_t chunk;          // largest chunk (packets), FP32 packet-buffer size
   const DevSubgrid *subs;
   const DevInstance *inst;
   const Chunk *chunks;
@@ -546,6 +611,89 @@ struct WalkShared {
   uint32_t claim;
   alignas(8) unsigned long long mbar;
 };
+
+struct Walk32Shared {
+  DirectionTables tab;
+  uint32_t ngb[kNumDirections];
+  int32_t n[3];
+  int32_t nyz;
+  int32_t ncells;
+  int32_t padded;
+  float cs_f[3];
+  float inv_cs_f[3];
+  float tally_scale;   // 2^22 / lref
+  double tally_unit;   // lref / 2^22 (m)
+  int64_t field_offset;
+  double sigma;
+  uint32_t instance;
+  // current run of chunks and segment of equal subgrid
+  uint32_t run_c0, run_c1;
+  uint32_t seg_sub, seg_begin, seg_chunks, seg_n, seg_next;
+  // packet ring: claims, per-slot copies, fills
+  uint32_t claim;
+  uint32_t loaded[2];
+  uint32_t uses[2];
+  uint32_t seg_use0[2];
+  alignas(8) unsigned long long mbar_field;
+  alignas(8) unsigned long long mbar_pk[2];
+};
+
+template <class Sh>
+__device__ __forceinline__ void load_subgrid(Sh &sh, const WalkParams &prm, uint32_t sub) {
+  const DevSubgrid &S = prm.subs[sub];
+  for (int d = 0; d < kNumDirections; ++d) sh.ngb[d] = S.ngb[d];
+  for (int a = 0; a < 3; ++a) {
+    sh.n[a] = S.ncell[a];
+    sh.cs_f[a] = S.cell_size_f[a];
+    sh.anchor[a] = S.anchor[a];
+    sh.cs[a] = S.cell_size[a];
+    sh.inv_cs[a] = S.inv_cell_size[a];
+  }
+  sh.nyz = S.ncell[1] * S.ncell[2];
+  sh.ncells = S.ncells;
+  sh.padded = S.padded_cells;
+  sh.field_offset = S.field_offset;
+  sh.instance = S.instance;
+  sh.sigma = prm.inst[S.instance].sigma;
+}
+
+__device__ __forceinline__ void load_subgrid32(Walk32Shared &sh, const DevSubgrid &S,
+                                               const WalkParams &prm) {
+  for (int d = 0; d < kNumDirections; ++d) sh.ngb[d] = S.ngb[d];
+  float lref = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    sh.n[a] = S.ncell[a];
+    sh.cs_f[a] = S.cell_size_f[a];
+    sh.inv_cs_f[a] = (float)S.inv_cell_size[a];
+    lref = fmaxf(lref, S.cell_size_f[a]);
+  }
+  sh.tally_scale = 4194304.f / lref;
+  sh.tally_unit = (double)lref / 4194304.0;
+  sh.nyz = S.ncell[1] * S.ncell[2];
+  sh.ncells = S.ncells;
+  sh.padded = S.padded_cells;
+  sh.field_offset = S.field_offset;
+  sh.instance = S.instance;
+  sh.sigma = prm.inst[S.instance].sigma;
+}
+
+// per-thread counters -> instance statistics (one atomic per warp and counter)
+__device__ __forceinline__ void flush_counters(DevStats *stats, uint32_t instance,
+                                               uint32_t &c_cross, uint32_t &c_trans,
+                                               uint32_t &c_abs, uint32_t &c_esc) {
+  const uint32_t wc = __reduce_add_sync(kFull, c_cross);
+  const uint32_t wt = __reduce_add_sync(kFull, c_trans);
+  const uint32_t wa = __reduce_add_sync(kFull, c_abs);
+  const uint32_t we = __reduce_add_sync(kFull, c_esc);
+  if ((threadIdx.x & 31) == 0) {
+    DevStats &S = stats[instance];
+    if (wc) atomicAdd(&S.crossings, (unsigned long long)wc);
+    if (wt) atomicAdd(&S.transits, (unsigned long long)wt);
+    if (wa) atomicAdd(&S.absorbed, (unsigned long long)wa);
+    if (we) atomicAdd(&S.escaped, (unsigned long long)we);
+  }
+  c_cross = c_trans = c_abs = c_esc = 0;
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -615,16 +763,14 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <bool kF32, bool kComp, int kThreads>
-__global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
+// FP64 wavefront round: the reference walk, fields staged by TMA, packets
+// read from the sorted arena, FP64 tallies in shared memory.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WalkShared &sh = *reinterpret_cast<WalkShared *>(smem_raw);
   const size_t head = (sizeof(WalkShared) + 15) & ~(size_t)15;
   const int P = prm.max_padded;
-  // FP32: kappa | hi | lo      FP64: nH | xH | J
-  float *s_kappa = reinterpret_cast<float *>(smem_raw + head);
-  float *s_hi = s_kappa + P;
-  float *s_lo = s_hi + P;
   double *s_n = reinterpret_cast<double *>(smem_raw + head);
   double *s_x = s_n + P;
   double *s_J = s_x + P;
@@ -638,14 +784,7 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
         reinterpret_cast<const uint32_t *>(&prm.tables)[tid];
   }
   if (tid == 0) mbar_init(&sh.mbar, 1);
-  if (kF32) {
-    for (int c = tid; c < P; c += kThreads) {
-      s_hi[c] = 0.f;
-      if (kComp) s_lo[c] = 0.f;
-    }
-  } else {
-    for (int c = tid; c < P; c += kThreads) s_J[c] = 0.;
-  }
+  for (int c = tid; c < P; c += kThreads) s_J[c] = 0.;
   __syncthreads();
 
   const int lane = tid & 31;
@@ -655,37 +794,13 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
   uint32_t c_cross = 0, c_trans = 0, c_abs = 0, c_esc = 0;
 
   auto flush = [&]() {
-    // tallies -> J (FP64, HBM), counters -> instance stats
     const int64_t off = sh.field_offset;
-    const int nc = sh.ncells;
-    if (kF32) {
-      const double sw = sh.sigma;  // sigma * weight; packets of the iteration have weight 1
-      for (int c = tid; c < nc; c += kThreads) {
-        const float h = s_hi[c];
-        const float l = kComp ? s_lo[c] : 0.f;
-        if (h != 0.f || l != 0.f) atomicAdd(&prm.J[off + c], ((double)h + (double)l) * sw);
-        s_hi[c] = 0.f;
-        if (kComp) s_lo[c] = 0.f;
-      }
-    } else {
-      for (int c = tid; c < nc; c += kThreads) {
-        const double v = s_J[c];
-        if (v != 0.) atomicAdd(&prm.J[off + c], v);
-        s_J[c] = 0.;
-      }
+    for (int c = tid; c < sh.ncells; c += kThreads) {
+      const double v = s_J[c];
+      if (v != 0.) atomicAdd(&prm.J[off + c], v);
+      s_J[c] = 0.;
     }
-    const uint32_t wc = __reduce_add_sync(kFull, c_cross);
-    const uint32_t wt = __reduce_add_sync(kFull, c_trans);
-    const uint32_t wa = __reduce_add_sync(kFull, c_abs);
-    const uint32_t we = __reduce_add_sync(kFull, c_esc);
-    if (lane == 0) {
-      DevStats &S = prm.stats[sh.instance];
-      if (wc) atomicAdd(&S.crossings, (unsigned long long)wc);
-      if (wt) atomicAdd(&S.transits, (unsigned long long)wt);
-      if (wa) atomicAdd(&S.absorbed, (unsigned long long)wa);
-      if (we) atomicAdd(&S.escaped, (unsigned long long)we);
-    }
-    c_cross = c_trans = c_abs = c_esc = 0;
+    flush_counters(prm.stats, sh.instance, c_cross, c_trans, c_abs, c_esc);
   };
 
   for (;;) {
@@ -709,32 +824,12 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
       if (staged != kNone) flush();
       __syncthreads();
       if (tid == 0) {
-        const DevSubgrid &S = prm.subs[sub];
-        for (int d = 0; d < kNumDirections; ++d) sh.ngb[d] = S.ngb[d];
-        for (int a = 0; a < 3; ++a) {
-          sh.n[a] = S.ncell[a];
-          sh.cs_f[a] = S.cell_size_f[a];
-          sh.anchor[a] = S.anchor[a];
-          sh.cs[a] = S.cell_size[a];
-          sh.inv_cs[a] = S.inv_cell_size[a];
-        }
-        sh.nyz = S.ncell[1] * S.ncell[2];
-        sh.ncells = S.ncells;
-        sh.padded = S.padded_cells;
-        sh.field_offset = S.field_offset;
-        sh.instance = S.instance;
-        sh.sigma = prm.inst[S.instance].sigma;
+        load_subgrid(sh, prm, sub);
         fence_proxy_async();
-        if (kF32) {
-          const uint32_t bytes = (uint32_t)S.padded_cells * 4u;
-          mbar_expect_tx(&sh.mbar, bytes);
-          tma_load_1d(s_kappa, prm.kappa + S.field_offset, bytes, &sh.mbar);
-        } else {
-          const uint32_t bytes = (uint32_t)S.padded_cells * 8u;
-          mbar_expect_tx(&sh.mbar, 2u * bytes);
-          tma_load_1d(s_n, prm.nH + S.field_offset, bytes, &sh.mbar);
-          tma_load_1d(s_x, prm.xH + S.field_offset, bytes, &sh.mbar);
-        }
+        const uint32_t bytes = (uint32_t)sh.padded * 8u;
+        mbar_expect_tx(&sh.mbar, 2u * bytes);
+        tma_load_1d(s_n, prm.nH + sh.field_offset, bytes, &sh.mbar);
+        tma_load_1d(s_x, prm.xH + sh.field_offset, bytes, &sh.mbar);
       }
       mbar_wait_bounded(&sh.mbar, phase, &st->flags);
       phase ^= 1u;
@@ -742,35 +837,19 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
       __syncthreads();
     }
 
-    // ---- trace the chunk's packets, one crossing per loop trip ----
     const uint32_t count = sh.chunk_count, begin = sh.chunk_begin;
     const int limit = sh.n[0] + sh.n[1] + sh.n[2] + 3;
-    View32 v32;
     View64 v64;
-    if (kF32) {
-      v32.kappa = s_kappa;
-      v32.tally_hi = s_hi;
-      v32.tally_lo = s_lo;
-      v32.n[0] = sh.n[0];
-      v32.n[1] = sh.n[1];
-      v32.n[2] = sh.n[2];
-      v32.nyz = sh.nyz;
-      v32.cs[0] = sh.cs_f[0];
-      v32.cs[1] = sh.cs_f[1];
-      v32.cs[2] = sh.cs_f[2];
-    } else {
-      v64.nH = s_n;
-      v64.xH = s_x;
-      v64.J = s_J;
-      for (int a = 0; a < 3; ++a) {
-        v64.n[a] = sh.n[a];
-        v64.anchor[a] = sh.anchor[a];
-        v64.cs[a] = sh.cs[a];
-        v64.inv_cs[a] = sh.inv_cs[a];
-      }
-      v64.nyz = sh.nyz;
+    v64.nH = s_n;
+    v64.xH = s_x;
+    v64.J = s_J;
+    for (int a = 0; a < 3; ++a) {
+      v64.n[a] = sh.n[a];
+      v64.anchor[a] = sh.anchor[a];
+      v64.cs[a] = sh.cs[a];
+      v64.inv_cs[a] = sh.inv_cs[a];
     }
-    Walk32<kComp> w32;
+    v64.nyz = sh.nyz;
     Walk64 w64;
     uint32_t wq_b = 0, wq_e = 0;
     bool exhausted = false, have = false, fresh = false;
@@ -793,14 +872,8 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
           const uint32_t take = min((uint32_t)__popc(idle), wq_e - wq_b);
           const uint32_t r = (uint32_t)__popc(idle & lt);
           if (!have && r < take) {
-            const uint32_t slot = begin + wq_b + r;
-            if (kF32) {
-              const Packet32 pk = load_packet(((const Packet32 *)prm.arena_in) + slot);
-              entry = w32.begin(pk, v32, sh.tab.sign_code);
-            } else {
-              const Packet64 pk = load_packet(((const Packet64 *)prm.arena_in) + slot);
-              entry = w64.begin(pk, v64, sh.tab.sign_code);
-            }
+            const Packet64 pk = load_packet(((const Packet64 *)prm.arena_in) + begin + wq_b + r);
+            entry = w64.begin(pk, v64, sh.tab.sign_code);
             have = true;
             fresh = true;
           }
@@ -818,9 +891,9 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
           fresh = false;
         }
         if (status == kRun) {
-          status = kF32 ? w32.step(v32) : w64.step(v64);
+          status = w64.step(v64);
           ++c_cross;
-          if (status == kRun && (kF32 ? w32.steps : w64.steps) > limit) status = kDrop;
+          if (status == kRun && w64.steps > limit) status = kDrop;
         }
       }
       const bool fin = have && status != kRun;
@@ -830,8 +903,7 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
         if (fin) {
           ++c_trans;
           if (status == kExited) {
-            const int mask = kF32 ? w32.exit_mask(v32) : w64.exit_mask(v64);
-            const int od = sh.tab.mask_dir[mask];
+            const int od = sh.tab.mask_dir[w64.exit_mask(v64)];
             if (od >= kNumDirections) {
               atomicOr(&st->flags, kFlagWalkLimit);
             } else {
@@ -845,22 +917,315 @@ __global__ void __launch_bounds__(kThreads) k_walk(WalkParams prm) {
             atomicOr(&st->flags, kFlagWalkLimit);
           }
         }
-        if (kF32) {
-          Packet32 rec{};
-          if (append) rec = w32.packet(meta);
-          warp_append(append, key, rec, (Packet32 *)prm.arena_out, prm.keys, prm.ranks,
-                      prm.hist, st, prm.capacity);
-        } else {
-          Packet64 rec{};
-          if (append) rec = w64.packet(v64, meta);
-          warp_append(append, key, rec, (Packet64 *)prm.arena_out, prm.keys, prm.ranks,
-                      prm.hist, st, prm.capacity);
-        }
+        Packet64 rec{};
+        if (append) rec = w64.packet(v64, meta);
+        warp_append(append, key, rec, (Packet64 *)prm.arena_out, prm.keys, prm.ranks, prm.hist,
+                    st, prm.capacity);
         if (fin) have = false;
       }
     }
     __syncthreads();
   }
+  if (staged != kNone) flush();
+}
+
+// FP32 wavefront round.
+//
+// Work distribution: the plan's chunks (<= CH packets, sorted by subgrid) are
+// claimed in runs of consecutive chunks (guided: shorter runs as the round
+// drains).  A run splits into segments of equal subgrid; per segment the CTA
+// stages the subgrid's kappa = sigma*n*x (TMA) unless it is already resident.
+//
+// Packet flow inside a segment: a two-slot shared-memory ring, each slot
+// filled with one chunk by a TMA bulk copy from the sorted arena.  Warps claim
+// exactly as many packets as they have idle lanes and copy them into
+// registers; the warp whose copy completes a slot issues the TMA of the chunk
+// after next into it.  Warps therefore flow across the chunks of a subgrid
+// without block-wide barriers; one barrier per segment remains (tally flush
+// and restaging happen there).
+//
+// Packets leaving the subgrid are staged per warp and appended 32 at a time
+// (one 1 KB coalesced store, one arena atomic, one bucket atomic per
+// destination).  Path lengths go to shared-memory tallies (Tally32), merged
+// into FP64 J in HBM when the CTA leaves the subgrid.
+constexpr int kStage = 64;  // staged output packets per warp
+
+template <int kThreads, int kTally>
+__global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Walk32Shared &sh = *reinterpret_cast<Walk32Shared *>(smem_raw);
+  constexpr int kWarps = kThreads / 32;
+  const int P = prm.max_padded;
+  const uint32_t CH = prm.chunk;
+  const uint32_t ch_shift = (uint32_t)(__ffs(CH) - 1);  // CH is a power of two
+  unsigned char *cur_ptr = smem_raw + ((sizeof(Walk32Shared) + 15) & ~(size_t)15);
+  float *s_kappa = reinterpret_cast<float *>(cur_ptr);
+  cur_ptr += (size_t)P * 4;
+  Tally32<kTally> tally;
+  tally.f_hi = tally.f_lo = nullptr;
+  tally.u_lo = tally.u_hi = nullptr;
+  tally.u64 = nullptr;
+  if (kTally == 3) {
+    cur_ptr = (unsigned char *)(((uintptr_t)cur_ptr + 15) & ~(uintptr_t)15);
+    tally.u64 = reinterpret_cast<unsigned long long *>(cur_ptr);
+    cur_ptr += (size_t)P * 8;
+  } else if (kTally == 2) {
+    tally.u_lo = reinterpret_cast<uint32_t *>(cur_ptr);
+    tally.u_hi = tally.u_lo + P;
+    cur_ptr += (size_t)P * 8;
+  } else {
+    tally.f_hi = reinterpret_cast<float *>(cur_ptr);
+    tally.f_lo = tally.f_hi + P;
+    cur_ptr += (size_t)P * (kTally == 1 ? 8 : 4);
+  }
+  Packet32 *s_pk = reinterpret_cast<Packet32 *>(cur_ptr);  // [2][CH]
+  cur_ptr += sizeof(Packet32) * 2 * (size_t)CH;
+  Packet32 *s_stage = reinterpret_cast<Packet32 *>(cur_ptr);  // [kWarps][kStage]
+  cur_ptr += sizeof(Packet32) * kWarps * kStage;
+  uint32_t *s_skey = reinterpret_cast<uint32_t *>(cur_ptr);  // [kWarps][kStage]
+
+  RoundState *st = prm.st;
+  const uint32_t nchunks = st->num_chunks;
+  if (nchunks == 0u) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  if (tid < (int)sizeof(DirectionTables) / 4) {
+    reinterpret_cast<uint32_t *>(&sh.tab)[tid] =
+        reinterpret_cast<const uint32_t *>(&prm.tables)[tid];
+  }
+  if (tid == 0) {
+    mbar_init(&sh.mbar_field, 1);
+    mbar_init(&sh.mbar_pk[0], 1);
+    mbar_init(&sh.mbar_pk[1], 1);
+    sh.uses[0] = sh.uses[1] = 0u;
+  }
+  for (int c = tid; c < P; c += kThreads) tally.zero(c);
+  __syncthreads();
+
+  // TMA of chunk k of the current segment into ring slot k & 1
+  auto issue = [&](uint32_t k) {
+    const uint32_t slot = k & 1u;
+    const uint32_t cnt = (k + 1u < sh.seg_chunks) ? CH : sh.seg_n - (k << ch_shift);
+    const uint32_t bytes = cnt * (uint32_t)sizeof(Packet32);
+    sh.uses[slot] += 1u;
+    fence_proxy_async();
+    mbar_expect_tx(&sh.mbar_pk[slot], bytes);
+    tma_load_1d(s_pk + (size_t)slot * CH,
+                ((const Packet32 *)prm.arena_in) + sh.seg_begin + (k << ch_shift), bytes,
+                &sh.mbar_pk[slot]);
+  };
+  // packets of chunk k copied out of the ring by this warp (lane 0): the copy
+  // that completes a chunk refills its slot with chunk k + 2
+  auto consumed = [&](uint32_t k, uint32_t n) {
+    const uint32_t slot = k & 1u;
+    const uint32_t cnt = (k + 1u < sh.seg_chunks) ? CH : sh.seg_n - (k << ch_shift);
+    __threadfence_block();
+    const uint32_t old = atomicAdd(&sh.loaded[slot], n);
+    if (old + n == cnt) {
+      __threadfence_block();
+      sh.loaded[slot] = 0u;
+      if (k + 2u < sh.seg_chunks) issue(k + 2u);
+    }
+  };
+  // wait until chunk k of the segment is in its slot (all lanes)
+  auto wait_chunk = [&](uint32_t k) {
+    const uint32_t slot = k & 1u;
+    const uint32_t use = sh.seg_use0[slot] + (k >> 1);  // this chunk is the use-th fill
+    mbar_wait_bounded(&sh.mbar_pk[slot], use & 1u, &st->flags);
+  };
+
+  uint32_t phase_field = 0;
+  uint32_t staged = kNone;
+  uint32_t c_cross = 0, c_trans = 0, c_abs = 0, c_esc = 0;
+  uint32_t nstage = 0;  // warp-uniform
+  Packet32 *my_stage = s_stage + warp * kStage;
+  uint32_t *my_skey = s_skey + warp * kStage;
+
+  auto flush = [&]() {
+    const int64_t off = sh.field_offset;
+    const double scale = (kTally >= 2) ? sh.tally_unit : 1.0;
+    for (int c = tid; c < sh.ncells; c += kThreads) {
+      const double v = tally.take(c, scale);
+      if (v != 0.) atomicAdd(&prm.J[off + c], v * sh.sigma);
+    }
+    flush_counters(prm.stats, sh.instance, c_cross, c_trans, c_abs, c_esc);
+  };
+
+  // append the first n staged packets of this warp, then move the rest down
+  auto flush_stage = [&](uint32_t n) {
+    __syncwarp();
+    const bool valid = (uint32_t)lane < n;
+    Packet32 rec{};
+    uint32_t key = 0;
+    if (valid) {
+      rec = my_stage[lane];
+      key = my_skey[lane];
+    }
+    warp_append(valid, key, rec, (Packet32 *)prm.arena_out, prm.keys, prm.ranks, prm.hist, st,
+                prm.capacity);
+    __syncwarp();
+    if ((uint32_t)lane + n < nstage) {
+      my_stage[lane] = my_stage[lane + n];
+      my_skey[lane] = my_skey[lane + n];
+    }
+    __syncwarp();
+    nstage -= n;
+  };
+
+  for (;;) {
+    if (tid == 0) {
+      // guided run length: about half of an even share of what is left
+      const uint32_t done = *(volatile uint32_t *)&st->chunk_next;
+      const uint32_t left = (nchunks > done) ? nchunks - done : 0u;
+      const uint32_t run = max(1u, min(64u, left / (2u * gridDim.x)));
+      const uint32_t c0 = atomicAdd(&st->chunk_next, run);
+      sh.run_c0 = c0;
+      sh.run_c1 = min(c0 + run, nchunks);
+    }
+    __syncthreads();
+    if (sh.run_c0 >= nchunks) break;
+    uint32_t a = sh.run_c0;
+    const uint32_t run_end = sh.run_c1;
+    while (a < run_end) {
+      if (tid == 0) {
+        const Chunk ca = prm.chunks[a];
+        const uint32_t b = min(run_end, a + ca.rem);
+        const Chunk cl = prm.chunks[b - 1u];
+        sh.seg_sub = ca.subgrid;
+        sh.seg_begin = ca.begin;
+        sh.seg_chunks = b - a;
+        sh.seg_n = ((b - 1u - a) << ch_shift) + cl.count;
+        sh.seg_next = b;
+      }
+      __syncthreads();
+      const uint32_t sub = sh.seg_sub;
+      const uint32_t nseg = sh.seg_n;
+      a = sh.seg_next;
+      if (sub != staged) {
+        if (staged != kNone) flush();
+        __syncthreads();
+        if (tid == 0) {
+          const DevSubgrid &S = prm.subs[sub];
+          load_subgrid32(sh, S, prm);
+          fence_proxy_async();
+          const uint32_t bytes = (uint32_t)S.padded_cells * 4u;
+          mbar_expect_tx(&sh.mbar_field, bytes);
+          tma_load_1d(s_kappa, prm.kappa + S.field_offset, bytes, &sh.mbar_field);
+        }
+        mbar_wait_bounded(&sh.mbar_field, phase_field, &st->flags);
+        phase_field ^= 1u;
+        staged = sub;
+      }
+      if (tid == 0) {
+        sh.claim = 0u;
+        sh.loaded[0] = sh.loaded[1] = 0u;
+        sh.seg_use0[0] = sh.uses[0];
+        sh.seg_use0[1] = sh.uses[1];
+        issue(0u);
+        if (sh.seg_chunks > 1u) issue(1u);
+      }
+      __syncthreads();
+
+      const int limit = sh.n[0] + sh.n[1] + sh.n[2] + 3;
+      View32 v;
+      v.kappa = s_kappa;
+      for (int ax = 0; ax < 3; ++ax) {
+        v.n[ax] = sh.n[ax];
+        v.cs[ax] = sh.cs_f[ax];
+        v.inv_cs[ax] = sh.inv_cs_f[ax];
+      }
+      v.nyz = sh.nyz;
+      tally.scale = sh.tally_scale;
+      Walk32 w;
+      bool exhausted = false, have = false, fresh = false;
+      int entry = kRun;
+      for (;;) {
+        const unsigned idle = __ballot_sync(kFull, !have);
+        if (idle != 0u && !exhausted) {
+          const uint32_t need = (uint32_t)__popc(idle);
+          uint32_t base = 0;
+          if (lane == 0) base = atomicAdd(&sh.claim, need);
+          base = __shfl_sync(kFull, base, 0);
+          if (base >= nseg) {
+            exhausted = true;
+          } else {
+            const uint32_t take = min(need, nseg - base);
+            const uint32_t k0 = base >> ch_shift, k1 = (base + take - 1u) >> ch_shift;
+            wait_chunk(k0);
+            if (k1 != k0) wait_chunk(k1);
+            const uint32_t r = (uint32_t)__popc(idle & lt);
+            if (!have && r < take) {
+              const uint32_t vi = base + r;
+              const uint32_t k = vi >> ch_shift;
+              const Packet32 pk = s_pk[(size_t)(k & 1u) * CH + (vi - (k << ch_shift))];
+              entry = w.begin(pk, v, sh.tab.sign_code);
+              have = true;
+              fresh = true;
+            }
+            __syncwarp();
+            if (lane == 0) {
+              const uint32_t n0 = min(take, ((k0 + 1u) << ch_shift) - base);
+              consumed(k0, n0);
+              if (take > n0) consumed(k1, take - n0);
+            }
+          }
+        }
+        if (!__any_sync(kFull, have)) {
+          if (exhausted) break;
+          continue;
+        }
+        int status = kRun;
+        if (have) {
+          if (fresh) {
+            status = entry;
+            fresh = false;
+          }
+          if (status == kRun) {
+            int tcell;
+            float len;
+            status = w.step(v, tcell, len);
+            tally.add(tcell, len);
+            ++c_cross;
+            if (status == kRun && w.steps > limit) status = kDrop;
+          }
+        }
+        const bool fin = have && status != kRun;
+        if (__any_sync(kFull, fin)) {
+          uint32_t key = kOutside, meta = 0;
+          bool append = false;
+          if (fin) {
+            ++c_trans;
+            if (status == kExited) {
+              const int od = sh.tab.mask_dir[w.exit_mask(v)];
+              if (od >= kNumDirections) {
+                atomicOr(&st->flags, kFlagWalkLimit);
+              } else {
+                key = sh.ngb[od];
+                meta = sh.tab.mirror[od];
+                if (key == kOutside) ++c_esc; else append = true;
+              }
+            } else if (status == kAbsorbed) {
+              ++c_abs;
+            } else {
+              atomicOr(&st->flags, kFlagWalkLimit);
+            }
+            have = false;
+          }
+          const unsigned am = __ballot_sync(kFull, append);
+          if (append) {
+            const uint32_t slot = nstage + (uint32_t)__popc(am & lt);
+            my_stage[slot] = w.packet(meta);
+            my_skey[slot] = key;
+          }
+          nstage += (uint32_t)__popc(am);
+          if (nstage >= 32u) flush_stage(32u);
+        }
+      }
+      __syncthreads();  // segment done: every packet of it is traced
+    }
+  }
+  if (nstage > 0u) flush_stage(nstage);
+  __syncthreads();
   if (staged != kNone) flush();
 }
 
@@ -1036,14 +1401,19 @@ __global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
   for (int a = 0; a < 3; ++a) {
     v32.n[a] = v64.n[a] = S.ncell[a];
     v32.cs[a] = S.cell_size_f[a];
+    v32.inv_cs[a] = (float)S.inv_cell_size[a];
     v64.anchor[a] = S.anchor[a];
     v64.cs[a] = S.cell_size[a];
     v64.inv_cs[a] = S.inv_cell_size[a];
   }
   v32.nyz = v64.nyz = S.ncell[1] * S.ncell[2];
   v32.kappa = s_kappa;
-  v32.tally_hi = s_hi;
-  v32.tally_lo = s_lo;
+  Tally32<1> tally32;
+  tally32.f_hi = s_hi;
+  tally32.f_lo = s_lo;
+  tally32.u_lo = tally32.u_hi = nullptr;
+  tally32.u64 = nullptr;
+  tally32.scale = 1.f;
   v64.nH = s_n;
   v64.xH = s_x;
   v64.J = s_J;
@@ -1063,12 +1433,13 @@ __global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
       }
       pk.tau = (float)ph.tau;
       pk.meta = ph.meta;
-      Walk32<true> w;
+      Walk32 w;
       status = w.begin(pk, v32, tab.sign_code);
       while (status == kRun) {
-        const int cell = w.cell;
+        int cell;
         float len;
-        status = w.step(v32, &len);
+        status = w.step(v32, cell, len);
+        tally32.add(cell, len);
         if (tracing && nsteps < prm.max_steps) {
           prm.trace_cells[nsteps] = cell;
           prm.trace_len[nsteps] = (double)len;
@@ -1078,7 +1449,7 @@ __global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
       }
       for (int a = 0; a < 3; ++a) ph.pos[a] = S.anchor[a] + (double)w.p[a] * S.cell_size[a];
       ph.tau = (double)__fsub_rn(w.tau_target, w.tau_done);
-      if (status == kExited) result = tab.mask_dir[w.exit_mask(v32)];
+      if (status == kExited) result = tab.mask_dir[w.exit_mask(v32, false)];
     } else {
       Walk64 w;
       status = w.begin(ph, v64, tab.sign_code);

@@ -8,8 +8,8 @@
 //    contracted and every result rounds exactly as on the host.
 //  * Walk32 -- FP32 in cell units: the position is kept relative to the
 //    subgrid in units of cells, so cell faces are exact small integers; path
-//    lengths stay in metres, l = (face - p) * (cell_size / d).  Tallies of
-//    path length go to compensated FP32 shared-memory accumulators.
+//    lengths stay in metres, l = (face - p) * (cell_size / d).  Path lengths
+//    go to shared-memory tallies (Tally32) merged into FP64 J.
 #pragma once
 
 #include "cmi_device.cuh"
@@ -26,11 +26,80 @@ __device__ __forceinline__ T min_ref(T a, T b) {  // std::min semantics
 // View of the staged subgrid in shared memory (FP32 mode).
 struct View32 {
   const float *kappa;  // sigma * n * x per cell (1/m)
-  float *tally_hi;     // path length sums (m)
-  float *tally_lo;     // their rounding errors (compensated mode)
   int n[3];
   int nyz;
-  float cs[3];
+  float cs[3];         // cell size (m)
+  float inv_cs[3];     // 1 / cell size, rounded from FP64
+};
+
+// Shared-memory path-length tallies of one staged subgrid.
+//  kTally 0: FP32 atomics
+//  kTally 1: FP32 atomics with the rounding error of each addition (TwoSum of
+//            the atomic's own old value) accumulated in a second FP32 array
+//  kTally 2: 64-bit fixed point (units of lref / 2^22) in two 32-bit words,
+//            low word by integer atomic add, carry counted in the high word
+//  kTally 3: 64-bit fixed point with 64-bit integer atomics
+// The fixed-point forms round len * 2^22 / lref (< 2^23 since len <= sqrt(3)
+// lref) half-to-even through the float adder: adding 2^23 leaves the
+// rounded integer in the mantissa bits, so no conversion instruction is used.
+template <int kTally>
+struct Tally32 {
+  float *f_hi, *f_lo;
+  uint32_t *u_lo, *u_hi;
+  unsigned long long *u64;
+  float scale;  // 2^22 / lref
+
+  static __device__ __forceinline__ uint32_t fixed(float len, float scale) {
+    const float q = fmaxf(__fmul_rn(len, scale), 0.f);
+    return __float_as_uint(__fadd_rn(q, 8388608.f)) - 0x4B000000u;
+  }
+
+  __device__ __forceinline__ void add(int cell, float len) const {
+    if (kTally == 0) {
+      atomicAdd(&f_hi[cell], len);
+    } else if (kTally == 1) {
+      const float old = atomicAdd(&f_hi[cell], len);
+      const float nw = __fadd_rn(old, len);
+      const float bv = __fsub_rn(nw, old);
+      const float err = __fadd_rn(__fsub_rn(old, __fsub_rn(nw, bv)), __fsub_rn(len, bv));
+      if (err != 0.f) atomicAdd(&f_lo[cell], err);
+    } else if (kTally == 2) {
+      const uint32_t v = fixed(len, scale);
+      const uint32_t old = atomicAdd(&u_lo[cell], v);
+      if (old + v < old) atomicAdd(&u_hi[cell], 1u);
+    } else {
+      atomicAdd(&u64[cell], (unsigned long long)fixed(len, scale));
+    }
+  }
+
+  // Sum of cell c in units of metres (lref / 2^22 for the fixed-point forms);
+  // resets the cell.
+  __device__ __forceinline__ double take(int c, double unit) const {
+    double v;
+    if (kTally == 0) {
+      v = (double)f_hi[c];
+      f_hi[c] = 0.f;
+    } else if (kTally == 1) {
+      v = (double)f_hi[c] + (double)f_lo[c];
+      f_hi[c] = 0.f;
+      f_lo[c] = 0.f;
+    } else if (kTally == 2) {
+      v = (double)(((unsigned long long)u_hi[c] << 32) | u_lo[c]) * unit;
+      u_lo[c] = 0u;
+      u_hi[c] = 0u;
+    } else {
+      v = (double)u64[c] * unit;
+      u64[c] = 0ull;
+    }
+    return v;
+  }
+
+  __device__ __forceinline__ void zero(int c) const {
+    if (kTally == 0) f_hi[c] = 0.f;
+    else if (kTally == 1) { f_hi[c] = 0.f; f_lo[c] = 0.f; }
+    else if (kTally == 2) { u_lo[c] = 0u; u_hi[c] = 0u; }
+    else u64[c] = 0ull;
+  }
 };
 
 // View of the staged subgrid in shared memory (FP64 mode).
@@ -48,15 +117,17 @@ struct View64 {
 // ----------------------------------------------------------------------------
 // FP32 cell-unit walk
 // ----------------------------------------------------------------------------
-template <bool kCompensated>
 struct Walk32 {
   float p[3], d[3], inv[3], dcs[3];
   float tau_done, tau_target;
+  float fidx[3];  // idx as float (exact): the cell faces without conversions
   int idx[3];
   int cell;
   int steps;
 
   // Entry: DensitySubGrid.hpp:1186-1219 (start index per get_start_index).
+  // inv = cell_size * (1/d) and dcs = d * (1/cell_size): correctly rounded
+  // reciprocals and products, no divisions.
   __device__ __forceinline__ int begin(const Packet32 &pk, const View32 &v,
                                       const uint8_t *sign_code) {
     const uint8_t code = sign_code[pk.meta & 31u];
@@ -64,10 +135,11 @@ struct Walk32 {
     for (int a = 0; a < 3; ++a) {
       p[a] = pk.pos[a];
       d[a] = pk.dir[a];
-      dcs[a] = __fdiv_rn(d[a], v.cs[a]);
-      inv[a] = __fdiv_rn(v.cs[a], d[a]);
+      dcs[a] = __fmul_rn(d[a], v.inv_cs[a]);
+      inv[a] = __fmul_rn(v.cs[a], __frcp_rn(d[a]));
       const int s = sign_of(code, a);
       idx[a] = (s == 0) ? __float2int_rz(p[a]) : ((s < 0) ? 0 : v.n[a] - 1);
+      fidx[a] = (float)idx[a];
     }
     cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
     tau_done = 0.f;
@@ -82,32 +154,21 @@ struct Walk32 {
            idx[2] < v.n[2] && idx[2] >= 0;
   }
 
-  __device__ __forceinline__ void tally(const View32 &v, float len) const {
-    if (kCompensated) {
-      // TwoSum of the atomic's own addition: old + len = nw + err exactly.
-      const float old = atomicAdd(&v.tally_hi[cell], len);
-      const float nw = __fadd_rn(old, len);
-      const float bv = __fsub_rn(nw, old);
-      const float err = __fadd_rn(__fsub_rn(old, __fsub_rn(nw, bv)), __fsub_rn(len, bv));
-      if (err != 0.f) atomicAdd(&v.tally_lo[cell], err);
-    } else {
-      atomicAdd(&v.tally_hi[cell], len);
-    }
-  }
-
-  // One iteration of the loop at DensitySubGrid.hpp:1221-1305.
-  __device__ __forceinline__ int step(const View32 &v, float *trace_len = nullptr) {
+  // One iteration of the loop at DensitySubGrid.hpp:1221-1305; the path
+  // length lmin of the crossed cell `tally_cell` is returned for the tally.
+  __device__ __forceinline__ int step(const View32 &v, int &tally_cell, float &lmin_out) {
     float lo[3], hi[3], l[3];
+    const float k = v.kappa[cell];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      lo[a] = __int2float_rn(idx[a]);
-      hi[a] = __int2float_rn(idx[a] + 1);
+      lo[a] = fidx[a];
+      hi[a] = __fadd_rn(fidx[a], 1.f);
       l[a] = (d[a] > 0.f)   ? __fmul_rn(__fsub_rn(hi[a], p[a]), inv[a])
              : (d[a] < 0.f) ? __fmul_rn(__fsub_rn(lo[a], p[a]), inv[a])
                             : FLT_MAX;
     }
     float lmin = min_ref(l[0], min_ref(l[1], l[2]));
-    const float tau = __fmul_rn(lmin, v.kappa[cell]);
+    const float tau = __fmul_rn(lmin, k);
     tau_done = __fadd_rn(tau_done, tau);
     const bool absorbed = tau_done >= tau_target;
     if (absorbed) {
@@ -116,11 +177,14 @@ struct Walk32 {
     } else {
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        if (l[a] == lmin) idx[a] += (d[a] > 0.f) ? 1 : -1;
+        if (l[a] == lmin) {
+          idx[a] += (d[a] > 0.f) ? 1 : -1;
+          fidx[a] = (d[a] > 0.f) ? hi[a] : __fsub_rn(lo[a], 1.f);
+        }
       }
     }
-    if (trace_len) *trace_len = lmin;
-    tally(v, lmin);
+    tally_cell = cell;
+    lmin_out = lmin;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       p[a] = (l[a] == lmin) ? ((d[a] > 0.f) ? hi[a] : lo[a]) : __fmaf_rn(lmin, dcs[a], p[a]);
@@ -132,19 +196,23 @@ struct Walk32 {
     return kRun;
   }
 
-  // Exit: 6-bit mask (DensitySubGrid.hpp:483-506) and the position moved into
-  // the neighbour's cell frame (exact: the exit coordinate is 0 or n).
-  __device__ __forceinline__ int exit_mask(const View32 &v) {
+  // Exit: 6-bit mask (DensitySubGrid.hpp:483-506).  With reanchor the
+  // position moves into the neighbour's cell frame (exact: the exit
+  // coordinate is 0 or n).
+  __device__ __forceinline__ int exit_mask(const View32 &v, bool reanchor = true) {
     int mask = 0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+      // (idx / n) > 0 of the reference; idx is in [-1, n] here
       const int low = idx[a] < 0;
-      const int high = (idx[a] / v.n[a]) > 0;
+      const int high = idx[a] >= v.n[a];
       mask |= (high << (5 - 2 * a)) | (low << (4 - 2 * a));
-      if (high) {
-        p[a] = __fsub_rn(p[a], __int2float_rn(v.n[a]));
-      } else if (low) {
-        p[a] = __fadd_rn(p[a], __int2float_rn(v.n[a]));
+      if (reanchor) {
+        if (high) {
+          p[a] = __fsub_rn(p[a], __int2float_rn(v.n[a]));
+        } else if (low) {
+          p[a] = __fadd_rn(p[a], __int2float_rn(v.n[a]));
+        }
       }
     }
     return mask;
@@ -170,6 +238,7 @@ struct Walk32 {
 struct Walk64 {
   double pos[3], d[3], inv[3];
   double tau_done, tau_target, sigma, weight;
+  double didx[3];  // idx as double (exact): idx * cs and (idx + 1.) * cs without conversions
   int idx[3];
   int cell;
   int steps;
@@ -186,6 +255,7 @@ struct Walk64 {
       pos[a] = pk.pos[a] - v.anchor[a];
       const int s = sign_of(code, a);
       idx[a] = (s == 0) ? __double2int_rz(pos[a] * v.inv_cs[a]) : ((s < 0) ? 0 : v.n[a] - 1);
+      didx[a] = (double)idx[a];
     }
     cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
     tau_done = 0.;
@@ -208,8 +278,8 @@ struct Walk64 {
     double lo[3], hi[3], l[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      lo[a] = idx[a] * v.cs[a];
-      hi[a] = (idx[a] + 1.) * v.cs[a];
+      lo[a] = didx[a] * v.cs[a];
+      hi[a] = (didx[a] + 1.) * v.cs[a];
       l[a] = (d[a] > 0.)   ? (hi[a] - pos[a]) * inv[a]
              : (d[a] < 0.) ? (lo[a] - pos[a]) * inv[a]
                            : DBL_MAX;
@@ -226,7 +296,10 @@ struct Walk64 {
     } else {
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        if (l[a] == lmin) idx[a] += (d[a] > 0.) ? 1 : -1;
+        if (l[a] == lmin) {
+          idx[a] += (d[a] > 0.) ? 1 : -1;
+          didx[a] += (d[a] > 0.) ? 1. : -1.;
+        }
       }
     }
     if (trace_len) *trace_len = lmin;

@@ -1,0 +1,114 @@
+// Stromgren-sphere driver on the GPU path, with the command line and
+// params.txt of the reference's OpenMP driver (testDensitySubGrid_omp.cpp):
+//
+//   stromgren_driver -t THREADS -p params.txt
+//
+// THREADS only seeds the host generator the way the reference does
+// (random_generator[0] seeded 42 + THREADS, testDensitySubGrid_omp.cpp:1786-1790),
+// so a random density field and random sources come out identical to a
+// reference run with the same -t.  The transport and balance run on the GPU.
+// Output: neutral_fractions.bin, the neutral fraction of every cell, subgrid
+// after subgrid (output_neutral_fractions_binary, testDensitySubGrid_omp.cpp:507-521).
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "cmacionize/DensityGrid.hpp"
+#include "cmacionize/Parameters.hpp"
+#include "cmacionize/RandomGenerator.hpp"
+
+int main(int argc, char **argv) {
+  int threads = 1;
+  std::string params_file;
+  for (int i = 1; i < argc; ++i) {
+    const std::string a = argv[i];
+    if ((a == "-t" || a == "--threads") && i + 1 < argc) threads = std::atoi(argv[++i]);
+    else if ((a == "-p" || a == "--params") && i + 1 < argc) params_file = argv[++i];
+  }
+  if (params_file.empty()) {
+    std::fprintf(stderr, "usage: %s -t THREADS -p PARAMS\n", argv[0]);
+    return 2;
+  }
+  try {
+    const PlainMethodParameters p(Parameters::from_file(params_file));
+    if (p.reemission_probability != 0.) {
+      std::fprintf(stderr, "reemission_probability > 0 is not supported by this driver\n");
+      return 2;
+    }
+    DensityGrid grid(p.box, p.ncell, p.num_subgrid);
+    RandomGenerator rng(42 + threads);
+
+    if (p.random_density) {
+      // 10-mode cosine field, testDensitySubGrid_omp.cpp:1881-1936
+      const unsigned int nk = 10;
+      std::vector<double> k(3 * nk), phase(3 * nk);
+      for (unsigned int i = 0; i < nk; ++i) {
+        double u[4];
+        for (double &x : u) x = rng.get_uniform_random_double();
+        const double kx = std::sqrt(-2. * std::log(u[0])) * std::cos(2. * M_PI * u[1]);
+        const double ky = std::sqrt(-2. * std::log(u[0])) * std::sin(2. * M_PI * u[1]);
+        const double kz = std::sqrt(-2. * std::log(u[2])) * std::cos(2. * M_PI * u[3]);
+        k[3 * i] = 4. * M_PI * kx / p.box[3];
+        k[3 * i + 1] = 4. * M_PI * ky / p.box[4];
+        k[3 * i + 2] = 4. * M_PI * kz / p.box[5];
+        for (int a = 0; a < 3; ++a) phase[3 * i + a] = 2. * M_PI * rng.get_uniform_random_double();
+      }
+      for (unsigned int s = 0; s < grid.number_of_subgrids(); ++s) {
+        DensitySubGrid sg = grid.subgrid(s);
+        double box[6];
+        sg.get_grid_box(box);
+        const int *n = grid.subgrid_cells();
+        for (unsigned int c = 0; c < sg.get_number_of_cells(); ++c) {
+          const int i3[3] = {(int)(c / (n[1] * n[2])), (int)((c / n[2]) % n[1]), (int)(c % n[2])};
+          double mid[3];
+          for (int a = 0; a < 3; ++a) mid[a] = box[a] + (i3[a] + 0.5) * (box[3 + a] / n[a]);
+          double nd = 0.;
+          for (unsigned int q = 0; q < nk; ++q) {
+            nd += 1.e8 * (std::cos(k[3 * q] * mid[0] + phase[3 * q]) *
+                              std::cos(k[3 * q + 1] * mid[1] + phase[3 * q + 1]) *
+                              std::cos(k[3 * q + 2] * mid[2] + phase[3 * q + 2]) +
+                          1.);
+          }
+          sg.set_number_density(c, nd / nk);
+        }
+      }
+    }
+
+    // sources, testDensitySubGrid_omp.cpp:1944-2016
+    std::vector<Source> sources;
+    if (p.number_of_sources > 1) {
+      for (unsigned int i = 0; i < p.number_of_sources; ++i) {
+        double pos[3];
+        for (int a = 0; a < 3; ++a) pos[a] = p.box[a] + rng.get_uniform_random_double() * p.box[3 + a];
+        sources.emplace_back(pos, 4.26e48);
+      }
+    } else {
+      const double origin[3] = {0., 0., 0.};
+      sources.emplace_back(origin, 4.26e49);
+    }
+    grid.set_sources(sources);
+    grid.set_num_photon(p.num_photon);
+
+    const auto t0 = std::chrono::steady_clock::now();
+    const std::vector<cmi_stats> st = grid.run_iterations((int)p.number_of_iterations, 42);
+    const double mc = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    unsigned long long crossings = 0;
+    for (const cmi_stats &s : st) crossings += s.cell_crossings;
+    std::fprintf(stderr, "Total Monte Carlo time: %g s.\n", mc);
+    std::fprintf(stderr, "Cell crossings: %llu (%.4g per second)\n", crossings, crossings / mc);
+
+    const double *x = grid.neutral_fractions();
+    std::ofstream out("neutral_fractions.bin", std::ios::binary);
+    out.write(reinterpret_cast<const char *>(x),
+              sizeof(double) * grid.cells_per_subgrid() * grid.number_of_subgrids());
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "error: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}

@@ -35,6 +35,10 @@ TRAVEL_DIRECTIONS = [
 ]
 TravelDirection = {name: i for i, name in enumerate(TRAVEL_DIRECTIONS)}
 
+# shared-memory path-length tallies of the FP32 transport (cmi_tally)
+TALLY_MODES = {"fp32": _lib.TALLY_FP32, "fp32_compensated": _lib.TALLY_FP32_COMPENSATED,
+               "fixed64": _lib.TALLY_FIXED64, "fixed64_atomic64": _lib.TALLY_FIXED64_ATOMIC64}
+
 
 @dataclass
 class GridSpec:
@@ -87,7 +91,7 @@ class TransportEngine:
     """A library context holding one or more grid instances on one GPU."""
 
     def __init__(self, grids, precision="fp32", balance="stable", rng="philox", device=0,
-                 packets_per_chunk=0, compensated_tally=True, use_graph=True, ctas_per_sm=0):
+                 packets_per_chunk=0, tally="fixed64", use_graph=True, ctas_per_sm=0):
         if isinstance(grids, GridSpec):
             grids = [grids]
         self.grids = list(grids)
@@ -97,7 +101,7 @@ class TransportEngine:
             balance_form={"reference": _lib.BALANCE_REFERENCE, "stable": _lib.BALANCE_STABLE}[balance],
             rng={"philox": _lib.RNG_PHILOX, "ranlux": _lib.RNG_RANLUX}[rng],
             device=device, packets_per_chunk=packets_per_chunk,
-            compensated_tally=int(bool(compensated_tally)), use_graph=int(bool(use_graph)),
+            tally_mode=TALLY_MODES[tally], use_graph=int(bool(use_graph)),
             ctas_per_sm=ctas_per_sm)
         descs = (_lib.GridDesc * len(self.grids))(*[g.desc() for g in self.grids])
         h = C.c_void_p()

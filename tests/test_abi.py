@@ -33,7 +33,7 @@ def test_default_options():
     o = _lib.default_options()
     assert o.transport_precision == _lib.TRANSPORT_FP32
     assert o.balance_form == _lib.BALANCE_STABLE
-    assert o.compensated_tally == 1 and o.use_graph == 1
+    assert o.tally_mode == _lib.TALLY_FIXED64 and o.use_graph == 1
     with pytest.raises(TypeError):
         _lib.default_options(no_such_option=1)
 

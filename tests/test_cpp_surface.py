@@ -1,0 +1,91 @@
+"""The C++ host surface (include/cmacionize/*.hpp) over the C ABI."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+DRIVER = os.path.join(ROOT, "parallelcmacionize_b200", "stromgren_driver")
+
+PARAMS = """## Physical parameters
+box:
+  anchor: [-5. pc, -5. pc, -5. pc]
+  sides: [10. pc, 10. pc, 10. pc]
+ncell: [{n}, {n}, {n}]
+num_photon: {photons}
+number_of_iterations: {iters}
+reemission_probability: 0.
+number_of_sources: 1
+random_density: false
+## Algorithm parameters
+num_subgrid: [{s}, {s}, {s}]
+queue_size_per_thread: 100
+memoryspace_size: 50000
+number_of_tasks: 500000
+MPI_buffer_size: 1000
+cost_copy_factor: 10
+edge_copy_factor: 0.01
+general_queue_size: 100000
+"""
+
+
+def test_headers_compile_against_the_abi(tmp_path):
+    src = tmp_path / "t.cpp"
+    src.write_text(
+        '#include "cmacionize/DensityGrid.hpp"\n#include "cmacionize/Parameters.hpp"\n'
+        '#include <cassert>\n#include <sstream>\n'
+        "int main() {\n"
+        "  assert(TravelDirections::output_to_input_direction(TRAVELDIRECTION_CORNER_PPN)"
+        " == TRAVELDIRECTION_CORNER_NNP);\n"
+        "  assert(TravelDirections::get_output_direction(9) == TRAVELDIRECTION_EDGE_X_PN);\n"
+        "  RandomGenerator r(42); double u = r.get_uniform_random_double(); assert(u >= 0 && u < 1);\n"
+        '  std::istringstream s("box:\\n  anchor: [0 pc, 0 pc, 0 pc]\\n");\n'
+        "  Parameters p(s); double a[3]; p.get_physical_vector(\"box:anchor\", a);\n"
+        "  PhotonBuffer b; b.grow(3); assert(b.size() == 3);\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "t"
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe)], check=True)
+    subprocess.run([str(exe)], check=True)
+
+
+def test_ranlxd_header_matches_reference_stream(tmp_path):
+    """The shared ranlxd header (host + device) reproduces RandomGenerator."""
+    from conftest import golden
+    g = golden("rng.npz")
+    src = tmp_path / "r.cpp"
+    src.write_text('#include "cmacionize/RandomGenerator.hpp"\n#include <cstdio>\n#include <cstdlib>\n'
+                   "int main(int c, char **v) { RandomGenerator r(atoi(v[1]));\n"
+                   "  for (int i = 0; i < 2500; ++i) printf(\"%a\\n\", r.get_uniform_random_double()); }\n")
+    exe = tmp_path / "r"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-o", str(exe)], check=True)
+    for seed, ref in zip(g["seeds"], g["streams"]):
+        out = subprocess.run([str(exe), str(int(seed))], check=True, capture_output=True,
+                             text=True).stdout.split()
+        assert np.array_equal(np.array([float.fromhex(x) for x in out]), ref)
+
+
+@pytest.mark.gpu
+def test_stromgren_driver_runs(tmp_path):
+    """The reference's command line and params.txt, on the GPU path."""
+    if not os.path.exists(DRIVER):
+        pytest.fail("stromgren_driver not built (make -C parallelcmacionize_b200/csrc)")
+    p = tmp_path / "params.txt"
+    p.write_text(PARAMS.format(n=32, s=4, photons=200000, iters=6))
+    r = subprocess.run([DRIVER, "-t", "1", "-p", str(p)], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "Total Monte Carlo time" in r.stderr
+    x = np.fromfile(tmp_path / "neutral_fractions.bin", dtype=np.float64)
+    assert x.size == 32 ** 3
+    assert np.all((x > 0) & (x <= 1))
+    from parallelcmacionize_b200.engine import blocked_to_cube
+    from parallelcmacionize_b200.problems import GridSpec, ionized_radius, stromgren_profile
+    spec = GridSpec(box=(-5 * 3.086e16,) * 3 + (10 * 3.086e16,) * 3, ncell=(32,) * 3,
+                    num_subgrid=(4,) * 3)
+    R = ionized_radius(blocked_to_cube(x, spec.ncell, spec.num_subgrid), spec)
+    _, _, Rs = stromgren_profile()
+    assert abs(R / Rs - 1) < 0.05  # coarse 32^3 grid

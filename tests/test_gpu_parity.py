@@ -106,7 +106,8 @@ def test_trace_fp32_matches_cpu_spec(case):
         q["pos"] = (ph["position"] - g["box"][:3]) * np.array(sg.inv_cell_size)
         q["dir"] = ph["direction"]
         q["tau"] = ph["tau"]
-        ores, ocells, olen, on = O.interact32(g["ncell"], cs, kappa, None, q, max_steps=4096)
+        ores, ocells, olen, on = O.interact32(g["ncell"], cs, kappa, None, q, max_steps=4096,
+                                              inv_cell_size=np.array(sg.inv_cell_size))
         assert res == ores and n == on
         assert np.array_equal(cells, ocells)
         assert np.array_equal(lengths.astype(np.float32), olen)
@@ -149,15 +150,28 @@ def test_transport_packets_fp32_matches_cpu_spec():
     q["dir"] = g["photons"]["direction"]
     q["tau"] = g["photons"]["tau"]
     tally = np.zeros(g["nH"].size)
-    cnt = lat.transport32(kappa, tally, q, g["start"])
+    fixed = np.zeros(g["nH"].size, np.uint64)
+    cnt = lat.transport32(kappa, tally, q.copy(), g["start"], fixed=fixed)
     assert st["packets_absorbed"] == cnt["absorbed"]
     assert st["packets_escaped"] == cnt["escaped"]
     assert st["cell_crossings"] == cnt["crossings"]
     _, J = eng.get_fields(0)
-    # compensated FP32 shared-memory sums merged into FP64
-    np.testing.assert_allclose(J, tally * 6.3e-22, rtol=1e-9, atol=0)
+    # default tally: exact 64-bit fixed-point sums, merged into FP64 once per
+    # subgrid residency -> equal to the oracle's integer sums to FP64 rounding
+    np.testing.assert_allclose(J, fixed.astype(np.float64) * lat.fixed_unit() * 6.3e-22,
+                               rtol=1e-12, atol=0)
+    # the fixed-point rounding: at most half a unit (lref / 2^25) per crossing
+    half_unit = 0.5 * lat.fixed_unit() * 6.3e-22
+    assert np.all(np.abs(J - tally * 6.3e-22) <= 1e-9 * np.abs(J) + 100 * half_unit)
     # and against the FP64 reference
     np.testing.assert_allclose(J.sum(), g["J"].sum(), rtol=1e-4)
+    eng.close()
+    # the compensated-FP32 tally variant: FP32 partials + their TwoSum errors
+    eng = TransportEngine(spec, precision="fp32", tally="fp32_compensated")
+    eng.set_fields(0, g["nH"], g["xH"])
+    eng.transport_packets(0, g["photons"], g["start"])
+    _, Jc = eng.get_fields(0)
+    np.testing.assert_allclose(Jc, tally * 6.3e-22, rtol=1e-9, atol=0)
     eng.close()
 
 

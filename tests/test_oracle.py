@@ -223,7 +223,8 @@ def test_fp32_walk_tracks_fp64(oracle_mod):
         q["pos"] = ((g["photons"]["position"][i] - g["box"][:3]) * np.array(sg.inv_cell_size))
         q["dir"] = g["photons"]["direction"][i]
         q["tau"] = g["photons"]["tau"][i]
-        _, cells32, len32, _ = O.interact32(g["ncell"], cs, kappa, None, q, max_steps=4096)
+        _, cells32, len32, _ = O.interact32(g["ncell"], cs, kappa, None, q, max_steps=4096,
+                                            inv_cell_size=np.array(sg.inv_cell_size))
         if np.array_equal(cells32, cells64):
             same_seq += 1
             # FP32 positions in cell units of a 16-cell subgrid: absolute error
