@@ -234,6 +234,40 @@ int cmi_set_kernel_timing(cmi_context *context, int32_t enable);
 int cmi_kernel_timing(cmi_context *context, double milliseconds[CMI_KERNEL_CLASSES],
                       uint64_t launches[CMI_KERNEL_CLASSES]);
 
+/* Allocation-free variant of cmi_traverse_buffer.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory, e.g.
+ * a host code whose GPU memory is owned by its own pool allocator, or a
+ * plug-in running inside another application's process, where a cudaMalloc
+ * or cudaFree would synchronize the whole device, fragment the host's pool or
+ * fail outright.  It needs no context: the caller passes the subgrid (box,
+ * cells, FP64 fields in DensitySubGrid cell order) and every input and output
+ * as device pointers; the library allocates nothing.  The walk's intermediate
+ * photons live in one fixed array in device global memory, the same for every
+ * call, sized for CMI_NOALLOC_MAX_PHOTONS photons (about 340 KiB, held by
+ * every GPU that loads the library until the process exits).
+ *
+ *   box, ncell        subgrid box (anchor, sides; m) and cells per axis
+ *                     (at most 4096 cells)
+ *   d_nH, d_xH, d_J   device fields; J receives the tallies (accumulated)
+ *   d_in, n           device photons, n <= CMI_NOALLOC_MAX_PHOTONS
+ *   output_enabled    host flags of the 27 output buffers (NULL: all)
+ *   d_out             device output, n photons, grouped by exit direction
+ *   d_out_count       device array of 27 group sizes
+ *   d_num_done        device counter of the photons in disabled groups
+ *   stream            cudaStream_t to run on (NULL: the default stream)
+ *
+ * Runs the reference FP64 walk on the calling thread's current device and
+ * returns when the stream has finished it.  The first call on a device looks
+ * up the array's device address (once per device), so make the first call
+ * before any stream capture.  Calls that overlap on the GPU (other host
+ * threads, other streams) share the array and race: serialise them. */
+#define CMI_NOALLOC_MAX_PHOTONS 4096
+int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
+                                const double *d_nH, const double *d_xH, double *d_J,
+                                int32_t input_direction, const cmi_photon *d_in, uint32_t n,
+                                const uint8_t *output_enabled, cmi_photon *d_out,
+                                uint32_t *d_out_count, uint32_t *d_num_done, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

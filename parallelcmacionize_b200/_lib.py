@@ -49,7 +49,7 @@ EXPORTED = [
     "cmi_transport_packets", "cmi_traverse_buffer", "cmi_trace_packet",
     "cmi_compute_neutral_fraction", "cmi_device_field", "cmi_get_stream", "cmi_synchronize",
     "cmi_last_launch_count", "cmi_set_kernel_timing", "cmi_kernel_timing",
-    "cmi_compute_neutral_fraction_subgrids",
+    "cmi_compute_neutral_fraction_subgrids", "cmi_traverse_buffer_noalloc",
 ]
 
 PHOTON_DTYPE = np.dtype(

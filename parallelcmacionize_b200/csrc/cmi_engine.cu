@@ -10,6 +10,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1246,3 +1247,206 @@ int cmi_last_launch_count(cmi_context *c, uint64_t *launches) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free buffer traversal (cmi_traverse_buffer_noalloc)
+// ===========================================================================
+namespace {
+
+// Layout of the fixed device array: walked photons, their exit directions,
+// the 27 output flags and an error word.
+constexpr size_t kNoAllocPhotonBytes = sizeof(Packet64) * CMI_NOALLOC_MAX_PHOTONS;
+constexpr size_t kNoAllocDirOffset = kNoAllocPhotonBytes;
+constexpr size_t kNoAllocFlagsOffset = kNoAllocDirOffset + sizeof(int32_t) * CMI_NOALLOC_MAX_PHOTONS;
+constexpr size_t kNoAllocErrOffset = kNoAllocFlagsOffset + 32;
+constexpr size_t kNoAllocBytes = kNoAllocErrOffset + 256;
+
+}  // namespace
+
+// The one scratch array of the allocation-free entry point.  In host code
+// this name is only a handle: its device address comes from
+// cudaGetSymbolAddress (see noalloc_scratch below).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+constexpr int kNoAllocMaxDevices = 64;
+unsigned char *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device with that device current.
+int noalloc_scratch(unsigned char **out) {
+  int dev = -1;
+  CMI_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(CMI_ERR_NOT_SUPPORTED, "device %d beyond the supported %d", dev,
+                kNoAllocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(CMI_ERR_CUDA, "cudaGetSymbolAddress of the traversal scratch failed: %s",
+                  cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return CMI_OK;
+}
+
+struct NoAllocParams {
+  DevSubgrid sub;  // geometry by value: no device-side subgrid table
+  uint8_t enabled[32];
+  uint8_t *enabled_out;  // flags for k_partition, written by block 0
+  int32_t input_direction;
+  const Packet64 *in;
+  uint32_t n;
+  const double *nH, *xH;
+  double *J;
+  Packet64 *walked;
+  int32_t *dir;
+  uint32_t *err;
+  DirectionTables tables;
+};
+
+// The reference FP64 walk of every photon through one subgrid (one photon
+// per thread), fields staged in shared memory, tallies flushed to J.
+__global__ void __launch_bounds__(256) k_traverse_noalloc(NoAllocParams prm) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ DirectionTables tab;
+  const DevSubgrid &S = prm.sub;
+  const int P = S.padded_cells;
+  double *s_n = reinterpret_cast<double *>(smem_raw);
+  double *s_x = s_n + P;
+  double *s_J = s_x + P;
+  if (threadIdx.x < sizeof(DirectionTables) / 4) {
+    reinterpret_cast<uint32_t *>(&tab)[threadIdx.x] =
+        reinterpret_cast<const uint32_t *>(&prm.tables)[threadIdx.x];
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 32) prm.enabled_out[threadIdx.x] = prm.enabled[threadIdx.x];
+  for (int c = threadIdx.x; c < S.ncells; c += blockDim.x) {
+    s_n[c] = prm.nH[c];
+    s_x[c] = prm.xH[c];
+    s_J[c] = 0.;
+  }
+  __syncthreads();
+  View64 v;
+  for (int a = 0; a < 3; ++a) {
+    v.n[a] = S.ncell[a];
+    v.anchor[a] = S.anchor[a];
+    v.cs[a] = S.cell_size[a];
+    v.inv_cs[a] = S.inv_cell_size[a];
+  }
+  v.nyz = S.ncell[1] * S.ncell[2];
+  v.nH = s_n;
+  v.xH = s_x;
+  v.J = s_J;
+  const int limit = S.ncell[0] + S.ncell[1] + S.ncell[2] + 3;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < prm.n) {
+    Packet64 ph = prm.in[i];
+    ph.meta = (uint32_t)prm.input_direction;
+    Walk64 w;
+    int status = w.begin(ph, v, tab.sign_code);
+    while (status == kRun) {
+      status = w.step(v);
+      if (status == kRun && w.steps > limit) status = kDrop;
+    }
+    int result = kInside;
+    ph = w.packet(v, 0u);
+    if (status == kExited) result = tab.mask_dir[w.exit_mask(v)];
+    if (status == kDrop || result >= kNumDirections) {
+      atomicOr(prm.err, kFlagWalkLimit);
+      result = kInside;
+    }
+    ph.meta = 0u;
+    prm.walked[i] = ph;
+    prm.dir[i] = result;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < S.ncells; c += blockDim.x) {
+    if (s_J[c] != 0.) atomicAdd(&prm.J[c], s_J[c]);
+  }
+}
+
+}  // namespace
+
+extern "C" int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
+                                           const double *d_nH, const double *d_xH, double *d_J,
+                                           int32_t input_direction, const cmi_photon *d_in,
+                                           uint32_t n, const uint8_t *output_enabled,
+                                           cmi_photon *d_out, uint32_t *d_out_count,
+                                           uint32_t *d_num_done, void *stream) {
+  if (!box || !ncell || !d_nH || !d_xH || !d_J || !d_out_count || !d_num_done)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  if (n > 0 && (!d_in || !d_out)) return fail(CMI_ERR_INVALID_ARGUMENT, "null photon buffer");
+  if (n > CMI_NOALLOC_MAX_PHOTONS)
+    return fail(CMI_ERR_CAPACITY,
+                "%u photons exceed the allocation-free scratch of %d photons; split the "
+                "buffer or use cmi_traverse_buffer",
+                n, CMI_NOALLOC_MAX_PHOTONS);
+  if (input_direction < 0 || input_direction >= kNumDirections)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "input direction %d out of range", input_direction);
+  DevSubgrid S{};
+  int64_t cells = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (ncell[a] <= 0 || !(box[3 + a] > 0.))
+      return fail(CMI_ERR_INVALID_ARGUMENT, "cells and box sides must be positive");
+    cells *= ncell[a];
+    // DensitySubGrid(box, ncell), DensitySubGrid.hpp:516-527
+    S.anchor[a] = box[a];
+    S.cell_size[a] = box[3 + a] / ncell[a];
+    S.inv_cell_size[a] = ncell[a] / box[3 + a];
+    S.cell_size_f[a] = (float)S.cell_size[a];
+    S.ncell[a] = ncell[a];
+  }
+  if (cells > 4096)
+    return fail(CMI_ERR_NOT_SUPPORTED, "%lld cells per subgrid exceed 4096",
+                (long long)cells);
+  S.ncells = (int32_t)cells;
+  S.padded_cells = (S.ncells + 3) & ~3;
+  for (int d = 0; d < kNumDirections; ++d) S.ngb[d] = kOutside;
+
+  unsigned char *scratch = nullptr;
+  CMI_TRY(noalloc_scratch(&scratch));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Packet64 *walked = reinterpret_cast<Packet64 *>(scratch);
+  int32_t *dir = reinterpret_cast<int32_t *>(scratch + kNoAllocDirOffset);
+  uint8_t *flags = scratch + kNoAllocFlagsOffset;
+  uint32_t *err = reinterpret_cast<uint32_t *>(scratch + kNoAllocErrOffset);
+  // the previous call's contents stay in the array: the error word is reset
+  // to zero here, the output flags are rewritten by the walk kernel, and
+  // walked/dir entries are written before they are read
+  CMI_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
+  {
+    NoAllocParams prm{};
+    for (int d = 0; d < 32; ++d)
+      prm.enabled[d] = (d < kNumDirections) ? (output_enabled ? output_enabled[d] : 1) : 0;
+    prm.enabled_out = flags;
+    prm.sub = S;
+    prm.input_direction = input_direction;
+    prm.in = reinterpret_cast<const Packet64 *>(d_in);
+    prm.n = n;
+    prm.nH = d_nH;
+    prm.xH = d_xH;
+    prm.J = d_J;
+    prm.walked = walked;
+    prm.dir = dir;
+    prm.err = err;
+    prm.tables = make_direction_tables();
+    const size_t smem = 24 * (size_t)S.padded_cells;
+    CMI_CUDA(cudaFuncSetAttribute(k_traverse_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    k_traverse_noalloc<<<n > 0 ? (n + 255) / 256 : 1, 256, smem, s>>>(prm);
+    CMI_CUDA(cudaGetLastError());
+  }
+  k_partition<<<1, 256, 0, s>>>(walked, dir, n, flags, reinterpret_cast<Packet64 *>(d_out),
+                                d_out_count, d_num_done);
+  CMI_CUDA(cudaGetLastError());
+  uint32_t herr = 0;
+  CMI_CUDA(cudaMemcpyAsync(&herr, err, sizeof(herr), cudaMemcpyDeviceToHost, s));
+  CMI_CUDA(cudaStreamSynchronize(s));
+  if (herr & kFlagWalkLimit) return fail(CMI_ERR_INVARIANT, "walk step bound exceeded");
+  return CMI_OK;
+}
