@@ -1,18 +1,30 @@
 #!/usr/bin/env python
 """Cell crossings per second of the plain photoionization method on B200.
 
-Workload (one "step" = one iteration of the plain method: emit the packets,
-trace them to absorption or escape, solve the ionization balance):
-  128^3 cells as 8^3 subgrids of 16^3, log-normal n_H (sigma_ln = 1, smoothed
-  over 4 cells, mean 1e8 m^-3), 4 sources at seeded random positions with
-  luminosities log-uniform in 1e48-1e49 s^-1, 1e7 packets per iteration,
-  FP32 transport with FP64 balance.  Inputs are seeded synthetic data.
+One "step" = one iteration of the plain method: emit the packets, trace them
+to absorption or escape, solve the ionization balance.  Workloads (seeded
+synthetic inputs; --workload):
+
+  lognormal128 (default)  128^3 cells as 8^3 subgrids of 16^3, log-normal n_H
+                          (sigma_ln = 1, smoothed over 4 cells, mean 1e8 m^-3),
+                          4 sources at seeded random positions, luminosities
+                          log-uniform in 1e48-1e49 s^-1, 1e7 packets/iteration
+  stromgren64             the reference's own test: 64^3 as 8^3 subgrids of
+                          8^3, n_H = 1e8, one 4.26e49 s^-1 source, 1e6 packets
+  batch64                 64 independent instances, sides 32-128 in 16^3
+                          subgrids, sigma_ln 0.5-1.5, 1-4 sources, 5 packets
+                          per cell per iteration
+  large256                256^3 as 16^3 subgrids of 16^3, sigma_ln = 1.5,
+                          16 sources, 1e8 packets/iteration
+
+FP32 transport with FP64 balance by default.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torchrun, one rank per GPU: every rank traces its own 1e7
-packets (weak scaling) and the ranks sum J with one NCCL all-reduce per
-iteration before each solves the balance.
+N > 1 runs under torchrun, one rank per GPU.  Single-instance workloads:
+every rank traces its own packets (weak scaling) and the ranks sum J with one
+NCCL all-reduce per iteration before each solves the balance.  batch64: the
+instances are sharded over the ranks (no collective on the data path).
 """
 from __future__ import annotations
 
@@ -30,11 +42,22 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CROSSING = 32  # FP64 n, x read + J read-modify-write per crossing
-WORKLOAD = ("lognormal128: 128^3 cells as 8^3 subgrids of 16^3, log-normal n_H "
-            "(sigma_ln=1, 4-cell smoothing, mean 1e8 m^-3), 4 sources L in 1e48-1e49 s^-1, "
-            "1e7 packets/iteration")
 METRIC = "cell-crossings/s"
 UNIT = "crossings/s"
+DESCRIPTIONS = {
+    "lognormal128": ("lognormal128: 128^3 cells as 8^3 subgrids of 16^3, log-normal n_H "
+                     "(sigma_ln=1, 4-cell smoothing, mean 1e8 m^-3), 4 sources L in "
+                     "1e48-1e49 s^-1, {packets:.0e} packets/iteration"),
+    "stromgren64": ("stromgren64: 64^3 cells as 8^3 subgrids of 8^3, uniform n_H = 1e8 m^-3, "
+                    "one source of 4.26e49 s^-1 at the centre, alpha = 4e-19, "
+                    "{packets:.0e} packets/iteration"),
+    "batch64": ("batch64: 64 independent log-normal instances, sides in {{32,48,64,96,128}} as "
+                "16^3-cell subgrids, sigma_ln in 0.5-1.5, 1-4 sources, 5 packets per cell per "
+                "iteration ({packets:.3e} packets/iteration in total)"),
+    "large256": ("large256: 256^3 cells as 16^3 subgrids of 16^3, log-normal n_H (sigma_ln=1.5), "
+                 "16 sources, {packets:.0e} packets/iteration"),
+}
+DEFAULT_PACKETS = {"lognormal128": 1e7, "stromgren64": 1e6, "large256": 1e8}
 
 
 def parse():
@@ -43,20 +66,52 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(DESCRIPTIONS), default="lognormal128")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
-    ap.add_argument("--packets", type=float, default=1e7)
-    ap.add_argument("--ncell", type=int, default=128)
-    ap.add_argument("--num-subgrid", type=int, default=8)
+    ap.add_argument("--packets", type=float, default=0.0,
+                    help="packets per iteration (single-instance workloads; 0 = default)")
     ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--cpu-packets", type=float, default=1e7,
+                    help="most packets per instance in the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
-def workload(args):
-    from parallelcmacionize_b200.problems import lognormal_config
-    return lognormal_config(ncell=args.ncell, num_subgrid=args.num_subgrid,
-                            num_photon=int(args.packets), num_sources=4, sigma_ln=1.0, seed=42)
+class Workload:
+    """Instances of a workload owned by one rank (all of them for replicas)."""
+
+    def __init__(self, name, specs, fields, sharded, total_packets):
+        self.name = name
+        self.specs = specs            # this rank's GridSpecs
+        self.fields = fields          # their n_H, blocked order
+        self.sharded = sharded        # instances split over ranks
+        self.total_packets = total_packets  # per iteration, whole job at one rank
+        self.description = DESCRIPTIONS[name].format(packets=total_packets)
+
+
+def workload(args, rank=0, world=1):
+    from parallelcmacionize_b200 import problems as P
+    name = args.workload
+    if name == "batch64":
+        from parallelcmacionize_b200.distributed import shard_instances
+        cfgs = P.batch_configs(count=64, select=set())
+        costs = [g.num_photon * sum(g.ncell) for g, _ in cfgs]
+        mine = shard_instances(costs, world)[rank]
+        cfgs = P.batch_configs(count=64, select=set(mine))
+        specs = [cfgs[i][0] for i in mine]
+        fields = [cfgs[i][1] for i in mine]
+        total = sum(g.num_photon for g, _ in cfgs)
+        return Workload(name, specs, fields, True, total)
+    packets = int(args.packets or DEFAULT_PACKETS[name])
+    if name == "lognormal128":
+        g, n = P.lognormal_config(ncell=128, num_subgrid=8, num_photon=packets, num_sources=4,
+                                  sigma_ln=1.0, seed=42)
+    elif name == "stromgren64":
+        g, n = P.stromgren(ncell=64, num_subgrid=8, num_photon=packets)
+    else:
+        g, n = P.large_config(num_photon=packets)
+    return Workload(name, [g], [n], False, packets)
 
 
 # ---------------------------------------------------------------------------
@@ -158,21 +213,43 @@ def cpu_reference_run(spec, nH, xH, packets, iterations, warmup=0):
             "seconds": secs, "crossings": cross, "iterations": iterations}
 
 
+def cpu_sample(wl, x_states, iterations, warmup=0, max_packets=1e7):
+    """Bounded CPU sample of a workload: single instance -> that instance with at
+    most ``max_packets`` packets; batch -> instances in order until their packets
+    reach ``max_packets``.  Returns (summary dict, sample text)."""
+    secs, cross, used, pk = 0.0, 0, [], 0
+    for i, (g, n) in enumerate(zip(wl.specs, wl.fields)):
+        packets = int(min(g.num_photon, max_packets)) if not wl.sharded else int(g.num_photon)
+        r = cpu_reference_run(g, n, x_states[i], packets, iterations, warmup=warmup)
+        secs += r["seconds"]
+        cross += r["crossings"]
+        used.append(i)
+        pk += packets
+        kind, cores = r["kind"], r["cores"]
+        if pk >= max_packets or not wl.sharded:
+            break
+    what = (f"instances {used[0]}-{used[-1]} of the batch ({pk:.3e} packets)" if wl.sharded
+            else f"{pk:.0e} packets")
+    return ({"value": cross / secs, "unit": UNIT, "cores": cores, "kind": kind,
+             "seconds": secs, "crossings": cross}, what)
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    spec, nH = workload(args)
-    xH = np.full(nH.size, 1e-6)
-    r = cpu_reference_run(spec, nH, xH, int(args.packets), args.steps, warmup=args.warmup)
+    wl = workload(args)
+    xs = [np.full(n.size, 1e-6) for n in wl.fields]
+    r, what = cpu_sample(wl, xs, args.steps, warmup=args.warmup, max_packets=args.cpu_packets)
     ms = 1000.0 * r["seconds"] / args.steps
-    sample = (f"{int(args.packets):.0e} packets x {args.steps} timed iterations after "
-              f"{args.warmup} warm-up iterations, from x_H = 1e-6, {r['cores']} threads")
+    sample = (f"{what} x {args.steps} timed iterations after {args.warmup} warm-up "
+              f"iterations, from x_H = 1e-6, {r['cores']} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
-        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "device": "host cores"},
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl.description, "device": "host cores"},
         "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"],
                          "kind": r["kind"], "sample": sample},
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -185,6 +262,9 @@ def reference_arm(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+TALLY_TEXT = {"fixed64": "fixed-point shared tallies (exact 64-bit sums) -> fp64 J"}
+
+
 def ours(args):
     import torch
     from parallelcmacionize_b200 import TransportEngine
@@ -204,11 +284,12 @@ def ours(args):
                                 device_id=torch.device("cuda", local))
         group = dist.group.WORLD
 
-    spec, nH = workload(args)
-    eng = TransportEngine(spec, precision=args.precision, device=local,
+    wl = workload(args, rank, world)
+    eng = TransportEngine(wl.specs, precision=args.precision, device=local,
                           packets_per_chunk=args.chunk)
-    eng.set_fields(0, nH, np.full(nH.size, 1e-6))
-    runner = ReplicaRunner(eng, group=group)
+    for i, n in enumerate(wl.fields):
+        eng.set_fields(i, n, np.full(n.size, 1e-6))
+    runner = ReplicaRunner(eng, group=group, mode="shards" if wl.sharded else "replicas")
     stream = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", local))
 
     # ---- warm-up (graph capture happens here) ----
@@ -226,7 +307,7 @@ def ours(args):
     torch.cuda.synchronize()
     ms_local = start.elapsed_time(stop)
     ms = runner.max_over_ranks(ms_local)
-    launches = eng.last_launch_count() if world == 1 else runner.launches
+    launches = runner.launches
     crossings_local = sum(s["cell_crossings"] for s in stats)
     crossings = runner.sum_over_ranks(crossings_local)
     value = crossings / (ms / 1000.0)
@@ -245,7 +326,9 @@ def ours(args):
     peak, peak_kind = measured_peak_hbm()
     total_kt = sum(v[0] for v in kt.values())
     roofline = {
-        "kernel": "k_walk (transport round)", "bound": "hbm", "achieved": achieved,
+        "kernel": "k_walk32 (transport round)" if args.precision == "fp32" else
+                  "k_walk64 (transport round)",
+        "bound": "hbm", "achieved": achieved,
         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
         "traffic": None, "algorithmic_bytes_per_crossing": BYTES_PER_CROSSING,
         "walk_ms_per_iteration": walk_ms, "walk_launches_per_iteration": walk_launches,
@@ -256,49 +339,59 @@ def ours(args):
     # ---- end to end through the public API with host buffers ----
     e2e = None
     if not args.no_e2e:
-        pin_n = torch.from_numpy(nH.copy()).pin_memory()
-        x_now, _ = eng.get_fields(0, intensity=False)
-        pin_x = torch.from_numpy(x_now).pin_memory()
-        out_x = torch.empty(nH.size, dtype=torch.float64).pin_memory()
+        pin_n = [torch.from_numpy(n.copy()).pin_memory() for n in wl.fields]
+        pin_x = [torch.from_numpy(eng.get_fields(i, intensity=False)[0]).pin_memory()
+                 for i in range(len(wl.fields))]
+        out_x = [torch.empty(n.size, dtype=torch.float64).pin_memory() for n in wl.fields]
+        ncells = sum(n.size for n in wl.fields)
         runner.barrier()
         t0 = time.perf_counter()
         e2e_cross = 0
         for k in range(args.steps):
-            eng.set_fields(0, pin_n.numpy(), pin_x.numpy())
+            for i in range(len(wl.fields)):
+                eng.set_fields(i, pin_n[i].numpy(), pin_x[i].numpy())
             st = runner.run(1, seed=1000 + k)
             e2e_cross += sum(s["cell_crossings"] for s in st)
-            eng.get_fields(0, intensity=False, out_x=out_x.numpy())
-            pin_x.copy_(out_x)
+            for i in range(len(wl.fields)):
+                eng.get_fields(i, intensity=False, out_x=out_x[i].numpy())
+                pin_x[i].copy_(out_x[i])
         e2e_s = runner.max_over_ranks(time.perf_counter() - t0)
         e2e_cross = runner.sum_over_ranks(e2e_cross)
         e2e = {"value": e2e_cross / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(2 * 8 * nH.size),
-               "d2h_bytes_per_step": int(8 * nH.size + 64),
+               "h2d_bytes_per_step": int(2 * 8 * ncells),
+               "d2h_bytes_per_step": int(8 * ncells + 64 * len(wl.fields)),
                "ms_per_step": 1000.0 * e2e_s / args.steps}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        x_state, _ = eng.get_fields(0, intensity=False)
-        r = cpu_reference_run(spec, nH, x_state, int(args.packets), 1)
+        xs = [eng.get_fields(i, intensity=False)[0] for i in range(len(wl.fields))]
+        r, what = cpu_sample(wl, xs, 1, max_packets=args.cpu_packets)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
-               "sample": (f"1 iteration of {int(args.packets):.0e} packets on the GPU run's "
-                          f"post-warm-up x_H field, {r['cores']} threads, "
-                          f"{r['seconds']:.2f} s of transport+balance, crossings counted by "
-                          "replaying the same packets through the oracle walk")}
+               "sample": (f"1 iteration of {what} on the GPU run's post-warm-up x_H field, "
+                          f"{r['cores']} threads, {r['seconds']:.2f} s of transport+balance, "
+                          "crossings counted by replaying the same packets through the "
+                          "oracle walk")}
 
     if rank == 0:
+        ncells = sum(int(np.prod(g.ncell)) for g in wl.specs)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.precision, "data": "synthetic (seeded log-normal density, random sources)",
             "config": {
-                "workload": WORKLOAD, "packets_per_step_per_gpu": int(args.packets),
-                "transport": args.precision + " walk, compensated fp32 tallies -> fp64 J, fp64 balance",
-                "l2": "inputs larger than L2: packet arenas 2 x 320 MB per GPU stream through HBM "
-                      "every round; fields (16 MB) stay L2-resident",
-                "parallelism": (f"{world} packet replicas + NCCL all-reduce of J per iteration"
-                                if world > 1 else "single GPU"),
+                "workload": wl.description,
+                "packets_per_step_per_gpu": int(sum(g.num_photon for g in wl.specs)),
+                "transport": (f"{args.precision} walk, "
+                              + (TALLY_TEXT["fixed64"] if args.precision == "fp32"
+                                 else "fp64 shared tallies -> fp64 J") + ", fp64 balance"),
+                "l2": ("inputs larger than L2: the packet arenas (32 B per packet in flight, "
+                       "in and out) stream through HBM every round; per-rank fields of "
+                       f"{ncells} cells"),
+                "parallelism": ("single GPU" if world == 1 else
+                                f"{world} ranks, instances sharded (no collective)"
+                                if wl.sharded else
+                                f"{world} packet replicas + NCCL all-reduce of J per iteration"),
             },
             "crossings_per_step": crossings / args.steps,
             "clocks": clocks.summary(),

@@ -131,6 +131,21 @@ class DensityGrid {
     _host_stale = true;
     return st;
   }
+  // iterate until the mean |delta x_H| of an iteration drops below tolerance
+  // (no reference counterpart); returns the stats of the iterations run and
+  // sets *converged_at (0: not within max_iterations)
+  std::vector<cmi_stats> run_until_converged(double tolerance, int max_iterations, uint64_t seed,
+                                             int *converged_at, int min_iterations = 2) {
+    push();
+    std::vector<cmi_stats> st((size_t)max_iterations);
+    int32_t done = 0, at = 0;
+    cmi_check(cmi_run_until_converged(_ctx, max_iterations, min_iterations, tolerance, seed,
+                                      st.data(), &done, &at));
+    _host_stale = true;
+    st.resize((size_t)done);
+    if (converged_at) *converged_at = at;
+    return st;
+  }
 };
 
 class DensitySubGrid {

@@ -86,7 +86,7 @@ enum cmi_balance_form {
 enum cmi_tally {
   CMI_TALLY_FP32 = 0,              /* FP32 shared-memory atomics */
   CMI_TALLY_FP32_COMPENSATED = 1,  /* FP32 atomics + TwoSum rounding error in a second FP32 word */
-  CMI_TALLY_FIXED64 = 2,           /* 64-bit fixed point (lref/2^24 units), 32-bit integer atomics + carry */
+  CMI_TALLY_FIXED64 = 2,           /* fixed point (lref/2^22 units), 32-bit integer atomics, carries to FP64 J */
   CMI_TALLY_FIXED64_ATOMIC64 = 3   /* 64-bit fixed point, 64-bit integer atomics */
 };
 enum cmi_rng {
@@ -109,10 +109,12 @@ typedef struct {
   int32_t device;              /* CUDA device ordinal */
   int32_t threads_per_cta;     /* 0 = library default (256) */
   int32_t ctas_per_sm;         /* 0 = as many as fit */
-  int32_t packets_per_chunk;   /* 0 = library default (512); power of two in [32, 4096] */
+  int32_t packets_per_chunk;   /* 0 = library default (128); power of two in [32, 4096] */
   int32_t tally_mode;          /* FP32 transport: cmi_tally (default CMI_TALLY_FIXED64) */
   int32_t use_graph;           /* 1 = capture each iteration as a CUDA graph (default) */
-  int32_t reserved[7];
+  int32_t max_run_chunks;      /* most chunks a CTA claims at once (0 = 64): how long a CTA
+                                  stays on one subgrid before flushing its tallies */
+  int32_t reserved[6];
 } cmi_options;
 
 /* Per-instance counters of one iteration. */
@@ -169,6 +171,22 @@ int cmi_set_packet_budget(cmi_context *context, int32_t instance, uint64_t num_p
  * num_instances records (iteration-major) and may be NULL. */
 int cmi_run_iterations(cmi_context *context, int32_t num_iterations, uint64_t seed,
                        cmi_stats *stats);
+/* Run iterations until every instance has converged or max_iterations have
+ * run.  No reference counterpart: the reference runs a fixed number of
+ * iterations (number of iterations in params.txt).  An instance has converged
+ * after iteration k (k >= min_iterations) when the mean over its cells of
+ * |x_H after - x_H before| in that iteration is below tolerance; from then on
+ * it is frozen for the rest of the call: it emits no packets and keeps its
+ * x_H.  The Monte Carlo noise of x_H sets a floor under the mean change
+ * (roughly proportional to 1/sqrt(packets per iteration)), so a tolerance
+ * below that floor runs to max_iterations.  stats receives iterations_done x
+ * num_instances records (iteration-major; capacity max_iterations x
+ * num_instances; may be NULL), *iterations_done the number of iterations run,
+ * converged_at[i] (num_instances entries, may be NULL) the 1-based iteration
+ * after which instance i converged, 0 if it did not. */
+int cmi_run_until_converged(cmi_context *context, int32_t max_iterations, int32_t min_iterations,
+                            double tolerance, uint64_t seed, cmi_stats *stats,
+                            int32_t *iterations_done, int32_t *converged_at);
 /* Transport phase only (no balance); J keeps accumulating. */
 int cmi_shoot_packets(cmi_context *context, uint64_t seed, uint32_t iteration, cmi_stats *stats);
 

@@ -45,7 +45,8 @@ NEIGHBOUR_OUTSIDE = 0xFFFFFFFF
 EXPORTED = [
     "cmi_default_options", "cmi_last_error_string", "cmi_abi_version", "cmi_create",
     "cmi_destroy", "cmi_set_fields", "cmi_get_fields", "cmi_set_intensity", "cmi_set_sources",
-    "cmi_set_packet_budget", "cmi_run_iterations", "cmi_shoot_packets",
+    "cmi_set_packet_budget", "cmi_run_iterations", "cmi_run_until_converged",
+    "cmi_shoot_packets",
     "cmi_transport_packets", "cmi_traverse_buffer", "cmi_trace_packet",
     "cmi_compute_neutral_fraction", "cmi_device_field", "cmi_get_stream", "cmi_synchronize",
     "cmi_last_launch_count", "cmi_set_kernel_timing", "cmi_kernel_timing",
@@ -87,7 +88,8 @@ class Options(C.Structure):
         ("packets_per_chunk", C.c_int32),
         ("tally_mode", C.c_int32),
         ("use_graph", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("max_run_chunks", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -143,6 +145,7 @@ def load():
     L.cmi_set_sources.argtypes = [ctx, i32, vp, vp, i32]
     L.cmi_set_packet_budget.argtypes = [ctx, i32, u64]
     L.cmi_run_iterations.argtypes = [ctx, i32, u64, vp]
+    L.cmi_run_until_converged.argtypes = [ctx, i32, i32, d, u64, vp, vp, vp]
     L.cmi_shoot_packets.argtypes = [ctx, u64, u32, vp]
     L.cmi_transport_packets.argtypes = [ctx, i32, vp, vp, u64, vp]
     L.cmi_traverse_buffer.argtypes = [ctx, i32, u32, i32, vp, u32, vp, vp, vp, vp]

@@ -1,0 +1,210 @@
+"""Autotuner for the transport's launch shape (no reference counterpart).
+
+The reference fixes its subgrid decomposition and buffer sizes in the
+parameter file (params.txt: ``num_subgrid``, ``PHOTONBUFFER_SIZE`` in
+PhotonBuffer.hpp:34).  On the GPU those choices set how many cells a CTA
+stages in shared memory, how many CTAs fit on an SM and how often a CTA flushes
+its tallies, and the best choice depends on the grid, the source layout and the
+packet count.  ``Autotuner`` times a short run of each candidate and keeps the
+fastest, cached on disk by device, grid shape, precision and packet count.
+
+A candidate (``WalkConfig``) chooses:
+
+* ``sub_side``          -- cells per subgrid along each axis (8 or 16 by
+  default); the grid is re-blocked for it,
+* ``packets_per_chunk`` -- packets a CTA takes per claim (the packet ring slot),
+* ``max_run_chunks``    -- most chunks claimed at once: how long a CTA stays on
+  one subgrid before it flushes its shared tallies to J,
+* ``tally``             -- shared-memory tally form of the FP32 walk,
+* ``ctas_per_sm``       -- 0 = the engine's occupancy choice.
+
+The subgrid decomposition changes where the FP32 walk re-anchors its
+positions, so results of two candidates agree to FP32 rounding, not bit for
+bit; every candidate is a correct transport.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import tempfile
+import time
+from dataclasses import asdict, dataclass
+
+import numpy as np
+
+from .engine import GridSpec, TransportEngine, cube_to_blocked
+
+
+@dataclass(frozen=True)
+class WalkConfig:
+    sub_side: int = 16
+    packets_per_chunk: int = 128
+    max_run_chunks: int = 64
+    tally: str = "fixed64"
+    ctas_per_sm: int = 0
+
+    def grid(self, base: GridSpec) -> GridSpec:
+        """``base`` re-decomposed into subgrids of ``sub_side`` cells per axis."""
+        nsub = tuple(int(n) // self.sub_side for n in base.ncell)
+        return GridSpec(box=base.box, ncell=base.ncell, num_subgrid=nsub,
+                        recombination_rate=base.recombination_rate,
+                        cross_section=base.cross_section, sources=list(base.sources),
+                        num_photon=base.num_photon)
+
+    def engine_options(self) -> dict:
+        return dict(packets_per_chunk=self.packets_per_chunk, tally=self.tally,
+                    ctas_per_sm=self.ctas_per_sm, max_run_chunks=self.max_run_chunks)
+
+
+def candidates(ncell, precision="fp32", sides=(8, 16), chunks=(64, 128, 256),
+               runs=(16, 64), tallies=("fixed64",), ctas=(0,)):
+    """Every valid combination for a grid of ``ncell`` cells per axis.
+
+    A side must divide every axis.  The FP64 walk has no shared tallies and no
+    packet ring, so only the decomposition is searched for it.
+    """
+    ncell = tuple(int(n) for n in ncell)
+    ok_sides = [s for s in sides if all(n % s == 0 for n in ncell)]
+    if not ok_sides:
+        raise ValueError(f"no subgrid side of {sides} divides the grid {ncell}")
+    if precision == "fp64":
+        return [WalkConfig(sub_side=s, packets_per_chunk=0, max_run_chunks=0, tally="fixed64",
+                           ctas_per_sm=0) for s in ok_sides]
+    return [WalkConfig(s, c, r, t, k) for s in ok_sides for c in chunks for r in runs
+            for t in tallies for k in ctas]
+
+
+def default_cache_path() -> str:
+    p = os.environ.get("CMI_AUTOTUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "parallelcmacionize_b200",
+                        "autotune.json")
+
+
+def cache_key(device_name: str, grid: GridSpec, precision: str) -> str:
+    """Grid shape, source count and packet count to the nearest power of two."""
+    bucket = int(round(math.log2(max(1, int(grid.num_photon)))))
+    n = "x".join(str(int(v)) for v in grid.ncell)
+    return f"{device_name}|{n}|src{len(grid.sources)}|pk2^{bucket}|{precision}"
+
+
+def _device_name(device: int) -> str:
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.cuda.get_device_name(device).replace("|", "/")
+    except Exception:
+        pass
+    return f"cuda{device}"
+
+
+class Autotuner:
+    """Pick the fastest ``WalkConfig`` for a grid by timing short runs.
+
+    ``measure(config, grid, nH_cube, xH_cube) -> crossings per second`` may be
+    replaced (tests use a model of it); the default builds an engine for the
+    candidate, runs ``warmup`` untimed and ``iterations`` timed iterations of
+    the transport + balance loop from the same initial fields and divides the
+    cell crossings by the time between two device synchronisations.
+    """
+
+    def __init__(self, cache_path=None, device=0, precision="fp32", iterations=2, warmup=1,
+                 seed=42, measure=None):
+        self.cache_path = cache_path or default_cache_path()
+        self.device = device
+        self.precision = precision
+        self.iterations = int(iterations)
+        self.warmup = int(warmup)
+        self.seed = int(seed)
+        self.measure = measure or self._measure
+        self.last_table = []
+
+    # ---- cache ----
+    def _load(self) -> dict:
+        try:
+            with open(self.cache_path) as f:
+                d = json.load(f)
+            return d if isinstance(d, dict) else {}
+        except (OSError, ValueError):
+            return {}
+
+    def _store(self, key: str, entry: dict):
+        d = self._load()
+        d[key] = entry
+        os.makedirs(os.path.dirname(os.path.abspath(self.cache_path)), exist_ok=True)
+        fd, tmp = tempfile.mkstemp(dir=os.path.dirname(os.path.abspath(self.cache_path)),
+                                   suffix=".tmp")
+        with os.fdopen(fd, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, self.cache_path)
+
+    def cached(self, grid: GridSpec):
+        e = self._load().get(cache_key(_device_name(self.device), grid, self.precision))
+        return WalkConfig(**e["config"]) if e else None
+
+    # ---- search ----
+    def _measure(self, cfg: WalkConfig, grid: GridSpec, nH_cube, xH_cube) -> float:
+        g = cfg.grid(grid)
+        with TransportEngine(g, precision=self.precision, device=self.device,
+                             **cfg.engine_options()) as eng:
+            nH = cube_to_blocked(nH_cube, g.ncell, g.num_subgrid)
+            xH = cube_to_blocked(xH_cube, g.ncell, g.num_subgrid)
+            eng.set_fields(0, nH, xH)
+            if self.warmup:
+                eng.run_iterations(self.warmup, seed=self.seed)
+            eng.set_fields(0, nH, xH)
+            eng.synchronize()
+            t0 = time.perf_counter()
+            st = eng.run_iterations(self.iterations, seed=self.seed + 1)
+            eng.synchronize()
+            dt = time.perf_counter() - t0
+        crossings = sum(s[0]["cell_crossings"] for s in st)
+        return crossings / dt
+
+    def tune(self, grid: GridSpec, nH_cube, xH_cube=None, configs=None, force=False):
+        """Best config for ``grid`` (from the cache unless ``force``).
+
+        ``nH_cube``/``xH_cube`` are (nx, ny, nz) cubes; xH defaults to the
+        reference's initial 1e-6 (DensitySubGrid.hpp:544-551).
+        """
+        key = cache_key(_device_name(self.device), grid, self.precision)
+        if not force:
+            hit = self._load().get(key)
+            if hit:
+                self.last_table = []
+                return WalkConfig(**hit["config"])
+        nH_cube = np.asarray(nH_cube, dtype=np.float64).reshape(tuple(grid.ncell))
+        xH_cube = (np.full_like(nH_cube, 1.0e-6) if xH_cube is None
+                   else np.asarray(xH_cube, dtype=np.float64).reshape(nH_cube.shape))
+        configs = list(configs) if configs is not None else candidates(grid.ncell,
+                                                                         self.precision)
+        if not configs:
+            raise ValueError("no candidate configurations")
+        table = []
+        for cfg in configs:
+            table.append((cfg, float(self.measure(cfg, grid, nH_cube, xH_cube))))
+        best, rate = max(table, key=lambda t: t[1])
+        self.last_table = table
+        self._store(key, {"config": asdict(best), "crossings_per_s": rate,
+                          "searched": len(table)})
+        return best
+
+    def engine(self, grid: GridSpec, nH_cube, xH_cube=None, **engine_kw):
+        """A ``TransportEngine`` for ``grid`` in the tuned decomposition, with
+        the fields set; returns (engine, config).  Fields read back from it are
+        in that decomposition's blocked order (``blocked_to_cube`` with
+        ``engine.grids[0]``)."""
+        cfg = self.tune(grid, nH_cube, xH_cube)
+        g = cfg.grid(grid)
+        kw = cfg.engine_options()
+        kw.update(engine_kw)
+        eng = TransportEngine(g, precision=self.precision, device=self.device, **kw)
+        nH = cube_to_blocked(np.asarray(nH_cube, np.float64).reshape(tuple(g.ncell)), g.ncell,
+                             g.num_subgrid)
+        xH = (np.full(nH.size, 1.0e-6) if xH_cube is None else
+              cube_to_blocked(np.asarray(xH_cube, np.float64).reshape(tuple(g.ncell)),
+                              g.ncell, g.num_subgrid))
+        eng.set_fields(0, nH, xH)
+        return eng, cfg

@@ -91,6 +91,8 @@ struct alignas(16) DevInstance {
   uint32_t first_subgrid, num_subgrids;
   uint32_t first_source, num_sources;
   int64_t num_cells;
+  uint32_t frozen;        // 1: converged, emits nothing and keeps x_H (run until converged)
+  uint32_t reserved;
 };
 
 struct alignas(16) DevSource {

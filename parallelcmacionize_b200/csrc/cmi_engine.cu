@@ -35,6 +35,7 @@ int fail(int code, const char *fmt, ...) {
   do {                                                                                     \
     const cudaError_t e_ = (call);                                                         \
     if (e_ != cudaSuccess) {                                                               \
+      (void)cudaGetLastError(); /* a non-sticky error must not fail the next check */      \
       return fail(e_ == cudaErrorMemoryAllocation ? CMI_ERR_OUT_OF_MEMORY : CMI_ERR_CUDA, \
                   "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,       \
                   __LINE__);                                                               \
@@ -334,6 +335,7 @@ int launch_plan(cmi_context *c) {
 WalkParams walk_params(cmi_context *c) {
   WalkParams p{};
   p.chunk = c->chunk;
+  p.max_run = c->opt.max_run_chunks > 0 ? (uint32_t)c->opt.max_run_chunks : 64u;
   p.subs = c->d_sub;
   p.inst = c->d_inst;
   p.chunks = c->d_chunks;
@@ -354,9 +356,14 @@ WalkParams walk_params(cmi_context *c) {
   return p;
 }
 
+// the fixed-point default is built for 4 resident CTAs per SM (<= 64 registers)
+template <int kTally>
+constexpr int walk32_min_blocks() { return kTally == 2 ? 4 : 1; }
+
 template <int kTally>
 void launch_walk32_t(cmi_context *c, const WalkParams &p) {
-  k_walk32<kWalkThreads, kTally><<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+  k_walk32<kWalkThreads, kTally, walk32_min_blocks<kTally>()>
+      <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
 }
 
 int launch_walk(cmi_context *c) {
@@ -378,6 +385,14 @@ int launch_walk(cmi_context *c) {
 
 template <class F>
 int config_kernel(cmi_context *c, F fn) {
+  int optin = 0;
+  CMI_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  if (c->walk_smem > (size_t)optin)
+    return fail(CMI_ERR_NOT_SUPPORTED,
+                "the %s walk needs %zu B of shared memory per CTA (largest subgrid %d cells%s), "
+                "the device allows %d B",
+                c->fp32() ? "FP32" : "FP64", c->walk_smem, (int)c->max_padded,
+                c->fp32() ? ", two packet-ring chunks: lower packets_per_chunk" : "", optin);
   CMI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)c->walk_smem));
   int per_sm = 0;
@@ -395,15 +410,15 @@ int config_walk(cmi_context *c) {
   if (c->fp32()) {
     const size_t head = (sizeof(Walk32Shared) + 15) & ~(size_t)15;
     const int tm = c->opt.tally_mode;
-    const size_t tally_bytes = (tm == 0 ? 4 : 8) * (size_t)c->max_padded + 16;
+    const size_t tally_bytes = (tm == 0 || tm == 2 ? 4 : 8) * (size_t)c->max_padded + 16;
     c->walk_smem = head + 4 * (size_t)c->max_padded + tally_bytes +
                    sizeof(Packet32) * 2 * (size_t)c->chunk +
                    (sizeof(Packet32) + 4) * (kWalkThreads / 32) * kStage;
     switch (tm) {
-      case 0: return config_kernel(c, k_walk32<kWalkThreads, 0>);
-      case 1: return config_kernel(c, k_walk32<kWalkThreads, 1>);
-      case 2: return config_kernel(c, k_walk32<kWalkThreads, 2>);
-      default: return config_kernel(c, k_walk32<kWalkThreads, 3>);
+      case 0: return config_kernel(c, k_walk32<kWalkThreads, 0, walk32_min_blocks<0>()>);
+      case 1: return config_kernel(c, k_walk32<kWalkThreads, 1, walk32_min_blocks<1>()>);
+      case 2: return config_kernel(c, k_walk32<kWalkThreads, 2, walk32_min_blocks<2>()>);
+      default: return config_kernel(c, k_walk32<kWalkThreads, 3, walk32_min_blocks<3>()>);
     }
   }
   const size_t head = (sizeof(WalkShared) + 15) & ~(size_t)15;
@@ -630,6 +645,7 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
        (opt.packets_per_chunk < 32 || (opt.packets_per_chunk & (opt.packets_per_chunk - 1)))))
     return fail(CMI_ERR_INVALID_ARGUMENT,
                 "packets_per_chunk must be 0 or a power of two in [32, 4096]");
+  if (opt.max_run_chunks < 0) return fail(CMI_ERR_INVALID_ARGUMENT, "negative max_run_chunks");
   if (opt.tally_mode < CMI_TALLY_FP32 || opt.tally_mode > CMI_TALLY_FIXED64_ATOMIC64)
     return fail(CMI_ERR_INVALID_ARGUMENT, "unknown tally mode %d", opt.tally_mode);
 
@@ -638,7 +654,7 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
   c->opt = opt;
   c->device = opt.device;
   c->tables = make_direction_tables();
-  c->chunk = opt.packets_per_chunk > 0 ? (uint32_t)opt.packets_per_chunk : 512u;
+  c->chunk = opt.packets_per_chunk > 0 ? (uint32_t)opt.packets_per_chunk : 128u;
   auto bail = [&](int rc) {
     cmi_destroy(c);
     return rc;
@@ -935,6 +951,60 @@ int cmi_run_iterations(cmi_context *c, int32_t iterations, uint64_t seed, cmi_st
                            c->stream));
   CMI_CUDA(cudaStreamSynchronize(c->stream));
   return run(c, iterations, seed, it0, true, stats);
+}
+
+static int set_frozen(cmi_context *c, int32_t i, uint32_t v) {
+  CMI_CUDA(cudaMemcpyAsync(&c->d_inst[i].frozen, &v, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           c->stream));
+  return CMI_OK;
+}
+
+int cmi_run_until_converged(cmi_context *c, int32_t max_iterations, int32_t min_iterations,
+                            double tolerance, uint64_t seed, cmi_stats *stats,
+                            int32_t *iterations_done, int32_t *converged_at) {
+  CMI_TRY(check_ctx(c));
+  if (max_iterations <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "max_iterations must be > 0");
+  if (min_iterations < 1 || min_iterations > max_iterations)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "min_iterations must be in [1, max_iterations]");
+  if (!(tolerance >= 0.) || !std::isfinite(tolerance))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "tolerance must be finite and >= 0");
+  const int ninst = (int)c->inst.size();
+  std::vector<int32_t> at(ninst, 0);
+  int remaining = ninst;
+  CMI_TRY(clear_flags(c));
+  uint32_t it0 = 0;
+  CMI_CUDA(cudaMemcpyAsync(&it0, &c->d_state->iteration, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  std::vector<cmi_stats> st(ninst);
+  int32_t done = 0;
+  int rc = CMI_OK;
+  while (done < max_iterations && remaining > 0) {
+    // one iteration (graph replay); the host reads the per-instance change
+    rc = run(c, 1, seed, it0 + (uint32_t)done, true, st.data());
+    if (rc != CMI_OK) break;
+    ++done;
+    if (stats) std::copy(st.begin(), st.end(), stats + (size_t)(done - 1) * ninst);
+    for (int i = 0; i < ninst && rc == CMI_OK; ++i) {
+      if (at[i] != 0 || done < min_iterations || !(st[i].mean_abs_dx < tolerance)) continue;
+      at[i] = done;
+      --remaining;
+      if (remaining > 0) rc = set_frozen(c, i, 1u);
+    }
+  }
+  // leave every instance active for later calls
+  for (int i = 0; i < ninst; ++i)
+    if (at[i] != 0) {
+      const int r = set_frozen(c, i, 0u);
+      if (rc == CMI_OK) rc = r;
+    }
+  if (rc == CMI_OK) {
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) rc = fail(CMI_ERR_CUDA, "unfreeze: %s", cudaGetErrorString(e));
+  }
+  if (iterations_done) *iterations_done = done;
+  if (converged_at) std::copy(at.begin(), at.end(), converged_at);
+  return rc;
 }
 
 int cmi_shoot_packets(cmi_context *c, uint64_t seed, uint32_t iteration, cmi_stats *stats) {

@@ -163,7 +163,8 @@ __global__ void k_emission_plan(const DevInstance *inst, int ninst, const DevSou
   const uint64_t seed = st->seed;
   const uint32_t it = st->iteration;
   for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
-    const DevInstance I = inst[i];
+    DevInstance I = inst[i];
+    if (I.frozen) I.num_photon = 0;
     double total = 0.;
     for (uint32_t k = 0; k < I.num_sources; ++k) total += src[I.first_source + k].luminosity;
     uint64_t assigned = 0;
@@ -578,6 +579,7 @@ __global__ void __launch_bounds__(256) k_scatter(const P *out, const uint32_t *k
 // ---------------------------------------------------------------------------
 struct WalkParams {
   uint32_t chunk;          // largest chunk (packets), FP32 packet-buffer size
+  uint32_t max_run;        // most chunks claimed at once
   const DevSubgrid *subs;
   const DevInstance *inst;
   const Chunk *chunks;
@@ -750,13 +752,28 @@ __device__ __forceinline__ void mbar_wait_bounded(unsigned long long *mbar, uint
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(mbar, phase)) {
     if (global_ns() - t0 > kStageWaitNs) {
-      if (threadIdx.x == 0) atomicOr(flags, kFlagStageTimeout);
+      atomicOr(flags, kFlagStageTimeout);
       const unsigned long long t1 = global_ns();
       while (!mbar_try_wait(mbar, phase) && global_ns() - t1 < kStageWaitNs) {
       }
       return;
     }
   }
+}
+
+// Bounded wait until the counter *p has passed `target` (a shared-memory
+// count bumped by another warp).
+__device__ __forceinline__ void wait_count_above(const uint32_t *p, uint32_t target,
+                                                 uint32_t *flags) {
+  if ((int32_t)(*(const volatile uint32_t *)p - target) > 0) return;
+  const unsigned long long t0 = global_ns();
+  while ((int32_t)(*(const volatile uint32_t *)p - target) <= 0) {
+    if (global_ns() - t0 > kStageWaitNs) {
+      atomicOr(flags, kFlagStageTimeout);
+      return;
+    }
+  }
+  __threadfence_block();
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
@@ -948,10 +965,13 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
 // (one 1 KB coalesced store, one arena atomic, one bucket atomic per
 // destination).  Path lengths go to shared-memory tallies (Tally32), merged
 // into FP64 J in HBM when the CTA leaves the subgrid.
-constexpr int kStage = 64;  // staged output packets per warp
+// per-warp output staging: flushed when it holds >= kStageFlush packets, so
+// it never holds more than kStageFlush - 1 + 32
+constexpr int kStage = 48;
+constexpr uint32_t kStageFlush = 16;
 
-template <int kThreads, int kTally>
-__global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
+template <int kThreads, int kTally, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Walk32Shared &sh = *reinterpret_cast<Walk32Shared *>(smem_raw);
   constexpr int kWarps = kThreads / 32;
@@ -971,13 +991,14 @@ __global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
     cur_ptr += (size_t)P * 8;
   } else if (kTally == 2) {
     tally.u_lo = reinterpret_cast<uint32_t *>(cur_ptr);
-    tally.u_hi = tally.u_lo + P;
-    cur_ptr += (size_t)P * 8;
+    cur_ptr += (size_t)P * 4;
   } else {
     tally.f_hi = reinterpret_cast<float *>(cur_ptr);
     tally.f_lo = tally.f_hi + P;
     cur_ptr += (size_t)P * (kTally == 1 ? 8 : 4);
   }
+  tally.carry_J = nullptr;
+  tally.carry_value = 0.;
   Packet32 *s_pk = reinterpret_cast<Packet32 *>(cur_ptr);  // [2][CH]
   cur_ptr += sizeof(Packet32) * 2 * (size_t)CH;
   Packet32 *s_stage = reinterpret_cast<Packet32 *>(cur_ptr);  // [kWarps][kStage]
@@ -1007,7 +1028,7 @@ __global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
     const uint32_t slot = k & 1u;
     const uint32_t cnt = (k + 1u < sh.seg_chunks) ? CH : sh.seg_n - (k << ch_shift);
     const uint32_t bytes = cnt * (uint32_t)sizeof(Packet32);
-    sh.uses[slot] += 1u;
+    *(volatile uint32_t *)&sh.uses[slot] = sh.uses[slot] + 1u;
     fence_proxy_async();
     mbar_expect_tx(&sh.mbar_pk[slot], bytes);
     tma_load_1d(s_pk + (size_t)slot * CH,
@@ -1023,14 +1044,21 @@ __global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
     const uint32_t old = atomicAdd(&sh.loaded[slot], n);
     if (old + n == cnt) {
       __threadfence_block();
-      sh.loaded[slot] = 0u;
+      *(volatile uint32_t *)&sh.loaded[slot] = 0u;
+      __threadfence_block();  // the reset is seen before the refill's issue count
       if (k + 2u < sh.seg_chunks) issue(k + 2u);
     }
   };
-  // wait until chunk k of the segment is in its slot (all lanes)
+  // wait until chunk k of the segment is in its slot (all lanes).  Claims run
+  // up to kThreads packets ahead of the copies, so a warp can claim chunk k
+  // while its slot still serves chunk k - 2 (or earlier).  A parity wait cannot
+  // tell fill `use` from fill `use - 2`, so the warp first waits until fill
+  // `use` has been issued: that happens only after chunk k - 2 was copied out
+  // completely, which leaves fill `use` as the barrier's current phase.
   auto wait_chunk = [&](uint32_t k) {
     const uint32_t slot = k & 1u;
     const uint32_t use = sh.seg_use0[slot] + (k >> 1);  // this chunk is the use-th fill
+    wait_count_above(&sh.uses[slot], use, &st->flags);
     mbar_wait_bounded(&sh.mbar_pk[slot], use & 1u, &st->flags);
   };
 
@@ -1077,7 +1105,7 @@ __global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
       // guided run length: about half of an even share of what is left
       const uint32_t done = *(volatile uint32_t *)&st->chunk_next;
       const uint32_t left = (nchunks > done) ? nchunks - done : 0u;
-      const uint32_t run = max(1u, min(64u, left / (2u * gridDim.x)));
+      const uint32_t run = max(1u, min(prm.max_run, left / (2u * gridDim.x)));
       const uint32_t c0 = atomicAdd(&st->chunk_next, run);
       sh.run_c0 = c0;
       sh.run_c1 = min(c0 + run, nchunks);
@@ -1136,6 +1164,8 @@ __global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
       }
       v.nyz = sh.nyz;
       tally.scale = sh.tally_scale;
+      tally.carry_J = prm.J + sh.field_offset;
+      tally.carry_value = 4294967296.0 * sh.tally_unit * sh.sigma;
       Walk32 w;
       bool exhausted = false, have = false, fresh = false;
       int entry = kRun;
@@ -1218,7 +1248,7 @@ __global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
             my_skey[slot] = key;
           }
           nstage += (uint32_t)__popc(am);
-          if (nstage >= 32u) flush_stage(32u);
+          if (nstage >= kStageFlush) flush_stage(min(nstage, 32u));
         }
       }
       __syncthreads();  // segment done: every packet of it is traced
@@ -1227,6 +1257,12 @@ __global__ void __launch_bounds__(kThreads) k_walk32(WalkParams prm) {
   if (nstage > 0u) flush_stage(nstage);
   __syncthreads();
   if (staged != kNone) flush();
+  // every issued ring fill has been waited on by its consumers; make sure no
+  // bulk copy into this CTA's shared memory outlives it
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s)
+      if (sh.uses[s] != 0u) mbar_wait_bounded(&sh.mbar_pk[s], (sh.uses[s] - 1u) & 1u, &st->flags);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1249,6 +1285,7 @@ __global__ void __launch_bounds__(256) k_balance(BalanceParams prm) {
   const uint32_t s = prm.first_sub + blockIdx.x;
   const DevSubgrid &S = prm.subs[s];
   const DevInstance &I = prm.inst[S.instance];
+  if (I.frozen) return;  // converged: x_H kept, J is zero (no packets)
   const double jfac = (prm.jfac_override >= 0.) ? prm.jfac_override : I.jfac;
   const double alpha = I.alpha;
   const double sigma = I.sigma;

@@ -36,8 +36,9 @@ struct View32 {
 //  kTally 0: FP32 atomics
 //  kTally 1: FP32 atomics with the rounding error of each addition (TwoSum of
 //            the atomic's own old value) accumulated in a second FP32 array
-//  kTally 2: 64-bit fixed point (units of lref / 2^22) in two 32-bit words,
-//            low word by integer atomic add, carry counted in the high word
+//  kTally 2: fixed point (units of lref / 2^22) in one 32-bit word per cell by
+//            integer atomic add; a wrap of the word (rare: 1024 cell lengths)
+//            adds its 2^32 units straight to the FP64 J array in HBM
 //  kTally 3: 64-bit fixed point with 64-bit integer atomics
 // The fixed-point forms round len * 2^22 / lref (< 2^23 since len <= sqrt(3)
 // lref) half-to-even through the float adder: adding 2^23 leaves the
@@ -47,6 +48,8 @@ struct Tally32 {
   float *f_hi, *f_lo;
   uint32_t *u_lo, *u_hi;
   unsigned long long *u64;
+  double *carry_J;      // kTally 2: J of the staged subgrid (HBM)
+  double carry_value;   // kTally 2: 2^32 units in J units
   float scale;  // 2^22 / lref
 
   static __device__ __forceinline__ uint32_t fixed(float len, float scale) {
@@ -66,7 +69,7 @@ struct Tally32 {
     } else if (kTally == 2) {
       const uint32_t v = fixed(len, scale);
       const uint32_t old = atomicAdd(&u_lo[cell], v);
-      if (old + v < old) atomicAdd(&u_hi[cell], 1u);
+      if (old + v < old) atomicAdd(&carry_J[cell], carry_value);
     } else {
       atomicAdd(&u64[cell], (unsigned long long)fixed(len, scale));
     }
@@ -84,9 +87,8 @@ struct Tally32 {
       f_hi[c] = 0.f;
       f_lo[c] = 0.f;
     } else if (kTally == 2) {
-      v = (double)(((unsigned long long)u_hi[c] << 32) | u_lo[c]) * unit;
+      v = (double)u_lo[c] * unit;
       u_lo[c] = 0u;
-      u_hi[c] = 0u;
     } else {
       v = (double)u64[c] * unit;
       u64[c] = 0ull;
@@ -97,7 +99,7 @@ struct Tally32 {
   __device__ __forceinline__ void zero(int c) const {
     if (kTally == 0) f_hi[c] = 0.f;
     else if (kTally == 1) { f_hi[c] = 0.f; f_lo[c] = 0.f; }
-    else if (kTally == 2) { u_lo[c] = 0u; u_hi[c] = 0u; }
+    else if (kTally == 2) u_lo[c] = 0u;
     else u64[c] = 0ull;
   }
 };

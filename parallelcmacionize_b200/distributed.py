@@ -1,11 +1,18 @@
-"""Packet-parallel replicas over several GPUs (one process per GPU).
+"""Work over several GPUs (one process per GPU).
 
-Every rank holds the whole grid and traces its own packets with a
-rank-specific seed; after the transport phase the ranks sum the intensity
-integrals J with one all-reduce over NCCL (NVLink / NVSwitch) and each solves
-the ionization balance for the combined packet count.  This is the
-replica form of the reference's MPI copy merge (testDensitySubGrid.cpp:3320-3379);
-with one rank it reduces to TransportEngine.run_iterations.
+Two forms, both without any exchange of packets:
+
+* replicas (one instance): every rank holds the whole grid and traces its own
+  packets with a rank-specific seed; after the transport phase the ranks sum
+  the intensity integrals J with one all-reduce over NCCL (NVLink / NVSwitch)
+  and each solves the ionization balance for the combined packet count.  This
+  is the replica form of the reference's MPI copy merge
+  (testDensitySubGrid.cpp:3320-3379).
+* shards (many independent instances): ``shard_instances`` gives every rank
+  a subset of the instances, balanced by their work; ranks run their own
+  instances and only the timing and counters are combined.
+
+With one rank both reduce to TransportEngine.run_iterations.
 """
 from __future__ import annotations
 
@@ -18,6 +25,20 @@ _MASK64 = (1 << 64) - 1
 def replica_seed(seed: int, rank: int) -> int:
     """Independent Philox key per rank (rank 0 keeps the plain seed)."""
     return (int(seed) + _GOLDEN * int(rank)) & _MASK64
+
+
+def shard_instances(costs, world):
+    """Assign independent instances to ``world`` ranks: longest first, each
+    to the least-loaded rank (ties to the lower rank).  Returns one sorted
+    list of instance indices per rank."""
+    costs = [float(c) for c in costs]
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(o) for o in out]
 
 
 class _CudaArray:
@@ -40,9 +61,13 @@ def intensity_tensor(engine, instance=0):
 class ReplicaRunner:
     """Iterations of the plain method on one engine, summed over ranks."""
 
-    def __init__(self, engine, group=None, instance=0, intensity=None, allreduce=None):
+    def __init__(self, engine, group=None, instance=0, intensity=None, allreduce=None,
+                 mode="replicas"):
+        if mode not in ("replicas", "shards"):
+            raise ValueError(f"mode must be 'replicas' or 'shards', not {mode!r}")
         self.eng = engine
         self.group = group
+        self.mode = mode
         self.instance = instance
         self._intensity = intensity or (lambda: intensity_tensor(engine, instance))
         self._allreduce = allreduce
@@ -89,7 +114,7 @@ class ReplicaRunner:
     # ---- iterations ----
     def run(self, iterations, seed=42):
         """Returns one summed stats dict per iteration (this rank's packets)."""
-        if self.world == 1:
+        if self.world == 1 or self.mode == "shards":
             out = []
             for it in self.eng.run_iterations(iterations, seed):
                 out.append(_sum_stats(it))

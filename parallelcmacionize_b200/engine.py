@@ -91,7 +91,8 @@ class TransportEngine:
     """A library context holding one or more grid instances on one GPU."""
 
     def __init__(self, grids, precision="fp32", balance="stable", rng="philox", device=0,
-                 packets_per_chunk=0, tally="fixed64", use_graph=True, ctas_per_sm=0):
+                 packets_per_chunk=0, tally="fixed64", use_graph=True, ctas_per_sm=0,
+                 max_run_chunks=0):
         if isinstance(grids, GridSpec):
             grids = [grids]
         self.grids = list(grids)
@@ -102,7 +103,7 @@ class TransportEngine:
             rng={"philox": _lib.RNG_PHILOX, "ranlux": _lib.RNG_RANLUX}[rng],
             device=device, packets_per_chunk=packets_per_chunk,
             tally_mode=TALLY_MODES[tally], use_graph=int(bool(use_graph)),
-            ctas_per_sm=ctas_per_sm)
+            ctas_per_sm=ctas_per_sm, max_run_chunks=max_run_chunks)
         descs = (_lib.GridDesc * len(self.grids))(*[g.desc() for g in self.grids])
         h = C.c_void_p()
         check(self._L.cmi_create(descs, len(self.grids), C.byref(opts), C.byref(h)))
@@ -181,6 +182,22 @@ class TransportEngine:
         st = (_lib.Stats * (iterations * ninst))()
         check(self._L.cmi_run_iterations(self._h, iterations, int(seed), st))
         return [[st[it * ninst + i].as_dict() for i in range(ninst)] for it in range(iterations)]
+
+    def run_until_converged(self, tolerance, max_iterations=100, min_iterations=2, seed=42):
+        """Iterate until each instance's mean |delta x_H| < tolerance (then it
+        is frozen for the rest of the call).  Returns (stats, converged_at):
+        stats[iteration][instance] dicts and, per instance, the 1-based
+        iteration after which it converged (0: not within max_iterations)."""
+        ninst = len(self.grids)
+        st = (_lib.Stats * (max_iterations * ninst))()
+        done = C.c_int32(0)
+        at = (C.c_int32 * ninst)()
+        check(self._L.cmi_run_until_converged(self._h, int(max_iterations), int(min_iterations),
+                                              float(tolerance), int(seed), st, C.byref(done),
+                                              at))
+        stats = [[st[it * ninst + i].as_dict() for i in range(ninst)]
+                 for it in range(done.value)]
+        return stats, list(at)
 
     def shoot_packets(self, seed=42, iteration=0):
         ninst = len(self.grids)

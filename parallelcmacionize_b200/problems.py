@@ -8,8 +8,9 @@
   mu = ln(mean) - s^2 / 2 so that <n> = mean.
 * ``random_sources`` -- positions uniform in the box, luminosities
   log-uniform between two bounds.
-* ``lognormal_config`` / ``batch_configs`` -- the log-normal plain-method
-  workload and the batched set of uneven instances.
+* ``lognormal_config`` / ``batch_configs`` / ``large_config`` -- the log-normal
+  plain-method workload, the batched set of uneven instances and the large
+  256^3 run.
 * ``stromgren_profile`` -- the semi-analytic neutral-fraction profile and
   Stromgren radius of scripts/plot_neutral_fraction_profile.py:60-82.
 """
@@ -67,10 +68,12 @@ def lognormal_config(ncell=128, num_subgrid=8, num_photon=10_000_000, num_source
 
 
 def batch_configs(count=64, sides=(32, 48, 64, 96, 128), sigma_range=(0.5, 1.5),
-                  max_sources=4, packets_per_cell=5, sub_cells=16, seed=7, alpha=4.0e-19):
+                  max_sources=4, packets_per_cell=5, sub_cells=16, seed=7, alpha=4.0e-19,
+                  select=None):
     """Independent instances of uneven size, density contrast and source count.
 
-    Returns a list of (GridSpec, n_H blocked)."""
+    Returns a list of (GridSpec, n_H blocked); with ``select`` (a set of
+    indices) the density of the other instances is None (not generated)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -81,9 +84,20 @@ def batch_configs(count=64, sides=(32, 48, 64, 96, 128), sigma_range=(0.5, 1.5),
         g = GridSpec(box=BOX_10PC, ncell=(side,) * 3, num_subgrid=(side // sc,) * 3,
                      recombination_rate=alpha, num_photon=packets_per_cell * side ** 3)
         g.sources = random_sources(g.box, nsrc, seed=seed * 1000 + i)
+        if select is not None and i not in select:
+            out.append((g, None))
+            continue
         cube = lognormal_density(side, sigma_ln=s_ln, seed=seed * 1000 + i)
         out.append((g, cube_to_blocked(cube, g.ncell, g.num_subgrid)))
     return out
+
+
+def large_config(ncell=256, num_subgrid=16, num_photon=100_000_000, num_sources=16,
+                 sigma_ln=1.5, seed=42, alpha=4.0e-19):
+    """The large log-normal run: 256^3 as 16^3 subgrids of 16^3, sigma_ln = 1.5,
+    16 sources, 1e8 packets per iteration."""
+    return lognormal_config(ncell=ncell, num_subgrid=num_subgrid, num_photon=num_photon,
+                            num_sources=num_sources, sigma_ln=sigma_ln, seed=seed, alpha=alpha)
 
 
 def stromgren_profile(alpha=4.0e-19, nH=1.0e8, Q=4.26e49, sigma=6.3e-22,

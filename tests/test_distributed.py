@@ -114,3 +114,33 @@ def test_replica_seeds_distinct():
     from parallelcmacionize_b200.distributed import replica_seed
     seeds = {replica_seed(42, r) for r in range(64)}
     assert len(seeds) == 64 and replica_seed(42, 0) == 42
+
+
+def test_shard_instances_balances_and_covers():
+    from parallelcmacionize_b200.distributed import shard_instances
+    from parallelcmacionize_b200.problems import batch_configs
+    cfgs = batch_configs(count=64, select=set())
+    assert all(n is None for _, n in cfgs)
+    costs = [g.num_photon * sum(g.ncell) for g, _ in cfgs]
+    for world in (1, 2, 3, 8):
+        parts = shard_instances(costs, world)
+        assert sorted(i for p in parts for i in p) == list(range(64))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        # longest-processing-time bound: max load <= mean + largest item
+        assert max(loads) <= sum(costs) / world + max(costs)
+    assert shard_instances([5.0, 1.0, 1.0], 2) == [[0], [1, 2]]
+    # the selected densities equal the full generation
+    full = batch_configs(count=6)
+    part = batch_configs(count=6, select={1, 4})
+    for i in range(6):
+        assert full[i][0] == part[i][0]
+        if i in (1, 4):
+            assert np.array_equal(full[i][1], part[i][1])
+        else:
+            assert part[i][1] is None
+
+
+def test_runner_modes():
+    from parallelcmacionize_b200.distributed import ReplicaRunner
+    with pytest.raises(ValueError):
+        ReplicaRunner(None, mode="bogus")

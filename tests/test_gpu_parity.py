@@ -175,6 +175,74 @@ def test_transport_packets_fp32_matches_cpu_spec():
     eng.close()
 
 
+def test_transport_fp32_independent_of_chunking():
+    """The FP32 walk's packet ring (chunks of 32 .. 1024 packets, claimed up
+    to 256 packets ahead of the copies, runs of 1 .. 64 chunks per claim):
+    every chunking traces the same packets, so the counts are identical and J
+    (exact fixed-point sums, merged into FP64 in varying order) agrees to FP64
+    rounding."""
+    spec, nH = lognormal_config(ncell=64, num_subgrid=4, num_photon=400_000, num_sources=3)
+    ref = None
+    for chunk, run in [(128, 0), (32, 0), (64, 0), (64, 1), (256, 8), (1024, 0)]:
+        eng = TransportEngine(spec, precision="fp32", packets_per_chunk=chunk,
+                              max_run_chunks=run)
+        eng.set_fields(0, nH)
+        st = [eng.shoot_packets(seed=9, iteration=i)[0] for i in range(2)]
+        _, J = eng.get_fields(0)
+        eng.close()
+        for s in st:
+            assert s["error_flags"] == 0, (chunk, run)
+            assert s["packets_absorbed"] + s["packets_escaped"] == 400_000
+        key = [(s["cell_crossings"], s["packets_absorbed"], s["subgrid_transits"]) for s in st]
+        if ref is None:
+            ref = (key, J)
+            continue
+        assert key == ref[0], (chunk, run)
+        np.testing.assert_allclose(J, ref[1], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_multi_tile_plan_matches_single_tile(precision):
+    """More than 4096 subgrids in a context: the round plan runs as
+    count / offsets / write over several tiles.  Instance 1's packets (Philox
+    keyed by the instance index) must be traced identically whether instance 0
+    has 4096 subgrids (4160 in all: two plan tiles) or 8 (one tile)."""
+    big, nbig = lognormal_config(ncell=128, num_subgrid=16, num_photon=300_000, num_sources=2,
+                                 seed=3)
+    tiny, ntiny = lognormal_config(ncell=16, num_subgrid=2, num_photon=1000, num_sources=1,
+                                   seed=5)
+    small, nsmall = lognormal_config(ncell=32, num_subgrid=4, num_photon=100_000, num_sources=2,
+                                     seed=4)
+    out = []
+    for first, nfirst in ((big, nbig), (tiny, ntiny)):
+        eng = TransportEngine([first, small], precision=precision)
+        eng.set_fields(0, nfirst)
+        eng.set_fields(1, nsmall)
+        st = [eng.shoot_packets(seed=8, iteration=i) for i in range(2)]
+        for s in st:
+            for k in s:
+                assert k["error_flags"] == 0
+                assert k["packets_absorbed"] + k["packets_escaped"] == k["packets_emitted"]
+        out.append(([(s[1]["cell_crossings"], s[1]["packets_absorbed"], s[1]["subgrid_transits"])
+                     for s in st], eng.get_fields(1)[1]))
+        eng.close()
+    assert out[0][0] == out[1][0]
+    np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-12, atol=0)
+
+
+def test_oversized_packet_ring_is_refused():
+    """Two 4096-packet chunks (256 KB) do not fit in a CTA's shared memory:
+    creation fails with NOT_SUPPORTED and the next context works."""
+    spec, nH = lognormal_config(ncell=32, num_subgrid=2, num_photon=10_000, num_sources=1)
+    with pytest.raises(CMIError) as e:
+        TransportEngine(spec, precision="fp32", packets_per_chunk=4096)
+    assert "shared memory" in str(e.value)
+    eng = TransportEngine(spec, precision="fp32")
+    eng.set_fields(0, nH)
+    assert eng.run_iterations(1, seed=1)[0][0]["error_flags"] == 0
+    eng.close()
+
+
 def test_balance_reference_form_bit_exact():
     g = golden("balance.npz")
     spec = GridSpec(box=tuple(g["box"]), ncell=tuple(int(v) for v in g["ncell"]),
