@@ -356,14 +356,22 @@ WalkParams walk_params(cmi_context *c) {
   return p;
 }
 
-// the fixed-point default is built for 4 resident CTAs per SM (<= 64 registers)
+// the fixed-point default is built for 4 resident CTAs per SM (<= 64
+// registers); ctas_per_sm = 3 selects a build for 3 (<= 85 registers)
 template <int kTally>
 constexpr int walk32_min_blocks() { return kTally == 2 ? 4 : 1; }
 
+bool walk32_three_per_sm(const cmi_context *c) {
+  return c->opt.tally_mode == CMI_TALLY_FIXED64 && c->opt.ctas_per_sm == 3;
+}
+
 template <int kTally>
 void launch_walk32_t(cmi_context *c, const WalkParams &p) {
-  k_walk32<kWalkThreads, kTally, walk32_min_blocks<kTally>()>
-      <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+  if (kTally == 2 && walk32_three_per_sm(c))
+    k_walk32<kWalkThreads, 2, 3><<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+  else
+    k_walk32<kWalkThreads, kTally, walk32_min_blocks<kTally>()>
+        <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
 }
 
 int launch_walk(cmi_context *c) {
@@ -417,7 +425,9 @@ int config_walk(cmi_context *c) {
     switch (tm) {
       case 0: return config_kernel(c, k_walk32<kWalkThreads, 0, walk32_min_blocks<0>()>);
       case 1: return config_kernel(c, k_walk32<kWalkThreads, 1, walk32_min_blocks<1>()>);
-      case 2: return config_kernel(c, k_walk32<kWalkThreads, 2, walk32_min_blocks<2>()>);
+      case 2:
+        return walk32_three_per_sm(c) ? config_kernel(c, k_walk32<kWalkThreads, 2, 3>)
+                                      : config_kernel(c, k_walk32<kWalkThreads, 2, 4>);
       default: return config_kernel(c, k_walk32<kWalkThreads, 3, walk32_min_blocks<3>()>);
     }
   }

@@ -1215,7 +1215,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
             float len;
             status = w.step(v, tcell, len);
             tally.add(tcell, len);
-            ++c_cross;
             if (status == kRun && w.steps > limit) status = kDrop;
           }
         }
@@ -1225,6 +1224,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
           bool append = false;
           if (fin) {
             ++c_trans;
+            c_cross += (uint32_t)w.steps;  // one step per crossed cell
             if (status == kExited) {
               const int od = sh.tab.mask_dir[w.exit_mask(v)];
               if (od >= kNumDirections) {

@@ -120,12 +120,20 @@ struct View64 {
 // FP32 cell-unit walk
 // ----------------------------------------------------------------------------
 struct Walk32 {
-  float p[3], d[3], inv[3], dcs[3];
+  // Per axis the packet looks only at the cell face ahead of it (direction
+  // of travel): face = idx + 1 for d > 0, idx for d < 0, +inf for d == 0.
+  // The path length to it is l = (face - p) * inv with inv = cs / d, the same
+  // operands and roundings as (hi - p) * inv / (lo - p) * inv of the
+  // reference loop, so the walk is unchanged; the per-axis branches, the
+  // integer index and the cell-index recomputation of each step are gone.
+  float p[3], d[3], face[3], inv[3], dcs[3];
+  float fstep[3];  // +1 / -1: the face after the next one
+  float fexit[3];  // the face whose crossing leaves the subgrid (n or 0)
+  int cstep[3];    // cell-index change when the face is crossed
   float tau_done, tau_target;
-  float fidx[3];  // idx as float (exact): the cell faces without conversions
-  int idx[3];
   int cell;
   int steps;
+  int exited;      // exit: bit a set when axis a left the subgrid
 
   // Entry: DensitySubGrid.hpp:1186-1219 (start index per get_start_index).
   // inv = cell_size * (1/d) and dcs = d * (1/cell_size): correctly rounded
@@ -133,68 +141,83 @@ struct Walk32 {
   __device__ __forceinline__ int begin(const Packet32 &pk, const View32 &v,
                                       const uint8_t *sign_code) {
     const uint8_t code = sign_code[pk.meta & 31u];
+    const int stride[3] = {v.nyz, v.n[2], 1};
+    int idx[3];
+    bool inside = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       p[a] = pk.pos[a];
       d[a] = pk.dir[a];
       dcs[a] = __fmul_rn(d[a], v.inv_cs[a]);
-      inv[a] = __fmul_rn(v.cs[a], __frcp_rn(d[a]));
       const int s = sign_of(code, a);
       idx[a] = (s == 0) ? __float2int_rz(p[a]) : ((s < 0) ? 0 : v.n[a] - 1);
-      fidx[a] = (float)idx[a];
+      inside = inside && idx[a] >= 0 && idx[a] < v.n[a];
+      const bool up = d[a] > 0.f;
+      const bool moving = up || d[a] < 0.f;
+      inv[a] = moving ? __fmul_rn(v.cs[a], __frcp_rn(d[a])) : __int_as_float(0x7f800000);
+      face[a] = moving ? (float)(up ? idx[a] + 1 : idx[a]) : __int_as_float(0x7f800000);
+      fstep[a] = up ? 1.f : -1.f;
+      fexit[a] = up ? (float)v.n[a] : 0.f;
+      cstep[a] = up ? stride[a] : -stride[a];
     }
-    cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
+    cell = idx[0] * stride[0] + idx[1] * stride[1] + idx[2];
     tau_done = 0.f;
     tau_target = pk.tau;
     steps = 0;
+    exited = 0;
     if (!(tau_done < tau_target)) return kAbsorbed;
-    return inside(v) ? kRun : kExited;
-  }
-
-  __device__ __forceinline__ bool inside(const View32 &v) const {
-    return idx[0] < v.n[0] && idx[0] >= 0 && idx[1] < v.n[1] && idx[1] >= 0 &&
-           idx[2] < v.n[2] && idx[2] >= 0;
+    if (!inside) {
+      // entered outside the index range (position on or beyond a face)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (idx[a] < 0 || idx[a] >= v.n[a]) {
+          exited |= 1 << a;
+          // the side it left through, for exit_mask
+          fstep[a] = idx[a] < 0 ? -1.f : 1.f;
+        }
+      }
+      return kExited;
+    }
+    return kRun;
   }
 
   // One iteration of the loop at DensitySubGrid.hpp:1221-1305; the path
   // length lmin of the crossed cell `tally_cell` is returned for the tally.
   __device__ __forceinline__ int step(const View32 &v, int &tally_cell, float &lmin_out) {
-    float lo[3], hi[3], l[3];
+    float l[3];
     const float k = v.kappa[cell];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = fidx[a];
-      hi[a] = __fadd_rn(fidx[a], 1.f);
-      l[a] = (d[a] > 0.f)   ? __fmul_rn(__fsub_rn(hi[a], p[a]), inv[a])
-             : (d[a] < 0.f) ? __fmul_rn(__fsub_rn(lo[a], p[a]), inv[a])
-                            : FLT_MAX;
-    }
+    for (int a = 0; a < 3; ++a) l[a] = __fmul_rn(__fsub_rn(face[a], p[a]), inv[a]);
     float lmin = min_ref(l[0], min_ref(l[1], l[2]));
     const float tau = __fmul_rn(lmin, k);
     tau_done = __fadd_rn(tau_done, tau);
-    const bool absorbed = tau_done >= tau_target;
-    if (absorbed) {
+    tally_cell = cell;
+    ++steps;
+    if (tau_done >= tau_target) {
       const float corr = __fdiv_rn(__fsub_rn(tau_done, tau_target), tau);
       lmin = __fmul_rn(lmin, __fsub_rn(1.f, corr));
-    } else {
+      lmin_out = lmin;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        if (l[a] == lmin) {
-          idx[a] += (d[a] > 0.f) ? 1 : -1;
-          fidx[a] = (d[a] > 0.f) ? hi[a] : __fsub_rn(lo[a], 1.f);
-        }
-      }
+      for (int a = 0; a < 3; ++a)
+        p[a] = (l[a] == lmin) ? face[a] : __fmaf_rn(lmin, dcs[a], p[a]);
+      return kAbsorbed;
     }
-    tally_cell = cell;
     lmin_out = lmin;
+    int out = 0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      p[a] = (l[a] == lmin) ? ((d[a] > 0.f) ? hi[a] : lo[a]) : __fmaf_rn(lmin, dcs[a], p[a]);
+      const bool cross = l[a] == lmin;
+      p[a] = cross ? face[a] : __fmaf_rn(lmin, dcs[a], p[a]);
+      if (cross) {
+        out |= (face[a] == fexit[a]) ? (1 << a) : 0;
+        face[a] = __fadd_rn(face[a], fstep[a]);
+        cell += cstep[a];
+      }
     }
-    ++steps;
-    if (absorbed) return kAbsorbed;
-    if (!inside(v)) return kExited;
-    cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
+    if (out) {
+      exited = out;
+      return kExited;
+    }
     return kRun;
   }
 
@@ -205,16 +228,12 @@ struct Walk32 {
     int mask = 0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      // (idx / n) > 0 of the reference; idx is in [-1, n] here
-      const int low = idx[a] < 0;
-      const int high = idx[a] >= v.n[a];
-      mask |= (high << (5 - 2 * a)) | (low << (4 - 2 * a));
+      if (!((exited >> a) & 1)) continue;
+      const bool high = fstep[a] > 0.f;
+      mask |= high ? (1 << (5 - 2 * a)) : (1 << (4 - 2 * a));
       if (reanchor) {
-        if (high) {
-          p[a] = __fsub_rn(p[a], __int2float_rn(v.n[a]));
-        } else if (low) {
-          p[a] = __fadd_rn(p[a], __int2float_rn(v.n[a]));
-        }
+        p[a] = high ? __fsub_rn(p[a], __int2float_rn(v.n[a]))
+                    : __fadd_rn(p[a], __int2float_rn(v.n[a]));
       }
     }
     return mask;
