@@ -286,6 +286,83 @@ int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
                                 const uint8_t *output_enabled, cmi_photon *d_out,
                                 uint32_t *d_out_count, uint32_t *d_num_done, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start.  No reference counterpart: the reference starts every
+ * run from x_H = 1e-6 (DensitySubGrid.hpp:544-551).  A 3-level 3D
+ * convolutional U-Net maps two input channels per cell, [log10 n_H, log10 of
+ * the source flux sum_i L_i / (4 pi r_i^2)] (normalised), to log10 x_H; the
+ * plain iteration then starts from that field and still decides convergence.
+ *
+ * Layers (c1, c2, c3 channels per level; 3x3x3 convolutions, zero padding,
+ * leaky ReLU; 2x2x2 average pooling down, nearest-neighbour upsampling up,
+ * skip connections concatenated after the upsampled channels):
+ *   level 1: conv(2 -> c1), conv(c1 -> c1)      pooled to level 2
+ *   level 2: conv(c1 -> c2), conv(c2 -> c2)     pooled to level 3
+ *   level 3: conv(c2 -> c3), conv(c3 -> c3)     upsampled to level 2
+ *   level 2: conv(c3 + c2 -> c2), conv(c2 -> c2) upsampled to level 1
+ *   level 1: conv(c2 + c1 -> c1), conv(c1 -> c1), 1x1 conv(c1 -> 1)
+ * Parameters (FP32 master copy, in this order per convolution): W[co][tap][ci]
+ * with tap = (dz * 3 + dy) * 3 + dx, then b[co]; last the head's w[c1], b.
+ * Weights and activations are BF16, accumulation FP32; the 3x3x3
+ * convolutions and their input gradients run on the tensor cores (tcgen05),
+ * the weight gradients on CUDA cores.  Training minimises the mean squared
+ * error of log10 x_H with Adam.
+ *
+ * Tensors handed to the network live in device memory, FP32, one sample
+ * after another in the engine's cube order (index (ix * ny + iy) * nz + iz):
+ * features [batch][cells][2], targets and predictions [batch][cells].  Grid
+ * sides must be multiples of 32.  Calls are synchronous.  Errors: the codes
+ * above, message in cmi_unet_last_error_string(). */
+typedef struct cmi_unet cmi_unet;
+typedef struct {
+  int32_t channels[3];  /* c1 (<= 16), c2, c3 (<= 64); default 12, 24, 48 (~2e5 parameters) */
+  float leaky_slope;    /* default 0.1 */
+  int32_t device;
+  int32_t reserved[8];
+} cmi_unet_config;
+
+void cmi_unet_default_config(cmi_unet_config *config);
+const char *cmi_unet_last_error_string(void);
+int cmi_unet_create(const cmi_unet_config *config, cmi_unet **net);
+int cmi_unet_destroy(cmi_unet *net);
+int cmi_unet_num_params(cmi_unet *net, int64_t *count);
+/* FP32 parameters to / from host memory (set also resets the optimiser) */
+int cmi_unet_get_params(cmi_unet *net, float *params);
+int cmi_unet_set_params(cmi_unet *net, const float *params);
+/* predictions of log10 x_H */
+int cmi_unet_forward(cmi_unet *net, const float *features, float *prediction, int32_t batch,
+                     const int32_t dims[3]);
+/* forward + backward without an update: mean squared error and the gradient
+ * of every parameter (host array, num_params entries; may be NULL) */
+int cmi_unet_gradients(cmi_unet *net, const float *features, const float *target, int32_t batch,
+                       const int32_t dims[3], float *loss, float *gradients);
+/* one Adam step (beta 0.9, 0.999, eps 1e-8) at learning rate lr */
+int cmi_unet_train_step(cmi_unet *net, const float *features, const float *target, int32_t batch,
+                        const int32_t dims[3], float lr, float *loss);
+/* features of one grid from its FP64 n_H (device, cube order) and sources
+ * (host, [x, y, z, L] each); norm = {n_mean, n_scale, f_mean, f_scale}:
+ * channel 0 = (log10 n_H - n_mean) / n_scale, channel 1 = (log10 flux -
+ * f_mean) / f_scale with r clamped to half a cell */
+int cmi_unet_features(cmi_unet *net, const double *nH_cube, const int32_t dims[3],
+                      const double box[6], const double *sources, int32_t num_sources,
+                      const float norm[4], float *features);
+/* x_H = 10^clamp(prediction, log10_min, 0) as FP64 (device), n values */
+int cmi_unet_to_neutral_fraction(cmi_unet *net, const float *prediction, double *xH, int64_t n,
+                                 float log10_min);
+/* Building blocks, exposed for testing: one 3x3x3 convolution on the tensor
+ * cores (BF16 channels-last device tensors, channel counts multiples of 16,
+ * weights packed by cmi_unet_pack_weights, bias FP32 or NULL, activation 1 =
+ * leaky ReLU); packing of FP32 W[cout][27][cin] (flip = 1: the input-gradient
+ * form); the weight gradient dW[cout][27][cin] (FP32, device) of a
+ * convolution from its input x and output gradient dy. */
+int cmi_unet_conv3(cmi_unet *net, const void *in, int32_t in_channels, const void *weights_packed,
+                   const float *bias, void *out, int32_t out_channels, int32_t activation,
+                   int32_t batch, const int32_t dims[3]);
+int cmi_unet_pack_weights(cmi_unet *net, const float *weights, int32_t cout, int32_t cin,
+                          int32_t flip, void *packed);
+int cmi_unet_conv3_wgrad(cmi_unet *net, const void *x, int32_t cin, const void *dy, int32_t cout,
+                         int32_t batch, const int32_t dims[3], float *dw);
+
 #ifdef __cplusplus
 }
 #endif

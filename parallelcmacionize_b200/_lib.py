@@ -51,6 +51,12 @@ EXPORTED = [
     "cmi_compute_neutral_fraction", "cmi_device_field", "cmi_get_stream", "cmi_synchronize",
     "cmi_last_launch_count", "cmi_set_kernel_timing", "cmi_kernel_timing",
     "cmi_compute_neutral_fraction_subgrids", "cmi_traverse_buffer_noalloc",
+    # learned warm start
+    "cmi_unet_default_config", "cmi_unet_last_error_string", "cmi_unet_create",
+    "cmi_unet_destroy", "cmi_unet_num_params", "cmi_unet_get_params", "cmi_unet_set_params",
+    "cmi_unet_forward", "cmi_unet_gradients", "cmi_unet_train_step", "cmi_unet_features",
+    "cmi_unet_to_neutral_fraction", "cmi_unet_conv3", "cmi_unet_pack_weights",
+    "cmi_unet_conv3_wgrad",
 ]
 
 PHOTON_DTYPE = np.dtype(
@@ -110,6 +116,15 @@ class Stats(C.Structure):
                 for k, _ in self._fields_}
 
 
+class UNetConfig(C.Structure):
+    _fields_ = [
+        ("channels", C.c_int32 * 3),
+        ("leaky_slope", C.c_float),
+        ("device", C.c_int32),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
 class CMIError(RuntimeError):
     """A library call returned a non-zero status."""
 
@@ -159,6 +174,23 @@ def load():
     L.cmi_last_launch_count.argtypes = [ctx, C.POINTER(u64)]
     L.cmi_set_kernel_timing.argtypes = [ctx, i32]
     L.cmi_kernel_timing.argtypes = [ctx, vp, vp]
+    f32, i64 = C.c_float, C.c_int64
+    L.cmi_unet_default_config.argtypes = [C.POINTER(UNetConfig)]
+    L.cmi_unet_default_config.restype = None
+    L.cmi_unet_last_error_string.restype = C.c_char_p
+    L.cmi_unet_create.argtypes = [C.POINTER(UNetConfig), C.POINTER(vp)]
+    L.cmi_unet_destroy.argtypes = [vp]
+    L.cmi_unet_num_params.argtypes = [vp, C.POINTER(i64)]
+    L.cmi_unet_get_params.argtypes = [vp, vp]
+    L.cmi_unet_set_params.argtypes = [vp, vp]
+    L.cmi_unet_forward.argtypes = [vp, vp, vp, i32, vp]
+    L.cmi_unet_gradients.argtypes = [vp, vp, vp, i32, vp, C.POINTER(f32), vp]
+    L.cmi_unet_train_step.argtypes = [vp, vp, vp, i32, vp, f32, C.POINTER(f32)]
+    L.cmi_unet_features.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp]
+    L.cmi_unet_to_neutral_fraction.argtypes = [vp, vp, vp, i64, f32]
+    L.cmi_unet_conv3.argtypes = [vp, vp, i32, vp, vp, vp, i32, i32, i32, vp]
+    L.cmi_unet_pack_weights.argtypes = [vp, vp, i32, i32, i32, vp]
+    L.cmi_unet_conv3_wgrad.argtypes = [vp, vp, i32, vp, i32, i32, vp, vp]
     for name in EXPORTED:
         f = getattr(L, name)
         if f.restype is C.c_int and name not in ("cmi_abi_version",):
@@ -170,6 +202,13 @@ def load():
 def check(rc):
     if rc != OK:
         msg = load().cmi_last_error_string()
+        raise CMIError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def check_unet(rc):
+    if rc != OK:
+        msg = load().cmi_unet_last_error_string()
         raise CMIError(rc, msg.decode() if msg else "")
     return rc
 

@@ -49,6 +49,7 @@ int fail(int code, const char *fmt, ...) {
   } while (0)
 
 constexpr int kWalkThreads = 256;
+constexpr int kSpareRounds = 3;  // wavefront rounds beyond the straight-line bound
 
 struct HostInstance {
   cmi_grid_desc desc;
@@ -750,7 +751,10 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
       c->h_sub.push_back(S);
     }
     c->max_padded = std::max(c->max_padded, I.padded_per_sub);
-    c->rounds = std::max(c->rounds, ns[0] + ns[1] + ns[2] - 2);
+    // a straight path visits at most ns[0] + ns[1] + ns[2] - 2 subgrids; a
+    // packet whose position rounds exactly onto a face of a neighbouring
+    // subgrid makes one extra transit that crosses no cell, hence the spares
+    c->rounds = std::max(c->rounds, ns[0] + ns[1] + ns[2] - 2 + kSpareRounds);
     c->inst.push_back(I);
   }
   c->S = (uint32_t)c->h_sub.size();

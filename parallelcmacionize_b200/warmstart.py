@@ -1,0 +1,473 @@
+"""Learned warm start for the plain method (no reference counterpart).
+
+The reference starts every photoionization run from x_H = 1e-6 everywhere
+(DensitySubGrid.hpp:544-551) and iterates.  Here a small 3D convolutional
+U-Net (the CUDA library's cmi_unet_*: BF16 tensor-core convolutions with FP32
+accumulation, trained by the library's own backward kernels) predicts log10
+x_H from [log10 n_H, log10 of the source flux sum_i L_i / (4 pi r_i^2)], and
+the plain iteration starts from that field.  The Monte Carlo iteration still
+decides convergence (cmi_run_until_converged); the network only chooses where
+it starts, so a bad prediction costs iterations, never correctness.
+
+* ``UNet``             -- the network (create, parameters, forward,
+  gradients, Adam step, features, save / load).
+* ``generate_runs``    -- training data: batched plain-method runs of the
+  log-normal generator, iterated to convergence; the label is log10 of x_H
+  averaged over the last iterations (less Monte Carlo noise).
+* ``train``            -- Adam on mean squared error of log10 x_H.
+* ``warm_start``       -- features -> prediction -> x_H of an engine instance.
+* ``time_to_converge`` -- iterations and wall time to convergence from the
+  plain start and from the warm start, on the same inputs.
+
+Device memory is handled with torch tensors (CUDA); the arithmetic is the
+library's.  Run ``python -m parallelcmacionize_b200.warmstart --help`` for the
+training pipeline that produced the shipped weights.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check_unet
+
+# log10 x_H below this is not predicted (the plain start is 1e-6)
+LOG10_XH_MIN = -8.0
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
+                               "warmstart_unet64.npz")
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _dims(ncell):
+    n = tuple(int(v) for v in ncell)
+    return (C.c_int32 * 3)(n[2], n[1], n[0])  # network X = iz (fastest), Z = ix
+
+
+class UNet:
+    """The warm-start network on one GPU."""
+
+    def __init__(self, channels=(12, 24, 48), slope=0.1, device=0, seed=0):
+        self._L = _lib.load()
+        cfg = _lib.UNetConfig()
+        self._L.cmi_unet_default_config(C.byref(cfg))
+        for k in range(3):
+            cfg.channels[k] = int(channels[k])
+        cfg.leaky_slope = float(slope)
+        cfg.device = int(device)
+        h = C.c_void_p()
+        check_unet(self._L.cmi_unet_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.channels = tuple(int(c) for c in channels)
+        self.slope = float(slope)
+        self.device = int(device)
+        n = C.c_int64()
+        check_unet(self._L.cmi_unet_num_params(self._h, C.byref(n)))
+        self.num_params = int(n.value)
+        # feature normalisation: (n_mean, n_scale, f_mean, f_scale)
+        self.norm = np.array([8.0, 1.0, 13.0, 1.5], dtype=np.float32)
+        self.set_params(self.initial_params(seed))
+
+    # ---- lifetime ----
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cmi_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- parameters ----
+    def layer_shapes(self):
+        c1, c2, c3 = self.channels
+        convs = [(c1, 2), (c1, c1), (c2, c1), (c2, c2), (c3, c2), (c3, c3), (c2, c3 + c2),
+                 (c2, c2), (c1, c2 + c1), (c1, c1)]
+        return convs
+
+    def initial_params(self, seed=0):
+        """He-normal convolution weights, zero biases."""
+        rng = np.random.default_rng(seed)
+        parts = []
+        for cout, cin in self.layer_shapes():
+            parts.append(rng.normal(0.0, np.sqrt(2.0 / (27 * cin)), cout * 27 * cin))
+            parts.append(np.zeros(cout))
+        c1 = self.channels[0]
+        parts.append(rng.normal(0.0, np.sqrt(1.0 / c1), c1))
+        parts.append(np.zeros(1))
+        p = np.concatenate(parts).astype(np.float32)
+        assert p.size == self.num_params
+        return p
+
+    def get_params(self):
+        p = np.empty(self.num_params, dtype=np.float32)
+        check_unet(self._L.cmi_unet_get_params(self._h, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.num_params:
+            raise ValueError(f"expected {self.num_params} parameters, got {p.size}")
+        check_unet(self._L.cmi_unet_set_params(self._h, p.ctypes.data))
+
+    def save(self, path, **meta):
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        np.savez_compressed(path, params=self.get_params(), channels=np.array(self.channels),
+                            slope=np.array(self.slope), norm=self.norm,
+                            **{k: np.asarray(v) for k, v in meta.items()})
+
+    @classmethod
+    def load(cls, path=DEFAULT_WEIGHTS, device=0):
+        d = np.load(path)
+        net = cls(channels=tuple(int(c) for c in d["channels"]), slope=float(d["slope"]),
+                  device=device)
+        net.set_params(d["params"])
+        net.norm = d["norm"].astype(np.float32)
+        net.meta = {k: d[k] for k in d.files if k not in ("params", "channels", "slope", "norm")}
+        return net
+
+    # ---- compute (torch CUDA tensors, float32, cube order) ----
+    # The library runs on its own stream and returns when that stream is done;
+    # inputs written by torch (its own stream) are made complete first.
+    def _sync(self):
+        import torch
+        torch.cuda.synchronize(self.device)
+
+    def forward(self, features, ncell):
+        """features [B, cells, 2] -> predicted log10 x_H [B, cells]."""
+        import torch
+        self._sync()
+        B = features.shape[0]
+        pred = torch.empty(features.shape[:2], dtype=torch.float32, device=features.device)
+        check_unet(self._L.cmi_unet_forward(self._h, _ptr(features), _ptr(pred), B,
+                                            _dims(ncell)))
+        return pred
+
+    def gradients(self, features, target, ncell):
+        """(loss, gradient of every parameter) without an update."""
+        self._sync()
+        g = np.empty(self.num_params, dtype=np.float32)
+        loss = C.c_float()
+        check_unet(self._L.cmi_unet_gradients(self._h, _ptr(features), _ptr(target),
+                                              features.shape[0], _dims(ncell), C.byref(loss),
+                                              g.ctypes.data))
+        return float(loss.value), g
+
+    def train_step(self, features, target, ncell, lr):
+        self._sync()
+        loss = C.c_float()
+        check_unet(self._L.cmi_unet_train_step(self._h, _ptr(features), _ptr(target),
+                                               features.shape[0], _dims(ncell), float(lr),
+                                               C.byref(loss)))
+        return float(loss.value)
+
+    def features(self, nH_cube, grid, out=None):
+        """Features [cells, 2] of one grid from its FP64 n_H (torch, device,
+        cube order) and the GridSpec's box and sources."""
+        import torch
+        self._sync()
+        n = int(np.prod(grid.ncell))
+        if out is None:
+            out = torch.empty((n, 2), dtype=torch.float32, device=nH_cube.device)
+        dims = (C.c_int32 * 3)(*[int(v) for v in grid.ncell])
+        box = np.ascontiguousarray(grid.box, dtype=np.float64)
+        src = np.ascontiguousarray(np.asarray(grid.sources, dtype=np.float64).reshape(-1, 4))
+        norm = np.ascontiguousarray(self.norm, dtype=np.float32)
+        check_unet(self._L.cmi_unet_features(self._h, _ptr(nH_cube), dims, box.ctypes.data,
+                                             src.ctypes.data, src.shape[0], norm.ctypes.data,
+                                             _ptr(out)))
+        return out
+
+    def to_neutral_fraction(self, pred, log10_min=LOG10_XH_MIN):
+        import torch
+        self._sync()
+        x = torch.empty(pred.numel(), dtype=torch.float64, device=pred.device)
+        check_unet(self._L.cmi_unet_to_neutral_fraction(self._h, _ptr(pred), _ptr(x),
+                                                        pred.numel(), float(log10_min)))
+        return x
+
+    def fit_normalisation(self, nH_cubes, grids):
+        """Feature means / scales from a set of grids (host arithmetic)."""
+        ln, lf = [], []
+        for n, g in zip(nH_cubes, grids):
+            ln.append(np.log10(n).ravel())
+            lf.append(flux_proxy(g).ravel())
+        ln, lf = np.concatenate(ln), np.concatenate(lf)
+        self.norm = np.array([ln.mean(), ln.std() + 1e-6, lf.mean(), lf.std() + 1e-6],
+                             dtype=np.float32)
+
+
+def flux_proxy(grid):
+    """log10 sum_i L_i / (4 pi r_i^2) at the cell centres (cube order), r
+    clamped to half a cell; the same quantity the features kernel computes."""
+    box = np.asarray(grid.box, dtype=np.float64)
+    n = tuple(int(v) for v in grid.ncell)
+    cell = box[3:] / np.array(n)
+    axes = [box[a] + (np.arange(n[a]) + 0.5) * cell[a] for a in range(3)]
+    X, Y, Z = np.meshgrid(*axes, indexing="ij")
+    flux = np.zeros(n)
+    rmin = 0.5 * cell.min()
+    for s in np.asarray(grid.sources, dtype=np.float64).reshape(-1, 4):
+        r = np.maximum(np.sqrt((X - s[0]) ** 2 + (Y - s[1]) ** 2 + (Z - s[2]) ** 2), rmin)
+        flux += s[3] / (4.0 * np.pi * r ** 2)
+    return np.log10(np.maximum(flux, 1e-300))
+
+
+# ---------------------------------------------------------------------------
+# training data from the plain method
+# ---------------------------------------------------------------------------
+def run_configs(seeds, ncell=64, packets_per_cell=5, num_sources=4, sigma_ln=1.0):
+    """Log-normal plain-method configurations (64^3 as 4^3 subgrids of 16^3)."""
+    from .problems import lognormal_config
+    out = []
+    for s in seeds:
+        g, nH = lognormal_config(ncell=ncell, num_subgrid=ncell // 16,
+                                 num_photon=int(round(packets_per_cell * ncell ** 3)),
+                                 num_sources=num_sources, sigma_ln=sigma_ln, seed=int(s))
+        out.append((g, nH))
+    return out
+
+
+def generate_runs(seeds, ncell=64, packets_per_cell=5, iterations=24, average=6, batch=64,
+                  device=0, log=None):
+    """Plain-method runs from x_H = 1e-6, ``batch`` instances per context,
+    ``iterations`` iterations each (well past convergence); the label is log10
+    of x_H averaged over the last ``average`` iterations (less Monte Carlo
+    noise).
+
+    Returns (grids, nH cubes [N, n, n, n], labels log10 x_H [N, n, n, n]
+    float32, dx [iterations, N]: the mean |delta x_H| of every iteration)."""
+    from .engine import TransportEngine, blocked_to_cube
+    grids, cubes, labels, dxs = [], [], [], []
+    seeds = list(seeds)
+    for b0 in range(0, len(seeds), batch):
+        cfgs = run_configs(seeds[b0: b0 + batch], ncell, packets_per_cell)
+        specs = [g for g, _ in cfgs]
+        t0 = time.perf_counter()
+        with TransportEngine(specs, precision="fp32", device=device) as eng:
+            for i, (_, nH) in enumerate(cfgs):
+                eng.set_fields(i, nH)
+            st = eng.run_iterations(iterations - average, seed=1000 + b0)
+            acc = [np.zeros(int(np.prod(g.ncell))) for g in specs]
+            for k in range(average):
+                st += eng.run_iterations(1, seed=5000 + b0 + k)
+                for i in range(len(specs)):
+                    acc[i] += eng.get_fields(i, layout="cube", intensity=False)[0]
+        dxs.append(np.array([[s[i]["mean_abs_dx"] for i in range(len(specs))] for s in st]))
+        for i, (g, nH) in enumerate(cfgs):
+            grids.append(g)
+            cubes.append(blocked_to_cube(nH, g.ncell, g.num_subgrid).astype(np.float64))
+            x = np.maximum(acc[i] / average, 10.0 ** LOG10_XH_MIN)
+            labels.append(np.log10(x).reshape(g.ncell).astype(np.float32))
+        if log:
+            log(f"runs {b0}-{b0 + len(cfgs) - 1}: {time.perf_counter() - t0:.1f} s; mean "
+                f"|dx| per iteration {np.round(dxs[-1].mean(axis=1), 4).tolist()}")
+    return grids, np.stack(cubes), np.stack(labels), np.concatenate(dxs, axis=1)
+
+
+def iterations_to_tolerance(dx, tolerance, min_iterations=2):
+    """First iteration (1-based) >= min_iterations whose mean |dx| < tolerance,
+    per run (0: never), from a [iterations, runs] array."""
+    ok = dx < tolerance
+    ok[: min_iterations - 1] = False
+    first = np.argmax(ok, axis=0) + 1
+    return np.where(ok.any(axis=0), first, 0)
+
+
+def build_features(net, grids, cubes):
+    """Features of every run on the GPU: torch [N, cells, 2]."""
+    import torch
+    n = int(np.prod(grids[0].ncell))
+    out = torch.empty((len(grids), n, 2), dtype=torch.float32, device=f"cuda:{net.device}")
+    for i, (g, c) in enumerate(zip(grids, cubes)):
+        nH = torch.from_numpy(np.ascontiguousarray(c).ravel()).to(out.device)
+        net.features(nH, g, out=out[i])
+    return out
+
+
+def train(net, feats, labels, ncell, epochs=10, batch=8, lr=2e-3, lr_final=2e-4, seed=0,
+          log=None):
+    """Adam over shuffled mini-batches, learning rate decaying geometrically
+    from lr to lr_final.  feats [N, cells, 2], labels [N, cells] (torch)."""
+    import torch
+    N = feats.shape[0]
+    rng = np.random.default_rng(seed)
+    steps = epochs * (N // batch)
+    history = []
+    k = 0
+    t0 = time.perf_counter()
+    for ep in range(epochs):
+        order = rng.permutation(N)
+        losses = []
+        for b in range(N // batch):
+            idx = torch.from_numpy(order[b * batch:(b + 1) * batch]).to(feats.device)
+            f = feats.index_select(0, idx).contiguous()
+            t = labels.index_select(0, idx).contiguous()
+            rate = lr * (lr_final / lr) ** (k / max(1, steps - 1))
+            losses.append(net.train_step(f, t, ncell, rate))
+            k += 1
+        history.append(float(np.mean(losses)))
+        if log:
+            log(f"epoch {ep}: loss {history[-1]:.5f} ({time.perf_counter() - t0:.1f} s)")
+    return history
+
+
+def evaluate_loss(net, feats, labels, ncell, batch=8):
+    import torch
+    tot, n = 0.0, 0
+    with torch.no_grad():
+        for b in range(0, feats.shape[0], batch):
+            f = feats[b: b + batch].contiguous()
+            p = net.forward(f, ncell)
+            tot += float(((p - labels[b: b + batch]) ** 2).sum())
+            n += p.numel()
+    return tot / n
+
+
+# ---------------------------------------------------------------------------
+# warm start and the convergence comparison
+# ---------------------------------------------------------------------------
+def warm_start(net, engine, instance, nH_cube, log10_min=LOG10_XH_MIN):
+    """Predict x_H for an engine instance and load it (cube order)."""
+    import torch
+    grid = engine.grids[instance]
+    dev = f"cuda:{net.device}"
+    nH = torch.from_numpy(np.ascontiguousarray(nH_cube, dtype=np.float64).ravel()).to(dev)
+    f = net.features(nH, grid).unsqueeze(0).contiguous()
+    pred = net.forward(f, grid.ncell)
+    x = net.to_neutral_fraction(pred, log10_min)
+    torch.cuda.synchronize(dev)
+    engine.set_fields_device(instance, 0, x.data_ptr(), layout="cube")
+    return x
+
+
+def time_to_converge(net, grid, nH_blocked, x_reference=None, tolerance=0.01,
+                     max_iterations=60, seed=7, device=0):
+    """Iterations and wall time (s) to convergence (mean |delta x_H| <
+    tolerance, cmi_run_until_converged) from x_H = 1e-6 and from the warm
+    start, same grid and packet seed.  Wall time covers the features, the
+    network and the iterations, with n_H already on the device and both paths
+    warmed up (graph capture, network buffers).  With ``x_reference`` (cube
+    order) also the mean |x - x_reference| of each converged field; always the
+    mean |x_plain - x_warm|."""
+    import torch
+    from .engine import TransportEngine, blocked_to_cube
+    cube = blocked_to_cube(nH_blocked, grid.ncell, grid.num_subgrid)
+    out = {}
+    fields = {}
+    for mode in ("plain", "warm"):
+        with TransportEngine(grid, precision="fp32", device=device) as eng:
+            eng.set_fields(0, nH_blocked, np.full(nH_blocked.size, 1e-6))
+            eng.run_iterations(1, seed=99)  # warm-up: graph capture, first touch
+            if mode == "warm":
+                warm_start(net, eng, 0, cube)  # warm-up of the network path
+            eng.set_fields(0, None, np.full(nH_blocked.size, 1e-6))
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            if mode == "warm":
+                warm_start(net, eng, 0, cube)
+            stats, at = eng.run_until_converged(tolerance, max_iterations=max_iterations,
+                                                min_iterations=2, seed=seed)
+            eng.synchronize()
+            dt = time.perf_counter() - t0
+            fields[mode] = eng.get_fields(0, layout="cube", intensity=False)[0]
+            out[mode] = {"iterations": int(at[0]) or len(stats), "converged": bool(at[0]),
+                         "seconds": dt,
+                         "dx": [round(s[0]["mean_abs_dx"], 5) for s in stats]}
+            if x_reference is not None:
+                out[mode]["error_vs_reference"] = float(
+                    np.mean(np.abs(fields[mode] - np.ravel(x_reference))))
+    out["mean_abs_dx_between"] = float(np.mean(np.abs(fields["plain"] - fields["warm"])))
+    out["speedup"] = out["plain"]["seconds"] / out["warm"]["seconds"]
+    return out
+
+
+def main(argv=None):
+    import argparse
+    import json
+
+    import torch
+    ap = argparse.ArgumentParser(description="train the warm-start U-Net on plain-method runs")
+    ap.add_argument("--runs", type=int, default=2000)
+    ap.add_argument("--ncell", type=int, default=64)
+    ap.add_argument("--packets-per-cell", type=float, default=5)
+    ap.add_argument("--label-iterations", type=int, default=24)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--tolerance", type=float, default=0.01)
+    ap.add_argument("--eval", type=int, default=16, help="held-out runs for the wall-time test")
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+    log = (lambda s: print(s, flush=True))
+    torch.cuda.set_device(0)
+    ntrain = int(round(0.8 * a.runs))
+    seeds = [100_000 + i for i in range(a.runs)]
+    t0 = time.perf_counter()
+    grids, cubes, labels, dx = generate_runs(seeds, ncell=a.ncell,
+                                             packets_per_cell=a.packets_per_cell,
+                                             iterations=a.label_iterations, log=log)
+    t_gen = time.perf_counter() - t0
+    plain_its = iterations_to_tolerance(dx, a.tolerance)
+    log(f"plain method: iterations to mean |dx| < {a.tolerance}: mean {plain_its.mean():.2f}, "
+        f"not reached {int(np.sum(plain_its == 0))}; noise floor (last iterations) "
+        f"{dx[-4:].mean():.4f}")
+    net = UNet()
+    net.fit_normalisation(cubes[:ntrain], grids[:ntrain])
+    feats = build_features(net, grids, cubes)
+    lab = torch.from_numpy(labels.reshape(len(grids), -1)).to(feats.device)
+    ncell = grids[0].ncell
+    t0 = time.perf_counter()
+    hist = train(net, feats[:ntrain], lab[:ntrain], ncell, epochs=a.epochs, batch=a.batch,
+                 lr=a.lr, log=log)
+    t_train = time.perf_counter() - t0
+    val = evaluate_loss(net, feats[ntrain:], lab[ntrain:], ncell)
+    base = float(((lab[ntrain:] - lab[:ntrain].mean(0)) ** 2).mean())
+    log(f"held-out MSE {val:.5f} (mean-field baseline {base:.5f})")
+    net.save(a.out, train_loss=np.array(hist), val_mse=val, baseline_mse=base,
+             runs=a.runs, ncell=a.ncell, tolerance=a.tolerance,
+             packets_per_cell=a.packets_per_cell)
+    ev = []
+    for i in range(ntrain, min(ntrain + a.eval, a.runs)):
+        g, nH = run_configs([seeds[i]], a.ncell, a.packets_per_cell)[0]
+        ev.append(time_to_converge(net, g, nH, x_reference=10.0 ** labels[i].astype(np.float64),
+                                   tolerance=a.tolerance))
+        log(json.dumps(ev[-1]))
+
+    def mean(key, sub):
+        return float(np.mean([e[key][sub] for e in ev]))
+    rep = {"runs": a.runs, "train": ntrain, "generation_s": t_gen, "training_s": t_train,
+           "train_loss": hist, "val_mse": val, "baseline_mse": base,
+           "tolerance": a.tolerance, "noise_floor_dx": float(dx[-4:].mean()),
+           "plain_iterations_mean": mean("plain", "iterations"),
+           "warm_iterations_mean": mean("warm", "iterations"),
+           "plain_seconds_mean": mean("plain", "seconds"),
+           "warm_seconds_mean": mean("warm", "seconds"),
+           "speedup_median": float(np.median([e["speedup"] for e in ev])),
+           "plain_error_vs_reference": mean("plain", "error_vs_reference"),
+           "warm_error_vs_reference": mean("warm", "error_vs_reference"),
+           "mean_abs_dx_between_mean": float(np.mean([e["mean_abs_dx_between"] for e in ev])),
+           "eval": ev}
+    if a.report:
+        with open(a.report, "w") as f:
+            json.dump(rep, f, indent=1)
+    log(json.dumps({k: v for k, v in rep.items() if k not in ("eval", "train_loss")}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -302,7 +302,7 @@ def test_iteration_conservation(precision):
         assert s["packets_emitted"] == 300_001
         assert s["packets_absorbed"] + s["packets_escaped"] == s["packets_emitted"]
         assert s["error_flags"] == 0
-        assert 1 <= s["rounds"] <= 4 + 4 + 4 - 2
+        assert 1 <= s["rounds"] <= 4 + 4 + 4 - 2 + 3  # straight-line bound + spares
         assert s["cell_crossings"] > s["subgrid_transits"] > 0
     eng.close()
 

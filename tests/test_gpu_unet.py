@@ -1,0 +1,181 @@
+"""The warm-start network's CUDA kernels against the CPU oracle
+(oracle/unet_oracle.py, pinned by finite differences on the CPU).
+
+BF16 storage makes GPU and oracle differ: the oracle rounds weights and every
+stored tensor to BF16 where the GPU does, so the remaining difference is FP32
+(GPU) vs FP64 (oracle) accumulation, plus occasional one-ulp BF16 flips that
+propagate.  Tolerances below are stated per check."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import unet_oracle as U
+from parallelcmacionize_b200 import _lib
+from parallelcmacionize_b200.problems import lognormal_config
+from parallelcmacionize_b200.warmstart import UNet, flux_proxy
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_tensor(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16).cuda()
+
+
+def _np(t):
+    return t.float().cpu().numpy().astype(np.float64)
+
+
+def _dims(X, Y, Z):
+    return (C.c_int32 * 3)(X, Y, Z)
+
+
+def _bf16_ulp(a):
+    """Spacing of BF16 values at |a| (8 significant bits)."""
+    e = np.floor(np.log2(np.maximum(np.abs(a), 1e-30)))
+    return 2.0 ** (e - 7)
+
+
+def _assert_bf16_rounded(got, ref):
+    """got = BF16(ref computed in FP32): within half a BF16 ulp of the FP64
+    value, except where FP32 accumulation lands on the other side of a
+    rounding boundary (then one ulp), for at most 2% of the values."""
+    err = np.abs(got - ref)
+    ulp = _bf16_ulp(ref)
+    # absolute terms: FP32 accumulation error of sums that cancel to ~0
+    assert np.all(err <= ulp + 1e-4), float((err / ulp).max())
+    assert np.mean(err <= 0.5 * ulp * (1 + 1e-3) + 1e-5) > 0.98
+
+
+def _pack(net, W, flip):
+    cout, _, cin = W.shape
+    w = torch.from_numpy(np.ascontiguousarray(W, dtype=np.float32)).cuda()
+    out = torch.zeros(27 * cin * cout, dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check_unet(net._L.cmi_unet_pack_weights(net._h, C.c_void_p(w.data_ptr()), cout, cin,
+                                                 flip, C.c_void_p(out.data_ptr())))
+    return out
+
+
+def _conv(net, x, cin, wp, bias, cout, act, shape):
+    B, Z, Y, X = shape
+    out = torch.zeros((B, Z, Y, X, cout), dtype=torch.bfloat16, device="cuda")
+    b = None if bias is None else torch.from_numpy(bias.astype(np.float32)).cuda()
+    torch.cuda.synchronize()
+    _lib.check_unet(net._L.cmi_unet_conv3(
+        net._h, C.c_void_p(x.data_ptr()), cin, C.c_void_p(wp.data_ptr()),
+        None if b is None else C.c_void_p(b.data_ptr()), C.c_void_p(out.data_ptr()), cout, act,
+        B, _dims(X, Y, Z)))
+    return out
+
+
+@pytest.fixture(scope="module")
+def net():
+    n = UNet()
+    yield n
+    n.close()
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 16), (32, 48), (80, 32)])
+def test_conv3_forward_matches_oracle(net, cin, cout):
+    rng = np.random.default_rng(cin + cout)
+    shape = (2, 8, 8, 16)  # B, Z, Y, X
+    x = U.bf16_round(rng.normal(size=shape + (cin,)))
+    W = rng.normal(0, 0.2, size=(cout, 27, cin))
+    bias = rng.normal(0, 0.1, size=cout).astype(np.float32).astype(np.float64)
+    y = _np(_conv(net, _bf16_tensor(x), cin, _pack(net, W, 0), bias, cout, 1, shape))
+    ref = U.leaky(U.conv3(x, U.bf16_round(W), bias))
+    _assert_bf16_rounded(y, ref)
+
+
+def test_conv3_input_gradient_matches_oracle(net):
+    rng = np.random.default_rng(5)
+    cin, cout = 48, 32
+    shape = (1, 8, 16, 8)
+    dy = U.bf16_round(rng.normal(size=shape + (cout,)))
+    W = rng.normal(0, 0.2, size=(cout, 27, cin))
+    dx = _np(_conv(net, _bf16_tensor(dy), cout, _pack(net, W, 1), None, cin, 0, shape))
+    ref = U.conv3_input_grad(dy, U.bf16_round(W))
+    _assert_bf16_rounded(dx, ref)
+
+
+def test_conv3_weight_gradient_matches_oracle(net):
+    rng = np.random.default_rng(6)
+    cin, cout = 32, 16
+    shape = (2, 8, 8, 16)
+    x = U.bf16_round(rng.normal(size=shape + (cin,)))
+    dy = U.bf16_round(rng.normal(size=shape + (cout,)))
+    dw = torch.zeros(cout * 27 * cin, dtype=torch.float32, device="cuda")
+    xt, dyt = _bf16_tensor(x), _bf16_tensor(dy)
+    torch.cuda.synchronize()
+    _lib.check_unet(net._L.cmi_unet_conv3_wgrad(net._h, C.c_void_p(xt.data_ptr()), cin,
+                                                C.c_void_p(dyt.data_ptr()), cout, 2,
+                                                _dims(16, 8, 8), C.c_void_p(dw.data_ptr())))
+    got = dw.cpu().numpy().reshape(cout, 27, cin)
+    ref = U.conv3_weight_grad(x, dy)
+    # sums of 2048 products in FP32 in another order
+    np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-3)
+
+
+def test_network_gradients_match_oracle(net):
+    rng = np.random.default_rng(7)
+    shape = (2, 32, 32, 32)
+    feats = rng.normal(size=shape + (2,)).astype(np.float32)
+    target = rng.normal(-1.0, 0.5, size=shape).astype(np.float32)
+    p = net.initial_params(seed=3)
+    p += rng.normal(0, 0.02, p.size).astype(np.float32)
+    net.set_params(p)
+    f = torch.from_numpy(feats.reshape(2, -1, 2)).cuda()
+    t = torch.from_numpy(target.reshape(2, -1)).cuda()
+    loss, g = net.gradients(f, t, (32, 32, 32))
+    o = U.UNetOracle(p.astype(np.float64), bf16=True)
+    oloss, og = o.gradients(feats.astype(np.float64), target.astype(np.float64))
+    assert abs(loss - oloss) <= 1e-3 * oloss
+    # per tensor: relative L2 error and direction (BF16 activations and
+    # gradients: ~1% relative)
+    off = 0
+    for cout, cin in net.layer_shapes():
+        for size in (cout * 27 * cin, cout):
+            a, b = g[off: off + size].astype(np.float64), og[off: off + size]
+            rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+            cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-300))
+            assert rel < 3e-2 and cos > 0.999, (off, size, rel, cos)
+            off += size
+    np.testing.assert_allclose(g[off:], og[off:], rtol=3e-2, atol=1e-6)
+    # prediction of the forward pass
+    pred = net.forward(f, (32, 32, 32)).cpu().numpy().reshape(shape)
+    # one-ulp BF16 differences compound over ten layers: bound the worst and
+    # the mean deviation
+    dev = np.abs(pred - o.forward(feats.astype(np.float64)))
+    assert dev.max() < 5e-2 and dev.mean() < 3e-3, (dev.max(), dev.mean())
+
+
+def test_features_match_host():
+    spec, nH = lognormal_config(ncell=32, num_subgrid=2, num_photon=1000, num_sources=3)
+    from parallelcmacionize_b200 import blocked_to_cube
+    cube = blocked_to_cube(nH, spec.ncell, spec.num_subgrid)
+    with UNet() as n:
+        n.norm = np.array([8.0, 0.5, 12.0, 2.0], np.float32)
+        f = n.features(torch.from_numpy(cube.ravel().copy()).cuda(), spec).cpu().numpy()
+    np.testing.assert_allclose(f[:, 0], (np.log10(cube.ravel()) - 8.0) / 0.5, rtol=1e-5,
+                               atol=1e-5)
+    np.testing.assert_allclose(f[:, 1], (flux_proxy(spec).ravel() - 12.0) / 2.0, rtol=1e-5,
+                               atol=1e-5)
+
+
+def test_training_reduces_loss():
+    """A learnable target (a smooth function of the features): Adam through the
+    library's kernels brings the loss well below its starting value."""
+    rng = np.random.default_rng(11)
+    shape = (4, 32, 32, 32)
+    f = rng.normal(size=shape + (2,)).astype(np.float32)
+    import scipy.ndimage as nd
+    f = np.stack([nd.gaussian_filter(f[..., k], (0, 2, 2, 2)) * 3 for k in range(2)], -1)
+    target = (np.tanh(f[..., 0]) - 0.5 * f[..., 1]).astype(np.float32)
+    ft = torch.from_numpy(f.reshape(4, -1, 2).astype(np.float32)).cuda()
+    tt = torch.from_numpy(target.reshape(4, -1)).cuda()
+    with UNet(seed=1) as n:
+        losses = [n.train_step(ft, tt, (32, 32, 32), 3e-3) for _ in range(60)]
+    assert np.all(np.isfinite(losses))
+    assert np.mean(losses[-5:]) < 0.2 * losses[0], losses[::10]
