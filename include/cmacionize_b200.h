@@ -289,14 +289,15 @@ int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
 /* ---------------------------------------------------------------------------
  * Learned warm start.  No reference counterpart: the reference starts every
  * run from x_H = 1e-6 (DensitySubGrid.hpp:544-551).  A 3-level 3D
- * convolutional U-Net maps two input channels per cell, [log10 n_H, log10 of
- * the source flux sum_i L_i / (4 pi r_i^2)] (normalised), to log10 x_H; the
- * plain iteration then starts from that field and still decides convergence.
+ * convolutional U-Net maps three input channels per cell (cmi_unet_features:
+ * density, unattenuated source flux and a Stromgren ratio along the rays
+ * from the sources) to log10 x_H; the plain iteration then starts from that
+ * field and still decides convergence.
  *
  * Layers (c1, c2, c3 channels per level; 3x3x3 convolutions, zero padding,
  * leaky ReLU; 2x2x2 average pooling down, nearest-neighbour upsampling up,
  * skip connections concatenated after the upsampled channels):
- *   level 1: conv(2 -> c1), conv(c1 -> c1)      pooled to level 2
+ *   level 1: conv(3 -> c1), conv(c1 -> c1)      pooled to level 2
  *   level 2: conv(c1 -> c2), conv(c2 -> c2)     pooled to level 3
  *   level 3: conv(c2 -> c3), conv(c3 -> c3)     upsampled to level 2
  *   level 2: conv(c3 + c2 -> c2), conv(c2 -> c2) upsampled to level 1
@@ -310,7 +311,7 @@ int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
  *
  * Tensors handed to the network live in device memory, FP32, one sample
  * after another in the engine's cube order (index (ix * ny + iy) * nz + iz):
- * features [batch][cells][2], targets and predictions [batch][cells].  Grid
+ * features [batch][cells][3], targets and predictions [batch][cells].  Grid
  * sides must be multiples of 32.  Calls are synchronous.  Errors: the codes
  * above, message in cmi_unet_last_error_string(). */
 typedef struct cmi_unet cmi_unet;
@@ -339,13 +340,18 @@ int cmi_unet_gradients(cmi_unet *net, const float *features, const float *target
 /* one Adam step (beta 0.9, 0.999, eps 1e-8) at learning rate lr */
 int cmi_unet_train_step(cmi_unet *net, const float *features, const float *target, int32_t batch,
                         const int32_t dims[3], float lr, float *loss);
-/* features of one grid from its FP64 n_H (device, cube order) and sources
- * (host, [x, y, z, L] each); norm = {n_mean, n_scale, f_mean, f_scale}:
- * channel 0 = (log10 n_H - n_mean) / n_scale, channel 1 = (log10 flux -
- * f_mean) / f_scale with r clamped to half a cell */
+/* The three input channels of one grid ([cells][3], FP32, device) from its
+ * FP64 n_H (device, cube order) and sources (host, [x, y, z, L] each), each
+ * channel (raw - norm[2k]) / norm[2k + 1]:
+ *   0: log10 n_H
+ *   1: log10 sum_i L_i / (4 pi r_i^2), r clamped to half a cell
+ *   2: log10 sum_i L_i / (4 pi alpha R_i), R_i = integral of n_H^2 r^2 dr
+ *      along the ray from source i to the cell centre (FP32 midpoint sum in
+ *      steps of at most half the smallest cell side, n_H of the cell holding
+ *      each sample), clamped to [1e-30, 1e30] */
 int cmi_unet_features(cmi_unet *net, const double *nH_cube, const int32_t dims[3],
                       const double box[6], const double *sources, int32_t num_sources,
-                      const float norm[4], float *features);
+                      double recombination_rate, const float norm[6], float *features);
 /* x_H = 10^clamp(prediction, log10_min, 0) as FP64 (device), n values */
 int cmi_unet_to_neutral_fraction(cmi_unet *net, const float *prediction, double *xH, int64_t n,
                                  float log10_min);

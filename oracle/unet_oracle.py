@@ -22,6 +22,7 @@ from __future__ import annotations
 import numpy as np
 
 SLOPE = 0.1
+NUM_FEATURES = 3  # input channels
 
 
 def bf16_round(a):
@@ -36,7 +37,7 @@ def bf16_round(a):
 
 def layer_specs(c1=12, c2=24, c3=48):
     """(cout, [input segment channels]) of the ten convolutions."""
-    return [(c1, [2]), (c1, [c1]), (c2, [c1]), (c2, [c2]), (c3, [c2]), (c3, [c3]),
+    return [(c1, [NUM_FEATURES]), (c1, [c1]), (c2, [c1]), (c2, [c2]), (c3, [c2]), (c3, [c3]),
             (c2, [c3, c2]), (c2, [c2]), (c1, [c2, c1]), (c1, [c1])]
 
 
@@ -155,7 +156,7 @@ class UNetOracle:
         return bf16_round(a) if self.bf16 else a
 
     def forward(self, feats):
-        """feats [B, Z, Y, X, 2] -> prediction [B, Z, Y, X]; keeps activations."""
+        """feats [B, Z, Y, X, 3] -> prediction [B, Z, Y, X]; keeps activations."""
         q = self._q
         W, b = self.W, self.b
         s = {}

@@ -186,7 +186,7 @@ def load():
     L.cmi_unet_forward.argtypes = [vp, vp, vp, i32, vp]
     L.cmi_unet_gradients.argtypes = [vp, vp, vp, i32, vp, C.POINTER(f32), vp]
     L.cmi_unet_train_step.argtypes = [vp, vp, vp, i32, vp, f32, C.POINTER(f32)]
-    L.cmi_unet_features.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp]
+    L.cmi_unet_features.argtypes = [vp, vp, vp, vp, vp, i32, d, vp, vp]
     L.cmi_unet_to_neutral_fraction.argtypes = [vp, vp, vp, i64, f32]
     L.cmi_unet_conv3.argtypes = [vp, vp, i32, vp, vp, vp, i32, i32, i32, vp]
     L.cmi_unet_pack_weights.argtypes = [vp, vp, i32, i32, i32, vp]

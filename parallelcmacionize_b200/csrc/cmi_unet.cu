@@ -53,6 +53,7 @@ constexpr int kTileX = 8, kTileY = 4, kTileZ = 4;  // 128 voxels
 constexpr int kABytes = 128 * 32;                  // one K step of the A operand
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr uint32_t kErrTimeout = 1u;
+constexpr int kFeatures = 3;  // input channels of the network
 
 // ---------------------------------------------------------------------------
 // error reporting (the engine's cmi_last_error_string is per thread; the
@@ -675,49 +676,98 @@ __global__ void k_adam(float *p, const float *g, float *m, float *v, long long n
   }
 }
 
-// input features -> the 16-channel BF16 input tensor (channels 2..15 zero)
+// input features -> the 16-channel BF16 input tensor (channels 3..15 zero)
 __global__ void k_input(const float *f, bf16 *x, long long nvox) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvox * 16;
        i += (long long)gridDim.x * blockDim.x) {
     const long long v = i / 16;
     const int k = (int)(i % 16);
-    x[i] = __float2bfloat16_rn(k < 2 ? f[v * 2 + k] : 0.f);
+    x[i] = __float2bfloat16_rn(k < kFeatures ? f[v * kFeatures + k] : 0.f);
   }
 }
 
-// Features of one grid (cube order, Z = ix slowest): channel 0 = (log10 n_H -
-// n_mean) / n_scale, channel 1 = (log10 sum_i L_i / (4 pi r_i^2) - f_mean) /
-// f_scale, r clamped to half a cell.
+// Features of one grid (cube order, Z = ix slowest), each (raw - mean) / scale:
+//  0: log10 n_H
+//  1: log10 sum_i L_i / (4 pi r_i^2), r clamped to half a cell
+//  2: log10 sum_i L_i / (4 pi alpha R_i), R_i = integral of n_H^2 r^2 dr along
+//     the ray from source i to the cell centre (the Stromgren condition: a
+//     source ionizes a ray up to where its recombinations use up L_i / 4 pi).
+//     The integral is a midpoint sum over ceil(r / (cell / 2)) steps with n_H
+//     of the cell that holds each sample point, in FP32 cell units with n_H in
+//     units of its grid mean, so the march costs a few FP32 operations per
+//     step.  Explicitly rounded operations (no contraction) make the sample
+//     cells reproducible by the same float32 sum on the host.
 struct FeatureArgs {
   const double *nH;
+  const float *nrel;    // n_H / n_ref (FP32), cube order
   float *out;
   int dims[3];          // X (iz), Y (iy), Z (ix)
+  int n3[3];            // cells along ix, iy, iz
   double origin[3];     // box corner along ix, iy, iz
   double cell[3];       // cell size along ix, iy, iz
   const double *src;    // [nsrc][4]: position (x, y, z), L
   int nsrc;
-  float norm[4];        // n_mean, n_scale, f_mean, f_scale
+  double alpha, nref;
+  float norm[2 * kFeatures];  // (mean, scale) per channel
 };
+
+__global__ void k_nrel(const double *nH, float *nrel, long long n, double inv_nref) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    nrel[i] = (float)__dmul_rn(nH[i], inv_nref);
+}
 
 __global__ void k_features(FeatureArgs a) {
   const long long nvox = (long long)a.dims[0] * a.dims[1] * a.dims[2];
-  const double rmin = 0.5 * fmin(a.cell[0], fmin(a.cell[1], a.cell[2]));
+  const double hmin = fmin(a.cell[0], fmin(a.cell[1], a.cell[2]));
+  const double rmin = 0.5 * hmin;
+  // march in units of cells along each axis; step length in units of hmin
+  const float hstep = 0.5f;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox;
        v += (long long)gridDim.x * blockDim.x) {
-    const int iz = (int)(v % a.dims[0]);
-    const int iy = (int)((v / a.dims[0]) % a.dims[1]);
-    const int ix = (int)(v / ((long long)a.dims[0] * a.dims[1]));
-    const double p[3] = {a.origin[0] + (ix + 0.5) * a.cell[0], a.origin[1] + (iy + 0.5) * a.cell[1],
-                         a.origin[2] + (iz + 0.5) * a.cell[2]};
-    double flux = 0.;
+    const int i3[3] = {(int)(v / ((long long)a.dims[0] * a.dims[1])),
+                       (int)((v / a.dims[0]) % a.dims[1]), (int)(v % a.dims[0])};
+    double flux = 0., strom = 0.;
     for (int s = 0; s < a.nsrc; ++s) {
-      const double dx = p[0] - a.src[4 * s], dy = p[1] - a.src[4 * s + 1],
-                   dz = p[2] - a.src[4 * s + 2];
-      const double r = fmax(sqrt(dx * dx + dy * dy + dz * dz), rmin);
-      flux += a.src[4 * s + 3] / (4. * 3.141592653589793 * r * r);
+      const double *S = a.src + 4 * s;
+      double dm[3], sc[3];
+      float dc[3];
+      for (int k = 0; k < 3; ++k) {
+        const double p = __dadd_rn(a.origin[k], __dmul_rn((double)i3[k] + 0.5, a.cell[k]));
+        dm[k] = __dsub_rn(p, S[k]);
+        sc[k] = __ddiv_rn(__dsub_rn(S[k], a.origin[k]), a.cell[k]);  // source in cell units
+        dc[k] = (float)__ddiv_rn(dm[k], a.cell[k]);                  // ray in cell units
+      }
+      const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dm[0], dm[0]),
+                                                      __dmul_rn(dm[1], dm[1])),
+                                            __dmul_rn(dm[2], dm[2])));
+      const double rc = fmax(r, rmin);
+      flux += S[3] / (4. * 3.141592653589793 * rc * rc);
+      const float rh = (float)__ddiv_rn(r, hmin);  // length in units of hmin
+      const int nstep = max(1, (int)ceilf(__fdiv_rn(rh, hstep)));
+      const float inv = __frcp_rn((float)nstep);
+      const float sf[3] = {(float)sc[0], (float)sc[1], (float)sc[2]};
+      float col = 0.f;
+      for (int k = 0; k < nstep; ++k) {
+        const float t = __fmul_rn(__fadd_rn((float)k, 0.5f), inv);
+        int c3[3];
+        for (int m = 0; m < 3; ++m) {
+          const int ci = (int)floorf(__fadd_rn(sf[m], __fmul_rn(t, dc[m])));
+          c3[m] = min(max(ci, 0), a.n3[m] - 1);
+        }
+        const float n = a.nrel[((long long)c3[0] * a.n3[1] + c3[1]) * a.n3[2] + c3[2]];
+        const float rr = __fmul_rn(t, rh);
+        col = __fadd_rn(col, __fmul_rn(__fmul_rn(n, n), __fmul_rn(rr, rr)));
+      }
+      // R = sum n^2 r^2 dr in SI: (n_ref^2) (hmin^3) col * (rh / nstep)
+      const double R = (double)col * ((double)rh * (double)inv) * a.nref * a.nref * hmin * hmin *
+                       hmin;
+      strom += S[3] / (4. * 3.141592653589793 * a.alpha * fmax(R, 1e-300));
     }
-    a.out[2 * v] = (float)((log10(a.nH[v]) - a.norm[0]) / a.norm[1]);
-    a.out[2 * v + 1] = (float)((log10(fmax(flux, 1e-300)) - a.norm[2]) / a.norm[3]);
+    float *o = a.out + kFeatures * v;
+    o[0] = (float)((log10(a.nH[v]) - a.norm[0]) / a.norm[1]);
+    o[1] = (float)((log10(fmax(flux, 1e-300)) - a.norm[2]) / a.norm[3]);
+    o[2] = (float)((log10(fmin(fmax(strom, 1e-30), 1e30)) - a.norm[4]) / a.norm[5]);
   }
 }
 
@@ -800,6 +850,10 @@ struct cmi_unet {
        *gP2 = nullptr, *gBA = nullptr, *gBB = nullptr, *gD2A = nullptr, *gD2B = nullptr,
        *gD1A = nullptr, *gD1B = nullptr;
   float *pred = nullptr, *feat = nullptr;
+  double *d_src = nullptr;  // sources of the features kernel
+  size_t src_cap = 0;
+  float *d_nrel = nullptr;  // n_H / n_ref for the features kernel
+  size_t nrel_cap = 0;
   bool packed = false;
 };
 
@@ -879,7 +933,7 @@ int ensure_buffers(cmi_unet *u, int batch, const int dims[3]) {
   UN_TRY(dev_zero_alloc(&p, sizeof(float) * (size_t)v1));
   u->bufs.push_back(p);
   u->pred = static_cast<float *>(p);
-  UN_TRY(dev_zero_alloc(&p, sizeof(float) * 2 * (size_t)v1));
+  UN_TRY(dev_zero_alloc(&p, sizeof(float) * kFeatures * (size_t)v1));
   u->bufs.push_back(p);
   u->feat = static_cast<float *>(p);
   u->batch = batch;
@@ -1228,7 +1282,7 @@ int cmi_unet_create(const cmi_unet_config *cfg, cmi_unet **out) {
     int seg_real[2], seg_store[2];
   };
   const Spec specs[10] = {
-      {c.c1, {2, 0}, {16, 0}},          {c.c1, {c.c1, 0}, {c.s1, 0}},
+      {c.c1, {kFeatures, 0}, {16, 0}},  {c.c1, {c.c1, 0}, {c.s1, 0}},
       {c.c2, {c.c1, 0}, {c.s1, 0}},     {c.c2, {c.c2, 0}, {c.s2, 0}},
       {c.c3, {c.c2, 0}, {c.s2, 0}},     {c.c3, {c.c3, 0}, {c.s3, 0}},
       {c.c2, {c.c3, c.c2}, {c.s3, c.s2}}, {c.c2, {c.c2, 0}, {c.s2, 0}},
@@ -1308,6 +1362,8 @@ int cmi_unet_destroy(cmi_unet *u) {
   cudaFree(u->v);
   cudaFree(u->d_err);
   cudaFree(u->d_loss);
+  cudaFree(u->d_src);
+  cudaFree(u->d_nrel);
   if (u->stream) cudaStreamDestroy(u->stream);
   delete u;
   return CMI_OK;
@@ -1400,36 +1456,56 @@ int cmi_unet_train_step(cmi_unet *u, const float *features, const float *target,
 
 int cmi_unet_features(cmi_unet *u, const double *nH_cube, const int32_t dims[3],
                       const double box[6], const double *sources, int32_t num_sources,
-                      const float norm[4], float *features) {
+                      double recombination_rate, const float norm[6], float *features) {
   if (!u || !nH_cube || !dims || !box || !norm || !features || (num_sources > 0 && !sources))
     return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
   if (num_sources < 0 || num_sources > 4096)
     return fail(CMI_ERR_INVALID_ARGUMENT, "0..4096 sources");
+  if (!(recombination_rate > 0.) || !std::isfinite(recombination_rate))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "recombination rate must be > 0");
+  for (int k = 0; k < 3; ++k)
+    if (dims[k] <= 0 || !(box[3 + k] > 0.))
+      return fail(CMI_ERR_INVALID_ARGUMENT, "grid sides and box sizes must be > 0");
   UN_CUDA(cudaSetDevice(u->device));
   FeatureArgs a{};
   a.nH = nH_cube;
+  a.alpha = recombination_rate;
   a.out = features;
   a.dims[0] = dims[2];  // X = iz (fastest)
   a.dims[1] = dims[1];
   a.dims[2] = dims[0];  // Z = ix
   for (int k = 0; k < 3; ++k) {
+    a.n3[k] = dims[k];
     a.origin[k] = box[k];
     a.cell[k] = box[3 + k] / dims[k];
   }
-  double *dsrc = nullptr;
-  if (num_sources > 0) {
-    UN_CUDA(cudaMalloc(&dsrc, sizeof(double) * 4 * num_sources));
-    UN_CUDA(cudaMemcpyAsync(dsrc, sources, sizeof(double) * 4 * num_sources,
-                            cudaMemcpyHostToDevice, u->stream));
+  if ((size_t)num_sources > u->src_cap) {
+    cudaFree(u->d_src);
+  cudaFree(u->d_nrel);
+    u->d_src = nullptr;
+    u->src_cap = 0;
+    UN_CUDA(cudaMalloc(&u->d_src, sizeof(double) * 4 * num_sources));
+    u->src_cap = (size_t)num_sources;
   }
-  a.src = dsrc;
+  if (num_sources > 0)
+    UN_CUDA(cudaMemcpyAsync(u->d_src, sources, sizeof(double) * 4 * num_sources,
+                            cudaMemcpyHostToDevice, u->stream));
+  a.src = u->d_src;
   a.nsrc = num_sources;
-  for (int k = 0; k < 4; ++k) a.norm[k] = norm[k];
+  for (int k = 0; k < 2 * kFeatures; ++k) a.norm[k] = norm[k];
   const long long nv = (long long)dims[0] * dims[1] * dims[2];
+  if ((size_t)nv > u->nrel_cap) {
+    cudaFree(u->d_nrel);
+    u->d_nrel = nullptr;
+    u->nrel_cap = 0;
+    UN_CUDA(cudaMalloc(&u->d_nrel, sizeof(float) * nv));
+    u->nrel_cap = (size_t)nv;
+  }
+  a.nref = 1e8;  // n_H unit of the ray sums (FP32 range)
+  a.nrel = u->d_nrel;
+  k_nrel<<<grid_for(nv), 256, 0, u->stream>>>(nH_cube, u->d_nrel, nv, 1. / a.nref);
   k_features<<<grid_for(nv), 256, 0, u->stream>>>(a);
-  const cudaError_t e = cudaStreamSynchronize(u->stream);
-  if (dsrc) cudaFree(dsrc);
-  if (e != cudaSuccess) return fail(CMI_ERR_CUDA, "features: %s", cudaGetErrorString(e));
+  UN_CUDA(cudaStreamSynchronize(u->stream));
   return CMI_OK;
 }
 

@@ -36,6 +36,7 @@ from ._lib import check_unet
 
 # log10 x_H below this is not predicted (the plain start is 1e-6)
 LOG10_XH_MIN = -8.0
+NUM_FEATURES = 3  # density, unattenuated flux, Stromgren ratio (cmi_unet_features)
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                "warmstart_unet64.npz")
 
@@ -69,8 +70,8 @@ class UNet:
         n = C.c_int64()
         check_unet(self._L.cmi_unet_num_params(self._h, C.byref(n)))
         self.num_params = int(n.value)
-        # feature normalisation: (n_mean, n_scale, f_mean, f_scale)
-        self.norm = np.array([8.0, 1.0, 13.0, 1.5], dtype=np.float32)
+        # feature normalisation: (mean, scale) of each of the three channels
+        self.norm = np.array([8.0, 1.0, 13.0, 1.5, 0.0, 3.0], dtype=np.float32)
         self.set_params(self.initial_params(seed))
 
     # ---- lifetime ----
@@ -94,7 +95,8 @@ class UNet:
     # ---- parameters ----
     def layer_shapes(self):
         c1, c2, c3 = self.channels
-        convs = [(c1, 2), (c1, c1), (c2, c1), (c2, c2), (c3, c2), (c3, c3), (c2, c3 + c2),
+        convs = [(c1, NUM_FEATURES), (c1, c1), (c2, c1), (c2, c2), (c3, c2), (c3, c3),
+                 (c2, c3 + c2),
                  (c2, c2), (c1, c2 + c1), (c1, c1)]
         return convs
 
@@ -147,7 +149,7 @@ class UNet:
         torch.cuda.synchronize(self.device)
 
     def forward(self, features, ncell):
-        """features [B, cells, 2] -> predicted log10 x_H [B, cells]."""
+        """features [B, cells, 3] -> predicted log10 x_H [B, cells]."""
         import torch
         self._sync()
         B = features.shape[0]
@@ -174,20 +176,22 @@ class UNet:
                                                C.byref(loss)))
         return float(loss.value)
 
-    def features(self, nH_cube, grid, out=None):
-        """Features [cells, 2] of one grid from its FP64 n_H (torch, device,
-        cube order) and the GridSpec's box and sources."""
+    def features(self, nH_cube, grid, out=None, norm=None):
+        """Features [cells, 3] of one grid from its FP64 n_H (torch, device,
+        cube order) and the GridSpec's box, sources and recombination rate;
+        ``norm`` defaults to the network's normalisation."""
         import torch
         self._sync()
         n = int(np.prod(grid.ncell))
         if out is None:
-            out = torch.empty((n, 2), dtype=torch.float32, device=nH_cube.device)
+            out = torch.empty((n, NUM_FEATURES), dtype=torch.float32, device=nH_cube.device)
         dims = (C.c_int32 * 3)(*[int(v) for v in grid.ncell])
         box = np.ascontiguousarray(grid.box, dtype=np.float64)
         src = np.ascontiguousarray(np.asarray(grid.sources, dtype=np.float64).reshape(-1, 4))
-        norm = np.ascontiguousarray(self.norm, dtype=np.float32)
+        nm = np.ascontiguousarray(self.norm if norm is None else norm, dtype=np.float32)
         check_unet(self._L.cmi_unet_features(self._h, _ptr(nH_cube), dims, box.ctypes.data,
-                                             src.ctypes.data, src.shape[0], norm.ctypes.data,
+                                             src.ctypes.data, src.shape[0],
+                                             float(grid.recombination_rate), nm.ctypes.data,
                                              _ptr(out)))
         return out
 
@@ -199,15 +203,56 @@ class UNet:
                                                         pred.numel(), float(log10_min)))
         return x
 
-    def fit_normalisation(self, nH_cubes, grids):
-        """Feature means / scales from a set of grids (host arithmetic)."""
-        ln, lf = [], []
-        for n, g in zip(nH_cubes, grids):
-            ln.append(np.log10(n).ravel())
-            lf.append(flux_proxy(g).ravel())
-        ln, lf = np.concatenate(ln), np.concatenate(lf)
-        self.norm = np.array([ln.mean(), ln.std() + 1e-6, lf.mean(), lf.std() + 1e-6],
-                             dtype=np.float32)
+    def fit_normalisation(self, nH_cubes, grids, sample=64):
+        """Feature means / scales from (up to ``sample`` of) a set of grids,
+        computed from the raw features on the GPU."""
+        import torch
+        raw = np.array([0.0, 1.0] * NUM_FEATURES, dtype=np.float32)
+        acc = []
+        for n, g in list(zip(nH_cubes, grids))[:sample]:
+            t = torch.from_numpy(np.ascontiguousarray(n, dtype=np.float64).ravel())
+            acc.append(self.features(t.to(f"cuda:{self.device}"), g, norm=raw).cpu().numpy())
+        a = np.concatenate(acc)
+        self.norm = np.stack([a.mean(axis=0), a.std(axis=0) + 1e-6], axis=1).ravel() \
+            .astype(np.float32)
+
+
+def stromgren_ratio(grid, nH_cube, nref=1e8):
+    """log10 sum_i L_i / (4 pi alpha R_i) at the cell centres (cube order), R_i
+    the midpoint sum of n_H^2 r^2 dr along the ray from source i in
+    ceil(r / (h / 2)) steps (h the smallest cell side), n_H of the cell holding
+    each sample: the features kernel's sum with the same FP32 operations, for
+    tests."""
+    f32 = np.float32
+    box = np.asarray(grid.box, dtype=np.float64)
+    n3 = tuple(int(v) for v in grid.ncell)
+    cell = box[3:] / np.array(n3, dtype=np.float64)
+    hmin = cell.min()
+    nrel = (np.asarray(nH_cube, dtype=np.float64).reshape(n3) * (1.0 / nref)).astype(f32)
+    idx = np.meshgrid(*[np.arange(n) for n in n3], indexing="ij")
+    total = np.zeros(n3)
+    for s in np.asarray(grid.sources, dtype=np.float64).reshape(-1, 4):
+        p = [box[a] + (idx[a] + 0.5) * cell[a] for a in range(3)]
+        dm = [p[a] - s[a] for a in range(3)]
+        sc = [f32((s[a] - box[a]) / cell[a]) for a in range(3)]
+        dc = [(dm[a] / cell[a]).astype(f32) for a in range(3)]
+        r = np.sqrt((dm[0] * dm[0] + dm[1] * dm[1]) + dm[2] * dm[2])
+        rh = (r / hmin).astype(f32)
+        nstep = np.maximum(1, np.ceil(rh / f32(0.5)).astype(np.int64))
+        inv = (f32(1.0) / nstep.astype(f32)).astype(f32)
+        col = np.zeros(n3, dtype=f32)
+        for k in range(int(nstep.max())):
+            on = k < nstep
+            t = ((f32(k) + f32(0.5)) * inv).astype(f32)
+            c = [np.clip(np.floor(sc[a] + t * dc[a]).astype(np.int64), 0, n3[a] - 1)
+                 for a in range(3)]
+            n = nrel[c[0], c[1], c[2]]
+            rr = (t * rh).astype(f32)
+            col = np.where(on, (col + (n * n) * (rr * rr)).astype(f32), col)
+        R = col.astype(np.float64) * (rh.astype(np.float64) * inv.astype(np.float64)) * \
+            nref * nref * hmin * hmin * hmin
+        total += s[3] / (4.0 * np.pi * grid.recombination_rate * np.maximum(R, 1e-300))
+    return np.log10(np.clip(total, 1e-30, 1e30))
 
 
 def flux_proxy(grid):
@@ -288,10 +333,11 @@ def iterations_to_tolerance(dx, tolerance, min_iterations=2):
 
 
 def build_features(net, grids, cubes):
-    """Features of every run on the GPU: torch [N, cells, 2]."""
+    """Features of every run on the GPU: torch [N, cells, 3]."""
     import torch
     n = int(np.prod(grids[0].ncell))
-    out = torch.empty((len(grids), n, 2), dtype=torch.float32, device=f"cuda:{net.device}")
+    out = torch.empty((len(grids), n, NUM_FEATURES), dtype=torch.float32,
+                      device=f"cuda:{net.device}")
     for i, (g, c) in enumerate(zip(grids, cubes)):
         nH = torch.from_numpy(np.ascontiguousarray(c).ravel()).to(out.device)
         net.features(nH, g, out=out[i])
@@ -341,11 +387,15 @@ def evaluate_loss(net, feats, labels, ncell, batch=8):
 # warm start and the convergence comparison
 # ---------------------------------------------------------------------------
 def warm_start(net, engine, instance, nH_cube, log10_min=LOG10_XH_MIN):
-    """Predict x_H for an engine instance and load it (cube order)."""
+    """Predict x_H for an engine instance and load it.  ``nH_cube``: n_H in
+    cube order, a torch CUDA tensor (FP64) or a host array (copied first)."""
     import torch
     grid = engine.grids[instance]
     dev = f"cuda:{net.device}"
-    nH = torch.from_numpy(np.ascontiguousarray(nH_cube, dtype=np.float64).ravel()).to(dev)
+    if isinstance(nH_cube, torch.Tensor):
+        nH = nH_cube.reshape(-1)
+    else:
+        nH = torch.from_numpy(np.ascontiguousarray(nH_cube, dtype=np.float64).ravel()).to(dev)
     f = net.features(nH, grid).unsqueeze(0).contiguous()
     pred = net.forward(f, grid.ncell)
     x = net.to_neutral_fraction(pred, log10_min)
@@ -354,8 +404,32 @@ def warm_start(net, engine, instance, nH_cube, log10_min=LOG10_XH_MIN):
     return x
 
 
+def warm_breakdown(net, engine, instance, nH_dev, repeats=5):
+    """Milliseconds of the warm start's stages (features, network, x_H into
+    the engine), each bracketed by device synchronisations."""
+    import torch
+    grid = engine.grids[instance]
+    t = {"features": 0.0, "network": 0.0, "load": 0.0}
+    for _ in range(repeats):
+        torch.cuda.synchronize(net.device)
+        t0 = time.perf_counter()
+        f = net.features(nH_dev, grid).unsqueeze(0).contiguous()
+        torch.cuda.synchronize(net.device)
+        t1 = time.perf_counter()
+        pred = net.forward(f, grid.ncell)
+        torch.cuda.synchronize(net.device)
+        t2 = time.perf_counter()
+        x = net.to_neutral_fraction(pred)
+        engine.set_fields_device(instance, 0, x.data_ptr(), layout="cube")
+        t3 = time.perf_counter()
+        t["features"] += (t1 - t0) * 1e3 / repeats
+        t["network"] += (t2 - t1) * 1e3 / repeats
+        t["load"] += (t3 - t2) * 1e3 / repeats
+    return t
+
+
 def time_to_converge(net, grid, nH_blocked, x_reference=None, tolerance=0.01,
-                     max_iterations=60, seed=7, device=0):
+                     max_iterations=60, seed=7, device=0, plain_spread=True):
     """Iterations and wall time (s) to convergence (mean |delta x_H| <
     tolerance, cmi_run_until_converged) from x_H = 1e-6 and from the warm
     start, same grid and packet seed.  Wall time covers the features, the
@@ -366,6 +440,8 @@ def time_to_converge(net, grid, nH_blocked, x_reference=None, tolerance=0.01,
     import torch
     from .engine import TransportEngine, blocked_to_cube
     cube = blocked_to_cube(nH_blocked, grid.ncell, grid.num_subgrid)
+    # n_H is resident on the device, like the engine's copy
+    cube_dev = torch.from_numpy(np.ascontiguousarray(cube).ravel()).to(f"cuda:{device}")
     out = {}
     fields = {}
     for mode in ("plain", "warm"):
@@ -373,12 +449,13 @@ def time_to_converge(net, grid, nH_blocked, x_reference=None, tolerance=0.01,
             eng.set_fields(0, nH_blocked, np.full(nH_blocked.size, 1e-6))
             eng.run_iterations(1, seed=99)  # warm-up: graph capture, first touch
             if mode == "warm":
-                warm_start(net, eng, 0, cube)  # warm-up of the network path
+                warm_start(net, eng, 0, cube_dev)  # warm-up of the network path
+                out["warm_breakdown_ms"] = warm_breakdown(net, eng, 0, cube_dev)
             eng.set_fields(0, None, np.full(nH_blocked.size, 1e-6))
             torch.cuda.synchronize(device)
             t0 = time.perf_counter()
             if mode == "warm":
-                warm_start(net, eng, 0, cube)
+                warm_start(net, eng, 0, cube_dev)
             stats, at = eng.run_until_converged(tolerance, max_iterations=max_iterations,
                                                 min_iterations=2, seed=seed)
             eng.synchronize()
@@ -392,6 +469,15 @@ def time_to_converge(net, grid, nH_blocked, x_reference=None, tolerance=0.01,
                     np.mean(np.abs(fields[mode] - np.ravel(x_reference))))
     out["mean_abs_dx_between"] = float(np.mean(np.abs(fields["plain"] - fields["warm"])))
     out["speedup"] = out["plain"]["seconds"] / out["warm"]["seconds"]
+    if plain_spread:
+        # the same plain run with other packets: the Monte Carlo spread that
+        # any two converged fields show
+        with TransportEngine(grid, precision="fp32", device=device) as eng:
+            eng.set_fields(0, nH_blocked, np.full(nH_blocked.size, 1e-6))
+            eng.run_until_converged(tolerance, max_iterations=max_iterations, min_iterations=2,
+                                    seed=seed + 1)
+            x2 = eng.get_fields(0, layout="cube", intensity=False)[0]
+        out["mean_abs_dx_plain_vs_plain"] = float(np.mean(np.abs(fields["plain"] - x2)))
     return out
 
 
@@ -461,6 +547,8 @@ def main(argv=None):
            "plain_error_vs_reference": mean("plain", "error_vs_reference"),
            "warm_error_vs_reference": mean("warm", "error_vs_reference"),
            "mean_abs_dx_between_mean": float(np.mean([e["mean_abs_dx_between"] for e in ev])),
+           "mean_abs_dx_plain_vs_plain_mean": float(np.mean(
+               [e["mean_abs_dx_plain_vs_plain"] for e in ev])),
            "eval": ev}
     if a.report:
         with open(a.report, "w") as f:

@@ -13,7 +13,7 @@ import pytest
 from oracle import unet_oracle as U
 from parallelcmacionize_b200 import _lib
 from parallelcmacionize_b200.problems import lognormal_config
-from parallelcmacionize_b200.warmstart import UNet, flux_proxy
+from parallelcmacionize_b200.warmstart import UNet, flux_proxy, stromgren_ratio
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -121,12 +121,12 @@ def test_conv3_weight_gradient_matches_oracle(net):
 def test_network_gradients_match_oracle(net):
     rng = np.random.default_rng(7)
     shape = (2, 32, 32, 32)
-    feats = rng.normal(size=shape + (2,)).astype(np.float32)
+    feats = rng.normal(size=shape + (3,)).astype(np.float32)
     target = rng.normal(-1.0, 0.5, size=shape).astype(np.float32)
     p = net.initial_params(seed=3)
     p += rng.normal(0, 0.02, p.size).astype(np.float32)
     net.set_params(p)
-    f = torch.from_numpy(feats.reshape(2, -1, 2)).cuda()
+    f = torch.from_numpy(feats.reshape(2, -1, 3)).cuda()
     t = torch.from_numpy(target.reshape(2, -1)).cuda()
     loss, g = net.gradients(f, t, (32, 32, 32))
     o = U.UNetOracle(p.astype(np.float64), bf16=True)
@@ -156,12 +156,15 @@ def test_features_match_host():
     from parallelcmacionize_b200 import blocked_to_cube
     cube = blocked_to_cube(nH, spec.ncell, spec.num_subgrid)
     with UNet() as n:
-        n.norm = np.array([8.0, 0.5, 12.0, 2.0], np.float32)
+        n.norm = np.array([8.0, 0.5, 12.0, 2.0, 1.0, 3.0], np.float32)
         f = n.features(torch.from_numpy(cube.ravel().copy()).cuda(), spec).cpu().numpy()
     np.testing.assert_allclose(f[:, 0], (np.log10(cube.ravel()) - 8.0) / 0.5, rtol=1e-5,
                                atol=1e-5)
     np.testing.assert_allclose(f[:, 1], (flux_proxy(spec).ravel() - 12.0) / 2.0, rtol=1e-5,
                                atol=1e-5)
+    # the ray sums use explicitly rounded FP64 on both sides: same sample cells
+    np.testing.assert_allclose(f[:, 2], (stromgren_ratio(spec, cube).ravel() - 1.0) / 3.0,
+                               rtol=1e-5, atol=1e-5)
 
 
 def test_training_reduces_loss():
@@ -173,7 +176,8 @@ def test_training_reduces_loss():
     import scipy.ndimage as nd
     f = np.stack([nd.gaussian_filter(f[..., k], (0, 2, 2, 2)) * 3 for k in range(2)], -1)
     target = (np.tanh(f[..., 0]) - 0.5 * f[..., 1]).astype(np.float32)
-    ft = torch.from_numpy(f.reshape(4, -1, 2).astype(np.float32)).cuda()
+    f = np.concatenate([f, f[..., :1] * f[..., 1:]], axis=-1)  # a third channel
+    ft = torch.from_numpy(f.reshape(4, -1, 3).astype(np.float32)).cuda()
     tt = torch.from_numpy(target.reshape(4, -1)).cuda()
     with UNet(seed=1) as n:
         losses = [n.train_step(ft, tt, (32, 32, 32), 3e-3) for _ in range(60)]

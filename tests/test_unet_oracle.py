@@ -45,7 +45,7 @@ def test_pool_and_upsample_adjoints():
 
 
 def test_parameter_count():
-    assert U.num_params() == 199_189  # the default 12/24/48 network (~2e5)
+    assert U.num_params() == 199_513  # the default 12/24/48 network (~2e5)
     p = U.init_params()
     assert p.size == U.num_params()
     convs, (hw, hb) = U.split_params(p)
@@ -58,7 +58,7 @@ def test_oracle_gradient_matches_finite_differences(seed):
     rng = np.random.default_rng(seed)
     p = U.init_params(*c, seed=seed)
     p[:] += rng.normal(0, 0.05, p.size)  # non-zero biases
-    feats = rng.normal(size=(2, 8, 8, 8, 2))
+    feats = rng.normal(size=(2, 8, 8, 8, 3))
     target = rng.normal(size=(2, 8, 8, 8))
     net = U.UNetOracle(p, *c)
     loss, g = net.gradients(feats, target)
