@@ -42,7 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CROSSING = 32  # FP64 n, x read + J read-modify-write per crossing
-METRIC = "cell-crossings/s"
+METRIC = "cell-crossings/s"  # plus time to converged x_H, warm start vs plain ("warm_start")
 UNIT = "crossings/s"
 DESCRIPTIONS = {
     "lognormal128": ("lognormal128: 128^3 cells as 8^3 subgrids of 16^3, log-normal n_H "
@@ -75,7 +75,49 @@ def parse():
                     help="most packets per instance in the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-warm-start", action="store_true",
+                    help="skip the time-to-convergence comparison (warm start vs plain)")
+    ap.add_argument("--warm-start-seeds", type=int, default=4)
     return ap.parse_args()
+
+
+WARM_WORKLOAD = ("warmstart64: 64^3 log-normal generator (sigma_ln=1, 4 sources, 5 packets per "
+                 "cell), held-out seeds of the shipped network; convergence = mean |delta x_H| "
+                 "< 0.01 (the plain method's criterion)")
+
+
+def warm_start_comparison(seeds):
+    """Time to converged x_H from x_H = 1e-6 and from the learned warm start
+    (features + network + iterations, n_H on the device), on held-out seeds;
+    accuracy against a long plain run (24 iterations, last 6 averaged)."""
+    from parallelcmacionize_b200.warmstart import (DEFAULT_WEIGHTS, UNet, generate_runs,
+                                                   run_configs, time_to_converge)
+    if not os.path.exists(DEFAULT_WEIGHTS):
+        return None
+    runs = []
+    with UNet.load(DEFAULT_WEIGHTS) as net:
+        for s in seeds:
+            g, nH = run_configs([s])[0]
+            _, _, labels, _ = generate_runs([s], batch=1)
+            runs.append(time_to_converge(net, g, nH, x_reference=10.0 ** labels[0].astype(float),
+                                         tolerance=0.01))
+
+    def mean(mode, key):
+        return float(np.mean([r[mode][key] for r in runs]))
+    return {
+        "workload": WARM_WORKLOAD, "seeds": list(seeds),
+        "plain_ms": 1e3 * mean("plain", "seconds"), "warm_ms": 1e3 * mean("warm", "seconds"),
+        "plain_iterations": mean("plain", "iterations"),
+        "warm_iterations": mean("warm", "iterations"),
+        "speedup": float(np.median([r["speedup"] for r in runs])),
+        "plain_error_vs_reference": mean("plain", "error_vs_reference"),
+        "warm_error_vs_reference": mean("warm", "error_vs_reference"),
+        "mean_abs_dx_warm_vs_plain": float(np.mean([r["mean_abs_dx_between"] for r in runs])),
+        "mean_abs_dx_plain_vs_plain": float(np.mean([r["mean_abs_dx_plain_vs_plain"]
+                                                     for r in runs])),
+        "warm_overhead_ms": {k: float(np.mean([r["warm_breakdown_ms"][k] for r in runs]))
+                             for k in runs[0]["warm_breakdown_ms"]},
+    }
 
 
 class Workload:
@@ -372,6 +414,10 @@ def ours(args):
                           "crossings counted by replaying the same packets through the "
                           "oracle walk")}
 
+    warm = None
+    if rank == 0 and world == 1 and not args.no_warm_start:
+        warm = warm_start_comparison([101_980 + k for k in range(args.warm_start_seeds)])
+
     if rank == 0:
         ncells = sum(int(np.prod(g.ncell)) for g in wl.specs)
         line = {
@@ -399,6 +445,7 @@ def ours(args):
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "warm_start": warm,
             "mean_abs_dx_last": stats[-1]["mean_abs_dx"],
             "rounds": stats[-1]["rounds"],
         }
