@@ -481,6 +481,41 @@ def time_to_converge(net, grid, nH_blocked, x_reference=None, tolerance=0.01,
     return out
 
 
+def time_steps(steps, batch=8, ncell=64, log=print, warmup=3):
+    """Wall time per training step and per inference pass of the default
+    network on synthetic features (device-synchronised, after warm-up)."""
+    import json
+
+    import torch
+    rng = np.random.default_rng(0)
+    n = ncell ** 3
+    f = torch.from_numpy(rng.normal(size=(batch, n, NUM_FEATURES)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.normal(-1, 1, size=(batch, n)).astype(np.float32)).cuda()
+    dims = (ncell,) * 3
+    with UNet() as net:
+        for _ in range(warmup):
+            net.train_step(f, t, dims, 1e-4)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            net.train_step(f, t, dims, 1e-4)
+        torch.cuda.synchronize()
+        train_ms = (time.perf_counter() - t0) * 1e3 / steps
+        f1 = f[:1].contiguous()
+        for _ in range(warmup):
+            net.forward(f1, dims)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            net.forward(f1, dims)
+        torch.cuda.synchronize()
+        infer_ms = (time.perf_counter() - t0) * 1e3 / steps
+    log(json.dumps({"train_step_ms": train_ms, "batch": batch, "ncell": ncell,
+                    "voxels_per_s": batch * n / (train_ms / 1e3),
+                    "inference_ms_batch1": infer_ms}))
+    return 0
+
+
 def main(argv=None):
     import argparse
     import json
@@ -498,9 +533,14 @@ def main(argv=None):
     ap.add_argument("--eval", type=int, default=16, help="held-out runs for the wall-time test")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--time-steps", type=int, default=0,
+                    help="only time this many training steps and inference passes on "
+                         "synthetic 64^3 data (batch --batch) and exit")
     a = ap.parse_args(argv)
     log = (lambda s: print(s, flush=True))
     torch.cuda.set_device(0)
+    if a.time_steps:
+        return time_steps(a.time_steps, a.batch, a.ncell, log)
     ntrain = int(round(0.8 * a.runs))
     seeds = [100_000 + i for i in range(a.runs)]
     t0 = time.perf_counter()

@@ -37,8 +37,10 @@ def test_warm_start_converges_faster_to_the_same_field(net, seed):
     assert r["plain"]["converged"] and r["warm"]["converged"]
     # at least 3 iterations fewer (plain needs 6-8 on this generator)
     assert r["warm"]["iterations"] <= r["plain"]["iterations"] - 3, r
-    # converged as accurately as the plain method, to the Monte Carlo spread
-    assert r["warm"]["error_vs_reference"] <= r["plain"]["error_vs_reference"] + 0.01, r
-    assert r["mean_abs_dx_between"] <= r["mean_abs_dx_plain_vs_plain"] + 0.01, r
+    # as accurate as the plain method's own converged field, against the long
+    # run (two plain runs share their start and so their remaining convergence
+    # error; the warm start reaches the fixed point from another side, so its
+    # distance to a plain run is no accuracy measure)
+    assert r["warm"]["error_vs_reference"] <= r["plain"]["error_vs_reference"] + 0.005, r
     # wall time, features and network included (the bench measures it precisely)
     assert r["speedup"] > 1.5, r
