@@ -258,9 +258,12 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
               smem_u32(&empty[s]))
           : "memory");
-      if (k + kStages < nsteps) {
-        ok = mbar_wait(&empty[s], ph, a.err);  // the MMA has read stage s
-        if (ok) load(k + kStages);
+      // refill the stage of the previous MMA (MMA k stays queued meanwhile)
+      const int kp = k - 1;
+      if (kp >= 0 && kp + kStages < nsteps) {
+        const int sp = kp % kStages;
+        ok = mbar_wait(&empty[sp], (uint32_t)(kp / kStages) & 1u, a.err);
+        if (ok) load(kp + kStages);
       }
     }
     asm volatile(
@@ -361,31 +364,27 @@ __global__ void __launch_bounds__(256) k_conv3_wgrad(WgradArgs a) {
       const uint4 raw = *reinterpret_cast<const uint4 *>(a.dy + (base + v) * a.dy_ctot + a.dy_c0 +
                                                          q * 8);
       const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw);
-      float *o = sdy + v * a.cout + q * 8;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float2 f = __bfloat1622float2(h[k]);
-        o[2 * k] = f.x;
-        o[2 * k + 1] = f.y;
-      }
+      const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]),
+                   f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
+      float4 *o = reinterpret_cast<float4 *>(sdy + v * a.cout + q * 8);
+      o[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
+      o[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
     }
     for (int i = threadIdx.x; i < X * xq; i += blockDim.x) {
       const int v = i / xq, q = i - v * xq;
       const int qx = v + dx;
-      float *o = sx + v * a.cin + q * 8;
+      float4 *o = reinterpret_cast<float4 *>(sx + v * a.cin + q * 8);
       if (row_in && qx >= 0 && qx < X) {
         const uint4 raw = *reinterpret_cast<const uint4 *>(a.x + (qbase + qx) * a.x_ctot +
                                                            a.x_c0 + q * 8);
         const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const float2 f = __bfloat1622float2(h[k]);
-          o[2 * k] = f.x;
-          o[2 * k + 1] = f.y;
-        }
+        const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]),
+                     f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
+        o[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
+        o[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
       } else {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) o[k] = 0.f;
+        o[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+        o[1] = o[0];
       }
     }
     __syncthreads();
