@@ -114,7 +114,9 @@ typedef struct {
   int32_t use_graph;           /* 1 = capture each iteration as a CUDA graph (default) */
   int32_t max_run_chunks;      /* most chunks a CTA claims at once (0 = 64): how long a CTA
                                   stays on one subgrid before flushing its tallies */
-  int32_t reserved[6];
+  int32_t refill_lanes;        /* FP32 walk: a warp routes finished packets and refills its
+                                  lanes once this many lanes are not walking (0 = 16; 1..32) */
+  int32_t reserved[5];
 } cmi_options;
 
 /* Per-instance counters of one iteration. */

@@ -95,7 +95,8 @@ class Options(C.Structure):
         ("tally_mode", C.c_int32),
         ("use_graph", C.c_int32),
         ("max_run_chunks", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("refill_lanes", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

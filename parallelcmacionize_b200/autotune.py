@@ -15,6 +15,8 @@ A candidate (``WalkConfig``) chooses:
 * ``packets_per_chunk`` -- packets a CTA takes per claim (the packet ring slot),
 * ``max_run_chunks``    -- most chunks claimed at once: how long a CTA stays on
   one subgrid before it flushes its shared tallies to J,
+* ``refill_lanes``      -- lanes a warp lets go idle before it routes finished
+  packets and refills them in one batch,
 * ``tally``             -- shared-memory tally form of the FP32 walk,
 * ``ctas_per_sm``       -- 0 = the engine's occupancy choice.
 
@@ -43,6 +45,7 @@ class WalkConfig:
     max_run_chunks: int = 64
     tally: str = "fixed64"
     ctas_per_sm: int = 0
+    refill_lanes: int = 16
 
     def grid(self, base: GridSpec) -> GridSpec:
         """``base`` re-decomposed into subgrids of ``sub_side`` cells per axis."""
@@ -54,11 +57,12 @@ class WalkConfig:
 
     def engine_options(self) -> dict:
         return dict(packets_per_chunk=self.packets_per_chunk, tally=self.tally,
-                    ctas_per_sm=self.ctas_per_sm, max_run_chunks=self.max_run_chunks)
+                    ctas_per_sm=self.ctas_per_sm, max_run_chunks=self.max_run_chunks,
+                    refill_lanes=self.refill_lanes)
 
 
 def candidates(ncell, precision="fp32", sides=(8, 16), chunks=(64, 128, 256),
-               runs=(16, 64), tallies=("fixed64",), ctas=(0,)):
+               runs=(16, 64), tallies=("fixed64",), ctas=(0,), refills=(16,)):
     """Every valid combination for a grid of ``ncell`` cells per axis.
 
     A side must divide every axis.  The FP64 walk has no shared tallies and no
@@ -71,8 +75,8 @@ def candidates(ncell, precision="fp32", sides=(8, 16), chunks=(64, 128, 256),
     if precision == "fp64":
         return [WalkConfig(sub_side=s, packets_per_chunk=0, max_run_chunks=0, tally="fixed64",
                            ctas_per_sm=0) for s in ok_sides]
-    return [WalkConfig(s, c, r, t, k) for s in ok_sides for c in chunks for r in runs
-            for t in tallies for k in ctas]
+    return [WalkConfig(s, c, r, t, k, f) for s in ok_sides for c in chunks for r in runs
+            for t in tallies for k in ctas for f in refills]
 
 
 def default_cache_path() -> str:

@@ -50,6 +50,7 @@ int fail(int code, const char *fmt, ...) {
 
 constexpr int kWalkThreads = 256;
 constexpr int kSpareRounds = 3;  // wavefront rounds beyond the straight-line bound
+constexpr uint32_t kDefaultRefill = 16;  // lanes not walking before a warp routes + refills
 
 struct HostInstance {
   cmi_grid_desc desc;
@@ -337,6 +338,7 @@ WalkParams walk_params(cmi_context *c) {
   WalkParams p{};
   p.chunk = c->chunk;
   p.max_run = c->opt.max_run_chunks > 0 ? (uint32_t)c->opt.max_run_chunks : 64u;
+  p.refill = c->opt.refill_lanes > 0 ? (uint32_t)c->opt.refill_lanes : kDefaultRefill;
   p.subs = c->d_sub;
   p.inst = c->d_inst;
   p.chunks = c->d_chunks;
@@ -657,6 +659,8 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
     return fail(CMI_ERR_INVALID_ARGUMENT,
                 "packets_per_chunk must be 0 or a power of two in [32, 4096]");
   if (opt.max_run_chunks < 0) return fail(CMI_ERR_INVALID_ARGUMENT, "negative max_run_chunks");
+  if (opt.refill_lanes < 0 || opt.refill_lanes > 32)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "refill_lanes must be in [0, 32]");
   if (opt.tally_mode < CMI_TALLY_FP32 || opt.tally_mode > CMI_TALLY_FIXED64_ATOMIC64)
     return fail(CMI_ERR_INVALID_ARGUMENT, "unknown tally mode %d", opt.tally_mode);
 

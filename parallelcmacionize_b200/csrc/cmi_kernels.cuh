@@ -580,6 +580,7 @@ __global__ void __launch_bounds__(256) k_scatter(const P *out, const uint32_t *k
 struct WalkParams {
   uint32_t chunk;          // largest chunk (packets), FP32 packet-buffer size
   uint32_t max_run;        // most chunks claimed at once
+  uint32_t refill;         // FP32 walk: lanes not walking before a warp routes + refills
   const DevSubgrid *subs;
   const DevInstance *inst;
   const Chunk *chunks;
@@ -1167,88 +1168,94 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
       tally.carry_J = prm.J + sh.field_offset;
       tally.carry_value = 4294967296.0 * sh.tally_unit * sh.sigma;
       Walk32 w;
-      bool exhausted = false, have = false, fresh = false;
-      int entry = kRun;
+      // lane states: active (walking), pending (finished, not yet routed), free
+      bool exhausted = false, active = false, pending = false;
+      int pstatus = kRun;
       for (;;) {
-        const unsigned idle = __ballot_sync(kFull, !have);
-        if (idle != 0u && !exhausted) {
-          const uint32_t need = (uint32_t)__popc(idle);
-          uint32_t base = 0;
-          if (lane == 0) base = atomicAdd(&sh.claim, need);
-          base = __shfl_sync(kFull, base, 0);
-          if (base >= nseg) {
-            exhausted = true;
-          } else {
-            const uint32_t take = min(need, nseg - base);
-            const uint32_t k0 = base >> ch_shift, k1 = (base + take - 1u) >> ch_shift;
-            wait_chunk(k0);
-            if (k1 != k0) wait_chunk(k1);
-            const uint32_t r = (uint32_t)__popc(idle & lt);
-            if (!have && r < take) {
-              const uint32_t vi = base + r;
-              const uint32_t k = vi >> ch_shift;
-              const Packet32 pk = s_pk[(size_t)(k & 1u) * CH + (vi - (k << ch_shift))];
-              entry = w.begin(pk, v, sh.tab.sign_code);
-              have = true;
-              fresh = true;
-            }
-            __syncwarp();
-            if (lane == 0) {
-              const uint32_t n0 = min(take, ((k0 + 1u) << ch_shift) - base);
-              consumed(k0, n0);
-              if (take > n0) consumed(k1, take - n0);
-            }
-          }
-        }
-        if (!__any_sync(kFull, have)) {
-          if (exhausted) break;
-          continue;
-        }
-        int status = kRun;
-        if (have) {
-          if (fresh) {
-            status = entry;
-            fresh = false;
-          }
-          if (status == kRun) {
-            int tcell;
-            float len;
-            status = w.step(v, tcell, len);
-            tally.add(tcell, len);
-            if (status == kRun && w.steps > limit) status = kDrop;
-          }
-        }
-        const bool fin = have && status != kRun;
-        if (__any_sync(kFull, fin)) {
-          uint32_t key = kOutside, meta = 0;
-          bool append = false;
-          if (fin) {
-            ++c_trans;
-            c_cross += (uint32_t)w.steps;  // one step per crossed cell
-            if (status == kExited) {
-              const int od = sh.tab.mask_dir[w.exit_mask(v)];
-              if (od >= kNumDirections) {
-                atomicOr(&st->flags, kFlagWalkLimit);
+        const unsigned running = __ballot_sync(kFull, active);
+        // Finished packets are routed and free lanes refilled in one batch,
+        // once at least `refill` lanes are not walking (or none is): both
+        // blocks are divergent, so running them for one or two lanes at a time
+        // would cost more than the crossings they serve.
+        if ((uint32_t)(32 - __popc(running)) >= prm.refill || running == 0u) {
+          if (__any_sync(kFull, pending)) {
+            uint32_t key = kOutside, meta = 0;
+            bool append = false;
+            if (pending) {
+              ++c_trans;
+              c_cross += (uint32_t)w.steps;  // one step per crossed cell
+              if (pstatus == kExited) {
+                const int od = sh.tab.mask_dir[w.exit_mask(v)];
+                if (od >= kNumDirections) {
+                  atomicOr(&st->flags, kFlagWalkLimit);
+                } else {
+                  key = sh.ngb[od];
+                  meta = sh.tab.mirror[od];
+                  if (key == kOutside) ++c_esc; else append = true;
+                }
+              } else if (pstatus == kAbsorbed) {
+                ++c_abs;
               } else {
-                key = sh.ngb[od];
-                meta = sh.tab.mirror[od];
-                if (key == kOutside) ++c_esc; else append = true;
+                atomicOr(&st->flags, kFlagWalkLimit);
               }
-            } else if (status == kAbsorbed) {
-              ++c_abs;
-            } else {
-              atomicOr(&st->flags, kFlagWalkLimit);
+              pending = false;
             }
-            have = false;
+            const unsigned am = __ballot_sync(kFull, append);
+            if (append) {
+              const uint32_t slot = nstage + (uint32_t)__popc(am & lt);
+              my_stage[slot] = w.packet(meta);
+              my_skey[slot] = key;
+            }
+            nstage += (uint32_t)__popc(am);
+            if (nstage >= kStageFlush) flush_stage(min(nstage, 32u));
           }
-          const unsigned am = __ballot_sync(kFull, append);
-          if (append) {
-            const uint32_t slot = nstage + (uint32_t)__popc(am & lt);
-            my_stage[slot] = w.packet(meta);
-            my_skey[slot] = key;
+          if (!exhausted) {
+            const unsigned idle = ~running;  // every lane that is not walking
+            const uint32_t need = (uint32_t)__popc(idle);
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&sh.claim, need);
+            base = __shfl_sync(kFull, base, 0);
+            if (base >= nseg) {
+              exhausted = true;
+            } else {
+              const uint32_t take = min(need, nseg - base);
+              const uint32_t k0 = base >> ch_shift, k1 = (base + take - 1u) >> ch_shift;
+              wait_chunk(k0);
+              if (k1 != k0) wait_chunk(k1);
+              const uint32_t r = (uint32_t)__popc(idle & lt);
+              if (!active && r < take) {
+                const uint32_t vi = base + r;
+                const uint32_t k = vi >> ch_shift;
+                const Packet32 pk = s_pk[(size_t)(k & 1u) * CH + (vi - (k << ch_shift))];
+                const int entry = w.begin(pk, v, sh.tab.sign_code);
+                if (entry == kRun) {
+                  active = true;
+                } else {  // absorbed or outside at entry: routed next batch
+                  pending = true;
+                  pstatus = entry;
+                }
+              }
+              __syncwarp();
+              if (lane == 0) {
+                const uint32_t n0 = min(take, ((k0 + 1u) << ch_shift) - base);
+                consumed(k0, n0);
+                if (take > n0) consumed(k1, take - n0);
+              }
+            }
           }
-          nstage += (uint32_t)__popc(am);
-          if (nstage >= kStageFlush) flush_stage(min(nstage, 32u));
+          if (exhausted && !__any_sync(kFull, active || pending)) break;
+        }
+        if (active) {
+          int tcell;
+          float len;
+          int status = w.step(v, tcell, len);
+          tally.add(tcell, len);
+          if (status == kRun && w.steps > limit) status = kDrop;
+          if (status != kRun) {
+            active = false;
+            pending = true;
+            pstatus = status;
+          }
         }
       }
       __syncthreads();  // segment done: every packet of it is traced

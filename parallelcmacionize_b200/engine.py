@@ -92,7 +92,7 @@ class TransportEngine:
 
     def __init__(self, grids, precision="fp32", balance="stable", rng="philox", device=0,
                  packets_per_chunk=0, tally="fixed64", use_graph=True, ctas_per_sm=0,
-                 max_run_chunks=0):
+                 max_run_chunks=0, refill_lanes=0):
         if isinstance(grids, GridSpec):
             grids = [grids]
         self.grids = list(grids)
@@ -103,7 +103,7 @@ class TransportEngine:
             rng={"philox": _lib.RNG_PHILOX, "ranlux": _lib.RNG_RANLUX}[rng],
             device=device, packets_per_chunk=packets_per_chunk,
             tally_mode=TALLY_MODES[tally], use_graph=int(bool(use_graph)),
-            ctas_per_sm=ctas_per_sm, max_run_chunks=max_run_chunks)
+            ctas_per_sm=ctas_per_sm, max_run_chunks=max_run_chunks, refill_lanes=refill_lanes)
         descs = (_lib.GridDesc * len(self.grids))(*[g.desc() for g in self.grids])
         h = C.c_void_p()
         check(self._L.cmi_create(descs, len(self.grids), C.byref(opts), C.byref(h)))

@@ -177,27 +177,29 @@ def test_transport_packets_fp32_matches_cpu_spec():
 
 def test_transport_fp32_independent_of_chunking():
     """The FP32 walk's packet ring (chunks of 32 .. 1024 packets, claimed up
-    to 256 packets ahead of the copies, runs of 1 .. 64 chunks per claim):
+    to 256 packets ahead of the copies, runs of 1 .. 64 chunks per claim, lanes
+    routed and refilled one at a time up to all 32 at once):
     every chunking traces the same packets, so the counts are identical and J
     (exact fixed-point sums, merged into FP64 in varying order) agrees to FP64
     rounding."""
     spec, nH = lognormal_config(ncell=64, num_subgrid=4, num_photon=400_000, num_sources=3)
     ref = None
-    for chunk, run in [(128, 0), (32, 0), (64, 0), (64, 1), (256, 8), (1024, 0)]:
+    for chunk, run, refill in [(128, 0, 0), (32, 0, 0), (64, 0, 0), (64, 1, 0), (256, 8, 0),
+                               (1024, 0, 0), (128, 0, 1), (128, 0, 32), (64, 4, 5)]:
         eng = TransportEngine(spec, precision="fp32", packets_per_chunk=chunk,
-                              max_run_chunks=run)
+                              max_run_chunks=run, refill_lanes=refill)
         eng.set_fields(0, nH)
         st = [eng.shoot_packets(seed=9, iteration=i)[0] for i in range(2)]
         _, J = eng.get_fields(0)
         eng.close()
         for s in st:
-            assert s["error_flags"] == 0, (chunk, run)
+            assert s["error_flags"] == 0, (chunk, run, refill)
             assert s["packets_absorbed"] + s["packets_escaped"] == 400_000
         key = [(s["cell_crossings"], s["packets_absorbed"], s["subgrid_transits"]) for s in st]
         if ref is None:
             ref = (key, J)
             continue
-        assert key == ref[0], (chunk, run)
+        assert key == ref[0], (chunk, run, refill)
         np.testing.assert_allclose(J, ref[1], rtol=1e-12, atol=0)
 
 
