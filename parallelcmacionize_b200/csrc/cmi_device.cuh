@@ -132,7 +132,8 @@ struct alignas(16) RoundState {
   uint32_t flags;          // CMI_FLAG_* of the whole context
   uint32_t rounds_active;
   uint32_t capacity;       // arena capacity (packets)
-  uint32_t pad[3];
+  uint32_t round_index;    // walks started this iteration (graph loop)
+  uint32_t pad[2];
 };
 
 // FP64 packet: the reference Photon layout (80 B); `meta` (the reserved

@@ -100,6 +100,7 @@ struct cmi_context {
   double *d_nH = nullptr, *d_xH = nullptr, *d_J = nullptr;
   float *d_kappa = nullptr;
   uint64_t *d_src_count = nullptr, *d_src_first = nullptr, *d_buf_first = nullptr;
+  uint32_t *d_src_rank0 = nullptr;  // first place of each source's packets in its bucket
   RoundState *d_state = nullptr;
   DevStats *d_stats = nullptr;
   uint32_t *d_hist = nullptr, *d_bucket_off = nullptr;
@@ -122,7 +123,10 @@ struct cmi_context {
   // graph of one iteration
   cudaGraphExec_t graph_exec = nullptr;
   bool graph_dirty = true;
-  uint64_t graph_kernels = 0;
+  bool capturing = false;        // enqueue_iteration is being captured
+  cudaStream_t body_stream = nullptr;  // captures the round loop's body
+  uint64_t graph_kernels = 0;    // kernels per iteration outside the round loop
+  uint64_t graph_body_kernels = 0;  // kernels per round of the loop
   uint64_t last_launches = 0;
   uint64_t enqueued = 0;  // kernel launches of the current enqueue
   DevStats *h_stats = nullptr;  // pinned
@@ -275,12 +279,15 @@ int upload_tables(cmi_context *c) {
   dev_free(c->d_src);
   dev_free(c->d_src_count);
   dev_free(c->d_src_first);
+  dev_free(c->d_src_rank0);
   dev_free(c->d_buf_first);
+  dev_free(c->d_src_rank0);
   c->nsrc_total = (int)ds.size();
   CMI_TRY(dev_alloc(&c->d_src, ds.size()));
   CMI_TRY(dev_alloc(&c->d_src_count, ds.size() + 1));
   CMI_TRY(dev_alloc(&c->d_src_first, ds.size() + 1));
   CMI_TRY(dev_alloc(&c->d_buf_first, ds.size() + 1));
+  CMI_TRY(dev_alloc(&c->d_src_rank0, ds.size() + 1));
   if (!ds.empty())
     CMI_CUDA(cudaMemcpyAsync(c->d_src, ds.data(), sizeof(DevSource) * ds.size(),
                              cudaMemcpyHostToDevice, c->stream));
@@ -303,7 +310,9 @@ int refresh_kappa(cmi_context *c, int32_t i) {
 // ---------------------------------------------------------------------------
 // launch helpers (each counts its kernel)
 // ---------------------------------------------------------------------------
-int launch_plan(cmi_context *c) {
+// Plan of a round from the bucket histogram; with scatter, the packets the
+// previous step appended are moved into their buckets.
+int launch_plan(cmi_context *c, bool scatter) {
   if (c->ntiles == 1) {
     k_plan_fused<<<1, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk, c->d_bucket_off,
                                                     c->d_chunks, c->d_state);
@@ -319,17 +328,19 @@ int launch_plan(cmi_context *c) {
                                                             c->d_bucket_off, c->d_chunks);
     c->enqueued += 3;
   }
-  const int grid = c->num_sms * 8;
-  if (c->fp32()) {
-    k_scatter<Packet32><<<grid, 256, 0, c->stream>>>(
-        (const Packet32 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
-        (Packet32 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
-  } else {
-    k_scatter<Packet64><<<grid, 256, 0, c->stream>>>(
-        (const Packet64 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
-        (Packet64 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
+  if (scatter) {
+    const int grid = c->num_sms * 8;
+    if (c->fp32()) {
+      k_scatter<Packet32><<<grid, 256, 0, c->stream>>>(
+          (const Packet32 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
+          (Packet32 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
+    } else {
+      k_scatter<Packet64><<<grid, 256, 0, c->stream>>>(
+          (const Packet64 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
+          (Packet64 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
+    }
+    c->enqueued += 1;
   }
-  c->enqueued += 1;
   CMI_CUDA(cudaGetLastError());
   return CMI_OK;
 }
@@ -453,42 +464,100 @@ EmitParams emit_params(cmi_context *c) {
   e.ranks = c->d_ranks;
   e.hist = c->d_hist;
   e.capacity = (uint32_t)c->capacity;
+  e.src_rank0 = c->d_src_rank0;
+  e.bucket_off = c->d_bucket_off;
+  e.arena_sorted = c->d_arena_in;
   return e;
 }
 
-// Wavefront rounds after packets were appended to the arena.
+// Wavefront rounds once round 0 is planned: walk, then plan (+ scatter) the
+// packets it passed on; the last plan counts what is left over (must be zero).
 int enqueue_rounds(cmi_context *c) {
   for (int r = 0; r < c->rounds; ++r) {
-    CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c); }));
     CMI_TRY(timed_launch(c, 0, [&] { return launch_walk(c); }));
+    CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c, true); }));
   }
-  // final plan: counts what the last round left over (must be zero)
-  CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c); }));
+  return CMI_OK;
+}
+
+// The rounds inside a captured iteration: a WHILE conditional node runs
+// (walk -> plan -> gate) while packets remain, so an iteration stops after the
+// rounds it needs instead of the worst-case count (k_round_gate).
+int enqueue_rounds_graph(cmi_context *c) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  CMI_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) return fail(CMI_ERR_CUDA, "stream is not capturing");
+  cudaGraphConditionalHandle h;
+  CMI_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  k_round_gate<<<1, 32, 0, c->stream>>>(c->d_state, h, (uint32_t)c->rounds);
+  c->enqueued += 1;
+  CMI_CUDA(cudaGetLastError());
+  CMI_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CMI_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  CMI_CUDA(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1,
+                                               cudaStreamSetCaptureDependencies));
+  // the loop body, captured on the second stream into the node's graph
+  CMI_CUDA(cudaStreamBeginCaptureToGraph(c->body_stream, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+  cudaStream_t outer = c->stream;
+  const uint64_t before = c->enqueued;
+  c->stream = c->body_stream;
+  int rc = launch_walk(c);
+  if (rc == CMI_OK) rc = launch_plan(c, true);
+  if (rc == CMI_OK) {
+    k_round_gate<<<1, 32, 0, c->stream>>>(c->d_state, h, (uint32_t)c->rounds);
+    c->enqueued += 1;
+    if (cudaGetLastError() != cudaSuccess) rc = fail(CMI_ERR_CUDA, "round gate launch");
+  }
+  c->stream = outer;
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(c->body_stream, &captured);
+  if (rc != CMI_OK) return rc;
+  if (ee != cudaSuccess)
+    return fail(CMI_ERR_CUDA, "round loop capture: %s", cudaGetErrorString(ee));
+  c->graph_body_kernels = c->enqueued - before;
+  c->enqueued = before;  // body kernels are counted per executed round
   return CMI_OK;
 }
 
 int enqueue_iteration(cmi_context *c, bool balance) {
   const int ninst = (int)c->inst.size();
   k_begin_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst);
+  // Philox packets are written straight into their sorted place: the
+  // emission plan fills the round-0 histogram, the plan places the buckets
+  const bool direct = c->opt.rng == CMI_RNG_PHILOX;
   k_emission_plan<<<1, 128, 0, c->stream>>>(c->d_inst, ninst, c->d_src, c->nsrc_total,
                                             c->d_state, c->d_src_count, c->d_src_first,
-                                            c->d_buf_first, c->d_stats);
+                                            c->d_buf_first, c->d_stats,
+                                            direct ? c->d_src_rank0 : nullptr, c->d_hist);
   c->enqueued += 2;
   const EmitParams e = emit_params(c);
   const int egrid = c->num_sms * 8;
+  if (direct) CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c, false); }));
   CMI_TRY(timed_launch(c, 2, [&] {
     if (c->opt.rng == CMI_RNG_RANLUX) {
       if (c->fp32()) k_emit_ranlux<true><<<egrid, 128, 0, c->stream>>>(e);
       else k_emit_ranlux<false><<<egrid, 128, 0, c->stream>>>(e);
     } else {
-      if (c->fp32()) k_emit_philox<true><<<egrid, 256, 0, c->stream>>>(e);
-      else k_emit_philox<false><<<egrid, 256, 0, c->stream>>>(e);
+      if (c->fp32()) k_emit_philox_direct<true><<<egrid, 256, 0, c->stream>>>(e);
+      else k_emit_philox_direct<false><<<egrid, 256, 0, c->stream>>>(e);
     }
     return CMI_OK;
   }));
   c->enqueued += 1;
   CMI_CUDA(cudaGetLastError());
-  CMI_TRY(enqueue_rounds(c));
+  if (!direct) CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c, true); }));
+  CMI_TRY(c->capturing ? enqueue_rounds_graph(c) : enqueue_rounds(c));
   if (balance) {
     BalanceParams b{};
     b.subs = c->d_sub;
@@ -562,7 +631,9 @@ int run(cmi_context *c, int32_t iterations, uint64_t seed, uint32_t first_iterat
     cudaGraph_t g = nullptr;
     CMI_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     c->enqueued = 0;
+    c->capturing = true;
     const int rc = enqueue_iteration(c, true);
+    c->capturing = false;
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     if (rc != CMI_OK) {
       if (g) cudaGraphDestroy(g);
@@ -590,12 +661,18 @@ int run(cmi_context *c, int32_t iterations, uint64_t seed, uint32_t first_iterat
   }
   CMI_CUDA(cudaStreamSynchronize(c->stream));
   uint32_t flags_any = 0;
-  for (int32_t it = 0; it < iterations; ++it)
+  for (int32_t it = 0; it < iterations; ++it) {
+    if (use_graph && ninst > 0) {  // the round loop ran once per round with packets
+      const uint32_t r = std::min<uint32_t>(c->h_stats[(size_t)it * ninst].rounds,
+                                            (uint32_t)c->rounds);
+      c->last_launches += c->graph_body_kernels * r;
+    }
     for (int i = 0; i < ninst; ++i) {
       const DevStats &d = c->h_stats[(size_t)it * ninst + i];
       flags_any |= d.flags;
       if (stats) to_stats(d, c->inst[i], stats[(size_t)it * ninst + i]);
     }
+  }
   if (flags_any & (kFlagArenaOverflow | kFlagLeftover))
     return fail(CMI_ERR_CAPACITY, "device queue overflow or packets left over (flags 0x%x)",
                 flags_any);
@@ -688,7 +765,9 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
     delete c;
     return fail(CMI_ERR_CUDA, "cudaSetDevice failed");
   }
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return fail(CMI_ERR_CUDA, "stream creation failed");
   }
@@ -839,6 +918,7 @@ int cmi_destroy(cmi_context *c) {
   }
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->body_stream) cudaStreamDestroy(c->body_stream);
   delete c;
   return CMI_OK;
 }
@@ -1071,6 +1151,7 @@ int cmi_transport_packets(cmi_context *c, int32_t instance, const cmi_photon *pa
   else k_upload<false><<<grid, 256, 0, c->stream>>>(u);
   CMI_CUDA(cudaGetLastError());
   c->enqueued = 0;
+  CMI_TRY(launch_plan(c, true));
   CMI_TRY(enqueue_rounds(c));
   k_end_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst, 0);
   CMI_CUDA(cudaGetLastError());

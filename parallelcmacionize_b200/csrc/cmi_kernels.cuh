@@ -133,6 +133,7 @@ __global__ void k_begin_iteration(RoundState *st, DevStats *stats, int ninst) {
   }
   if (threadIdx.x == 0) {
     st->rounds_active = 0;
+    st->round_index = 0;
     st->arena_count = 0;
     st->num_chunks = 0;
     st->chunk_next = 0;
@@ -153,13 +154,29 @@ __global__ void k_end_iteration(RoundState *st, DevStats *stats, int ninst, int 
   }
 }
 
+// Condition of the graph's round loop: another walk when the last plan left
+// packets and fewer than max_rounds walks ran (a packet still in flight after
+// that is reported as left over by k_end_iteration).
+__global__ void k_round_gate(RoundState *st, cudaGraphConditionalHandle h, uint32_t max_rounds) {
+  if (threadIdx.x == 0) {
+    const bool more = st->num_chunks > 0u && st->round_index < max_rounds;
+    if (more) st->round_index += 1u;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+  }
+}
+
 // Packets per source of every instance for this iteration: the reference split
 // (testDensitySubGrid_omp.cpp:2199-2208) with the remainder given to the
 // sources holding the smallest Philox draws (stand-in for distribute(),
 // :1650-1677).  One block.
+// With src_rank0 (direct emission) it also counts every source's packets into
+// the bucket histogram of its subgrid and records where in that bucket the
+// source's packets start, so the emitted packets can be written in sorted
+// order (k_emit_philox_direct) without appends or a scatter.
 __global__ void k_emission_plan(const DevInstance *inst, int ninst, const DevSource *src,
                                 int nsrc_total, RoundState *st, uint64_t *src_count,
-                                uint64_t *src_first, uint64_t *buf_first, DevStats *stats) {
+                                uint64_t *src_first, uint64_t *buf_first, DevStats *stats,
+                                uint32_t *src_rank0, uint32_t *hist) {
   const uint64_t seed = st->seed;
   const uint32_t it = st->iteration;
   for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
@@ -211,6 +228,13 @@ __global__ void k_emission_plan(const DevInstance *inst, int ninst, const DevSou
     buf_first[nsrc_total] = bacc;
     st->emit_total = (uint32_t)acc;
     st->arena_count = 0;
+    if (src_rank0) {  // sources in order: ranks inside each subgrid's bucket
+      for (int s = 0; s < nsrc_total; ++s) {
+        const uint32_t sub = src[s].subgrid;
+        src_rank0[s] = hist[sub];
+        hist[sub] += (uint32_t)src_count[s];
+      }
+    }
   }
 }
 
@@ -229,6 +253,8 @@ struct EmitParams {
   const DevSource *src;
   int nsrc_total;
   const uint64_t *src_count, *src_first, *buf_first;
+  const uint32_t *src_rank0, *bucket_off;  // direct emission
+  void *arena_sorted;                      // direct emission: the walk's input arena
   RoundState *st;
   void *arena;
   uint32_t *keys, *ranks, *hist;
@@ -261,38 +287,36 @@ __device__ __forceinline__ void make_emitted(const DevSource &S, const DevInstan
   }
 }
 
-// Emission with Philox: packet g of the batch belongs to source s; its id in
-// the instance is g - first packet of the instance.
+// Philox emission straight into the sorted arena.  Packet g of the iteration
+// belongs to source s (src_first) and has id g - first packet of its instance
+// in the instance's Philox stream; it goes to bucket_off[subgrid of s] +
+// src_rank0[s] + (g - src_first[s]) (the plan ran on the histogram
+// k_emission_plan filled), so no append atomics and no scatter are needed.
 template <bool kF32>
-__global__ void __launch_bounds__(256) k_emit_philox(EmitParams prm) {
+__global__ void __launch_bounds__(256) k_emit_philox_direct(EmitParams prm) {
   const RoundState *st = prm.st;
   const uint64_t N = st->emit_total;
   const uint64_t seed = st->seed;
   const uint32_t it = st->iteration;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < N; base += stride) {
-    const uint64_t g = base + threadIdx.x;
-    const bool valid = g < N;
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += stride) {
+    const int s = find_bin(prm.src_first, prm.nsrc_total + 1, g);
+    const DevSource S = prm.src[s];
+    const DevInstance I = prm.inst[S.instance];
+    const uint64_t id = g - prm.src_first[I.first_source];
+    double dir[3], tau;
+    philox_packet(seed, S.instance, it, id, dir, tau);
     Packet32 p32{};
     Packet64 p64{};
-    uint32_t key = 0;
-    if (valid) {
-      const int s = find_bin(prm.src_first, prm.nsrc_total + 1, g);
-      const DevSource S = prm.src[s];
-      const DevInstance I = prm.inst[S.instance];
-      const uint64_t id = g - prm.src_first[I.first_source];
-      double dir[3], tau;
-      philox_packet(seed, S.instance, it, id, dir, tau);
-      make_emitted<kF32>(S, I, dir, tau, p32, p64);
-      key = S.subgrid;
+    make_emitted<kF32>(S, I, dir, tau, p32, p64);
+    const uint64_t dst = (uint64_t)prm.bucket_off[S.subgrid] + prm.src_rank0[s] +
+                         (g - prm.src_first[s]);
+    if (dst >= prm.capacity) {
+      atomicOr(&prm.st->flags, kFlagArenaOverflow);
+      continue;
     }
-    if (kF32) {
-      warp_append(valid, key, p32, (Packet32 *)prm.arena, prm.keys, prm.ranks, prm.hist,
-                  prm.st, prm.capacity);
-    } else {
-      warp_append(valid, key, p64, (Packet64 *)prm.arena, prm.keys, prm.ranks, prm.hist,
-                  prm.st, prm.capacity);
-    }
+    if (kF32) store_packet((Packet32 *)prm.arena_sorted + dst, p32);
+    else store_packet((Packet64 *)prm.arena_sorted + dst, p64);
   }
 }
 
