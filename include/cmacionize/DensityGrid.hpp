@@ -122,6 +122,11 @@ class DensityGrid {
     _num_photon = n;
     cmi_check(cmi_set_packet_budget(_ctx, 0, n));
   }
+  // reemission_probability (params.txt): absorbed packets are re-emitted with
+  // this probability (do_reemission, testDensitySubGrid_omp.cpp:675-702)
+  void set_reemission_probability(double p) {
+    cmi_check(cmi_set_reemission_probability(_ctx, 0, p));
+  }
   // shoot num_photon packets from the sources and solve the balance
   // (testDensitySubGrid_omp.cpp:2213-2434), `iterations` times
   std::vector<cmi_stats> run_iterations(int iterations, uint64_t seed) {

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define CMI_ABI_VERSION 1
+#define CMI_ABI_VERSION 2
 #define CMI_NUM_DIRECTIONS 27           /* TRAVELDIRECTION_NUMBER, TravelDirections.hpp:74 */
 #define CMI_NEIGHBOUR_OUTSIDE 0xffffffffu /* NEIGHBOUR_OUTSIDE, DensitySubGrid.hpp:53 */
 #define CMI_PHOTONBUFFER_SIZE 200       /* PHOTONBUFFER_SIZE, PhotonBuffer.hpp:42 */
@@ -129,6 +129,7 @@ typedef struct {
   double mean_abs_dx;        /* mean |x_new - x_old| over the cells of the instance */
   uint32_t error_flags;      /* CMI_FLAG_* bits raised on the device */
   uint32_t rounds;           /* wavefront rounds that carried packets */
+  uint64_t packets_reemitted; /* absorptions followed by a reemission */
 } cmi_stats;
 
 #define CMI_FLAG_ARENA_OVERFLOW 1u
@@ -166,6 +167,14 @@ int cmi_set_sources(cmi_context *context, int32_t instance, const double *positi
                     const double *luminosities, int32_t num_sources);
 /* Packets emitted per iteration by an instance (num_photon). */
 int cmi_set_packet_budget(cmi_context *context, int32_t instance, uint64_t num_photon);
+/* reemission_probability (params.txt; do_reemission,
+ * testDensitySubGrid_omp.cpp:675-702): an absorbed packet is re-emitted from
+ * its absorption point with this probability, in a new isotropic direction
+ * with a new optical depth, and walks on (default 0: absorbed packets are
+ * done).  The draws come from Philox keyed like the instance's emission, with
+ * the absorption position as counter.  packets_absorbed counts the final
+ * absorptions only. */
+int cmi_set_reemission_probability(cmi_context *context, int32_t instance, double probability);
 
 /* Run whole iterations of the plain method on every instance: emit the
  * packets, trace them to absorption or escape, solve the ionization balance

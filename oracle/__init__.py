@@ -85,12 +85,22 @@ class Lattice(C.Structure):
     ]
 
 
+class Reemission(C.Structure):
+    _fields_ = [
+        ("probability", C.c_double),
+        ("seed", C.c_uint64),
+        ("instance", C.c_uint32),
+        ("iteration", C.c_uint32),
+    ]
+
+
 class Counts(C.Structure):
     _fields_ = [
         ("absorbed", C.c_uint64),
         ("escaped", C.c_uint64),
         ("crossings", C.c_uint64),
         ("transits", C.c_uint64),
+        ("reemitted", C.c_uint64),
     ]
 
     def as_dict(self):
@@ -145,6 +155,10 @@ def lib():
                                      C.POINTER(Counts)]
         L.cmio_transport32.argtypes = [C.POINTER(Lattice), pf, pd, C.POINTER(u64), C.c_void_p,
                                        pu32, i64, C.POINTER(Counts)]
+        L.cmio_transport_r.argtypes = [C.POINTER(Lattice), pd, pd, pd, C.c_void_p, pu32, i64,
+                                       C.POINTER(Counts), C.c_void_p]
+        L.cmio_transport32_r.argtypes = [C.POINTER(Lattice), pf, pd, C.POINTER(u64),
+                                         C.c_void_p, pu32, i64, C.POINTER(Counts), C.c_void_p]
         L.cmio_split_packets.argtypes = [i32, pd, u64, u64, u32, C.POINTER(u64)]
         L.cmio_kappa32.argtypes = [i64, pd, pd, d, pf]
         L.cmio_iteration_omp.argtypes = [C.POINTER(Lattice), pd, pd, pd, pd, i32, pd, pd, u64,
@@ -330,23 +344,26 @@ class LatticeGrid:
         return lib().cmio_lattice_locate(C.byref(self.lat), _ptr(self.box, C.c_double),
                                          _ptr(p, C.c_double))
 
-    def transport(self, nH, xH, J, packets, start_subgrid):
+    def transport(self, nH, xH, J, packets, start_subgrid, reemission=None):
+        """FP64 transport; reemission = (probability, seed, instance, iteration)."""
         counts = Counts()
         s = np.ascontiguousarray(start_subgrid, dtype=np.uint32)
-        lib().cmio_transport(C.byref(self.lat), _ptr(nH, C.c_double), _ptr(xH, C.c_double),
-                             _ptr(J, C.c_double), packets.ctypes.data, _ptr(s, C.c_uint32),
-                             packets.size, C.byref(counts))
+        r = Reemission(*reemission) if reemission else None
+        lib().cmio_transport_r(C.byref(self.lat), _ptr(nH, C.c_double), _ptr(xH, C.c_double),
+                               _ptr(J, C.c_double), packets.ctypes.data, _ptr(s, C.c_uint32),
+                               packets.size, C.byref(counts), C.byref(r) if r else None)
         return counts.as_dict()
 
-    def transport32(self, kappa, tally, packets, start_subgrid, fixed=None):
+    def transport32(self, kappa, tally, packets, start_subgrid, fixed=None, reemission=None):
         """FP32 transport; tally: double sums of lmin, fixed: uint64 fixed-point sums."""
         counts = Counts()
         s = np.ascontiguousarray(start_subgrid, dtype=np.uint32)
-        lib().cmio_transport32(C.byref(self.lat), _ptr(kappa, C.c_float),
-                               _ptr(tally, C.c_double) if tally is not None else None,
-                               _ptr(fixed, C.c_uint64) if fixed is not None else None,
-                               packets.ctypes.data, _ptr(s, C.c_uint32), packets.size,
-                               C.byref(counts))
+        r = Reemission(*reemission) if reemission else None
+        lib().cmio_transport32_r(C.byref(self.lat), _ptr(kappa, C.c_float),
+                                 _ptr(tally, C.c_double) if tally is not None else None,
+                                 _ptr(fixed, C.c_uint64) if fixed is not None else None,
+                                 packets.ctypes.data, _ptr(s, C.c_uint32), packets.size,
+                                 C.byref(counts), C.byref(r) if r else None)
         return counts.as_dict()
 
     def fixed_unit(self, s=0):

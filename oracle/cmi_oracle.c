@@ -631,9 +631,41 @@ uint32_t cmio_lattice_locate(const cmio_lattice *lat, const double box[6],
 /* do_photon_traversal + routing (testDensitySubGrid_omp.cpp:607-666,
  * 1178-1191) applied to one packet at a time until absorption (INSIDE with
  * reemission off) or escape (neighbour NEIGHBOUR_OUTSIDE). */
-void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH, double *J,
-                    cmio_photon *packets, const uint32_t *start_subgrid, int64_t n,
-                    cmio_counts *counts) {
+uint32_t cmio_reemit_hash(double x) {
+  uint64_t b;
+  memcpy(&b, &x, sizeof(b));
+  return (uint32_t)b ^ (uint32_t)(b >> 32);
+}
+
+static uint32_t float_bits(float x) {
+  uint32_t b;
+  memcpy(&b, &x, sizeof(b));
+  return b;
+}
+
+/* do_reemission (testDensitySubGrid_omp.cpp:675-702) with counter-based draws */
+int cmio_reemit_draw(const cmio_reemission *r, uint32_t h0, uint32_t h1, uint32_t h2,
+                     double direction[3], double *tau) {
+  const uint32_t ctr[4] = {h0, h1, h2 ^ r->iteration, 0x434D4952u};
+  const uint32_t key[2] = {(uint32_t)r->seed, (uint32_t)(r->seed >> 32) + r->instance};
+  uint32_t w[4];
+  cmio_philox4x32(ctr, key, w);
+  const double u = ((double)w[0] + 0.5) * (1.0 / 4294967296.0);
+  if (!(u < r->probability)) return 0;
+  const double cost = 2. * (((double)w[1] + 0.5) * (1.0 / 4294967296.0)) - 1.;
+  const double phi = 2. * M_PI * (((double)w[2] + 0.5) * (1.0 / 4294967296.0));
+  const double s2 = 1. - cost * cost;
+  const double sint = sqrt((s2 < 0.) ? 0. : s2);
+  direction[0] = sint * cos(phi);
+  direction[1] = sint * sin(phi);
+  direction[2] = cost;
+  *tau = -log(((double)w[3] + 0.5) * (1.0 / 4294967296.0));
+  return 1;
+}
+
+void cmio_transport_r(const cmio_lattice *lat, const double *nH, const double *xH, double *J,
+                      cmio_photon *packets, const uint32_t *start_subgrid, int64_t n,
+                      cmio_counts *counts, const cmio_reemission *r) {
   const int64_t C = lat->cells_per_subgrid;
   for (int64_t i = 0; i < n; ++i) {
     uint32_t s = start_subgrid[i];
@@ -645,6 +677,18 @@ void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH,
       counts->crossings += (uint64_t)steps;
       counts->transits += 1;
       if (out == CMIO_INSIDE) {
+        double d[3], tau;
+        cmio_photon *ph = &packets[i];
+        if (r && r->probability > 0. &&
+            cmio_reemit_draw(r, cmio_reemit_hash(ph->position[0]),
+                             cmio_reemit_hash(ph->position[1]),
+                             cmio_reemit_hash(ph->position[2]), d, &tau)) {
+          counts->reemitted += 1;
+          for (int a = 0; a < 3; ++a) ph->direction[a] = d[a];
+          ph->target_optical_depth = tau;
+          in_dir = CMIO_INSIDE;
+          continue;  /* a new traversal of the same subgrid */
+        }
         counts->absorbed += 1;
         break;
       }
@@ -659,9 +703,15 @@ void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH,
   }
 }
 
-void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally,
-                      uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
-                      int64_t n, cmio_counts *counts) {
+void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH, double *J,
+                    cmio_photon *packets, const uint32_t *start_subgrid, int64_t n,
+                    cmio_counts *counts) {
+  cmio_transport_r(lat, nH, xH, J, packets, start_subgrid, n, counts, NULL);
+}
+
+void cmio_transport32_r(const cmio_lattice *lat, const float *kappa, double *tally,
+                        uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
+                        int64_t n, cmio_counts *counts, const cmio_reemission *r) {
   const int64_t C = lat->cells_per_subgrid;
   for (int64_t i = 0; i < n; ++i) {
     uint32_t s = start_subgrid[i];
@@ -678,6 +728,18 @@ void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally
       counts->crossings += (uint64_t)steps;
       counts->transits += 1;
       if (out == CMIO_INSIDE) {
+        double d[3], tau;
+        cmio_packet32 *pk = &packets[i];
+        if (r && r->probability > 0. &&
+            cmio_reemit_draw(r, float_bits(pk->pos[0]) ^ s,
+                             float_bits(pk->pos[1]) ^ (s * 0x9E3779B9u), float_bits(pk->pos[2]),
+                             d, &tau)) {
+          counts->reemitted += 1;
+          for (int a = 0; a < 3; ++a) pk->dir[a] = (float)d[a];
+          pk->tau_left = (float)tau;
+          pk->meta = (pk->meta & ~31u) | (uint32_t)CMIO_INSIDE;
+          continue;
+        }
         counts->absorbed += 1;
         break;
       }
@@ -691,6 +753,13 @@ void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally
     }
   }
 }
+
+void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally,
+                      uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
+                      int64_t n, cmio_counts *counts) {
+  cmio_transport32_r(lat, kappa, tally, fixed, packets, start_subgrid, n, counts, NULL);
+}
+
 
 void cmio_kappa32(int64_t ncell, const double *nH, const double *xH, double sigma,
                   float *kappa) {
@@ -770,7 +839,7 @@ void cmio_iteration_omp(const cmio_lattice *lat, const double box[6], const doub
     tid = omp_get_thread_num();
 #endif
     double *Jt = priv + (size_t)tid * (size_t)ncell;
-    cmio_counts local = {0, 0, 0, 0};
+    cmio_counts local = {0, 0, 0, 0, 0};
 #pragma omp for schedule(dynamic, 4096)
     for (int64_t p = 0; p < (int64_t)num_photon; ++p) {
       int32_t src = 0;

@@ -150,8 +150,23 @@ uint32_t cmio_lattice_locate(const cmio_lattice *lat, const double box[6],
                              const double position[3]);
 
 typedef struct {
-  uint64_t absorbed, escaped, crossings, transits;
+  uint64_t absorbed, escaped, crossings, transits, reemitted;
 } cmio_counts;
+
+/* Reemission (do_reemission, testDensitySubGrid_omp.cpp:675-702) with the
+ * GPU's draws: Philox4x32-10, key {seed_lo, seed_hi + instance}, counter
+ * {h0, h1, h2 ^ iteration, 0x434D4952}; w0 decides (u < p), w1 -> cos(theta),
+ * w2 -> phi, w3 -> optical depth.  Returns 1 and fills direction / tau when
+ * the packet is re-emitted. */
+typedef struct {
+  double probability;
+  uint64_t seed;
+  uint32_t instance, iteration;
+} cmio_reemission;
+int cmio_reemit_draw(const cmio_reemission *r, uint32_t h0, uint32_t h1, uint32_t h2,
+                     double direction[3], double *tau);
+/* hash of an FP64 coordinate for the counter: low ^ high word */
+uint32_t cmio_reemit_hash(double x);
 
 /* Transport packets to absorption/escape (fields in subgrid-blocked order). */
 void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH,
@@ -162,6 +177,16 @@ void cmio_transport(const cmio_lattice *lat, const double *nH, const double *xH,
 void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally,
                       uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
                       int64_t n, cmio_counts *counts);
+/* The same with reemission (r may be NULL).  FP64: counter from the absolute
+ * absorption position (cmio_reemit_hash per axis).  FP32: counter from the
+ * cell-unit position bits mixed with the subgrid index s: {bits(x) ^ s,
+ * bits(y) ^ (s * 0x9E3779B9), bits(z)}; draws in FP64, rounded to FP32. */
+void cmio_transport_r(const cmio_lattice *lat, const double *nH, const double *xH, double *J,
+                      cmio_photon *packets, const uint32_t *start_subgrid, int64_t n,
+                      cmio_counts *counts, const cmio_reemission *r);
+void cmio_transport32_r(const cmio_lattice *lat, const float *kappa, double *tally,
+                        uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
+                        int64_t n, cmio_counts *counts, const cmio_reemission *r);
 /* scale of the fixed-point tally of a subgrid: 2^24 / max float cell size */
 float cmio_fixed_scale(const cmio_subgrid *sg);
 

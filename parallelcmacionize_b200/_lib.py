@@ -45,7 +45,8 @@ NEIGHBOUR_OUTSIDE = 0xFFFFFFFF
 EXPORTED = [
     "cmi_default_options", "cmi_last_error_string", "cmi_abi_version", "cmi_create",
     "cmi_destroy", "cmi_set_fields", "cmi_get_fields", "cmi_set_intensity", "cmi_set_sources",
-    "cmi_set_packet_budget", "cmi_run_iterations", "cmi_run_until_converged",
+    "cmi_set_packet_budget", "cmi_set_reemission_probability", "cmi_run_iterations",
+    "cmi_run_until_converged",
     "cmi_shoot_packets",
     "cmi_transport_packets", "cmi_traverse_buffer", "cmi_trace_packet",
     "cmi_compute_neutral_fraction", "cmi_device_field", "cmi_get_stream", "cmi_synchronize",
@@ -110,6 +111,7 @@ class Stats(C.Structure):
         ("mean_abs_dx", C.c_double),
         ("error_flags", C.c_uint32),
         ("rounds", C.c_uint32),
+        ("packets_reemitted", C.c_uint64),
     ]
 
     def as_dict(self):
@@ -160,6 +162,7 @@ def load():
     L.cmi_set_intensity.argtypes = [ctx, i32, i32, i32, vp]
     L.cmi_set_sources.argtypes = [ctx, i32, vp, vp, i32]
     L.cmi_set_packet_budget.argtypes = [ctx, i32, u64]
+    L.cmi_set_reemission_probability.argtypes = [ctx, i32, d]
     L.cmi_run_iterations.argtypes = [ctx, i32, u64, vp]
     L.cmi_run_until_converged.argtypes = [ctx, i32, i32, d, u64, vp, vp, vp]
     L.cmi_shoot_packets.argtypes = [ctx, u64, u32, vp]

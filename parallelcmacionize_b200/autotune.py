@@ -53,7 +53,8 @@ class WalkConfig:
         return GridSpec(box=base.box, ncell=base.ncell, num_subgrid=nsub,
                         recombination_rate=base.recombination_rate,
                         cross_section=base.cross_section, sources=list(base.sources),
-                        num_photon=base.num_photon)
+                        num_photon=base.num_photon,
+                        reemission_probability=base.reemission_probability)
 
     def engine_options(self) -> dict:
         return dict(packets_per_chunk=self.packets_per_chunk, tally=self.tally,

@@ -92,7 +92,7 @@ struct alignas(16) DevInstance {
   uint32_t first_source, num_sources;
   int64_t num_cells;
   uint32_t frozen;        // 1: converged, emits nothing and keeps x_H (run until converged)
-  uint32_t reserved;
+  float reemission;       // probability that an absorbed packet is re-emitted
 };
 
 struct alignas(16) DevSource {
@@ -118,6 +118,7 @@ struct alignas(16) DevStats {
   unsigned long long emitted, absorbed, escaped, crossings, transits;
   double dx_sum;
   uint32_t flags, rounds;
+  unsigned long long reemitted;
 };
 
 // Control block of the wavefront.
@@ -227,6 +228,39 @@ __device__ __forceinline__ void philox_packet(uint64_t seed, uint32_t instance,
   dir[1] = sint * sp;
   dir[2] = cost;
   tau = -log(u2);
+}
+
+// Reemission of an absorbed packet (do_reemission, testDensitySubGrid_omp.cpp:
+// 675-702): with probability p a new isotropic direction and optical depth.
+// The draws come from Philox with the instance's emission key and a counter
+// made of the absorption position (h0..h2, see reemit_hash_*), the iteration
+// and a tag of its own, so they are independent of the emission streams.
+constexpr uint32_t kPhiloxReemitTag = 0x434D4952u;
+
+__device__ __forceinline__ uint32_t reemit_hash(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (uint32_t)b ^ (uint32_t)(b >> 32);
+}
+
+__device__ __forceinline__ bool reemit_draw(uint64_t seed, uint32_t instance, uint32_t iteration,
+                                            uint32_t h0, uint32_t h1, uint32_t h2, double p,
+                                            double dir[3], double &tau) {
+  const uint32_t ctr[4] = {h0, h1, h2 ^ iteration, kPhiloxReemitTag};
+  uint32_t w[4];
+  philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32) + instance, w);
+  const double u = ((double)w[0] + 0.5) * (1.0 / 4294967296.0);
+  if (!(u < p)) return false;
+  const double cost = 2. * (((double)w[1] + 0.5) * (1.0 / 4294967296.0)) - 1.;
+  const double phi = 2. * 3.14159265358979323846 * (((double)w[2] + 0.5) * (1.0 / 4294967296.0));
+  const double s2 = 1. - cost * cost;
+  const double sint = sqrt((s2 < 0.) ? 0. : s2);
+  double sp, cp;
+  sincos(phi, &sp, &cp);
+  dir[0] = sint * cp;
+  dir[1] = sint * sp;
+  dir[2] = cost;
+  tau = -log(((double)w[3] + 0.5) * (1.0 / 4294967296.0));
+  return true;
 }
 
 // ranlxd, the reference's generator (shared with the host C++ surface)

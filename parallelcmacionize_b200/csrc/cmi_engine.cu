@@ -62,6 +62,7 @@ struct HostInstance {
   int64_t ncells;
   std::vector<double> src_pos, src_lum;
   uint64_t num_photon = 0;
+  double reemission = 0.;  // reemission_probability (params.txt)
 };
 
 template <class T>
@@ -253,6 +254,7 @@ int upload_tables(cmi_context *c) {
     D.first_source = (uint32_t)ds.size();
     D.num_sources = (uint32_t)I.src_lum.size();
     D.num_cells = I.ncells;
+    D.reemission = (float)I.reemission;
     const int32_t *ns = I.desc.num_subgrid;
     for (size_t k = 0; k < I.src_lum.size(); ++k) {
       DevSource s{};
@@ -602,6 +604,7 @@ void to_stats(const DevStats &d, const HostInstance &I, cmi_stats &s) {
   s.mean_abs_dx = (I.ncells > 0) ? d.dx_sum / (double)I.ncells : 0.;
   s.error_flags = d.flags;
   s.rounds = d.rounds;
+  s.packets_reemitted = d.reemitted;
 }
 
 int ensure_host_stats(cmi_context *c, size_t n) {
@@ -1037,6 +1040,15 @@ int cmi_set_packet_budget(cmi_context *c, int32_t instance, uint64_t num_photon)
   c->inst[instance].num_photon = num_photon;
   CMI_TRY(upload_tables(c));
   return ensure_capacity(c, total_budget(c));
+}
+
+int cmi_set_reemission_probability(cmi_context *c, int32_t instance, double probability) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  if (!(probability >= 0. && probability < 1.))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "reemission probability must be in [0, 1)");
+  c->inst[instance].reemission = probability;
+  return upload_tables(c);
 }
 
 int cmi_run_iterations(cmi_context *c, int32_t iterations, uint64_t seed, cmi_stats *stats) {

@@ -632,6 +632,7 @@ struct WalkShared {
   double anchor[3], cs[3], inv_cs[3];
   int64_t field_offset;
   double sigma;
+  double reemission;
   uint32_t instance;
   int32_t chunk_id;
   uint32_t chunk_sub, chunk_begin, chunk_count;
@@ -652,6 +653,7 @@ struct Walk32Shared {
   double tally_unit;   // lref / 2^22 (m)
   int64_t field_offset;
   double sigma;
+  double reemission;
   uint32_t instance;
   // current run of chunks and segment of equal subgrid
   uint32_t run_c0, run_c1;
@@ -682,6 +684,7 @@ __device__ __forceinline__ void load_subgrid(Sh &sh, const WalkParams &prm, uint
   sh.field_offset = S.field_offset;
   sh.instance = S.instance;
   sh.sigma = prm.inst[S.instance].sigma;
+  sh.reemission = prm.inst[S.instance].reemission;
 }
 
 __device__ __forceinline__ void load_subgrid32(Walk32Shared &sh, const DevSubgrid &S,
@@ -702,24 +705,28 @@ __device__ __forceinline__ void load_subgrid32(Walk32Shared &sh, const DevSubgri
   sh.field_offset = S.field_offset;
   sh.instance = S.instance;
   sh.sigma = prm.inst[S.instance].sigma;
+  sh.reemission = prm.inst[S.instance].reemission;
 }
 
 // per-thread counters -> instance statistics (one atomic per warp and counter)
 __device__ __forceinline__ void flush_counters(DevStats *stats, uint32_t instance,
                                                uint32_t &c_cross, uint32_t &c_trans,
-                                               uint32_t &c_abs, uint32_t &c_esc) {
+                                               uint32_t &c_abs, uint32_t &c_esc,
+                                               uint32_t &c_reem) {
   const uint32_t wc = __reduce_add_sync(kFull, c_cross);
   const uint32_t wt = __reduce_add_sync(kFull, c_trans);
   const uint32_t wa = __reduce_add_sync(kFull, c_abs);
   const uint32_t we = __reduce_add_sync(kFull, c_esc);
+  const uint32_t wr = __reduce_add_sync(kFull, c_reem);
   if ((threadIdx.x & 31) == 0) {
     DevStats &S = stats[instance];
     if (wc) atomicAdd(&S.crossings, (unsigned long long)wc);
     if (wt) atomicAdd(&S.transits, (unsigned long long)wt);
     if (wa) atomicAdd(&S.absorbed, (unsigned long long)wa);
     if (we) atomicAdd(&S.escaped, (unsigned long long)we);
+    if (wr) atomicAdd(&S.reemitted, (unsigned long long)wr);
   }
-  c_cross = c_trans = c_abs = c_esc = 0;
+  c_cross = c_trans = c_abs = c_esc = c_reem = 0;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -833,7 +840,9 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
   const unsigned lt = (1u << lane) - 1u;
   uint32_t phase = 0;
   uint32_t staged = kNone;
-  uint32_t c_cross = 0, c_trans = 0, c_abs = 0, c_esc = 0;
+  uint32_t c_cross = 0, c_trans = 0, c_abs = 0, c_esc = 0, c_reem = 0;
+  const uint64_t rseed = st->seed;
+  const uint32_t riter = st->iteration;
 
   auto flush = [&]() {
     const int64_t off = sh.field_offset;
@@ -842,7 +851,7 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
       if (v != 0.) atomicAdd(&prm.J[off + c], v);
       s_J[c] = 0.;
     }
-    flush_counters(prm.stats, sh.instance, c_cross, c_trans, c_abs, c_esc);
+    flush_counters(prm.stats, sh.instance, c_cross, c_trans, c_abs, c_esc, c_reem);
   };
 
   for (;;) {
@@ -941,7 +950,7 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
       const bool fin = have && status != kRun;
       if (__any_sync(kFull, fin)) {
         uint32_t key = kOutside, meta = 0;
-        bool append = false;
+        bool append = false, reemitted = false;
         if (fin) {
           ++c_trans;
           if (status == kExited) {
@@ -954,7 +963,23 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
               if (key == kOutside) ++c_esc; else append = true;
             }
           } else if (status == kAbsorbed) {
-            ++c_abs;
+            // reemission from the absorption point (the photon as the
+            // reference's next traversal task would receive it)
+            Packet64 rp = w64.packet(v64, (uint32_t)kInside);
+            double rd[3], rtau;
+            if (sh.reemission > 0. &&
+                reemit_draw(rseed, sh.instance, riter, reemit_hash(rp.pos[0]),
+                            reemit_hash(rp.pos[1]), reemit_hash(rp.pos[2]), sh.reemission, rd,
+                            rtau)) {
+              ++c_reem;
+              for (int a = 0; a < 3; ++a) rp.dir[a] = rd[a];
+              rp.tau = rtau;
+              entry = w64.begin(rp, v64, sh.tab.sign_code);
+              fresh = true;
+              reemitted = true;
+            } else {
+              ++c_abs;
+            }
           } else {
             atomicOr(&st->flags, kFlagWalkLimit);
           }
@@ -963,7 +988,7 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
         if (append) rec = w64.packet(v64, meta);
         warp_append(append, key, rec, (Packet64 *)prm.arena_out, prm.keys, prm.ranks, prm.hist,
                     st, prm.capacity);
-        if (fin) have = false;
+        if (fin && !reemitted) have = false;
       }
     }
     __syncthreads();
@@ -1089,7 +1114,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
 
   uint32_t phase_field = 0;
   uint32_t staged = kNone;
-  uint32_t c_cross = 0, c_trans = 0, c_abs = 0, c_esc = 0;
+  uint32_t c_cross = 0, c_trans = 0, c_abs = 0, c_esc = 0, c_reem = 0;
+  const uint64_t rseed = st->seed;
+  const uint32_t riter = st->iteration;
   uint32_t nstage = 0;  // warp-uniform
   Packet32 *my_stage = s_stage + warp * kStage;
   uint32_t *my_skey = s_skey + warp * kStage;
@@ -1101,7 +1128,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
       const double v = tally.take(c, scale);
       if (v != 0.) atomicAdd(&prm.J[off + c], v * sh.sigma);
     }
-    flush_counters(prm.stats, sh.instance, c_cross, c_trans, c_abs, c_esc);
+    flush_counters(prm.stats, sh.instance, c_cross, c_trans, c_abs, c_esc, c_reem);
   };
 
   // append the first n staged packets of this warp, then move the rest down
@@ -1205,9 +1232,33 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
           if (__any_sync(kFull, pending)) {
             uint32_t key = kOutside, meta = 0;
             bool append = false;
+            bool route = pending;
             if (pending) {
               ++c_trans;
               c_cross += (uint32_t)w.steps;  // one step per crossed cell
+              double rd[3], rtau;
+              if (pstatus == kAbsorbed && sh.reemission > 0. &&
+                  reemit_draw(rseed, sh.instance, riter, __float_as_uint(w.p[0]) ^ staged,
+                              __float_as_uint(w.p[1]) ^ (staged * 0x9E3779B9u),
+                              __float_as_uint(w.p[2]), sh.reemission, rd, rtau)) {
+                // re-emitted in place: the lane walks on from the absorption point
+                ++c_reem;
+                Packet32 rp;
+                for (int a = 0; a < 3; ++a) {
+                  rp.pos[a] = w.p[a];
+                  rp.dir[a] = (float)rd[a];
+                }
+                rp.tau = (float)rtau;
+                rp.meta = (uint32_t)kInside;
+                pstatus = w.begin(rp, v, sh.tab.sign_code);
+                route = false;
+                if (pstatus == kRun) {
+                  active = true;
+                  pending = false;
+                }
+              }
+            }
+            if (route) {
               if (pstatus == kExited) {
                 const int od = sh.tab.mask_dir[w.exit_mask(v)];
                 if (od >= kNumDirections) {
@@ -1234,12 +1285,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
             if (nstage >= kStageFlush) flush_stage(min(nstage, 32u));
           }
           if (!exhausted) {
-            const unsigned idle = ~running;  // every lane that is not walking
+            // every lane neither walking nor holding a packet (a re-emitted
+            // packet walks on, or waits to be routed in the next batch)
+            const unsigned idle = __ballot_sync(kFull, !active && !pending);
             const uint32_t need = (uint32_t)__popc(idle);
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(&sh.claim, need);
             base = __shfl_sync(kFull, base, 0);
-            if (base >= nseg) {
+            if (need == 0u) {
+              // every lane busy after reemission: claim nothing this batch
+            } else if (base >= nseg) {
               exhausted = true;
             } else {
               const uint32_t take = min(need, nseg - base);
@@ -1247,7 +1302,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
               wait_chunk(k0);
               if (k1 != k0) wait_chunk(k1);
               const uint32_t r = (uint32_t)__popc(idle & lt);
-              if (!active && r < take) {
+              if (((idle >> lane) & 1u) && r < take) {
                 const uint32_t vi = base + r;
                 const uint32_t k = vi >> ch_shift;
                 const Packet32 pk = s_pk[(size_t)(k & 1u) * CH + (vi - (k << ch_shift))];

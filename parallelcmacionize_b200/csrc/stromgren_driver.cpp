@@ -36,11 +36,8 @@ int main(int argc, char **argv) {
   }
   try {
     const PlainMethodParameters p(Parameters::from_file(params_file));
-    if (p.reemission_probability != 0.) {
-      std::fprintf(stderr, "reemission_probability > 0 is not supported by this driver\n");
-      return 2;
-    }
     DensityGrid grid(p.box, p.ncell, p.num_subgrid);
+    grid.set_reemission_probability(p.reemission_probability);
     RandomGenerator rng(42 + threads);
 
     if (p.random_density) {

@@ -51,6 +51,7 @@ class GridSpec:
     cross_section: float = 6.3e-22       # testDensitySubGrid_omp.cpp:589
     sources: list = field(default_factory=list)  # [(x, y, z, L), ...]
     num_photon: int = 0
+    reemission_probability: float = 0.0          # params.txt reemission_probability
 
     def desc(self) -> _lib.GridDesc:
         g = _lib.GridDesc()
@@ -115,6 +116,8 @@ class TransportEngine:
                 self.set_sources(i, s[:, :3], s[:, 3])
             if g.num_photon:
                 self.set_packet_budget(i, g.num_photon)
+            if g.reemission_probability:
+                self.set_reemission_probability(i, g.reemission_probability)
 
     # ---- lifetime ----
     def close(self):
@@ -171,6 +174,9 @@ class TransportEngine:
         if p.size != 3 * l.size:
             raise ValueError("3 coordinates per source")
         check(self._L.cmi_set_sources(self._h, instance, ptr(p), ptr(l), l.size))
+
+    def set_reemission_probability(self, instance, probability):
+        check(self._L.cmi_set_reemission_probability(self._h, instance, float(probability)))
 
     def set_packet_budget(self, instance, num_photon):
         check(self._L.cmi_set_packet_budget(self._h, instance, int(num_photon)))

@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
     L = _lib.load()
     for name in declared_functions():
         assert hasattr(L, name), name
-    assert L.cmi_abi_version() == 1
+    assert L.cmi_abi_version() == 2  # 2: cmi_stats.packets_reemitted
 
 
 def test_default_options():
@@ -41,7 +41,7 @@ def test_default_options():
 def test_struct_layouts_match_header():
     assert C.sizeof(_lib.GridDesc) == 6 * 8 + 6 * 4 + 2 * 8
     assert C.sizeof(_lib.Options) == 16 * 4
-    assert C.sizeof(_lib.Stats) == 6 * 8 + 2 * 4
+    assert C.sizeof(_lib.Stats) == 6 * 8 + 2 * 4 + 8
     assert _lib.PHOTON_DTYPE.itemsize == 80
 
 
