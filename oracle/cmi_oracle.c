@@ -643,23 +643,55 @@ static uint32_t float_bits(float x) {
   return b;
 }
 
-/* do_reemission (testDensitySubGrid_omp.cpp:675-702) with counter-based draws */
+/* -ln(u), the GPU's series: u = m 2^e with m in [sqrt(1/2), sqrt(2)),
+ * ln m = 2 (s + s^3/3 + ... + s^31/31), s = (m - 1) / (m + 1) */
+static double reemit_neg_log(double u) {
+  int e;
+  double m = frexp(u, &e);
+  if (m < 0.70710678118654752440) {
+    m *= 2.;
+    e -= 1;
+  }
+  const double s = (m - 1.) / (m + 1.);
+  const double s2 = s * s;
+  double term = s, sum = s;
+  for (int k = 3; k <= 31; k += 2) {
+    term *= s2;
+    sum += term / (double)k;
+  }
+  return -(2. * sum + (double)e * 0.69314718055994530942);
+}
+
+/* do_reemission (testDensitySubGrid_omp.cpp:675-702) with the GPU's
+ * counter-based draws: Marsaglia's direction (attempt k uses tag + k) and the
+ * series above, correctly rounded operations only, so both sides agree bit
+ * for bit */
 int cmio_reemit_draw(const cmio_reemission *r, uint32_t h0, uint32_t h1, uint32_t h2,
-                     double direction[3], double *tau) {
-  const uint32_t ctr[4] = {h0, h1, h2 ^ r->iteration, 0x434D4952u};
+                     uint32_t count, double direction[3], double *tau) {
+  const double inv32 = 1.0 / 4294967296.0;
   const uint32_t key[2] = {(uint32_t)r->seed, (uint32_t)(r->seed >> 32) + r->instance};
-  uint32_t w[4];
-  cmio_philox4x32(ctr, key, w);
-  const double u = ((double)w[0] + 0.5) * (1.0 / 4294967296.0);
-  if (!(u < r->probability)) return 0;
-  const double cost = 2. * (((double)w[1] + 0.5) * (1.0 / 4294967296.0)) - 1.;
-  const double phi = 2. * M_PI * (((double)w[2] + 0.5) * (1.0 / 4294967296.0));
-  const double s2 = 1. - cost * cost;
-  const double sint = sqrt((s2 < 0.) ? 0. : s2);
-  direction[0] = sint * cos(phi);
-  direction[1] = sint * sin(phi);
-  direction[2] = cost;
-  *tau = -log(((double)w[3] + 0.5) * (1.0 / 4294967296.0));
+  if (count >= 1024u) return 0; /* the GPU's cap per subgrid visit */
+  for (uint32_t k = 0; k < 16u; ++k) {
+    const uint32_t ctr[4] = {h0, h1, h2 ^ r->iteration, 0x434D4952u + (count << 4) + k};
+    uint32_t w[4];
+    cmio_philox4x32(ctr, key, w);
+    if (k == 0u && !(((double)w[0] + 0.5) * inv32 < r->probability)) return 0;
+    const double x1 = 2. * (((double)w[1] + 0.5) * inv32) - 1.;
+    const double x2 = 2. * (((double)w[2] + 0.5) * inv32) - 1.;
+    const double s = x1 * x1 + x2 * x2;
+    if (s < 1.) {
+      const double f = 2. * sqrt(1. - s);
+      direction[0] = x1 * f;
+      direction[1] = x2 * f;
+      direction[2] = 1. - 2. * s;
+      *tau = reemit_neg_log(((double)w[3] + 0.5) * inv32);
+      return 1;
+    }
+  }
+  direction[0] = 0.;
+  direction[1] = 0.;
+  direction[2] = 1.;
+  *tau = 1.;
   return 1;
 }
 
@@ -670,6 +702,7 @@ void cmio_transport_r(const cmio_lattice *lat, const double *nH, const double *x
   for (int64_t i = 0; i < n; ++i) {
     uint32_t s = start_subgrid[i];
     int in_dir = CMIO_INSIDE;
+    uint32_t rcount = 0; /* reemissions in this subgrid visit */
     for (;;) {
       int32_t steps = 0;
       const int out = cmio_interact(&lat->sub[s], nH + s * C, xH + s * C, J + s * C, &packets[i],
@@ -682,8 +715,9 @@ void cmio_transport_r(const cmio_lattice *lat, const double *nH, const double *x
         if (r && r->probability > 0. &&
             cmio_reemit_draw(r, cmio_reemit_hash(ph->position[0]),
                              cmio_reemit_hash(ph->position[1]),
-                             cmio_reemit_hash(ph->position[2]), d, &tau)) {
+                             cmio_reemit_hash(ph->position[2]), rcount, d, &tau)) {
           counts->reemitted += 1;
+          rcount += 1;
           for (int a = 0; a < 3; ++a) ph->direction[a] = d[a];
           ph->target_optical_depth = tau;
           in_dir = CMIO_INSIDE;
@@ -699,6 +733,7 @@ void cmio_transport_r(const cmio_lattice *lat, const double *nH, const double *x
       }
       s = ngb;
       in_dir = cmio_output_to_input_direction(out);
+      rcount = 0;
     }
   }
 }
@@ -715,6 +750,7 @@ void cmio_transport32_r(const cmio_lattice *lat, const float *kappa, double *tal
   const int64_t C = lat->cells_per_subgrid;
   for (int64_t i = 0; i < n; ++i) {
     uint32_t s = start_subgrid[i];
+    uint32_t rcount = 0; /* reemissions in this subgrid visit */
     for (;;) {
       const cmio_subgrid *sg = &lat->sub[s];
       const float cs[3] = {(float)sg->cell_size[0], (float)sg->cell_size[1],
@@ -733,8 +769,9 @@ void cmio_transport32_r(const cmio_lattice *lat, const float *kappa, double *tal
         if (r && r->probability > 0. &&
             cmio_reemit_draw(r, float_bits(pk->pos[0]) ^ s,
                              float_bits(pk->pos[1]) ^ (s * 0x9E3779B9u), float_bits(pk->pos[2]),
-                             d, &tau)) {
+                             rcount, d, &tau)) {
           counts->reemitted += 1;
+          rcount += 1;
           for (int a = 0; a < 3; ++a) pk->dir[a] = (float)d[a];
           pk->tau_left = (float)tau;
           pk->meta = (pk->meta & ~31u) | (uint32_t)CMIO_INSIDE;
@@ -750,6 +787,7 @@ void cmio_transport32_r(const cmio_lattice *lat, const float *kappa, double *tal
       }
       s = ngb;
       packets[i].meta = (packets[i].meta & ~31u) | (uint32_t)cmio_output_to_input_direction(out);
+      rcount = 0;
     }
   }
 }

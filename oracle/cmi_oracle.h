@@ -155,16 +155,18 @@ typedef struct {
 
 /* Reemission (do_reemission, testDensitySubGrid_omp.cpp:675-702) with the
  * GPU's draws: Philox4x32-10, key {seed_lo, seed_hi + instance}, counter
- * {h0, h1, h2 ^ iteration, 0x434D4952}; w0 decides (u < p), w1 -> cos(theta),
- * w2 -> phi, w3 -> optical depth.  Returns 1 and fills direction / tau when
- * the packet is re-emitted. */
+ * {h0, h1, h2 ^ iteration, 0x434D4952 + (count << 4) + attempt}, count = the
+ * packet's earlier reemissions in this subgrid visit (at most 1024); w0 of
+ * attempt 0 decides (u < p), w1, w2 a point of the unit disc (Marsaglia's
+ * isotropic direction), w3 the optical depth (series logarithm).  Returns 1
+ * and fills direction / tau when the packet is re-emitted. */
 typedef struct {
   double probability;
   uint64_t seed;
   uint32_t instance, iteration;
 } cmio_reemission;
 int cmio_reemit_draw(const cmio_reemission *r, uint32_t h0, uint32_t h1, uint32_t h2,
-                     double direction[3], double *tau);
+                     uint32_t count, double direction[3], double *tau);
 /* hash of an FP64 coordinate for the counter: low ^ high word */
 uint32_t cmio_reemit_hash(double x);
 

@@ -233,33 +233,87 @@ __device__ __forceinline__ void philox_packet(uint64_t seed, uint32_t instance,
 // Reemission of an absorbed packet (do_reemission, testDensitySubGrid_omp.cpp:
 // 675-702): with probability p a new isotropic direction and optical depth.
 // The draws come from Philox with the instance's emission key and a counter
-// made of the absorption position (h0..h2, see reemit_hash_*), the iteration
-// and a tag of its own, so they are independent of the emission streams.
+// made of the absorption position (h0..h2), the iteration, the number of
+// earlier reemissions of the packet in this subgrid visit and a tag of their
+// own, so they are independent of the emission streams and a packet absorbed
+// twice at the same position (a move below the coordinate's resolution) still
+// draws afresh.  They use only
+// correctly rounded operations (no sin/cos/log), so the oracle's host copy of
+// this function draws the same bits: the direction by Marsaglia's method (a
+// point of the unit disc, rejection from the square; attempt k uses tag + k),
+// the optical depth -ln u by the series ln m = 2 atanh((m - 1) / (m + 1))
+// after an exact power-of-two range reduction.
 constexpr uint32_t kPhiloxReemitTag = 0x434D4952u;
+// reemissions of one packet in one subgrid visit before it counts as
+// absorbed (probability p^1024): keeps every walk finite whatever the draws
+constexpr uint32_t kMaxReemissions = 1024u;
 
 __device__ __forceinline__ uint32_t reemit_hash(double x) {
   const unsigned long long b = (unsigned long long)__double_as_longlong(x);
   return (uint32_t)b ^ (uint32_t)(b >> 32);
 }
 
+// -ln(u) for u in (0, 1): u = m 2^e with m in [sqrt(1/2), sqrt(2)), then
+// ln m = 2 (s + s^3/3 + ... + s^31/31), s = (m - 1) / (m + 1), |s| < 0.1716
+__device__ __forceinline__ double reemit_neg_log(double u) {
+  int e;
+  double m = frexp(u, &e);
+  if (m < 0.70710678118654752440) {
+    m *= 2.;
+    e -= 1;
+  }
+  const double s = (m - 1.) / (m + 1.);
+  const double s2 = s * s;
+  double term = s, sum = s;
+  for (int k = 3; k <= 31; k += 2) {
+    term *= s2;
+    sum += term / (double)k;
+  }
+  return -(2. * sum + (double)e * 0.69314718055994530942);
+}
+
 __device__ __forceinline__ bool reemit_draw(uint64_t seed, uint32_t instance, uint32_t iteration,
-                                            uint32_t h0, uint32_t h1, uint32_t h2, double p,
-                                            double dir[3], double &tau) {
-  const uint32_t ctr[4] = {h0, h1, h2 ^ iteration, kPhiloxReemitTag};
-  uint32_t w[4];
-  philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32) + instance, w);
-  const double u = ((double)w[0] + 0.5) * (1.0 / 4294967296.0);
-  if (!(u < p)) return false;
-  const double cost = 2. * (((double)w[1] + 0.5) * (1.0 / 4294967296.0)) - 1.;
-  const double phi = 2. * 3.14159265358979323846 * (((double)w[2] + 0.5) * (1.0 / 4294967296.0));
-  const double s2 = 1. - cost * cost;
-  const double sint = sqrt((s2 < 0.) ? 0. : s2);
-  double sp, cp;
-  sincos(phi, &sp, &cp);
-  dir[0] = sint * cp;
-  dir[1] = sint * sp;
-  dir[2] = cost;
-  tau = -log(((double)w[3] + 0.5) * (1.0 / 4294967296.0));
+                                            uint32_t h0, uint32_t h1, uint32_t h2, uint32_t count,
+                                            double p, double dir[3], double &tau) {
+  const double inv32 = 1.0 / 4294967296.0;
+  for (uint32_t k = 0; k < 16u; ++k) {
+    const uint32_t ctr[4] = {h0, h1, h2 ^ iteration, kPhiloxReemitTag + (count << 4) + k};
+    uint32_t w[4];
+    philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32) + instance, w);
+    if (k == 0u && !(((double)w[0] + 0.5) * inv32 < p)) return false;
+    const double x1 = 2. * (((double)w[1] + 0.5) * inv32) - 1.;
+    const double x2 = 2. * (((double)w[2] + 0.5) * inv32) - 1.;
+    const double s = x1 * x1 + x2 * x2;
+    if (s < 1.) {
+      const double f = 2. * sqrt(1. - s);
+      dir[0] = x1 * f;
+      dir[1] = x2 * f;
+      dir[2] = 1. - 2. * s;
+      tau = reemit_neg_log(((double)w[3] + 0.5) * inv32);
+      return true;
+    }
+  }
+  dir[0] = 0.;  // 16 rejections in a row: probability 0.21^16
+  dir[1] = 0.;
+  dir[2] = 1.;
+  tau = 1.;
+  return true;
+}
+
+// Out-of-line copy for the walk kernels (the draw is rare; inlined it would
+// cost the walk loop registers): out = direction (3), optical depth.
+__device__ __noinline__ bool reemit_draw_call(uint64_t seed, uint32_t instance,
+                                              uint32_t iteration, uint32_t h0, uint32_t h1,
+                                              uint32_t h2, uint32_t count, double p,
+                                              double *out) {
+  double d[3], tau;
+  if (count >= kMaxReemissions ||
+      !reemit_draw(seed, instance, iteration, h0, h1, h2, count, p, d, tau))
+    return false;
+  out[0] = d[0];
+  out[1] = d[1];
+  out[2] = d[2];
+  out[3] = tau;
   return true;
 }
 

@@ -50,6 +50,10 @@ int fail(int code, const char *fmt, ...) {
 
 constexpr int kWalkThreads = 256;
 constexpr int kSpareRounds = 3;  // wavefront rounds beyond the straight-line bound
+// With reemission a packet starts new straight paths, so its subgrid transits
+// have no fixed bound: the round loop runs until no packet is left, capped
+// here only against a runaway loop.
+constexpr int kReemissionRoundCap = 4096;
 constexpr uint32_t kDefaultRefill = 16;  // lanes not walking before a warp routes + refills
 
 struct HostInstance {
@@ -91,7 +95,9 @@ struct cmi_context {
   uint32_t S = 0;
   int64_t total_padded = 0;
   int32_t max_padded = 0;
-  int rounds = 1;
+  int rounds = 1;     // straight-line bound + spares
+  int round_cap = 1;  // rounds an iteration may run (rounds, or more with reemission)
+  bool reemission = false;  // some instance re-emits absorbed packets
   DirectionTables tables{};
 
   DevSubgrid *d_sub = nullptr;
@@ -233,6 +239,10 @@ uint64_t total_budget(const cmi_context *c) {
 
 // Upload instance + source tables (after sources or budgets change).
 int upload_tables(cmi_context *c) {
+  bool reemission = false;
+  for (const HostInstance &I : c->inst) reemission = reemission || I.reemission > 0.;
+  c->round_cap = reemission ? std::max(c->rounds, kReemissionRoundCap) : c->rounds;
+  c->reemission = reemission;
   std::vector<DevInstance> di(c->inst.size());
   std::vector<DevSource> ds;
   for (size_t i = 0; i < c->inst.size(); ++i) {
@@ -381,13 +391,20 @@ bool walk32_three_per_sm(const cmi_context *c) {
   return c->opt.tally_mode == CMI_TALLY_FIXED64 && c->opt.ctas_per_sm == 3;
 }
 
+template <int kTally, bool kReemit>
+void launch_walk32_r(cmi_context *c, const WalkParams &p) {
+  if (kTally == 2 && walk32_three_per_sm(c))
+    k_walk32<kWalkThreads, 2, 3, kReemit>
+        <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+  else
+    k_walk32<kWalkThreads, kTally, walk32_min_blocks<kTally>(), kReemit>
+        <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+}
+
 template <int kTally>
 void launch_walk32_t(cmi_context *c, const WalkParams &p) {
-  if (kTally == 2 && walk32_three_per_sm(c))
-    k_walk32<kWalkThreads, 2, 3><<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
-  else
-    k_walk32<kWalkThreads, kTally, walk32_min_blocks<kTally>()>
-        <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+  if (c->reemission) launch_walk32_r<kTally, true>(c, p);
+  else launch_walk32_r<kTally, false>(c, p);
 }
 
 int launch_walk(cmi_context *c) {
@@ -438,13 +455,25 @@ int config_walk(cmi_context *c) {
     c->walk_smem = head + 4 * (size_t)c->max_padded + tally_bytes +
                    sizeof(Packet32) * 2 * (size_t)c->chunk +
                    (sizeof(Packet32) + 4) * (kWalkThreads / 32) * kStage;
+    // both builds (with and without reemission) get the attribute; the grid
+    // comes from the build without (the same 64-register occupancy bound)
     switch (tm) {
-      case 0: return config_kernel(c, k_walk32<kWalkThreads, 0, walk32_min_blocks<0>()>);
-      case 1: return config_kernel(c, k_walk32<kWalkThreads, 1, walk32_min_blocks<1>()>);
+      case 0:
+        CMI_TRY(config_kernel(c, k_walk32<kWalkThreads, 0, walk32_min_blocks<0>(), true>));
+        return config_kernel(c, k_walk32<kWalkThreads, 0, walk32_min_blocks<0>(), false>);
+      case 1:
+        CMI_TRY(config_kernel(c, k_walk32<kWalkThreads, 1, walk32_min_blocks<1>(), true>));
+        return config_kernel(c, k_walk32<kWalkThreads, 1, walk32_min_blocks<1>(), false>);
       case 2:
-        return walk32_three_per_sm(c) ? config_kernel(c, k_walk32<kWalkThreads, 2, 3>)
-                                      : config_kernel(c, k_walk32<kWalkThreads, 2, 4>);
-      default: return config_kernel(c, k_walk32<kWalkThreads, 3, walk32_min_blocks<3>()>);
+        if (walk32_three_per_sm(c)) {
+          CMI_TRY(config_kernel(c, k_walk32<kWalkThreads, 2, 3, true>));
+          return config_kernel(c, k_walk32<kWalkThreads, 2, 3, false>);
+        }
+        CMI_TRY(config_kernel(c, k_walk32<kWalkThreads, 2, 4, true>));
+        return config_kernel(c, k_walk32<kWalkThreads, 2, 4, false>);
+      default:
+        CMI_TRY(config_kernel(c, k_walk32<kWalkThreads, 3, walk32_min_blocks<3>(), true>));
+        return config_kernel(c, k_walk32<kWalkThreads, 3, walk32_min_blocks<3>(), false>);
     }
   }
   const size_t head = (sizeof(WalkShared) + 15) & ~(size_t)15;
@@ -474,8 +503,15 @@ EmitParams emit_params(cmi_context *c) {
 
 // Wavefront rounds once round 0 is planned: walk, then plan (+ scatter) the
 // packets it passed on; the last plan counts what is left over (must be zero).
+// Outside a graph the host reads the plan's chunk count and stops when no
+// packet is left (the graph's round loop does the same on the device).
 int enqueue_rounds(cmi_context *c) {
-  for (int r = 0; r < c->rounds; ++r) {
+  for (int r = 0; r < c->round_cap; ++r) {
+    uint32_t remaining = 0;
+    CMI_CUDA(cudaMemcpyAsync(&remaining, &c->d_state->num_chunks, sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, c->stream));
+    CMI_CUDA(cudaStreamSynchronize(c->stream));
+    if (remaining == 0u) break;
     CMI_TRY(timed_launch(c, 0, [&] { return launch_walk(c); }));
     CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c, true); }));
   }
@@ -494,7 +530,7 @@ int enqueue_rounds_graph(cmi_context *c) {
   if (cs != cudaStreamCaptureStatusActive) return fail(CMI_ERR_CUDA, "stream is not capturing");
   cudaGraphConditionalHandle h;
   CMI_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-  k_round_gate<<<1, 32, 0, c->stream>>>(c->d_state, h, (uint32_t)c->rounds);
+  k_round_gate<<<1, 32, 0, c->stream>>>(c->d_state, h, (uint32_t)c->round_cap);
   c->enqueued += 1;
   CMI_CUDA(cudaGetLastError());
   CMI_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
@@ -517,7 +553,7 @@ int enqueue_rounds_graph(cmi_context *c) {
   int rc = launch_walk(c);
   if (rc == CMI_OK) rc = launch_plan(c, true);
   if (rc == CMI_OK) {
-    k_round_gate<<<1, 32, 0, c->stream>>>(c->d_state, h, (uint32_t)c->rounds);
+    k_round_gate<<<1, 32, 0, c->stream>>>(c->d_state, h, (uint32_t)c->round_cap);
     c->enqueued += 1;
     if (cudaGetLastError() != cudaSuccess) rc = fail(CMI_ERR_CUDA, "round gate launch");
   }
@@ -667,7 +703,7 @@ int run(cmi_context *c, int32_t iterations, uint64_t seed, uint32_t first_iterat
   for (int32_t it = 0; it < iterations; ++it) {
     if (use_graph && ninst > 0) {  // the round loop ran once per round with packets
       const uint32_t r = std::min<uint32_t>(c->h_stats[(size_t)it * ninst].rounds,
-                                            (uint32_t)c->rounds);
+                                            (uint32_t)c->round_cap);
       c->last_launches += c->graph_body_kernels * r;
     }
     for (int i = 0; i < ninst; ++i) {

@@ -905,6 +905,7 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
     uint32_t wq_b = 0, wq_e = 0;
     bool exhausted = false, have = false, fresh = false;
     int entry = kRun;
+    uint32_t rcount = 0;  // reemissions of the lane's packet in this visit
     for (;;) {
       const unsigned idle = __ballot_sync(kFull, !have);
       if (idle != 0u && !exhausted) {
@@ -925,6 +926,7 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
           if (!have && r < take) {
             const Packet64 pk = load_packet(((const Packet64 *)prm.arena_in) + begin + wq_b + r);
             entry = w64.begin(pk, v64, sh.tab.sign_code);
+            rcount = 0u;
             have = true;
             fresh = true;
           }
@@ -966,14 +968,15 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
             // reemission from the absorption point (the photon as the
             // reference's next traversal task would receive it)
             Packet64 rp = w64.packet(v64, (uint32_t)kInside);
-            double rd[3], rtau;
+            double rd[4];
             if (sh.reemission > 0. &&
-                reemit_draw(rseed, sh.instance, riter, reemit_hash(rp.pos[0]),
-                            reemit_hash(rp.pos[1]), reemit_hash(rp.pos[2]), sh.reemission, rd,
-                            rtau)) {
+                reemit_draw_call(rseed, sh.instance, riter, reemit_hash(rp.pos[0]),
+                                 reemit_hash(rp.pos[1]), reemit_hash(rp.pos[2]), rcount,
+                                 sh.reemission, rd)) {
               ++c_reem;
+              ++rcount;
               for (int a = 0; a < 3; ++a) rp.dir[a] = rd[a];
-              rp.tau = rtau;
+              rp.tau = rd[3];
               entry = w64.begin(rp, v64, sh.tab.sign_code);
               fresh = true;
               reemitted = true;
@@ -1020,7 +1023,9 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
 constexpr int kStage = 48;
 constexpr uint32_t kStageFlush = 16;
 
-template <int kThreads, int kTally, int kMinBlocks>
+// kReemit: the build with reemission (any instance with p > 0); without it
+// the absorbed-packet path carries no reemission code.
+template <int kThreads, int kTally, int kMinBlocks, bool kReemit>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Walk32Shared &sh = *reinterpret_cast<Walk32Shared *>(smem_raw);
@@ -1222,6 +1227,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
       // lane states: active (walking), pending (finished, not yet routed), free
       bool exhausted = false, active = false, pending = false;
       int pstatus = kRun;
+      uint32_t rcount = 0;  // reemissions of the lane's packet in this visit
       for (;;) {
         const unsigned running = __ballot_sync(kFull, active);
         // Finished packets are routed and free lanes refilled in one batch,
@@ -1236,19 +1242,20 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
             if (pending) {
               ++c_trans;
               c_cross += (uint32_t)w.steps;  // one step per crossed cell
-              double rd[3], rtau;
-              if (pstatus == kAbsorbed && sh.reemission > 0. &&
-                  reemit_draw(rseed, sh.instance, riter, __float_as_uint(w.p[0]) ^ staged,
-                              __float_as_uint(w.p[1]) ^ (staged * 0x9E3779B9u),
-                              __float_as_uint(w.p[2]), sh.reemission, rd, rtau)) {
+              double rd[4];
+              if (kReemit && pstatus == kAbsorbed && sh.reemission > 0. &&
+                  reemit_draw_call(rseed, sh.instance, riter, __float_as_uint(w.p[0]) ^ staged,
+                                   __float_as_uint(w.p[1]) ^ (staged * 0x9E3779B9u),
+                                   __float_as_uint(w.p[2]), rcount, sh.reemission, rd)) {
                 // re-emitted in place: the lane walks on from the absorption point
                 ++c_reem;
+                ++rcount;
                 Packet32 rp;
                 for (int a = 0; a < 3; ++a) {
                   rp.pos[a] = w.p[a];
                   rp.dir[a] = (float)rd[a];
                 }
-                rp.tau = (float)rtau;
+                rp.tau = (float)rd[3];
                 rp.meta = (uint32_t)kInside;
                 pstatus = w.begin(rp, v, sh.tab.sign_code);
                 route = false;
@@ -1307,6 +1314,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
                 const uint32_t k = vi >> ch_shift;
                 const Packet32 pk = s_pk[(size_t)(k & 1u) * CH + (vi - (k << ch_shift))];
                 const int entry = w.begin(pk, v, sh.tab.sign_code);
+                rcount = 0u;
                 if (entry == kRun) {
                   active = true;
                 } else {  // absorbed or outside at entry: routed next batch
