@@ -363,6 +363,14 @@ int cmi_unet_train_step(cmi_unet *net, const float *features, const float *targe
 int cmi_unet_features(cmi_unet *net, const double *nH_cube, const int32_t dims[3],
                       const double box[6], const double *sources, int32_t num_sources,
                       double recombination_rate, const float norm[6], float *features);
+/* Resampling for grids finer than the network's training grid (cube order,
+ * device): block mean of an FP64 field by `factor` per axis (dims of the
+ * source, multiples of factor), nearest-neighbour upsampling of an FP32
+ * field by `factor` per axis (dims of the source). */
+int cmi_unet_block_mean(cmi_unet *net, const double *src, const int32_t dims[3], int32_t factor,
+                        double *dst);
+int cmi_unet_upsample_nearest(cmi_unet *net, const float *src, const int32_t dims[3],
+                              int32_t factor, float *dst);
 /* x_H = 10^clamp(prediction, log10_min, 0) as FP64 (device), n values */
 int cmi_unet_to_neutral_fraction(cmi_unet *net, const float *prediction, double *xH, int64_t n,
                                  float log10_min);

@@ -57,7 +57,7 @@ EXPORTED = [
     "cmi_unet_destroy", "cmi_unet_num_params", "cmi_unet_get_params", "cmi_unet_set_params",
     "cmi_unet_forward", "cmi_unet_gradients", "cmi_unet_train_step", "cmi_unet_features",
     "cmi_unet_to_neutral_fraction", "cmi_unet_conv3", "cmi_unet_pack_weights",
-    "cmi_unet_conv3_wgrad",
+    "cmi_unet_conv3_wgrad", "cmi_unet_block_mean", "cmi_unet_upsample_nearest",
 ]
 
 PHOTON_DTYPE = np.dtype(
@@ -195,6 +195,8 @@ def load():
     L.cmi_unet_conv3.argtypes = [vp, vp, i32, vp, vp, vp, i32, i32, i32, vp]
     L.cmi_unet_pack_weights.argtypes = [vp, vp, i32, i32, i32, vp]
     L.cmi_unet_conv3_wgrad.argtypes = [vp, vp, i32, vp, i32, i32, vp, vp]
+    L.cmi_unet_block_mean.argtypes = [vp, vp, vp, i32, vp]
+    L.cmi_unet_upsample_nearest.argtypes = [vp, vp, vp, i32, vp]
     for name in EXPORTED:
         f = getattr(L, name)
         if f.restype is C.c_int and name not in ("cmi_abi_version",):

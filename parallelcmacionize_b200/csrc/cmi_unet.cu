@@ -770,6 +770,34 @@ __global__ void k_features(FeatureArgs a) {
   }
 }
 
+// block mean of an FP64 cube (dims of the source, cube order) by `f` per axis
+__global__ void k_block_mean(const double *src, double *dst, int n0, int n1, int n2, int f) {
+  const int m0 = n0 / f, m1 = n1 / f, m2 = n2 / f;
+  const long long n = (long long)m0 * m1 * m2;
+  const double inv = 1. / ((double)f * f * f);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c2 = (int)(i % m2), c1 = (int)((i / m2) % m1), c0 = (int)(i / ((long long)m1 * m2));
+    double s = 0.;
+    for (int a = 0; a < f; ++a)
+      for (int b = 0; b < f; ++b)
+        for (int d = 0; d < f; ++d)
+          s += src[((long long)(c0 * f + a) * n1 + (c1 * f + b)) * n2 + (c2 * f + d)];
+    dst[i] = s * inv;
+  }
+}
+
+// nearest-neighbour upsampling of an FP32 cube by `f` per axis
+__global__ void k_upsample_nearest(const float *src, float *dst, int n0, int n1, int n2, int f) {
+  const int M0 = n0 * f, M1 = n1 * f, M2 = n2 * f;
+  const long long n = (long long)M0 * M1 * M2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c2 = (int)(i % M2), c1 = (int)((i / M2) % M1), c0 = (int)(i / ((long long)M1 * M2));
+    dst[i] = src[((long long)(c0 / f) * n1 + c1 / f) * n2 + c2 / f];
+  }
+}
+
 // x_H = 10^clamp(pred, lo, 0) as FP64 (the engine's field)
 __global__ void k_to_xH(const float *pred, double *xH, long long n, float lo) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -1513,6 +1541,34 @@ int cmi_unet_to_neutral_fraction(cmi_unet *u, const float *pred, double *xH, int
   if (!u || !pred || !xH || n < 0) return fail(CMI_ERR_INVALID_ARGUMENT, "bad argument");
   UN_CUDA(cudaSetDevice(u->device));
   k_to_xH<<<grid_for(n), 256, 0, u->stream>>>(pred, xH, n, log10_min);
+  UN_CUDA(cudaStreamSynchronize(u->stream));
+  return CMI_OK;
+}
+
+int cmi_unet_block_mean(cmi_unet *u, const double *src, const int32_t dims[3], int32_t factor,
+                        double *dst) {
+  if (!u || !src || !dst || !dims || factor < 1)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "bad argument");
+  for (int a = 0; a < 3; ++a)
+    if (dims[a] <= 0 || dims[a] % factor)
+      return fail(CMI_ERR_INVALID_ARGUMENT, "grid sides must be positive multiples of factor");
+  UN_CUDA(cudaSetDevice(u->device));
+  const long long n = (long long)(dims[0] / factor) * (dims[1] / factor) * (dims[2] / factor);
+  k_block_mean<<<grid_for(n), 256, 0, u->stream>>>(src, dst, dims[0], dims[1], dims[2], factor);
+  UN_CUDA(cudaGetLastError());
+  UN_CUDA(cudaStreamSynchronize(u->stream));
+  return CMI_OK;
+}
+
+int cmi_unet_upsample_nearest(cmi_unet *u, const float *src, const int32_t dims[3],
+                              int32_t factor, float *dst) {
+  if (!u || !src || !dst || !dims || factor < 1 || dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "bad argument");
+  UN_CUDA(cudaSetDevice(u->device));
+  const long long n = (long long)dims[0] * dims[1] * dims[2] * factor * factor * factor;
+  k_upsample_nearest<<<grid_for(n), 256, 0, u->stream>>>(src, dst, dims[0], dims[1], dims[2],
+                                                        factor);
+  UN_CUDA(cudaGetLastError());
   UN_CUDA(cudaStreamSynchronize(u->stream));
   return CMI_OK;
 }

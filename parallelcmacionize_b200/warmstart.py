@@ -386,6 +386,45 @@ def evaluate_loss(net, feats, labels, ncell, batch=8):
 # ---------------------------------------------------------------------------
 # warm start and the convergence comparison
 # ---------------------------------------------------------------------------
+def training_ncell(net):
+    """Cells per axis of the grids the network was trained on (64 unless its
+    weights say otherwise)."""
+    meta = getattr(net, "meta", {}) or {}
+    return int(meta["ncell"]) if "ncell" in meta else 64
+
+
+def predict_log_xH(net, grid, nH_dev):
+    """log10 x_H predicted for ``grid`` (torch FP32, cube order).
+
+    A grid finer than the training grid by an integer factor per axis is
+    predicted at the training resolution: n_H is block-averaged to it (the
+    sources keep their positions), the network runs there and its prediction is
+    upsampled back (nearest neighbour).  The features and the receptive field
+    are then the ones the network was trained on; the plain iterations that
+    follow resolve the finer structure."""
+    import torch
+    from .engine import GridSpec
+    n = tuple(int(v) for v in grid.ncell)
+    base = training_ncell(net)
+    f = n[0] // base if n[0] % base == 0 else 1
+    if f > 1 and all(v == base * f for v in n):
+        coarse = GridSpec(box=grid.box, ncell=(base,) * 3, num_subgrid=(1, 1, 1),
+                          recombination_rate=grid.recombination_rate,
+                          cross_section=grid.cross_section, sources=list(grid.sources))
+        nc = torch.empty(base ** 3, dtype=torch.float64, device=nH_dev.device)
+        net._sync()
+        check_unet(net._L.cmi_unet_block_mean(net._h, _ptr(nH_dev), (C.c_int32 * 3)(*n), f,
+                                              _ptr(nc)))
+        feats = net.features(nc, coarse).unsqueeze(0).contiguous()
+        pc = net.forward(feats, coarse.ncell)
+        out = torch.empty(int(np.prod(n)), dtype=torch.float32, device=nH_dev.device)
+        check_unet(net._L.cmi_unet_upsample_nearest(net._h, _ptr(pc), (C.c_int32 * 3)(*(base,) * 3),
+                                                    f, _ptr(out)))
+        return out
+    feats = net.features(nH_dev, grid).unsqueeze(0).contiguous()
+    return net.forward(feats, grid.ncell).reshape(-1)
+
+
 def warm_start(net, engine, instance, nH_cube, log10_min=LOG10_XH_MIN):
     """Predict x_H for an engine instance and load it.  ``nH_cube``: n_H in
     cube order, a torch CUDA tensor (FP64) or a host array (copied first)."""
@@ -396,8 +435,7 @@ def warm_start(net, engine, instance, nH_cube, log10_min=LOG10_XH_MIN):
         nH = nH_cube.reshape(-1)
     else:
         nH = torch.from_numpy(np.ascontiguousarray(nH_cube, dtype=np.float64).ravel()).to(dev)
-    f = net.features(nH, grid).unsqueeze(0).contiguous()
-    pred = net.forward(f, grid.ncell)
+    pred = predict_log_xH(net, grid, nH)
     x = net.to_neutral_fraction(pred, log10_min)
     torch.cuda.synchronize(dev)
     engine.set_fields_device(instance, 0, x.data_ptr(), layout="cube")
@@ -405,27 +443,38 @@ def warm_start(net, engine, instance, nH_cube, log10_min=LOG10_XH_MIN):
 
 
 def warm_breakdown(net, engine, instance, nH_dev, repeats=5):
-    """Milliseconds of the warm start's stages (features, network, x_H into
-    the engine), each bracketed by device synchronisations."""
+    """Milliseconds of the warm start's stages (prediction: features and
+    network, at the training resolution for finer grids; x_H into the engine),
+    each bracketed by device synchronisations."""
     import torch
     grid = engine.grids[instance]
-    t = {"features": 0.0, "network": 0.0, "load": 0.0}
+    t = {"predict": 0.0, "load": 0.0}
     for _ in range(repeats):
         torch.cuda.synchronize(net.device)
         t0 = time.perf_counter()
-        f = net.features(nH_dev, grid).unsqueeze(0).contiguous()
+        pred = predict_log_xH(net, grid, nH_dev)
         torch.cuda.synchronize(net.device)
         t1 = time.perf_counter()
-        pred = net.forward(f, grid.ncell)
-        torch.cuda.synchronize(net.device)
-        t2 = time.perf_counter()
         x = net.to_neutral_fraction(pred)
         engine.set_fields_device(instance, 0, x.data_ptr(), layout="cube")
-        t3 = time.perf_counter()
-        t["features"] += (t1 - t0) * 1e3 / repeats
-        t["network"] += (t2 - t1) * 1e3 / repeats
-        t["load"] += (t3 - t2) * 1e3 / repeats
+        t2 = time.perf_counter()
+        t["predict"] += (t1 - t0) * 1e3 / repeats
+        t["load"] += (t2 - t1) * 1e3 / repeats
     return t
+
+
+def reference_field(grid, nH_blocked, iterations=24, average=6, seed=5000, device=0):
+    """x_H (cube order) of a long plain run: ``iterations`` from x_H = 1e-6,
+    averaged over the last ``average`` (the converged answer, less noise)."""
+    from .engine import TransportEngine
+    with TransportEngine(grid, precision="fp32", device=device) as eng:
+        eng.set_fields(0, nH_blocked, np.full(nH_blocked.size, 1e-6))
+        eng.run_iterations(iterations - average, seed=seed)
+        acc = np.zeros(int(np.prod(grid.ncell)))
+        for k in range(average):
+            eng.run_iterations(1, seed=seed + 1 + k)
+            acc += eng.get_fields(0, layout="cube", intensity=False)[0]
+    return acc / average
 
 
 def time_to_converge(net, grid, nH_blocked, x_reference=None, tolerance=0.01,

@@ -44,3 +44,30 @@ def test_warm_start_converges_faster_to_the_same_field(net, seed):
     assert r["warm"]["error_vs_reference"] <= r["plain"]["error_vs_reference"] + 0.005, r
     # wall time, features and network included (the bench measures it precisely)
     assert r["speedup"] > 1.5, r
+
+
+def test_finer_grids_are_predicted_at_the_training_resolution(net):
+    """A 128^3 grid: n_H is block-averaged to 64^3 (checked against numpy),
+    the network predicts there and the prediction is upsampled (nearest)."""
+    import ctypes as C
+
+    from parallelcmacionize_b200 import GridSpec, _lib
+    from parallelcmacionize_b200.problems import BOX_10PC, lognormal_density, random_sources
+    from parallelcmacionize_b200.warmstart import predict_log_xH
+
+    fine = lognormal_density(128, seed=3)
+    srcs = random_sources(BOX_10PC, 3, seed=4)
+    g128 = GridSpec(box=BOX_10PC, ncell=(128,) * 3, num_subgrid=(8,) * 3, sources=srcs)
+    g64 = GridSpec(box=BOX_10PC, ncell=(64,) * 3, num_subgrid=(4,) * 3, sources=srcs)
+    dev = torch.from_numpy(fine.ravel().copy()).cuda()
+    coarse = torch.empty(64 ** 3, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check_unet(net._L.cmi_unet_block_mean(net._h, C.c_void_p(dev.data_ptr()),
+                                               (C.c_int32 * 3)(128, 128, 128), 2,
+                                               C.c_void_p(coarse.data_ptr())))
+    ref = fine.reshape(64, 2, 64, 2, 64, 2).mean(axis=(1, 3, 5))
+    np.testing.assert_allclose(coarse.cpu().numpy().reshape(64, 64, 64), ref, rtol=1e-14)
+    p128 = predict_log_xH(net, g128, dev).cpu().numpy().reshape(128, 128, 128)
+    p64 = predict_log_xH(net, g64, coarse).cpu().numpy().reshape(64, 64, 64)
+    up = np.repeat(np.repeat(np.repeat(p64, 2, 0), 2, 1), 2, 2)
+    assert np.array_equal(p128, up)
