@@ -42,6 +42,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CROSSING = 32  # FP64 n, x read + J read-modify-write per crossing
+# DRAM bytes (read + write) per k_walk32 launch, averaged over the 12 walk
+# launches of one iteration of the default workload (1e7 packets, FP32 walk),
+# from an ncu capture of `bench.py --steps 3 --warmup 3`; other workloads and
+# settings were not captured and report null.
+WALK_TRAFFIC_PER_LAUNCH = {("lognormal128", 1e7, "fp32"): 94.02e6}
 METRIC = "cell-crossings/s"  # plus time to converged x_H, warm start vs plain ("warm_start")
 UNIT = "crossings/s"
 DESCRIPTIONS = {
@@ -78,6 +83,8 @@ def parse():
     ap.add_argument("--no-warm-start", action="store_true",
                     help="skip the time-to-convergence comparison (warm start vs plain)")
     ap.add_argument("--warm-start-seeds", type=int, default=4)
+    ap.add_argument("--no-fp64-check", action="store_true",
+                    help="skip the FP32-vs-FP64 mean-intensity comparison (large256 only)")
     return ap.parse_args()
 
 
@@ -124,6 +131,42 @@ def warm_start_comparison(seeds, workload="warmstart64"):
                                                      for r in runs])),
         "warm_overhead_ms": {k: float(np.mean([r["warm_breakdown_ms"][k] for r in runs]))
                              for k in runs[0]["warm_breakdown_ms"]},
+    }
+
+
+def intensity_error_vs_fp64(spec, nH, x_start, seed=61, device=0):
+    """One iteration from the same x_H field and the same Philox packets through
+    the FP32 walk and the FP64 walk (the reference's interact arithmetic, bit
+    for bit): the error of the FP32 mean intensity J and of the x_H that the
+    FP64 balance makes of it."""
+    from parallelcmacionize_b200 import TransportEngine
+    res = {}
+    for prec in ("fp64", "fp32"):
+        with TransportEngine(spec, precision=prec, device=device) as eng:
+            eng.set_fields(0, nH, x_start)
+            st = eng.shoot_packets(seed=seed, iteration=0)[0]
+            J = eng.get_fields(0)[1]
+            eng.set_fields(0, None, x_start)
+            eng.run_iterations(1, seed=seed)
+            x = eng.get_fields(0, intensity=False)[0]
+        res[prec] = (st, x, J)
+    (s64, x64, J64), (s32, x32, J32) = res["fp64"], res["fp32"]
+    lit = J64 > 1e-3 * J64.max()
+    if not lit.any():
+        raise SystemExit("FP64 walk left J = 0 everywhere")
+    rel = np.abs(J32[lit] - J64[lit]) / J64[lit]
+    return {
+        "what": ("one iteration from the same x_H and the same packets, FP32 walk vs FP64 "
+                 "walk; J relative error over cells with J > 1e-3 max J"),
+        "cells_compared": int(lit.sum()),
+        "J_rel_error_median": float(np.median(rel)),
+        "J_rel_error_p99": float(np.quantile(rel, 0.99)),
+        "J_rel_error_max": float(rel.max()),
+        "J_sum_rel_error": float(abs(J32.sum() - J64.sum()) / J64.sum()),
+        "x_H_mean_abs_error": float(np.mean(np.abs(x32 - x64))),
+        "crossings_rel_difference": float(abs(int(s32["cell_crossings"]) -
+                                              int(s64["cell_crossings"])) /
+                                          s64["cell_crossings"]),
     }
 
 
@@ -379,7 +422,9 @@ def ours(args):
                   "k_walk64 (transport round)",
         "bound": "hbm", "achieved": achieved,
         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-        "traffic": None, "algorithmic_bytes_per_crossing": BYTES_PER_CROSSING,
+        "traffic": WALK_TRAFFIC_PER_LAUNCH.get((args.workload, wl.total_packets, args.precision)),
+        "algorithmic_bytes_per_launch": kt_cross * BYTES_PER_CROSSING / max(walk_launches, 1),
+        "algorithmic_bytes_per_crossing": BYTES_PER_CROSSING,
         "walk_ms_per_iteration": walk_ms, "walk_launches_per_iteration": walk_launches,
         "walk_share_of_iteration": walk_ms / total_kt if total_kt else None,
         "kernel_ms": {k: v[0] for k, v in kt.items()},
@@ -429,6 +474,11 @@ def ours(args):
         else:
             warm = warm_start_comparison([101_980 + k for k in range(args.warm_start_seeds)])
 
+    jerr = None
+    if rank == 0 and world == 1 and args.workload == "large256" and not args.no_fp64_check:
+        jerr = intensity_error_vs_fp64(wl.specs[0], wl.fields[0],
+                                       eng.get_fields(0, intensity=False)[0], device=local)
+
     if rank == 0:
         ncells = sum(int(np.prod(g.ncell)) for g in wl.specs)
         line = {
@@ -457,6 +507,7 @@ def ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "warm_start": warm,
+            "fp32_vs_fp64": jerr,
             "mean_abs_dx_last": stats[-1]["mean_abs_dx"],
             "rounds": stats[-1]["rounds"],
         }
