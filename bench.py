@@ -93,9 +93,10 @@ WARM_WORKLOADS = {
                     "per cell), held-out seeds of the shipped network; convergence = mean "
                     "|delta x_H| < 0.01 (the plain method's criterion)"),
     "large256": ("large256: 256^3 as 16^3 subgrids of 16^3, sigma_ln=1.5, 16 sources, 1e8 "
-                 "packets/iteration; the network (trained at 64^3) predicts on n_H averaged "
-                 "to 64^3, upsampled; convergence = mean |delta x_H| < 0.01 (1e-3 is below "
-                 "the Monte Carlo floor at 6 packets per cell)"),
+                 "packets/iteration, seeds the 256^3 network did not train on; the network "
+                 "predicts at 256^3 (channel 2 marched on the 64^3 block mean); convergence = "
+                 "mean |delta x_H| < 0.01 (1e-3 is below the Monte Carlo floor at 6 packets "
+                 "per cell)"),
 }
 
 
@@ -105,14 +106,16 @@ def warm_start_comparison(seeds, workload="warmstart64"):
     did not train on; accuracy against a long plain run (24 iterations, last 6
     averaged)."""
     from parallelcmacionize_b200.problems import large_config
-    from parallelcmacionize_b200.warmstart import (DEFAULT_WEIGHTS, UNet, reference_field,
-                                                   run_configs, time_to_converge)
-    if not os.path.exists(DEFAULT_WEIGHTS):
+    from parallelcmacionize_b200.warmstart import (UNet, reference_field, run_configs,
+                                                   time_to_converge, weights_for)
+    cfgs = [large_config(seed=s) if workload == "large256" else run_configs([s])[0]
+            for s in seeds]
+    weights = weights_for(cfgs[0][0])
+    if not os.path.exists(weights):
         return None
     runs = []
-    with UNet.load(DEFAULT_WEIGHTS) as net:
-        for s in seeds:
-            g, nH = large_config(seed=s) if workload == "large256" else run_configs([s])[0]
+    with UNet.load(weights) as net:
+        for g, nH in cfgs:
             ref = reference_field(g, nH)
             runs.append(time_to_converge(net, g, nH, x_reference=ref, tolerance=0.01))
 
@@ -120,6 +123,7 @@ def warm_start_comparison(seeds, workload="warmstart64"):
         return float(np.mean([r[mode][key] for r in runs]))
     return {
         "workload": WARM_WORKLOADS[workload], "seeds": list(seeds),
+        "weights": os.path.basename(weights),
         "plain_ms": 1e3 * mean("plain", "seconds"), "warm_ms": 1e3 * mean("warm", "seconds"),
         "plain_iterations": mean("plain", "iterations"),
         "warm_iterations": mean("warm", "iterations"),

@@ -363,6 +363,18 @@ int cmi_unet_train_step(cmi_unet *net, const float *features, const float *targe
 int cmi_unet_features(cmi_unet *net, const double *nH_cube, const int32_t dims[3],
                       const double box[6], const double *sources, int32_t num_sources,
                       double recombination_rate, const float norm[6], float *features);
+/* The same channels with channel 2 computed on the grid coarser by
+ * ratio_factor per axis (n_H block-averaged, dims multiples of the factor) and
+ * interpolated trilinearly in log10 to the cell centres: the ray march costs
+ * ratio_factor^4 times less.  ratio_factor = 1 is cmi_unet_features. */
+int cmi_unet_features_coarse_ratio(cmi_unet *net, const double *nH_cube, const int32_t dims[3],
+                                   const double box[6], const double *sources,
+                                   int32_t num_sources, double recombination_rate,
+                                   const float norm[6], int32_t ratio_factor, float *features);
+/* Weight of the squared error of predictions above the target (a neutral
+ * fraction too high) in the loss of cmi_unet_gradients / cmi_unet_train_step;
+ * 1 (the default) is the mean squared error. */
+int cmi_unet_set_loss_weight(cmi_unet *net, float over_weight);
 /* Resampling for grids finer than the network's training grid (cube order,
  * device): block mean of an FP64 field by `factor` per axis (dims of the
  * source, multiples of factor), nearest-neighbour upsampling of an FP32

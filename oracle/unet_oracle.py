@@ -179,18 +179,25 @@ class UNetOracle:
         self.s = s
         return s["pred"]
 
-    def loss(self, feats, target):
-        p = self.forward(feats)
-        return float(np.mean((p - target) ** 2))
+    @staticmethod
+    def _weights(diff, over_weight):
+        """Per-voxel loss weights: over_weight where the prediction is above
+        the target (the library's cmi_unet_set_loss_weight), else 1."""
+        return np.where(diff > 0, over_weight, 1.0)
 
-    def gradients(self, feats, target):
+    def loss(self, feats, target, over_weight=1.0):
+        d = self.forward(feats) - target
+        return float(np.mean(self._weights(d, over_weight) * d ** 2))
+
+    def gradients(self, feats, target, over_weight=1.0):
         """(loss, gradient in the library's parameter order)."""
         q = self._q
         pred = self.forward(feats)
         s = self.s
         n = pred.size
         c1, c2, c3 = self.c
-        gp = 2.0 * (pred - target) / n
+        w = self._weights(pred - target, over_weight)
+        gp = 2.0 * w * (pred - target) / n
         g_hw = np.einsum("bzyxc,bzyx->c", s["d1b"], gp)
         g_hb = np.array([gp.sum()])
         gW = [None] * 10
@@ -232,5 +239,5 @@ class UNetOracle:
             parts.append(gb[i])
         parts.append(g_hw)
         parts.append(g_hb)
-        loss = float(np.mean((pred - target) ** 2))
+        loss = float(np.mean(w * (pred - target) ** 2))
         return loss, np.concatenate(parts)

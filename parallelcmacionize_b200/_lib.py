@@ -58,6 +58,7 @@ EXPORTED = [
     "cmi_unet_forward", "cmi_unet_gradients", "cmi_unet_train_step", "cmi_unet_features",
     "cmi_unet_to_neutral_fraction", "cmi_unet_conv3", "cmi_unet_pack_weights",
     "cmi_unet_conv3_wgrad", "cmi_unet_block_mean", "cmi_unet_upsample_nearest",
+    "cmi_unet_features_coarse_ratio", "cmi_unet_set_loss_weight",
 ]
 
 PHOTON_DTYPE = np.dtype(
@@ -197,6 +198,9 @@ def load():
     L.cmi_unet_conv3_wgrad.argtypes = [vp, vp, i32, vp, i32, i32, vp, vp]
     L.cmi_unet_block_mean.argtypes = [vp, vp, vp, i32, vp]
     L.cmi_unet_upsample_nearest.argtypes = [vp, vp, vp, i32, vp]
+    L.cmi_unet_features_coarse_ratio.argtypes = [vp, vp, vp, vp, vp, i32, C.c_double, vp, i32,
+                                                 vp]
+    L.cmi_unet_set_loss_weight.argtypes = [vp, C.c_float]
     for name in EXPORTED:
         f = getattr(L, name)
         if f.restype is C.c_int and name not in ("cmi_abi_version",):

@@ -566,7 +566,7 @@ __global__ void k_up2_bwd(const bf16 *din, int ictot, int ic0, bf16 *dout, int o
 // db += dpred.
 __global__ void k_head(const bf16 *h, int hctot, int c, const float *w, const float *b,
                        long long nvox, float *pred, const float *target, bf16 *dh,
-                       float *dw, float *db, float *loss) {
+                       float *dw, float *db, float *loss, float over_weight) {
   __shared__ float red[256];
   __shared__ float redw[16][33];
   float l = 0.f, gb = 0.f;
@@ -582,8 +582,11 @@ __global__ void k_head(const bf16 *h, int hctot, int c, const float *w, const fl
     if (pred) pred[v] = p;
     if (target) {
       const float diff = p - target[v];
-      l += diff * diff;
-      const float g = 2.f * diff / (float)nvox;
+      // squared errors of predictions above the target (too neutral) weigh
+      // over_weight: those fronts recover one cell per plain iteration
+      const float wl = diff > 0.f ? over_weight : 1.f;
+      l += wl * diff * diff;
+      const float g = 2.f * wl * diff / (float)nvox;
       gb += g;
       for (int k = 0; k < hctot; ++k)
         dh[v * hctot + k] = __float2bfloat16_rn(k < c ? g * w[k] : 0.f);
@@ -708,7 +711,38 @@ struct FeatureArgs {
   int nsrc;
   double alpha, nref;
   float norm[2 * kFeatures];  // (mean, scale) per channel
+  // 0: all three channels; 1: raw log10 of channel 2 only (out holds one
+  // float per cell); 2: channels 0-1 here, channel 2 interpolated
+  // (trilinear, in log10) from `ratio`, a raw mode-1 field on the grid
+  // coarser by `rf` per axis (rm cells along ix, iy, iz)
+  int mode;
+  const float *ratio;
+  int rm[3];
+  int rf;
 };
+
+// channel 2 of a fine cell from the coarse raw field: coarse cell centres
+// sit at fine coordinate (c + 0.5) rf - 0.5; outside them the edge value holds
+__device__ float ratio_from_coarse(const FeatureArgs &a, const int i3[3]) {
+  int lo[3], hi[3];
+  float t[3];
+  for (int k = 0; k < 3; ++k) {
+    float u = ((float)i3[k] + 0.5f) / (float)a.rf - 0.5f;
+    u = fminf(fmaxf(u, 0.f), (float)(a.rm[k] - 1));
+    lo[k] = min((int)u, a.rm[k] - 1);
+    hi[k] = min(lo[k] + 1, a.rm[k] - 1);
+    t[k] = u - (float)lo[k];
+  }
+  float acc = 0.f;
+  for (int c = 0; c < 8; ++c) {
+    const int j0 = (c & 4) ? hi[0] : lo[0], j1 = (c & 2) ? hi[1] : lo[1],
+              j2 = (c & 1) ? hi[2] : lo[2];
+    const float w = ((c & 4) ? t[0] : 1.f - t[0]) * ((c & 2) ? t[1] : 1.f - t[1]) *
+                    ((c & 1) ? t[2] : 1.f - t[2]);
+    acc += w * a.ratio[((long long)j0 * a.rm[1] + j1) * a.rm[2] + j2];
+  }
+  return acc;
+}
 
 __global__ void k_nrel(const double *nH, float *nrel, long long n, double inv_nref) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -742,6 +776,7 @@ __global__ void k_features(FeatureArgs a) {
                                             __dmul_rn(dm[2], dm[2])));
       const double rc = fmax(r, rmin);
       flux += S[3] / (4. * 3.141592653589793 * rc * rc);
+      if (a.mode == 2) continue;  // channel 2 comes from the coarse field
       const float rh = (float)__ddiv_rn(r, hmin);  // length in units of hmin
       const int nstep = max(1, (int)ceilf(__fdiv_rn(rh, hstep)));
       const float inv = __frcp_rn((float)nstep);
@@ -763,10 +798,16 @@ __global__ void k_features(FeatureArgs a) {
                        hmin;
       strom += S[3] / (4. * 3.141592653589793 * a.alpha * fmax(R, 1e-300));
     }
+    const double lratio = log10(fmin(fmax(strom, 1e-30), 1e30));
+    if (a.mode == 1) {
+      a.out[v] = (float)lratio;
+      continue;
+    }
     float *o = a.out + kFeatures * v;
     o[0] = (float)((log10(a.nH[v]) - a.norm[0]) / a.norm[1]);
     o[1] = (float)((log10(fmax(flux, 1e-300)) - a.norm[2]) / a.norm[3]);
-    o[2] = (float)((log10(fmin(fmax(strom, 1e-30), 1e30)) - a.norm[4]) / a.norm[5]);
+    const float l2 = a.mode == 2 ? ratio_from_coarse(a, i3) : (float)lratio;
+    o[2] = (l2 - a.norm[4]) / a.norm[5];
   }
 }
 
@@ -881,6 +922,11 @@ struct cmi_unet {
   size_t src_cap = 0;
   float *d_nrel = nullptr;  // n_H / n_ref for the features kernel
   size_t nrel_cap = 0;
+  double *d_ncoarse = nullptr;  // block-mean n_H of the coarse ratio pass
+  size_t ncoarse_cap = 0;
+  float *d_ratio = nullptr;     // raw coarse channel 2
+  size_t ratio_cap = 0;
+  float over_weight = 1.f;      // loss weight of predictions above the target
   bool packed = false;
 };
 
@@ -1153,7 +1199,8 @@ int backward(cmi_unet *u, const float *target, int batch, const int d1[3]) {
   UN_CUDA(cudaMemsetAsync(u->d_loss, 0, sizeof(float), u->stream));
   k_head<<<grid_for(v1), 256, 0, u->stream>>>(u->D1B, c.s1, c.c1, u->p + u->head_w,
                                                u->p + u->head_b, v1, u->pred, target, u->gD1B,
-                                               u->g + u->head_w, u->g + u->head_b, u->d_loss);
+                                               u->g + u->head_w, u->g + u->head_b, u->d_loss,
+                                               u->over_weight);
   const float sl = u->slope;
   // one convolution layer backwards: dy (in place) *= act'(y); wgrad; input gradient
   auto layer_bwd = [&](int li, const Slice &x, const Slice &y, const Slice &dy, const Slice *dx,
@@ -1391,6 +1438,8 @@ int cmi_unet_destroy(cmi_unet *u) {
   cudaFree(u->d_loss);
   cudaFree(u->d_src);
   cudaFree(u->d_nrel);
+  cudaFree(u->d_ncoarse);
+  cudaFree(u->d_ratio);
   if (u->stream) cudaStreamDestroy(u->stream);
   delete u;
   return CMI_OK;
@@ -1434,7 +1483,7 @@ int cmi_unet_forward(cmi_unet *u, const float *features, float *pred, int32_t ba
   const Chans c = chans(u);
   k_head<<<grid_for(v1), 256, 0, u->stream>>>(u->D1B, c.s1, c.c1, u->p + u->head_w,
                                                u->p + u->head_b, v1, pred, nullptr, nullptr,
-                                               nullptr, nullptr, nullptr);
+                                               nullptr, nullptr, nullptr, 1.f);
   UN_CUDA(cudaGetLastError());
   return check_err(u);
 }
@@ -1481,23 +1530,24 @@ int cmi_unet_train_step(cmi_unet *u, const float *features, const float *target,
   return CMI_OK;
 }
 
-int cmi_unet_features(cmi_unet *u, const double *nH_cube, const int32_t dims[3],
-                      const double box[6], const double *sources, int32_t num_sources,
-                      double recombination_rate, const float norm[6], float *features) {
-  if (!u || !nH_cube || !dims || !box || !norm || !features || (num_sources > 0 && !sources))
-    return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
-  if (num_sources < 0 || num_sources > 4096)
-    return fail(CMI_ERR_INVALID_ARGUMENT, "0..4096 sources");
-  if (!(recombination_rate > 0.) || !std::isfinite(recombination_rate))
-    return fail(CMI_ERR_INVALID_ARGUMENT, "recombination rate must be > 0");
-  for (int k = 0; k < 3; ++k)
-    if (dims[k] <= 0 || !(box[3 + k] > 0.))
-      return fail(CMI_ERR_INVALID_ARGUMENT, "grid sides and box sizes must be > 0");
-  UN_CUDA(cudaSetDevice(u->device));
-  FeatureArgs a{};
-  a.nH = nH_cube;
-  a.alpha = recombination_rate;
-  a.out = features;
+}  // extern "C"
+
+namespace cmiu {
+
+// grow-only device scratch
+template <class T>
+int ensure(T **p, size_t *cap, size_t n) {
+  if (n <= *cap) return CMI_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  UN_CUDA(cudaMalloc(p, sizeof(T) * n));
+  *cap = n;
+  return CMI_OK;
+}
+
+// geometry of a (dims, box) grid in the kernel's axis conventions
+void grid_args(FeatureArgs &a, const int32_t dims[3], const double box[6]) {
   a.dims[0] = dims[2];  // X = iz (fastest)
   a.dims[1] = dims[1];
   a.dims[2] = dims[0];  // Z = ix
@@ -1506,14 +1556,31 @@ int cmi_unet_features(cmi_unet *u, const double *nH_cube, const int32_t dims[3],
     a.origin[k] = box[k];
     a.cell[k] = box[3 + k] / dims[k];
   }
-  if ((size_t)num_sources > u->src_cap) {
-    cudaFree(u->d_src);
-  cudaFree(u->d_nrel);
-    u->d_src = nullptr;
-    u->src_cap = 0;
-    UN_CUDA(cudaMalloc(&u->d_src, sizeof(double) * 4 * num_sources));
-    u->src_cap = (size_t)num_sources;
+}
+
+int features_impl(cmi_unet *u, const double *nH_cube, const int32_t dims[3], const double box[6],
+                  const double *sources, int32_t num_sources, double recombination_rate,
+                  const float norm[6], int32_t ratio_factor, float *features) {
+  if (!u || !nH_cube || !dims || !box || !norm || !features || (num_sources > 0 && !sources))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  if (num_sources < 0 || num_sources > 4096)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "0..4096 sources");
+  if (!(recombination_rate > 0.) || !std::isfinite(recombination_rate))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "recombination rate must be > 0");
+  if (ratio_factor < 1 || ratio_factor > 64)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "ratio factor must be in 1..64");
+  for (int k = 0; k < 3; ++k) {
+    if (dims[k] <= 0 || !(box[3 + k] > 0.))
+      return fail(CMI_ERR_INVALID_ARGUMENT, "grid sides and box sizes must be > 0");
+    if (dims[k] % ratio_factor)
+      return fail(CMI_ERR_INVALID_ARGUMENT, "grid sides must be multiples of the ratio factor");
   }
+  UN_CUDA(cudaSetDevice(u->device));
+  FeatureArgs a{};
+  a.nH = nH_cube;
+  a.alpha = recombination_rate;
+  a.nref = 1e8;  // n_H unit of the ray sums (FP32 range)
+  UN_TRY(ensure(&u->d_src, &u->src_cap, (size_t)4 * std::max(num_sources, 1)));
   if (num_sources > 0)
     UN_CUDA(cudaMemcpyAsync(u->d_src, sources, sizeof(double) * 4 * num_sources,
                             cudaMemcpyHostToDevice, u->stream));
@@ -1521,18 +1588,69 @@ int cmi_unet_features(cmi_unet *u, const double *nH_cube, const int32_t dims[3],
   a.nsrc = num_sources;
   for (int k = 0; k < 2 * kFeatures; ++k) a.norm[k] = norm[k];
   const long long nv = (long long)dims[0] * dims[1] * dims[2];
-  if ((size_t)nv > u->nrel_cap) {
-    cudaFree(u->d_nrel);
-    u->d_nrel = nullptr;
-    u->nrel_cap = 0;
-    UN_CUDA(cudaMalloc(&u->d_nrel, sizeof(float) * nv));
-    u->nrel_cap = (size_t)nv;
+  if (ratio_factor == 1) {
+    UN_TRY(ensure(&u->d_nrel, &u->nrel_cap, (size_t)nv));
+    grid_args(a, dims, box);
+    a.nrel = u->d_nrel;
+    a.out = features;
+    k_nrel<<<grid_for(nv), 256, 0, u->stream>>>(nH_cube, u->d_nrel, nv, 1. / a.nref);
+    k_features<<<grid_for(nv), 256, 0, u->stream>>>(a);
+  } else {
+    // channel 2 on the grid coarser by ratio_factor (block-mean n_H), then
+    // interpolated: the march costs ratio_factor^4 times less
+    const int f = ratio_factor;
+    const int32_t cd[3] = {dims[0] / f, dims[1] / f, dims[2] / f};
+    const long long nc = (long long)cd[0] * cd[1] * cd[2];
+    UN_TRY(ensure(&u->d_ncoarse, &u->ncoarse_cap, (size_t)nc));
+    UN_TRY(ensure(&u->d_nrel, &u->nrel_cap, (size_t)nc));
+    UN_TRY(ensure(&u->d_ratio, &u->ratio_cap, (size_t)nc));
+    k_block_mean<<<grid_for(nc), 256, 0, u->stream>>>(nH_cube, u->d_ncoarse, dims[0], dims[1],
+                                                      dims[2], f);
+    k_nrel<<<grid_for(nc), 256, 0, u->stream>>>(u->d_ncoarse, u->d_nrel, nc, 1. / a.nref);
+    FeatureArgs c = a;
+    grid_args(c, cd, box);
+    c.nH = u->d_ncoarse;
+    c.nrel = u->d_nrel;
+    c.out = u->d_ratio;
+    c.mode = 1;
+    k_features<<<grid_for(nc), 256, 0, u->stream>>>(c);
+    grid_args(a, dims, box);
+    a.out = features;
+    a.mode = 2;
+    a.ratio = u->d_ratio;
+    a.rf = f;
+    for (int k = 0; k < 3; ++k) a.rm[k] = cd[k];
+    k_features<<<grid_for(nv), 256, 0, u->stream>>>(a);
   }
-  a.nref = 1e8;  // n_H unit of the ray sums (FP32 range)
-  a.nrel = u->d_nrel;
-  k_nrel<<<grid_for(nv), 256, 0, u->stream>>>(nH_cube, u->d_nrel, nv, 1. / a.nref);
-  k_features<<<grid_for(nv), 256, 0, u->stream>>>(a);
+  UN_CUDA(cudaGetLastError());
   UN_CUDA(cudaStreamSynchronize(u->stream));
+  return CMI_OK;
+}
+
+}  // namespace cmiu
+
+extern "C" {
+
+int cmi_unet_features(cmi_unet *u, const double *nH_cube, const int32_t dims[3],
+                      const double box[6], const double *sources, int32_t num_sources,
+                      double recombination_rate, const float norm[6], float *features) {
+  return cmiu::features_impl(u, nH_cube, dims, box, sources, num_sources, recombination_rate,
+                             norm, 1, features);
+}
+
+int cmi_unet_features_coarse_ratio(cmi_unet *u, const double *nH_cube, const int32_t dims[3],
+                                   const double box[6], const double *sources,
+                                   int32_t num_sources, double recombination_rate,
+                                   const float norm[6], int32_t ratio_factor, float *features) {
+  return cmiu::features_impl(u, nH_cube, dims, box, sources, num_sources, recombination_rate,
+                             norm, ratio_factor, features);
+}
+
+int cmi_unet_set_loss_weight(cmi_unet *u, float over_weight) {
+  if (!u) return fail(CMI_ERR_INVALID_ARGUMENT, "null network");
+  if (!(over_weight > 0.f) || !std::isfinite(over_weight))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "loss weight must be finite and > 0");
+  u->over_weight = over_weight;
   return CMI_OK;
 }
 

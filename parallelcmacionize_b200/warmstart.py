@@ -15,6 +15,16 @@ it starts, so a bad prediction costs iterations, never correctness.
   log-normal generator, iterated to convergence; the label is log10 of x_H
   averaged over the last iterations (less Monte Carlo noise).
 * ``train``            -- Adam on mean squared error of log10 x_H.
+* ``generate_large_runs`` / ``train_crops`` -- the same for the 256^3
+  generator (problems.large_config): long plain runs kept on the device,
+  training on random 64^3 windows, fine-tuned from the 64^3 weights with an
+  asymmetric loss (``UNet.set_loss_weight``) that penalises predicting x_H too
+  high: an ionization front predicted too far in towards the source moves out
+  by about one cell per plain iteration (one neutral cell is tens of optical
+  depths), while one predicted too far out is pulled back in one iteration.
+* ``weights_for``      -- the shipped weights for a grid: trained at its own
+  side if there are such (256^3), else the 64^3 network, which predicts finer
+  grids on block-averaged n_H.
 * ``warm_start``       -- features -> prediction -> x_H of an engine instance.
 * ``time_to_converge`` -- iterations and wall time to convergence from the
   plain start and from the warm start, on the same inputs.
@@ -37,8 +47,20 @@ from ._lib import check_unet
 # log10 x_H below this is not predicted (the plain start is 1e-6)
 LOG10_XH_MIN = -8.0
 NUM_FEATURES = 3  # density, unattenuated flux, Stromgren ratio (cmi_unet_features)
-DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
-                               "warmstart_unet64.npz")
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "warmstart_unet64.npz")
+LARGE_WEIGHTS = os.path.join(WEIGHTS_DIR, "warmstart_unet256.npz")
+# grid side -> shipped weights trained at that side
+SHIPPED = {64: DEFAULT_WEIGHTS, 256: LARGE_WEIGHTS}
+
+
+def weights_for(grid):
+    """Shipped weights for ``grid``: the network trained on grids of its side
+    when there is one, else the 64^3 network."""
+    n = tuple(int(v) for v in grid.ncell)
+    if n[0] == n[1] == n[2] and n[0] in SHIPPED and os.path.exists(SHIPPED[n[0]]):
+        return SHIPPED[n[0]]
+    return DEFAULT_WEIGHTS
 
 
 def _ptr(t):
@@ -176,10 +198,17 @@ class UNet:
                                                C.byref(loss)))
         return float(loss.value)
 
-    def features(self, nH_cube, grid, out=None, norm=None):
+    def set_loss_weight(self, over_weight):
+        """Weight of the squared error where the prediction is above the target
+        (x_H too high) in the training loss; 1 = mean squared error."""
+        check_unet(self._L.cmi_unet_set_loss_weight(self._h, float(over_weight)))
+
+    def features(self, nH_cube, grid, out=None, norm=None, ratio_factor=None):
         """Features [cells, 3] of one grid from its FP64 n_H (torch, device,
         cube order) and the GridSpec's box, sources and recombination rate;
-        ``norm`` defaults to the network's normalisation."""
+        ``norm`` defaults to the network's normalisation.  ``ratio_factor`` >
+        1 computes channel 2 on the grid that much coarser and interpolates it
+        (default: the network's own setting, 1 unless its weights say)."""
         import torch
         self._sync()
         n = int(np.prod(grid.ncell))
@@ -189,11 +218,17 @@ class UNet:
         box = np.ascontiguousarray(grid.box, dtype=np.float64)
         src = np.ascontiguousarray(np.asarray(grid.sources, dtype=np.float64).reshape(-1, 4))
         nm = np.ascontiguousarray(self.norm if norm is None else norm, dtype=np.float32)
-        check_unet(self._L.cmi_unet_features(self._h, _ptr(nH_cube), dims, box.ctypes.data,
-                                             src.ctypes.data, src.shape[0],
-                                             float(grid.recombination_rate), nm.ctypes.data,
-                                             _ptr(out)))
+        if ratio_factor is None:
+            ratio_factor = self.ratio_factor
+        check_unet(self._L.cmi_unet_features_coarse_ratio(
+            self._h, _ptr(nH_cube), dims, box.ctypes.data, src.ctypes.data, src.shape[0],
+            float(grid.recombination_rate), nm.ctypes.data, int(ratio_factor), _ptr(out)))
         return out
+
+    @property
+    def ratio_factor(self):
+        meta = getattr(self, "meta", {}) or {}
+        return int(meta["ratio_factor"]) if "ratio_factor" in meta else 1
 
     def to_neutral_fraction(self, pred, log10_min=LOG10_XH_MIN):
         import torch
@@ -253,6 +288,40 @@ def stromgren_ratio(grid, nH_cube, nref=1e8):
             nref * nref * hmin * hmin * hmin
         total += s[3] / (4.0 * np.pi * grid.recombination_rate * np.maximum(R, 1e-300))
     return np.log10(np.clip(total, 1e-30, 1e30))
+
+
+def stromgren_ratio_coarse(grid, nH_cube, factor):
+    """Channel 2 as cmi_unet_features_coarse_ratio computes it, for tests: the
+    ray sums of ``stromgren_ratio`` on n_H block-averaged by ``factor``, then
+    trilinear interpolation in log10 (coarse cell centres at fine coordinate
+    (c + 0.5) factor - 0.5, edge values held outside them)."""
+    from .engine import GridSpec
+    n3 = tuple(int(v) for v in grid.ncell)
+    m3 = tuple(v // factor for v in n3)
+    cube = np.asarray(nH_cube, dtype=np.float64).reshape(n3)
+    coarse = cube.reshape(m3[0], factor, m3[1], factor, m3[2], factor).mean(axis=(1, 3, 5))
+    cg = GridSpec(box=grid.box, ncell=m3, num_subgrid=(1, 1, 1),
+                  recombination_rate=grid.recombination_rate,
+                  cross_section=grid.cross_section, sources=list(grid.sources))
+    lr = stromgren_ratio(cg, coarse).reshape(m3).astype(np.float32).astype(np.float64)
+    axes = []
+    for k in range(3):
+        u = np.clip((np.arange(n3[k]) + 0.5) / factor - 0.5, 0.0, m3[k] - 1)
+        lo = np.minimum(np.floor(u).astype(np.int64), m3[k] - 1)
+        axes.append((lo, np.minimum(lo + 1, m3[k] - 1), u - lo))
+    out = np.zeros(n3)
+    for c in range(8):
+        idx, w = [], 1.0
+        for k, bit in enumerate((4, 2, 1)):
+            lo, hi, t = axes[k]
+            sel = hi if c & bit else lo
+            wk = t if c & bit else 1.0 - t
+            shape = [1, 1, 1]
+            shape[k] = n3[k]
+            idx.append(sel.reshape(shape))
+            w = w * wk.reshape(shape)
+        out += w * lr[idx[0], idx[1], idx[2]]
+    return out
 
 
 def flux_proxy(grid):
@@ -369,6 +438,81 @@ def train(net, feats, labels, ncell, epochs=10, batch=8, lr=2e-3, lr_final=2e-4,
         if log:
             log(f"epoch {ep}: loss {history[-1]:.5f} ({time.perf_counter() - t0:.1f} s)")
     return history
+
+
+def generate_large_runs(net, seeds, iterations=24, average=6, ratio_factor=4, device=0,
+                        log=None):
+    """Runs of the large generator (256^3 as 16^3 subgrids of 16^3, sigma_ln =
+    1.5, 16 sources, 1e8 packets per iteration; problems.large_config), kept on
+    the device: raw features [N, cells, 3] (channel 2 from the grid coarser by
+    ``ratio_factor``) and labels log10 x_H [N, cells] of the long plain run
+    (``iterations`` from x_H = 1e-6, the last ``average`` averaged)."""
+    import torch
+    from .engine import blocked_to_cube
+    from .problems import large_config
+    raw = np.array([0.0, 1.0] * NUM_FEATURES, dtype=np.float32)
+    feats, labels, grids = None, None, []
+    t0 = time.perf_counter()
+    for i, sd in enumerate(seeds):
+        g, nH = large_config(seed=int(sd))
+        ncell = int(np.prod(g.ncell))
+        if feats is None:
+            feats = torch.empty((len(seeds), ncell, NUM_FEATURES), dtype=torch.float32,
+                                device=f"cuda:{device}")
+            labels = torch.empty((len(seeds), ncell), dtype=torch.float32, device=feats.device)
+        x = reference_field(g, nH, iterations=iterations, average=average, seed=7000 + i,
+                            device=device)
+        labels[i] = torch.from_numpy(np.log10(np.maximum(x, 10.0 ** LOG10_XH_MIN))
+                                     .astype(np.float32)).to(feats.device)
+        cube = torch.from_numpy(blocked_to_cube(nH, g.ncell, g.num_subgrid)).to(feats.device)
+        net.features(cube, g, out=feats[i], norm=raw, ratio_factor=ratio_factor)
+        grids.append(g)
+        if log and (i % 8 == 7 or i == len(seeds) - 1):
+            log(f"large runs {i + 1}/{len(seeds)}: {time.perf_counter() - t0:.1f} s")
+    return grids, feats, labels
+
+
+def random_crops(feats, labels, ncell, crop, batch, rng):
+    """``batch`` random crop^3 windows of random runs: features [batch, crop^3,
+    3] and labels [batch, crop^3], contiguous (the network's zero padding sees
+    the window edge; the features already carry the whole grid's sources)."""
+    import torch
+    n0, n1, n2 = ncell
+    f = feats.view(feats.shape[0], n0, n1, n2, NUM_FEATURES)
+    t = labels.view(labels.shape[0], n0, n1, n2)
+    fo, to = [], []
+    for _ in range(batch):
+        r = int(rng.integers(feats.shape[0]))
+        z, y, x = (int(rng.integers(n - crop + 1)) for n in ncell)
+        fo.append(f[r, z:z + crop, y:y + crop, x:x + crop])
+        to.append(t[r, z:z + crop, y:y + crop, x:x + crop])
+    return (torch.stack(fo).reshape(batch, -1, NUM_FEATURES).contiguous(),
+            torch.stack(to).reshape(batch, -1).contiguous())
+
+
+def train_crops(net, feats, labels, ncell, steps=3000, crop=64, batch=8, lr=1e-3,
+                lr_final=1e-4, seed=0, log=None):
+    """Adam on random crop^3 windows of the large runs (normalised features),
+    learning rate decaying geometrically from lr to lr_final."""
+    rng = np.random.default_rng(seed)
+    hist, acc = [], []
+    t0 = time.perf_counter()
+    for k in range(steps):
+        f, t = random_crops(feats, labels, ncell, crop, batch, rng)
+        rate = lr * (lr_final / lr) ** (k / max(1, steps - 1))
+        acc.append(net.train_step(f, t, (crop,) * 3, rate))
+        if (k + 1) % 250 == 0:
+            hist.append(float(np.mean(acc)))
+            acc = []
+            if log:
+                log(f"step {k + 1}: loss {hist[-1]:.5f} ({time.perf_counter() - t0:.1f} s)")
+    return hist
+
+
+def normalise_features(feats, norm):
+    """In place: (raw - norm[2k]) / norm[2k + 1] per channel."""
+    for k in range(NUM_FEATURES):
+        feats[..., k].sub_(float(norm[2 * k])).div_(float(norm[2 * k + 1]))
 
 
 def evaluate_loss(net, feats, labels, ncell, batch=8):
@@ -565,6 +709,37 @@ def time_steps(steps, batch=8, ncell=64, log=print, warmup=3):
     return 0
 
 
+def train_large(runs, steps, over_weight, out, log, ratio_factor=4, crop=64, batch=8,
+                label_iterations=16, label_average=4):
+    """The 256^3 weights: ``runs`` long plain runs of large_config (seeds
+    300000 + i, the last sixth held out), features with channel 2 from the
+    grid coarser by ``ratio_factor``, the 64^3 weights (and normalisation)
+    fine-tuned on random crop^3 windows under the asymmetric loss."""
+    ntrain = runs - max(1, runs // 6)
+    seeds = [300_000 + i for i in range(runs)]
+    net = UNet.load(DEFAULT_WEIGHTS)
+    grids, feats, labels = generate_large_runs(net, seeds, iterations=label_iterations,
+                                               average=label_average,
+                                               ratio_factor=ratio_factor, log=log)
+    normalise_features(feats, net.norm)
+    ncell = grids[0].ncell
+    base = float(((labels[ntrain:] - labels[:ntrain].mean(0)) ** 2).mean())
+    net.set_loss_weight(over_weight)
+    hist = train_crops(net, feats[:ntrain], labels[:ntrain], ncell, steps=steps, crop=crop,
+                       batch=batch, log=log)
+    net.set_loss_weight(1.0)
+    val = evaluate_loss(net, feats[ntrain:], labels[ntrain:], ncell, batch=1)
+    log(f"held-out MSE {val:.4f} (mean-field baseline {base:.4f})")
+    net.save(out, ncell=int(ncell[0]), ratio_factor=ratio_factor, val_mse=val,
+             baseline_mse=base, over_weight=over_weight, train_loss=np.array(hist),
+             generator="large_config: 256^3, sigma_ln=1.5, 16 sources, 1e8 packets",
+             train_seeds=np.array([seeds[0], seeds[ntrain]]),
+             val_seeds=np.array([seeds[ntrain], seeds[-1] + 1]), steps=steps, crop=crop,
+             batch=batch, label_iterations=label_iterations, label_average=label_average,
+             init=os.path.basename(DEFAULT_WEIGHTS), lr=np.array([1e-3, 1e-4]))
+    return 0
+
+
 def main(argv=None):
     import argparse
     import json
@@ -585,11 +760,20 @@ def main(argv=None):
     ap.add_argument("--time-steps", type=int, default=0,
                     help="only time this many training steps and inference passes on "
                          "synthetic 64^3 data (batch --batch) and exit")
+    ap.add_argument("--large", action="store_true",
+                    help="fine-tune the 64^3 weights on the 256^3 generator instead "
+                         "(--runs long runs, 1/6 held out; writes the 256^3 weights)")
+    ap.add_argument("--steps", type=int, default=6000, help="--large: training steps")
+    ap.add_argument("--over-weight", type=float, default=16.0,
+                    help="--large: loss weight of predictions above the target")
     a = ap.parse_args(argv)
     log = (lambda s: print(s, flush=True))
     torch.cuda.set_device(0)
     if a.time_steps:
         return time_steps(a.time_steps, a.batch, a.ncell, log)
+    if a.large:
+        return train_large(a.runs, a.steps, a.over_weight,
+                           LARGE_WEIGHTS if a.out == DEFAULT_WEIGHTS else a.out, log)
     ntrain = int(round(0.8 * a.runs))
     seeds = [100_000 + i for i in range(a.runs)]
     t0 = time.perf_counter()

@@ -13,7 +13,8 @@ import pytest
 from oracle import unet_oracle as U
 from parallelcmacionize_b200 import _lib
 from parallelcmacionize_b200.problems import lognormal_config
-from parallelcmacionize_b200.warmstart import UNet, flux_proxy, stromgren_ratio
+from parallelcmacionize_b200.warmstart import (UNet, flux_proxy, stromgren_ratio,
+                                               stromgren_ratio_coarse)
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -118,7 +119,8 @@ def test_conv3_weight_gradient_matches_oracle(net):
     np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-3)
 
 
-def test_network_gradients_match_oracle(net):
+@pytest.mark.parametrize("over_weight", [1.0, 3.0])
+def test_network_gradients_match_oracle(net, over_weight):
     rng = np.random.default_rng(7)
     shape = (2, 32, 32, 32)
     feats = rng.normal(size=shape + (3,)).astype(np.float32)
@@ -128,9 +130,11 @@ def test_network_gradients_match_oracle(net):
     net.set_params(p)
     f = torch.from_numpy(feats.reshape(2, -1, 3)).cuda()
     t = torch.from_numpy(target.reshape(2, -1)).cuda()
+    net.set_loss_weight(over_weight)
     loss, g = net.gradients(f, t, (32, 32, 32))
+    net.set_loss_weight(1.0)
     o = U.UNetOracle(p.astype(np.float64), bf16=True)
-    oloss, og = o.gradients(feats.astype(np.float64), target.astype(np.float64))
+    oloss, og = o.gradients(feats.astype(np.float64), target.astype(np.float64), over_weight)
     assert abs(loss - oloss) <= 1e-3 * oloss
     # per tensor: relative L2 error and direction (BF16 activations and
     # gradients: ~1% relative)
@@ -165,6 +169,27 @@ def test_features_match_host():
     # the ray sums use explicitly rounded FP64 on both sides: same sample cells
     np.testing.assert_allclose(f[:, 2], (stromgren_ratio(spec, cube).ravel() - 1.0) / 3.0,
                                rtol=1e-5, atol=1e-5)
+
+
+def test_features_with_coarse_ratio_match_host():
+    """Channel 2 on the grid coarser by 2 (n_H block-averaged), interpolated:
+    the host restatement with the same FP32 sums; channels 0-1 unchanged."""
+    spec, nH = lognormal_config(ncell=32, num_subgrid=2, num_photon=1000, num_sources=3)
+    from parallelcmacionize_b200 import blocked_to_cube
+    cube = blocked_to_cube(nH, spec.ncell, spec.num_subgrid)
+    norm = np.array([8.0, 0.5, 12.0, 2.0, 1.0, 3.0], np.float32)
+    with UNet() as n:
+        n.norm = norm
+        d = torch.from_numpy(cube.ravel().copy()).cuda()
+        full = n.features(d, spec).cpu().numpy()
+        f = n.features(d, spec, ratio_factor=2).cpu().numpy()
+        with pytest.raises(_lib.CMIError):
+            n.features(d, spec, ratio_factor=3)  # 32 is not a multiple of 3
+    np.testing.assert_array_equal(f[:, :2], full[:, :2])
+    ref = (stromgren_ratio_coarse(spec, cube, 2).ravel() - 1.0) / 3.0
+    np.testing.assert_allclose(f[:, 2], ref, rtol=1e-5, atol=1e-5)
+    # the coarse channel tracks the full march (smooth along the rays)
+    assert np.corrcoef(f[:, 2], full[:, 2])[0, 1] > 0.98
 
 
 def test_training_reduces_loss():

@@ -52,8 +52,8 @@ def test_parameter_count():
     assert convs[6][0].shape == (24, 27, 72) and hw.shape == (12,)
 
 
-@pytest.mark.parametrize("seed", [0, 1])
-def test_oracle_gradient_matches_finite_differences(seed):
+@pytest.mark.parametrize("seed,over_weight", [(0, 1.0), (1, 1.0), (2, 4.0)])
+def test_oracle_gradient_matches_finite_differences(seed, over_weight):
     c = (3, 4, 5)
     rng = np.random.default_rng(seed)
     p = U.init_params(*c, seed=seed)
@@ -61,14 +61,14 @@ def test_oracle_gradient_matches_finite_differences(seed):
     feats = rng.normal(size=(2, 8, 8, 8, 3))
     target = rng.normal(size=(2, 8, 8, 8))
     net = U.UNetOracle(p, *c)
-    loss, g = net.gradients(feats, target)
-    assert np.isclose(loss, net.loss(feats, target))
+    loss, g = net.gradients(feats, target, over_weight)
+    assert np.isclose(loss, net.loss(feats, target, over_weight))
     idx = rng.choice(p.size, 60, replace=False)
     eps = 1e-6
     for i in idx:
         pp, pm = p.copy(), p.copy()
         pp[i] += eps
         pm[i] -= eps
-        fd = (U.UNetOracle(pp, *c).loss(feats, target) -
-              U.UNetOracle(pm, *c).loss(feats, target)) / (2 * eps)
+        fd = (U.UNetOracle(pp, *c).loss(feats, target, over_weight) -
+              U.UNetOracle(pm, *c).loss(feats, target, over_weight)) / (2 * eps)
         assert abs(fd - g[i]) <= 1e-5 * max(abs(fd), 1e-3), (i, fd, g[i])

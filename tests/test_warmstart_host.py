@@ -40,3 +40,21 @@ def test_run_configs_shapes():
     assert nH.shape == (32 ** 3,) and np.all(nH > 0)
     # seeds differ
     assert not np.array_equal(nH, cfgs[1][1])
+
+
+def test_weights_selection_and_large_weights_metadata():
+    from parallelcmacionize_b200 import GridSpec
+    from parallelcmacionize_b200.problems import BOX_10PC
+    from parallelcmacionize_b200.warmstart import DEFAULT_WEIGHTS, LARGE_WEIGHTS, weights_for
+
+    def grid(n):
+        return GridSpec(box=BOX_10PC, ncell=(n,) * 3, num_subgrid=(n // 16,) * 3)
+    assert weights_for(grid(256)) == LARGE_WEIGHTS
+    assert weights_for(grid(64)) == DEFAULT_WEIGHTS
+    assert weights_for(grid(128)) == DEFAULT_WEIGHTS  # predicted on the 64^3 block mean
+    d = np.load(LARGE_WEIGHTS)
+    assert int(d["ncell"]) == 256 and int(d["ratio_factor"]) == 4
+    assert d["params"].size == 199_513 and float(d["over_weight"]) > 1
+    # trained and validated on seeds away from the bench's and the tests' (7, 8)
+    assert int(d["train_seeds"][0]) >= 300_000 and int(d["val_seeds"][0]) >= 300_000
+    assert float(d["val_mse"]) < 0.25 * float(d["baseline_mse"])
