@@ -1022,6 +1022,10 @@ __global__ void __launch_bounds__(kThreads) k_walk64(WalkParams prm) {
 // it never holds more than kStageFlush - 1 + 32
 constexpr int kStage = 48;
 constexpr uint32_t kStageFlush = 16;
+// crossings per lane between warp-level batch tests (swept on B200: 1 -> 7.5e10,
+// 2 -> 8.3e10, 4 -> 8.7e10, 8 -> 9.0e10, 12 -> 8.4e10 crossings/s on the 128^3
+// log-normal workload)
+constexpr int kStepsPerCheck = 8;
 
 // kReemit: the build with reemission (any instance with p > 0); without it
 // the absorbed-packet path carries no reemission code.
@@ -1337,6 +1341,15 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
           float len;
           int status = w.step(v, tcell, len);
           tally.add(tcell, len);
+          // up to kStepsPerCheck crossings per lane between two looks at the
+          // warp (ballot, batch test, reconvergence), which cost more than the
+          // idle lanes the longer stretch leaves
+#pragma unroll
+          for (int u = 1; u < kStepsPerCheck; ++u) {
+            if (status != kRun) break;
+            status = w.step(v, tcell, len);
+            tally.add(tcell, len);
+          }
           if (status == kRun && w.steps > limit) status = kDrop;
           if (status != kRun) {
             active = false;
