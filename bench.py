@@ -63,12 +63,16 @@ DESCRIPTIONS = {
                  "16 sources, {packets:.0e} packets/iteration"),
 }
 DEFAULT_PACKETS = {"lognormal128": 1e7, "stromgren64": 1e6, "large256": 1e8}
+# timed iterations of a run without --steps: about a second of device time on
+# a B200, so that the clock samples (every 100 ms) fall inside the timed region
+DEFAULT_STEPS = {"lognormal128": 400, "stromgren64": 1000, "batch64": 20, "large256": 20}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=0,
+                    help="timed iterations (0: about a second of device time for the workload)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(DESCRIPTIONS), default="lognormal128")
@@ -85,7 +89,11 @@ def parse():
     ap.add_argument("--warm-start-seeds", type=int, default=4)
     ap.add_argument("--no-fp64-check", action="store_true",
                     help="skip the FP32-vs-FP64 mean-intensity comparison (large256 only)")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.steps <= 0:
+        # the reference arm times host cores: a few bounded iterations
+        a.steps = 5 if a.impl == "reference" else DEFAULT_STEPS[a.workload]
+    return a
 
 
 WARM_WORKLOADS = {
@@ -214,13 +222,14 @@ def workload(args, rank=0, world=1):
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
+        self.window = None  # (start, end) of the timed region, host clock
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
 
     def __enter__(self):
@@ -229,11 +238,23 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # wait (at most 3 s) for the first sample, so sampling covers the region
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
         return self
+
+    def start(self):
+        self.window = [time.time(), None]
+
+    def stop(self):
+        if self.window is not None:
+            self.window[1] = time.time()
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -247,24 +268,30 @@ class ClockSampler:
     def summary(self):
         if self.proc is None or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        import datetime
+        rows = []
         for line in open(self.path):
             f = [v.strip() for v in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                t = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((t, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        # samples inside the timed region (nvidia-smi prints local time)
+        if self.window and self.window[1] is not None:
+            inside = [r for r in rows if self.window[0] <= r[0] <= self.window[1] + 0.05]
+        else:
+            inside = rows
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None,
+                    "reasons": ["no samples inside the timed region"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {n for r in inside for n, v in zip(names, r[3]) if v.lower().startswith("active")}
+        return {"sm_mhz": statistics.median(r[1] for r in inside),
+                "sm_max_mhz": max(r[2] for r in inside), "reasons": sorted(reasons),
+                "samples": len(inside)}
 
 
 def measured_peak_hbm():
@@ -396,10 +423,12 @@ def ours(args):
     runner.barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        clocks.start()
         start.record(stream)
         stats = runner.run(args.steps, seed=42)
         stop.record(stream)
         stop.synchronize()
+        clocks.stop()
     torch.cuda.synchronize()
     ms_local = start.elapsed_time(stop)
     ms = runner.max_over_ranks(ms_local)
@@ -437,10 +466,12 @@ def ours(args):
     # ---- end to end through the public API with host buffers ----
     e2e = None
     if not args.no_e2e:
+        # the host owns n_H and x_H in pinned memory, as a hydro code owns its
+        # grid: every step sends both and reads x_H back into the same array,
+        # which the next step sends again
         pin_n = [torch.from_numpy(n.copy()).pin_memory() for n in wl.fields]
         pin_x = [torch.from_numpy(eng.get_fields(i, intensity=False)[0]).pin_memory()
                  for i in range(len(wl.fields))]
-        out_x = [torch.empty(n.size, dtype=torch.float64).pin_memory() for n in wl.fields]
         ncells = sum(n.size for n in wl.fields)
         runner.barrier()
         t0 = time.perf_counter()
@@ -451,8 +482,7 @@ def ours(args):
             st = runner.run(1, seed=1000 + k)
             e2e_cross += sum(s["cell_crossings"] for s in st)
             for i in range(len(wl.fields)):
-                eng.get_fields(i, intensity=False, out_x=out_x[i].numpy())
-                pin_x[i].copy_(out_x[i])
+                eng.get_fields(i, intensity=False, out_x=pin_x[i].numpy())
         e2e_s = runner.max_over_ranks(time.perf_counter() - t0)
         e2e_cross = runner.sum_over_ranks(e2e_cross)
         e2e = {"value": e2e_cross / e2e_s, "unit": UNIT,
