@@ -18,6 +18,8 @@
 #define CMACIONIZE_DENSITYGRID_HPP
 
 #include <cstdint>
+#include <fstream>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -102,6 +104,7 @@ class DensityGrid {
   double *host_nH() { pull(); _fields_dirty = true; return _nH.data(); }
   double *host_xH() { pull(); _fields_dirty = true; return _xH.data(); }
   const double *neutral_fractions() { pull(); return _xH.data(); }
+  const double *number_densities() const { return _nH.data(); }
   const double *intensity_integrals() { pull(); return _J.data(); }
 
   // ---- sources and the whole iteration ----
@@ -249,9 +252,61 @@ class DensitySubGrid {
     _grid->mark_device_changed();
   }
 
+  // Result-file records (DensitySubGrid.hpp:1738-1796, NO_HYDRO build): per
+  // cell in index order the centre x, y, z, x_H and n_H as FP64, then five
+  // zero 4-byte hydro slots; 60 bytes per cell.
+  size_t get_output_size() const { return get_number_of_cells() * (5 * sizeof(double) + 20); }
+  void output_intensities(std::ostream &stream) {
+    double box[6];
+    get_grid_box(box);
+    const int *n = _grid->subgrid_cells();
+    double cs[3];
+    for (int a = 0; a < 3; ++a) cs[a] = box[3 + a] / n[a];
+    const double *x = _grid->neutral_fractions() + offset();
+    const double *nh = _grid->number_densities() + offset();
+    const char zeros[20] = {0};
+    for (int ix = 0; ix < n[0]; ++ix) {
+      const double px = box[0] + (ix + 0.5) * cs[0];
+      for (int iy = 0; iy < n[1]; ++iy) {
+        const double py = box[1] + (iy + 0.5) * cs[1];
+        for (int iz = 0; iz < n[2]; ++iz) {
+          const double pz = box[2] + (iz + 0.5) * cs[2];
+          const size_t c = (size_t)(ix * n[1] + iy) * n[2] + iz;
+          const double rec[5] = {px, py, pz, x[c], nh[c]};
+          stream.write(reinterpret_cast<const char *>(rec), sizeof(rec));
+          stream.write(zeros, sizeof(zeros));
+        }
+      }
+    }
+  }
+
   unsigned int index() const { return _index; }
   DensityGrid *grid() { return _grid; }
 };
+
+// The reference driver's result files (testDensitySubGrid_omp.cpp:394-521):
+// neutral_fractions.dat (the records above, subgrid after subgrid) and
+// neutral_fractions.bin (x_H as FP64 in the same order).  Return the bytes
+// written.
+inline size_t output_neutral_fractions(DensityGrid &grid, const char *path) {
+  std::ofstream out(path, std::ios::binary);
+  size_t size = 0;
+  for (unsigned int s = 0; s < grid.number_of_subgrids(); ++s) {
+    DensitySubGrid sg = grid.subgrid(s);
+    sg.output_intensities(out);
+    size += sg.get_output_size();
+  }
+  if (!out) throw std::runtime_error(std::string("cannot write ") + path);
+  return size;
+}
+
+inline size_t output_neutral_fractions_binary(DensityGrid &grid, const char *path) {
+  std::ofstream out(path, std::ios::binary);
+  const size_t n = grid.cells_per_subgrid() * grid.number_of_subgrids();
+  out.write(reinterpret_cast<const char *>(grid.neutral_fractions()), sizeof(double) * n);
+  if (!out) throw std::runtime_error(std::string("cannot write ") + path);
+  return sizeof(double) * n;
+}
 
 inline DensitySubGrid DensityGrid::subgrid(unsigned int index) {
   if (index >= number_of_subgrids()) throw std::runtime_error("subgrid index out of range");

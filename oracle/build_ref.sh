@@ -6,6 +6,9 @@
 #                      (timed CPU baseline for generated inputs)
 #   testDensitySubGrid_omp  the reference's own OpenMP driver, compile_omp.sh
 #                      flags plus -DMEANING_OF_HASTE (timed CPU baseline, C1)
+#   testDensitySubGrid_omp_files  the same driver with its result files
+#                      switched on (-DMM_FILE -DBIN_FILE: neutral_fractions.dat
+#                      and .bin), no fast-math (golden output files)
 # Deviations from compile_omp.sh, all needed to build on this image:
 #   -march=x86-64-v3 instead of -march=native (the binary runs on another host),
 #   -include cstdint (CommandLineOption.hpp uses int_fast32_t without it),
@@ -37,5 +40,12 @@ for f in testDensitySubGrid_omp.cpp CommandLineOption.cpp CommandLineParser.cpp;
     2> "$TMP/${f%.cpp}.log" || { cat "$TMP/${f%.cpp}.log" >&2; exit 1; }
 done
 $CXX -fopenmp -o "$OUT/testDensitySubGrid_omp" "$TMP"/*.o
+rm -f "$TMP"/*.o
+for f in testDensitySubGrid_omp.cpp CommandLineOption.cpp CommandLineParser.cpp; do
+  $CXX -std=c++11 -fopenmp -Wall -Wno-catch-value -O2 -ffp-contract=off -fno-fast-math \
+    -DMM_FILE -DBIN_FILE -include cstdint -I"$HERE/hdf5_stub" -I"$REF_DIR" \
+    -c "$REF_DIR/$f" -o "$TMP/${f%.cpp}.o" 2> "$TMP/${f%.cpp}.log" || { cat "$TMP/${f%.cpp}.log" >&2; exit 1; }
+done
+$CXX -fopenmp -o "$OUT/testDensitySubGrid_omp_files" "$TMP"/*.o
 rm -rf "$TMP"
 echo "built: $(ls "$OUT" | tr '\n' ' ')"

@@ -7,8 +7,10 @@
 // (random_generator[0] seeded 42 + THREADS, testDensitySubGrid_omp.cpp:1786-1790),
 // so a random density field and random sources come out identical to a
 // reference run with the same -t.  The transport and balance run on the GPU.
-// Output: neutral_fractions.bin, the neutral fraction of every cell, subgrid
-// after subgrid (output_neutral_fractions_binary, testDensitySubGrid_omp.cpp:507-521).
+// Output: the reference's two result files, subgrid after subgrid:
+// neutral_fractions.dat (cell centre, x_H, n_H and zero hydro slots, 60 bytes
+// per cell; output_neutral_fractions, testDensitySubGrid_omp.cpp:394-442) and
+// neutral_fractions.bin (x_H only; output_neutral_fractions_binary, :507-521).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -99,10 +101,9 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "Total Monte Carlo time: %g s.\n", mc);
     std::fprintf(stderr, "Cell crossings: %llu (%.4g per second)\n", crossings, crossings / mc);
 
-    const double *x = grid.neutral_fractions();
-    std::ofstream out("neutral_fractions.bin", std::ios::binary);
-    out.write(reinterpret_cast<const char *>(x),
-              sizeof(double) * grid.cells_per_subgrid() * grid.number_of_subgrids());
+    // the reference's result files (MM_FILE and BIN_FILE outputs)
+    output_neutral_fractions(grid, "neutral_fractions.dat");
+    output_neutral_fractions_binary(grid, "neutral_fractions.bin");
   } catch (const std::exception &e) {
     std::fprintf(stderr, "error: %s\n", e.what());
     return 1;

@@ -15,6 +15,10 @@ inputs and stores inputs + reference outputs as compressed .npz files:
   transport.npz    interact + neighbour routing through a lattice of subgrids
   stromgren_ensemble.npz  64^3 Stromgren runs (reference code, 8 seeds):
                    radial x_H profiles and ionized radii
+  outputs.npz      the result files of the reference's own driver
+                   (oracle/_ref/testDensitySubGrid_omp_files, -DMM_FILE
+                   -DBIN_FILE): neutral_fractions.dat and .bin of a small
+                   non-cubic run, one thread (files written in subgrid order)
 
 Usage: python tests/golden/make_golden.py [--skip-ensemble]
 """
@@ -261,10 +265,52 @@ def gen_ensemble(seeds=8, packets=1_000_000, iterations=10):
          radii=np.array(radii), packets=packets, iterations=iterations)
 
 
+OUTPUT_CASE = {"ncell": (16, 16, 8), "num_subgrid": (2, 2, 1),
+               "anchor_pc": (-5.0, -4.0, -3.0), "sides_pc": (10.0, 8.0, 6.0),
+               "num_photon": 20000, "iterations": 2}
+
+
+def gen_outputs():
+    """Runs the reference driver with its file output switched on in a
+    temporary directory (params written here: the keys of
+    params_single_uniform.txt) and stores both files byte for byte."""
+    import subprocess
+    import tempfile
+    b = O.ref_binary("testDensitySubGrid_omp_files")
+    if b is None:
+        sys.exit("oracle/_ref/testDensitySubGrid_omp_files missing: run oracle/build_ref.sh")
+    c = OUTPUT_CASE
+    v = lambda t: "[" + ", ".join(str(int(x)) for x in t) + "]"
+    pcs = lambda t: "[" + ", ".join(f"{x} pc" for x in t) + "]"
+    params = "\n".join([
+        "box:", f"  anchor: {pcs(c['anchor_pc'])}", f"  sides: {pcs(c['sides_pc'])}",
+        f"ncell: {v(c['ncell'])}", f"num_photon: {c['num_photon']}",
+        f"number_of_iterations: {c['iterations']}", "reemission_probability: 0.",
+        "number_of_sources: 1", "random_density: false", f"num_subgrid: {v(c['num_subgrid'])}",
+        "queue_size_per_thread: 100", "memoryspace_size: 50000", "number_of_tasks: 500000",
+        "MPI_buffer_size: 1000", "cost_copy_factor: 10", "edge_copy_factor: 0.01",
+        "general_queue_size: 100000", ""])
+    with tempfile.TemporaryDirectory() as td:
+        with open(os.path.join(td, "params.txt"), "w") as f:
+            f.write(params)
+        subprocess.run([b, "-p", "params.txt", "-t", "1"], cwd=td, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        dat = np.fromfile(os.path.join(td, "neutral_fractions.dat"), dtype=np.uint8)
+        binf = np.fromfile(os.path.join(td, "neutral_fractions.bin"), dtype=np.float64)
+    save("outputs.npz", dat=dat, bin=binf, ncell=np.array(c["ncell"]),
+         num_subgrid=np.array(c["num_subgrid"]), anchor_pc=np.array(c["anchor_pc"]),
+         sides_pc=np.array(c["sides_pc"]))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-ensemble", action="store_true")
+    ap.add_argument("--only-outputs", action="store_true",
+                    help="regenerate outputs.npz only")
     args = ap.parse_args()
+    if args.only_outputs:
+        gen_outputs()
+        return
     if O.ref_binary() is None:
         sys.exit("oracle/_ref/ref_harness_exact missing: run oracle/build_ref.sh first")
     gen_directions()
@@ -273,6 +319,7 @@ def main():
     gen_walks()
     gen_balance()
     gen_transport()
+    gen_outputs()
     if not args.skip_ensemble:
         gen_ensemble()
 

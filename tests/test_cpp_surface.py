@@ -89,3 +89,10 @@ def test_stromgren_driver_runs(tmp_path):
     R = ionized_radius(blocked_to_cube(x, spec.ncell, spec.num_subgrid), spec)
     _, _, Rs = stromgren_profile()
     assert abs(R / Rs - 1) < 0.05  # coarse 32^3 grid
+    # the .dat file: the same x_H, n_H = 1e8 (uniform params), and the
+    # reference's record layout and cell centres (Python writer, pinned to
+    # the reference's own files in tests/test_outputs.py)
+    from parallelcmacionize_b200.outputs import neutral_fractions_dat
+    dat = np.fromfile(tmp_path / "neutral_fractions.dat", dtype=np.uint8)
+    ref = neutral_fractions_dat(spec, x, np.full(x.size, 1e8))
+    assert np.array_equal(dat, ref.view(np.uint8))

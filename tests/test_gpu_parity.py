@@ -424,3 +424,24 @@ def test_invalid_arguments():
     with pytest.raises(CMIError):
         TransportEngine(GridSpec(box=(0, 0, 0, 1, 1, 1), ncell=(10, 8, 8), num_subgrid=(3, 2, 2)))
     eng.close()
+
+
+def test_result_files_from_the_engine(tmp_path):
+    """write_outputs: the engine's x_H in the reference's .bin and .dat files,
+    read back unchanged; the radial profile of a Stromgren run drops across R_S."""
+    import os
+    from parallelcmacionize_b200.outputs import (radial_profile, read_neutral_fractions_binary,
+                                                  read_neutral_fractions_dat, write_outputs)
+    spec, nH = stromgren(ncell=32, num_subgrid=4, num_photon=200_000)
+    eng = TransportEngine(spec)
+    eng.set_fields(0, nH)
+    eng.run_iterations(6, seed=3)
+    x, _ = eng.get_fields(0, intensity=False)
+    paths = write_outputs(eng, 0, prefix=os.path.join(tmp_path, "nf"), nH_blocked=nH)
+    eng.close()
+    assert np.array_equal(read_neutral_fractions_binary(paths["bin"]), x)
+    rec = read_neutral_fractions_dat(paths["dat"])
+    assert np.array_equal(rec["xH"], x) and np.array_equal(rec["nH"], nH)
+    _, _, Rs = stromgren_profile()
+    r, prof = radial_profile(rec, bins=16, r_max=1.5 * Rs)
+    assert np.nanmax(prof[r < 0.7 * Rs]) < 0.1 and np.nanmin(prof[r > 1.3 * Rs]) > 0.5
