@@ -298,6 +298,43 @@ int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
                                 uint32_t *d_out_count, uint32_t *d_num_done, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Dust scattering with forced first scattering and a peel-off image: the
+ * photon loop of the reference's dust driver (testDensitySubGrid_omp_dust.cpp:
+ * fill_buffer :564-620 with FORCED_SCATTERING, execute_relaunch_photon_task
+ * :1200-1260, do_photon_traversal :621-722, do_reemission :730-760,
+ * execute_photon_reemit_task :1484-1560) on an instance's current n_H, x_H:
+ *   - num_photon packets leave `source` isotropically (weight 1, cross
+ *     section 1) and add up the optical depth tau0 to the box edge
+ *     (DensitySubGrid::compute_optical_depth, DensitySubGrid.hpp:1482-1604);
+ *   - each restarts at the source with weight 1 - exp(-tau0) and target depth
+ *     -ln(1 - u (1 - exp(-tau0))) and walks to it without tallies
+ *     (DensitySubGrid::propagate, DensitySubGrid.hpp:1333-1472);
+ *   - an absorbed packet scatters with probability `albedo` (the driver's
+ *     reemission_probability): isotropic direction, target -ln u, weight / 4pi;
+ *     a copy of it walks along +z to the box edge and adds weight * exp(-depth)
+ *     to the pixel under its exit point (npix_x columns over the box's x
+ *     side, npix_y rows over its y side; pixel (ix, iy) at image[ix * npix_y +
+ *     iy]); repeated until no packet is left.
+ * `image` (host, npix_x * npix_y) receives the sums divided by num_photon, as
+ * the driver writes image.dat.  FP64 throughout, the reference's walk
+ * arithmetic; counter-based draws (seed, iteration) replace the reference's
+ * per-thread generators.  albedo in [0, 1); num_photon <= 2^30. */
+typedef struct cmi_dust_stats {
+  uint64_t emitted;            /* source packets */
+  uint64_t scatterings;        /* scattered packets (= peel-off packets) */
+  uint64_t absorbed;           /* absorbed and not scattered */
+  uint64_t escaped;            /* relaunched or scattered packets that left the box */
+  uint64_t cell_crossings;     /* every walk: TAU, DIRECT and PEELOFF */
+  uint64_t subgrid_transits;
+  uint64_t peeloffs_off_image; /* peel-offs whose exit point is off the image */
+  uint32_t generations;        /* walk + scatter rounds run */
+  uint32_t error_flags;
+} cmi_dust_stats;
+int cmi_dust_run(cmi_context *ctx, int32_t instance, uint64_t num_photon, uint64_t seed,
+                 uint32_t iteration, double albedo, const double source[3], int32_t npix_x,
+                 int32_t npix_y, double *image, cmi_dust_stats *stats);
+
+/* ---------------------------------------------------------------------------
  * Learned warm start.  No reference counterpart: the reference starts every
  * run from x_H = 1e-6 (DensitySubGrid.hpp:544-551).  A 3-level 3D
  * convolutional U-Net maps three input channels per cell (cmi_unet_features:

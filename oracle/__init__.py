@@ -107,6 +107,16 @@ class Counts(C.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
+class DustStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("emitted", "scatterings", "absorbed", "escaped",
+                                          "cell_crossings", "subgrid_transits",
+                                          "peeloffs_off_image")] + \
+               [("generations", C.c_uint32), ("error_flags", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 def _ptr(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
@@ -163,6 +173,13 @@ def lib():
         L.cmio_kappa32.argtypes = [i64, pd, pd, d, pf]
         L.cmio_iteration_omp.argtypes = [C.POINTER(Lattice), pd, pd, pd, pd, i32, pd, pd, u64,
                                          u64, u32, d, d, C.c_int, C.c_int, C.POINTER(Counts)]
+        L.cmio_propagate.argtypes = [C.POINTER(Subgrid), pd, pd, C.c_void_p, C.c_int, pi32]
+        L.cmio_compute_optical_depth.argtypes = [C.POINTER(Subgrid), pd, pd, C.c_void_p,
+                                                 C.c_int, pi32]
+        L.cmio_dust_exp.argtypes = [d]
+        L.cmio_dust_exp.restype = d
+        L.cmio_dust_run.argtypes = [C.POINTER(Lattice), pd, pd, pd, u32, u64, u32, u32, d, pd,
+                                    u32, i32, i32, pd, C.POINTER(DustStats)]
         _lib = L
     return _lib
 
@@ -223,6 +240,27 @@ def interact(sg: Subgrid, nH, xH, J, photon, input_direction: int, max_steps: in
         _ptr(lengths, C.c_double) if max_steps else None, max_steps, C.byref(nsteps))
     n = min(nsteps.value, max_steps)
     return res, cells[:n].copy(), lengths[:n].copy(), nsteps.value
+
+
+def propagate(sg: Subgrid, nH, xH, photon, input_direction: int):
+    """DensitySubGrid::propagate on one photon (modified in place): (result, steps)."""
+    nsteps = C.c_int32(0)
+    res = lib().cmio_propagate(C.byref(sg), _ptr(nH, C.c_double), _ptr(xH, C.c_double),
+                               photon.ctypes.data, input_direction, C.byref(nsteps))
+    return res, nsteps.value
+
+
+def compute_optical_depth(sg: Subgrid, nH, xH, photon, input_direction: int):
+    """DensitySubGrid::compute_optical_depth on one photon (in place): (result, steps)."""
+    nsteps = C.c_int32(0)
+    res = lib().cmio_compute_optical_depth(C.byref(sg), _ptr(nH, C.c_double),
+                                           _ptr(xH, C.c_double), photon.ctypes.data,
+                                           input_direction, C.byref(nsteps))
+    return res, nsteps.value
+
+
+def dust_exp(x: float) -> float:
+    return lib().cmio_dust_exp(float(x))
 
 
 def interact32(ncell, cell_size, kappa, tally, packet, max_steps: int = 0,
@@ -369,6 +407,21 @@ class LatticeGrid:
     def fixed_unit(self, s=0):
         """Metres per fixed-point tally unit of subgrid s (lref / 2^22)."""
         return float(max(np.float32(v) for v in self.lat.sub[s].cell_size)) / 4194304.0
+
+    def dust_run(self, nH, xH, num_photon, seed, albedo, source, source_subgrid,
+                 npix=(101, 101), instance=0, iteration=0):
+        """Dust photon loop (cmio_dust_run): (image [npix_x, npix_y] / num_photon, stats)."""
+        img = np.zeros(int(npix[0]) * int(npix[1]))
+        src = np.ascontiguousarray(source, dtype=np.float64)
+        nh = np.ascontiguousarray(nH, np.float64)
+        xh = np.ascontiguousarray(xH, np.float64)
+        st = DustStats()
+        lib().cmio_dust_run(C.byref(self.lat), _ptr(self.box, C.c_double), _ptr(nh, C.c_double),
+                            _ptr(xh, C.c_double), int(num_photon), int(seed), int(instance),
+                            int(iteration), float(albedo), _ptr(src, C.c_double),
+                            int(source_subgrid), int(npix[0]), int(npix[1]),
+                            _ptr(img, C.c_double), C.byref(st))
+        return img.reshape(int(npix[0]), int(npix[1])), st.as_dict()
 
     def iteration_omp(self, nH, xH, J, src_pos, src_lum, num_photon, seed, iteration,
                       alpha_H=4e-19, cross_section=6.3e-22, balance_form=1, threads=0):

@@ -151,9 +151,12 @@ static inline double min_d(double a, double b) { return (b < a) ? b : a; }
 static inline float min_f(float a, float b) { return (b < a) ? b : a; }
 
 /* DensitySubGrid::interact, DensitySubGrid.hpp:1180-1323. */
-int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, double *J,
-                  cmio_photon *photon, int input_direction, int32_t *trace_cells,
-                  double *trace_lengths, int32_t max_steps, int32_t *nsteps) {
+/* mode 0: DensitySubGrid::interact (DensitySubGrid.hpp:1180-1323); 1: propagate, the same
+ * walk without the J tally (:1333-1472); 2: compute_optical_depth, no target, the depth of
+ * the whole crossing added to the photon (:1482-1604). */
+static int walk_mode(const cmio_subgrid *sg, const double *nH, const double *xH, double *J,
+                     cmio_photon *photon, int input_direction, int32_t *trace_cells,
+                     double *trace_lengths, int32_t max_steps, int32_t *nsteps, int mode) {
   const double *d = photon->direction;
   const double inv[3] = {1. / d[0], 1. / d[1], 1. / d[2]};
   double pos[3] = {photon->position[0] - sg->anchor[0], photon->position[1] - sg->anchor[1],
@@ -165,7 +168,7 @@ int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, do
   int32_t idx[3];
   int cell = cmio_get_start_index(sg, pos, input_direction, idx);
   int32_t steps = 0;
-  while (tau_done < tau_target && is_inside3(idx, sg->ncell)) {
+  while ((mode == 2 || tau_done < tau_target) && is_inside3(idx, sg->ncell)) {
     const double lo[3] = {idx[0] * sg->cell_size[0], idx[1] * sg->cell_size[1],
                           idx[2] * sg->cell_size[2]};
     const double hi[3] = {(idx[0] + 1.) * sg->cell_size[0], (idx[1] + 1.) * sg->cell_size[1],
@@ -184,7 +187,7 @@ int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, do
     double lminsigma = lmin * sigma;
     const double tau = lminsigma * nH[cell] * xH[cell];
     tau_done += tau;
-    if (tau_done >= tau_target) {
+    if (mode != 2 && tau_done >= tau_target) {
       const double correction = (tau_done - tau_target) / tau;
       lmin *= (1. - correction);
       lminsigma = lmin * sigma;
@@ -195,7 +198,7 @@ int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, do
         }
       }
     }
-    J[cell] += lminsigma * weight;
+    if (mode == 0) J[cell] += lminsigma * weight;
     if (trace_cells != NULL && steps < max_steps) {
       trace_cells[steps] = cell;
       trace_lengths[steps] = lmin;
@@ -206,17 +209,34 @@ int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, do
     }
     cell = idx[0] * sg->ncell[3] + idx[1] * sg->ncell[2] + idx[2];
   }
-  photon->target_optical_depth = tau_target - tau_done;
+  photon->target_optical_depth = (mode == 2) ? tau_target + tau_done : tau_target - tau_done;
   for (int a = 0; a < 3; ++a) {
     photon->position[a] = pos[a] + sg->anchor[a];
   }
   if (nsteps != NULL) {
     *nsteps = steps;
   }
-  if (tau_done >= tau_target) {
+  if (mode != 2 && tau_done >= tau_target) {
     return CMIO_INSIDE;
   }
   return cmio_get_output_direction(sg, idx);
+}
+
+int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH, double *J,
+                  cmio_photon *photon, int input_direction, int32_t *trace_cells,
+                  double *trace_lengths, int32_t max_steps, int32_t *nsteps) {
+  return walk_mode(sg, nH, xH, J, photon, input_direction, trace_cells, trace_lengths,
+                   max_steps, nsteps, 0);
+}
+
+int cmio_propagate(const cmio_subgrid *sg, const double *nH, const double *xH,
+                   cmio_photon *photon, int input_direction, int32_t *nsteps) {
+  return walk_mode(sg, nH, xH, NULL, photon, input_direction, NULL, NULL, 0, nsteps, 1);
+}
+
+int cmio_compute_optical_depth(const cmio_subgrid *sg, const double *nH, const double *xH,
+                               cmio_photon *photon, int input_direction, int32_t *nsteps) {
+  return walk_mode(sg, nH, xH, NULL, photon, input_direction, NULL, NULL, 0, nsteps, 2);
 }
 
 /* FP32 cell-unit walk.  Same loop as interact above, with positions in cell
@@ -922,4 +942,183 @@ void cmio_iteration_omp(const cmio_lattice *lat, const double box[6], const doub
   free(numbers);
   free(first);
   free(src_sub);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dust scattering with forced first scattering and peel-off image: the      */
+/* photon loop of testDensitySubGrid_omp_dust.cpp (fill_buffer :564-620,     */
+/* relaunch :1200-1260, do_photon_traversal :621-722, do_reemission          */
+/* :730-760, peel-offs :1533-1560), with counter-based draws in place of the */
+/* per-thread generators: the CUDA library's cmi_dust_run draws the same     */
+/* numbers with the same correctly rounded operations.                       */
+/* ------------------------------------------------------------------------ */
+#define DUST_TAG 0x44555354u
+
+/* exp(x), x <= 0: Cody-Waite reduction x = k ln2 + r, Taylor series of
+ * exp(r) to r^18/18!, scaled by 2^k; 0 below e^-700 */
+double cmio_dust_exp(double x) {
+  if (!(x >= -700.)) return 0.;
+  if (x > 0.) x = 0.;
+  const double k = rint(x * 0x1.71547652b82fep+0);
+  const double r = (x - k * 0x1.62e42fefa3800p-1) - k * 0x1.ef35793c76730p-45;
+  double term = 1., sum = 1.;
+  for (int n = 1; n <= 18; ++n) {
+    term = term * r / (double)n;
+    sum += term;
+  }
+  return ldexp(sum, (int)k);
+}
+
+static double dust_uniform(uint32_t w) { return ((double)w + 0.5) * (1.0 / 4294967296.0); }
+
+static void dust_words(uint64_t seed, uint32_t instance, uint32_t iteration, uint32_t id,
+                       uint32_t gen, uint32_t purpose, uint32_t attempt, uint32_t w[4]) {
+  const uint32_t ctr[4] = {id, gen, iteration, DUST_TAG + (purpose << 8) + attempt};
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32) + instance};
+  cmio_philox4x32(ctr, key, w);
+}
+
+static void dust_direction(uint64_t seed, uint32_t instance, uint32_t iteration, uint32_t id,
+                           uint32_t gen, uint32_t purpose, double dir[3], uint32_t *w0,
+                           uint32_t *w3) {
+  for (uint32_t k = 0; k < 16u; ++k) {
+    uint32_t w[4];
+    dust_words(seed, instance, iteration, id, gen, purpose, k, w);
+    if (k == 0u && w0) *w0 = w[0];
+    const double x1 = 2. * dust_uniform(w[1]) - 1.;
+    const double x2 = 2. * dust_uniform(w[2]) - 1.;
+    const double ss = x1 * x1 + x2 * x2;
+    if (ss < 1.) {
+      const double f = 2. * sqrt(1. - ss);
+      dir[0] = x1 * f;
+      dir[1] = x2 * f;
+      dir[2] = 1. - 2. * ss;
+      if (w3) *w3 = w[3];
+      return;
+    }
+  }
+  dir[0] = 0.;
+  dir[1] = 0.;
+  dir[2] = 1.;
+  if (w3) *w3 = 0x80000000u;
+}
+
+/* one packet from subgrid to subgrid; 0: absorbed, 1: left the box */
+static int dust_walk(const cmio_lattice *lat, const double *nH, const double *xH,
+                     cmio_photon *ph, uint32_t *sub, int mode, cmio_dust_stats *st) {
+  const int64_t C = (int64_t)lat->sub_ncell[0] * lat->sub_ncell[1] * lat->sub_ncell[2];
+  int in_dir = (int)ph->reserved;
+  for (;;) {
+    const uint32_t s = *sub;
+    int32_t steps = 0;
+    const int out = walk_mode(&lat->sub[s], nH + s * C, xH + s * C, NULL, ph, in_dir, NULL,
+                              NULL, 0, &steps, mode);
+    st->cell_crossings += (uint64_t)steps;
+    st->subgrid_transits += 1;
+    if (out == CMIO_INSIDE) return 0;
+    const uint32_t ngb = lat->ngb[s * CMIO_NUM_DIRECTIONS + out];
+    in_dir = cmio_output_to_input_direction(out);
+    ph->reserved = in_dir;
+    if (ngb == CMIO_NEIGHBOUR_OUTSIDE) return 1;
+    *sub = ngb;
+  }
+}
+
+void cmio_dust_run(const cmio_lattice *lat, const double box[6], const double *nH,
+                   const double *xH, uint32_t num_photon, uint64_t seed, uint32_t instance,
+                   uint32_t iteration, double albedo, const double source[3],
+                   uint32_t source_subgrid, int32_t npix_x, int32_t npix_y, double *image,
+                   cmio_dust_stats *st) {
+  memset(st, 0, sizeof(*st));
+  st->emitted = num_photon;
+  const size_t npix = (size_t)npix_x * npix_y;
+  for (size_t k = 0; k < npix; ++k) image[k] = 0.;
+  const size_t cap = num_photon ? num_photon : 1;
+  cmio_photon *cur = (cmio_photon *)malloc(sizeof(cmio_photon) * cap);
+  uint32_t *sub = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+  uint32_t *id = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+  uint32_t *gen = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+  /* 1. TAU packets to the box edge, 2. relaunch */
+  for (uint32_t i = 0; i < num_photon; ++i) {
+    cmio_photon *ph = &cur[i];
+    memset(ph, 0, sizeof(*ph));
+    for (int a = 0; a < 3; ++a) ph->position[a] = source[a];
+    dust_direction(seed, instance, iteration, i, 0u, 0u, ph->direction, NULL, NULL);
+    ph->target_optical_depth = 0.;
+    ph->cross_section = 1.;
+    ph->weight = 1.;
+    ph->type = 1; /* TAU */
+    ph->reserved = 0;
+    sub[i] = source_subgrid;
+    id[i] = i;
+    gen[i] = 0u;
+    (void)dust_walk(lat, nH, xH, ph, &sub[i], 2, st);
+    const double weight = 1. - cmio_dust_exp(-ph->target_optical_depth);
+    uint32_t w[4];
+    dust_words(seed, instance, iteration, i, 0u, 1u, 0u, w);
+    for (int a = 0; a < 3; ++a) ph->position[a] = source[a];
+    ph->weight = weight;
+    ph->target_optical_depth = reemit_neg_log(1. - dust_uniform(w[0]) * weight);
+    ph->type = 0; /* DIRECT */
+    ph->reserved = 0;
+    sub[i] = source_subgrid;
+  }
+  /* 3-4. walks and scatterings until no packet is left */
+  uint32_t n = num_photon;
+  for (uint32_t g = 0; g < 4096u && n > 0; ++g) {
+    st->generations += 1;
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      cmio_photon ph = cur[i];
+      uint32_t s = sub[i];
+      if (dust_walk(lat, nH, xH, &ph, &s, 1, st) == 1) {
+        st->escaped += 1;
+        continue;
+      }
+      const uint32_t gg = gen[i] + 1u;
+      double dir[3];
+      uint32_t w0 = 0, w3 = 0;
+      dust_direction(seed, instance, iteration, id[i], gg, 2u, dir, &w0, &w3);
+      if (!(dust_uniform(w0) < albedo)) {
+        st->absorbed += 1;
+        continue;
+      }
+      st->scatterings += 1;
+      for (int a = 0; a < 3; ++a) ph.direction[a] = dir[a];
+      ph.target_optical_depth = reemit_neg_log(dust_uniform(w3));
+      ph.weight = ph.weight * 0.25 * 0.318309886183790671538;
+      ph.type = 0;
+      ph.reserved = 0;
+      /* peel-off copy along +z */
+      cmio_photon e = ph;
+      e.direction[0] = 0.;
+      e.direction[1] = 0.;
+      e.direction[2] = 1.;
+      e.target_optical_depth = 0.;
+      e.type = 2; /* PEELOFF */
+      uint32_t es = s;
+      if (dust_walk(lat, nH, xH, &e, &es, 2, st) == 1) {
+        const double fx = ((e.position[0] - box[0]) / box[3]) * (double)npix_x;
+        const double fy = ((e.position[1] - box[1]) / box[4]) * (double)npix_y;
+        if (fx >= 0. && fx < (double)npix_x && fy >= 0. && fy < (double)npix_y) {
+          image[(size_t)(int)fx * npix_y + (int)fy] +=
+              e.weight * cmio_dust_exp(-e.target_optical_depth);
+        } else {
+          st->peeloffs_off_image += 1;
+        }
+      }
+      /* scattered packets move to the front, in order */
+      cur[m] = ph;
+      sub[m] = s;
+      id[m] = id[i];
+      gen[m] = gg;
+      ++m;
+    }
+    n = m;
+  }
+  for (size_t k = 0; k < npix; ++k) image[k] /= (double)num_photon;
+  free(cur);
+  free(sub);
+  free(id);
+  free(gen);
 }

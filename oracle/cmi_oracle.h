@@ -74,6 +74,14 @@ int cmio_interact(const cmio_subgrid *sg, const double *nH, const double *xH,
                   int32_t *trace_cells, double *trace_lengths, int32_t max_steps,
                   int32_t *nsteps);
 
+/* DensitySubGrid::propagate (DensitySubGrid.hpp:1333-1472: interact without the J
+ * tally) and DensitySubGrid::compute_optical_depth (:1482-1604: no target; the depth
+ * of the crossing is added to target_optical_depth). */
+int cmio_propagate(const cmio_subgrid *sg, const double *nH, const double *xH,
+                   cmio_photon *photon, int input_direction, int32_t *nsteps);
+int cmio_compute_optical_depth(const cmio_subgrid *sg, const double *nH, const double *xH,
+                               cmio_photon *photon, int input_direction, int32_t *nsteps);
+
 /* FP32 cell-unit walk used by the CUDA single-precision transport (the
  * project's own formulation; restated here so the GPU kernel can be checked
  * bit for bit).  pos is in cell units relative to the subgrid; kappa is
@@ -209,6 +217,21 @@ void cmio_iteration_omp(const cmio_lattice *lat, const double box[6], const doub
                         const double *src_lum, uint64_t num_photon, uint64_t seed,
                         uint32_t iteration, double alpha_H, double cross_section,
                         int balance_form, int threads, cmio_counts *counts);
+
+/* Dust scattering with forced first scattering and a peel-off image (the photon loop
+ * of testDensitySubGrid_omp_dust.cpp), restating cmi_dust_run of the CUDA library with
+ * the same counter-based draws. */
+typedef struct {
+  uint64_t emitted, scatterings, absorbed, escaped, cell_crossings, subgrid_transits,
+      peeloffs_off_image;
+  uint32_t generations, error_flags;
+} cmio_dust_stats;
+double cmio_dust_exp(double x);
+void cmio_dust_run(const cmio_lattice *lat, const double box[6], const double *nH,
+                   const double *xH, uint32_t num_photon, uint64_t seed, uint32_t instance,
+                   uint32_t iteration, double albedo, const double source[3],
+                   uint32_t source_subgrid, int32_t npix_x, int32_t npix_y, double *image,
+                   cmio_dust_stats *st);
 
 #ifdef __cplusplus
 }

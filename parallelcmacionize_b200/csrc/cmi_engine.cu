@@ -4,6 +4,7 @@
 #include "cmacionize_b200.h"
 
 #include "cmi_kernels.cuh"
+#include "cmi_dust.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -1464,6 +1465,185 @@ int cmi_last_launch_count(cmi_context *c, uint64_t *launches) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Dust scattering with peel-off image (cmi_dust_run; cmi_dust.cuh)
+// ===========================================================================
+namespace {
+
+// device buffers of one cmi_dust_run call, freed on every exit
+struct DustBuffers {
+  Packet64 *pk[2] = {nullptr, nullptr}, *peel = nullptr;
+  uint32_t *sub[2] = {nullptr, nullptr}, *id[2] = {nullptr, nullptr}, *gen[2] = {nullptr, nullptr};
+  uint32_t *peel_sub = nullptr, *counts = nullptr;
+  int32_t *status = nullptr;
+  unsigned long long *counters = nullptr;
+  double *image = nullptr;
+  ~DustBuffers() {
+    for (int k = 0; k < 2; ++k) {
+      cudaFree(pk[k]);
+      cudaFree(sub[k]);
+      cudaFree(id[k]);
+      cudaFree(gen[k]);
+    }
+    cudaFree(peel);
+    cudaFree(peel_sub);
+    cudaFree(counts);
+    cudaFree(status);
+    cudaFree(counters);
+    cudaFree(image);
+  }
+};
+
+unsigned dust_blocks(uint64_t n, int threads) {
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + threads - 1) / threads, 148 * 32));
+}
+
+}  // namespace
+
+extern "C" int cmi_dust_run(cmi_context *c, int32_t instance, uint64_t num_photon, uint64_t seed,
+                            uint32_t iteration, double albedo, const double source[3],
+                            int32_t npix_x, int32_t npix_y, double *image,
+                            cmi_dust_stats *stats) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  if (num_photon == 0 || num_photon > (1ull << 30))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "num_photon must be in [1, 2^30]");
+  if (!(albedo >= 0. && albedo < 1.))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "albedo must be in [0, 1)");
+  if (npix_x < 1 || npix_y < 1 || npix_x > 65536 || npix_y > 65536 ||
+      (int64_t)npix_x * npix_y > (1ll << 26))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "image size out of range");
+  if (!source || !image) return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  const HostInstance &I = c->inst[instance];
+  const double *box = I.desc.box;
+  // Source::get_subgrid_index: the subgrid holding the source
+  int si[3];
+  for (int a = 0; a < 3; ++a) {
+    if (!(source[a] >= box[a] && source[a] <= box[a] + box[3 + a]))
+      return fail(CMI_ERR_INVALID_ARGUMENT, "the source lies outside the box");
+    si[a] = (int)((source[a] - box[a]) / box[3 + a] * I.desc.num_subgrid[a]);
+    si[a] = std::min(si[a], I.desc.num_subgrid[a] - 1);
+  }
+  const uint32_t n = (uint32_t)num_photon;
+  DustBuffers B;
+  for (int k = 0; k < 2; ++k) {
+    CMI_TRY(dev_alloc(&B.pk[k], n));
+    CMI_TRY(dev_alloc(&B.sub[k], n));
+    CMI_TRY(dev_alloc(&B.id[k], n));
+    CMI_TRY(dev_alloc(&B.gen[k], n));
+  }
+  CMI_TRY(dev_alloc(&B.peel, n));
+  CMI_TRY(dev_alloc(&B.peel_sub, n));
+  CMI_TRY(dev_alloc(&B.status, n));
+  CMI_TRY(dev_alloc(&B.counts, 4));
+  CMI_TRY(dev_alloc(&B.counters, 8));
+  const size_t npix = (size_t)npix_x * npix_y;
+  CMI_TRY(dev_alloc(&B.image, npix));
+  cudaStream_t st = c->stream;
+  CMI_CUDA(cudaMemsetAsync(B.counters, 0, sizeof(unsigned long long) * 8, st));
+  CMI_CUDA(cudaMemsetAsync(B.image, 0, sizeof(double) * npix, st));
+  // counts: [0] live packets of pass 0, [1] of pass 1
+  const uint32_t counts0[4] = {n, 0u, 0u, 0u};
+  CMI_CUDA(cudaMemcpyAsync(B.counts, counts0, sizeof(counts0), cudaMemcpyHostToDevice, st));
+
+  DustParams p{};
+  p.subs = c->d_sub;
+  p.nH = c->d_nH;
+  p.xH = c->d_xH;
+  p.tables = c->tables;
+  p.status = B.status;
+  p.seed = seed;
+  p.instance = (uint32_t)instance;
+  p.iteration = iteration;
+  for (int a = 0; a < 3; ++a) p.src[a] = source[a];
+  p.src_sub = I.first_sub + (uint32_t)((si[0] * I.desc.num_subgrid[1] + si[1]) *
+                                           I.desc.num_subgrid[2] + si[2]);
+  p.counters = B.counters;
+  auto pass = [&](int k) {
+    p.pk = B.pk[k];
+    p.sub = B.sub[k];
+    p.id = B.id[k];
+    p.gen = B.gen[k];
+    p.count = B.counts + k;
+  };
+  const unsigned wb = dust_blocks(n, 128);
+  // 1. TAU packets to the box edge, 2. forced-scattering relaunch
+  pass(0);
+  k_dust_emit<<<dust_blocks(n, 256), 256, 0, st>>>(p, n);
+  k_dust_walk<kDepth><<<wb, 128, 0, st>>>(p);
+  k_dust_relaunch<<<dust_blocks(n, 256), 256, 0, st>>>(p);
+  CMI_CUDA(cudaGetLastError());
+  uint32_t generations = 0;
+  int cur = 0;
+  for (uint32_t g = 0; g < 4096u; ++g) {
+    // 3. DIRECT packets to absorption or out of the box
+    pass(cur);
+    k_dust_walk<kPropagate><<<wb, 128, 0, st>>>(p);
+    // 4. scattering + peel-off copies into the other pass
+    CMI_CUDA(cudaMemsetAsync(B.counts + (1 - cur), 0, sizeof(uint32_t), st));
+    DustScatterParams q{};
+    q.pk = B.pk[cur];
+    q.sub = B.sub[cur];
+    q.id = B.id[cur];
+    q.gen = B.gen[cur];
+    q.status = B.status;
+    q.count = B.counts + cur;
+    q.out_pk = B.pk[1 - cur];
+    q.out_sub = B.sub[1 - cur];
+    q.out_id = B.id[1 - cur];
+    q.out_gen = B.gen[1 - cur];
+    q.peel_pk = B.peel;
+    q.peel_sub = B.peel_sub;
+    q.out_count = B.counts + (1 - cur);
+    q.seed = seed;
+    q.instance = (uint32_t)instance;
+    q.iteration = iteration;
+    q.albedo = albedo;
+    q.counters = B.counters;
+    k_dust_scatter<<<dust_blocks(n, 256), 256, 0, st>>>(q);
+    ++generations;
+    uint32_t m = 0;
+    CMI_CUDA(cudaMemcpyAsync(&m, B.counts + (1 - cur), sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             st));
+    CMI_CUDA(cudaStreamSynchronize(st));
+    if (m == 0u) break;
+    // peel-offs (one per scattered packet) to the box edge, into the image
+    DustParams pp = p;
+    pp.pk = B.peel;
+    pp.sub = B.peel_sub;
+    pp.id = nullptr;
+    pp.gen = nullptr;
+    pp.count = B.counts + (1 - cur);
+    k_dust_walk<kDepth><<<dust_blocks(m, 128), 128, 0, st>>>(pp);
+    k_dust_image<<<dust_blocks(m, 256), 256, 0, st>>>(B.peel, B.status, B.counts + (1 - cur),
+                                                      box[0], box[3], box[1], box[4], npix_x,
+                                                      npix_y, B.image, B.counters + 6);
+    CMI_CUDA(cudaGetLastError());
+    cur = 1 - cur;
+  }
+  std::vector<double> img(npix);
+  unsigned long long ctr[8];
+  CMI_CUDA(cudaMemcpyAsync(img.data(), B.image, sizeof(double) * npix, cudaMemcpyDeviceToHost, st));
+  CMI_CUDA(cudaMemcpyAsync(ctr, B.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+  CMI_CUDA(cudaStreamSynchronize(st));
+  // the driver's image.dat holds the sums divided by the packet count
+  for (size_t k = 0; k < npix; ++k) image[k] = img[k] / (double)num_photon;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->emitted = num_photon;
+    stats->cell_crossings = ctr[0];
+    stats->subgrid_transits = ctr[1];
+    stats->absorbed = ctr[3];
+    stats->escaped = ctr[4];
+    stats->scatterings = ctr[5];
+    stats->peeloffs_off_image = ctr[6];
+    stats->generations = generations;
+    stats->error_flags = ctr[2] ? (uint32_t)kFlagWalkLimit : 0u;
+  }
+  if (ctr[2]) return fail(CMI_ERR_INVARIANT, "dust walk: step or visit bound exceeded");
+  return CMI_OK;
+}
 
 // ===========================================================================
 // Allocation-free buffer traversal (cmi_traverse_buffer_noalloc)

@@ -18,6 +18,14 @@ namespace cmi {
 
 enum WalkStatus : int { kRun = 0, kAbsorbed = 1, kExited = 2 };
 
+// What a FP64 walk does in each cell (the dust path, testDensitySubGrid_omp_dust.cpp):
+//  kInteract  DensitySubGrid::interact: path length into J, stop at the target depth
+//  kPropagate DensitySubGrid::propagate (DensitySubGrid.hpp:1333-1472): the same walk
+//             without the J tally
+//  kDepth     DensitySubGrid::compute_optical_depth (DensitySubGrid.hpp:1482-1604): no
+//             target, the optical depth of the whole crossing is added to the packet
+enum WalkMode : int { kInteract = 0, kPropagate = 1, kDepth = 2 };
+
 template <class T>
 __device__ __forceinline__ T min_ref(T a, T b) {  // std::min semantics
   return (b < a) ? b : a;
@@ -294,7 +302,18 @@ struct Walk64 {
            idx[2] < v.n[2] && idx[2] >= 0;
   }
 
-  // DensitySubGrid.hpp:1221-1305, one iteration.
+  // compute_optical_depth's entry (DensitySubGrid.hpp:1495-1519): no target,
+  // so no absorption test; the packet's depth so far is kept in tau_target
+  __device__ __forceinline__ int begin_depth(const Packet64 &pk, const View64 &v,
+                                            const uint8_t *sign_code) {
+    (void)begin(pk, v, sign_code);
+    tau_target = pk.tau;
+    tau_done = 0.;
+    return inside(v) ? kRun : kExited;
+  }
+
+  // DensitySubGrid.hpp:1221-1305, one iteration (kMode: what the cell does).
+  template <int kMode = kInteract>
   __device__ __forceinline__ int step(const View64 &v, double *trace_len = nullptr) {
     double lo[3], hi[3], l[3];
 #pragma unroll
@@ -309,7 +328,7 @@ struct Walk64 {
     double lminsigma = lmin * sigma;
     const double tau = lminsigma * v.nH[cell] * v.xH[cell];
     tau_done += tau;
-    const bool absorbed = tau_done >= tau_target;
+    const bool absorbed = kMode != kDepth && tau_done >= tau_target;
     if (absorbed) {
       const double correction = (tau_done - tau_target) / tau;
       lmin *= (1. - correction);
@@ -324,7 +343,7 @@ struct Walk64 {
       }
     }
     if (trace_len) *trace_len = lmin;
-    atomicAdd(&v.J[cell], lminsigma * weight);
+    if (kMode == kInteract) atomicAdd(&v.J[cell], lminsigma * weight);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       pos[a] = (l[a] == lmin) ? ((d[a] > 0.) ? hi[a] : lo[a]) : pos[a] + lmin * d[a];

@@ -205,6 +205,20 @@ class TransportEngine:
                  for it in range(done.value)]
         return stats, list(at)
 
+    def dust_image(self, instance, num_photon, albedo, source=(0.0, 0.0, 0.0), npix=(101, 101),
+                   seed=42, iteration=0):
+        """The reference dust driver's photon loop on this instance's n_H and x_H
+        (cmi_dust_run: forced first scattering, isotropic scattering with
+        probability `albedo`, peel-off image along +z).  Returns (image
+        [npix_x, npix_y] divided by num_photon, stats dict)."""
+        img = np.zeros(int(npix[0]) * int(npix[1]))
+        src = np.ascontiguousarray(source, dtype=np.float64)
+        st = _lib.DustStats()
+        check(self._L.cmi_dust_run(self._h, int(instance), int(num_photon), int(seed),
+                                   int(iteration), float(albedo), src.ctypes.data,
+                                   int(npix[0]), int(npix[1]), img.ctypes.data, C.byref(st)))
+        return img.reshape(int(npix[0]), int(npix[1])), st.as_dict()
+
     def shoot_packets(self, seed=42, iteration=0):
         ninst = len(self.grids)
         st = (_lib.Stats * ninst)()
