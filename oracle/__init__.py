@@ -452,6 +452,29 @@ def ref_run(args, binary: str = "ref_harness_exact", **kw):
     return subprocess.run([b] + [str(a) for a in args], check=True, capture_output=True, **kw)
 
 
+def ref_dust_walk(box, ncell, nH, xH, photons, in_dirs, depth=False):
+    """Reference DensitySubGrid::propagate (depth=False) or compute_optical_depth
+    on each photon, each on the same grid: (photons_out, results)."""
+    with tempfile.TemporaryDirectory() as td:
+        inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(inp, "wb") as f:
+            f.write(np.asarray(box, "<f8").tobytes())
+            f.write(np.asarray(ncell, "<i4").tobytes())
+            f.write(np.zeros(1, "<i4").tobytes())
+            f.write(np.asarray(nH, "<f8").tobytes())
+            f.write(np.asarray(xH, "<f8").tobytes())
+            f.write(np.asarray([photons.size], "<i8").tobytes())
+            rec = np.zeros(photons.size, dtype=[("p", PHOTON_DTYPE), ("d", "<i4")])
+            rec["p"] = photons
+            rec["d"] = in_dirs
+            f.write(rec.tobytes())
+        ref_run(["depth" if depth else "propagate", inp, out])
+        raw = open(out, "rb").read()
+    rec_dt = np.dtype([("p", PHOTON_DTYPE), ("r", "<i4")])
+    head = np.frombuffer(raw, dtype=rec_dt, count=photons.size)
+    return head["p"].copy(), head["r"].copy()
+
+
 def ref_walk(box, ncell, nH, xH, photons, in_dirs):
     """Reference DensitySubGrid::interact on each photon (in order).
 

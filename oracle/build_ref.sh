@@ -9,6 +9,9 @@
 #   testDensitySubGrid_omp_files  the same driver with its result files
 #                      switched on (-DMM_FILE -DBIN_FILE: neutral_fractions.dat
 #                      and .bin), no fast-math (golden output files)
+#   testDensitySubGrid_omp_dust  the reference's dust driver (forced first
+#                      scattering, peel-off image.dat), no fast-math (statistical
+#                      golden image of the dust path)
 # Deviations from compile_omp.sh, all needed to build on this image:
 #   -march=x86-64-v3 instead of -march=native (the binary runs on another host),
 #   -include cstdint (CommandLineOption.hpp uses int_fast32_t without it),
@@ -47,5 +50,12 @@ for f in testDensitySubGrid_omp.cpp CommandLineOption.cpp CommandLineParser.cpp;
     -c "$REF_DIR/$f" -o "$TMP/${f%.cpp}.o" 2> "$TMP/${f%.cpp}.log" || { cat "$TMP/${f%.cpp}.log" >&2; exit 1; }
 done
 $CXX -fopenmp -o "$OUT/testDensitySubGrid_omp_files" "$TMP"/*.o
+rm -f "$TMP"/*.o
+for f in testDensitySubGrid_omp_dust.cpp CommandLineOption.cpp CommandLineParser.cpp; do
+  $CXX -std=c++11 -fopenmp -Wall -Wno-catch-value -O2 -ffp-contract=off -fno-fast-math \
+    -include cstdint -I"$HERE/hdf5_stub" -I"$REF_DIR" \
+    -c "$REF_DIR/$f" -o "$TMP/${f%.cpp}.o" 2> "$TMP/${f%.cpp}.log" || { cat "$TMP/${f%.cpp}.log" >&2; exit 1; }
+done
+$CXX -fopenmp -o "$OUT/testDensitySubGrid_omp_dust" "$TMP"/*.o
 rm -rf "$TMP"
 echo "built: $(ls "$OUT" | tr '\n' ' ')"

@@ -580,6 +580,41 @@ int cmd_run(const char *in_path, const char *out_path, long packets, int iterati
 
 }  // namespace
 
+/* ---- dust walks: DensitySubGrid::propagate (DensitySubGrid.hpp:1333) or
+ * DensitySubGrid::compute_optical_depth (:1482) on a list of photons, each on
+ * the same grid ----
+ * in:  as cmd_walk
+ * out: {PhotonRecord, int32 result}*n */
+int cmd_dust_walk(const char *in_path, const char *out_path, bool depth) {
+  Reader r(in_path);
+  double box[6];
+  r.get(box, 6);
+  int ncell[3];
+  r.get(ncell, 3);
+  (void)r.get<int32_t>();
+  const long C = (long)ncell[0] * ncell[1] * ncell[2];
+  std::vector<double> nH(C), xH(C);
+  r.get(nH.data(), C);
+  r.get(xH.data(), C);
+  const long n = r.get<int64_t>();
+  DensitySubGrid grid(box, ncell);
+  for (long c = 0; c < C; ++c) {
+    grid.set_number_density(c, nH[c]);
+    grid.set_neutral_fraction(c, xH[c]);
+  }
+  Writer w(out_path);
+  for (long i = 0; i < n; ++i) {
+    const PhotonRecord rec = r.get<PhotonRecord>();
+    const int32_t in_dir = r.get<int32_t>();
+    Photon p;
+    to_photon(rec, p);
+    const int res = depth ? grid.compute_optical_depth(p, in_dir) : grid.propagate(p, in_dir);
+    w.put(from_photon(p));
+    w.put((int32_t)res);
+  }
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc < 2) {
     std::fprintf(stderr,
@@ -596,6 +631,8 @@ int main(int argc, char **argv) {
     return cmd_emit(std::atoi(argv[2]), std::atoi(argv[3]), std::atof(argv[4]),
                     std::atof(argv[5]), std::atof(argv[6]), argv[7]);
   if (cmd == "walk" && argc == 4) return cmd_walk(argv[2], argv[3]);
+  if (cmd == "propagate" && argc == 4) return cmd_dust_walk(argv[2], argv[3], false);
+  if (cmd == "depth" && argc == 4) return cmd_dust_walk(argv[2], argv[3], true);
   if (cmd == "balance" && argc == 4) return cmd_balance(argv[2], argv[3]);
   if (cmd == "transport" && argc == 4) return cmd_transport(argv[2], argv[3]);
   if (cmd == "run" && argc == 9)

@@ -100,6 +100,20 @@ def large_config(ncell=256, num_subgrid=16, num_photon=100_000_000, num_sources=
                             num_sources=num_sources, sigma_ln=sigma_ln, seed=seed, alpha=alpha)
 
 
+def dust_sphere(ncell=32, num_subgrid=4):
+    """The dust driver's test medium (testDensitySubGrid_omp_dust.cpp:2073-2091):
+    box [-1, 1]^3 (m), n_H = 1 in cells whose midpoint lies within radius 1,
+    0 outside; x_H = 1 (the state after the driver's first balance, whose J
+    is 0).  Returns (GridSpec, n_H blocked, x_H blocked)."""
+    from .outputs import cell_centres_blocked
+    g = GridSpec(box=(-1.0, -1.0, -1.0, 2.0, 2.0, 2.0), ncell=(ncell,) * 3,
+                 num_subgrid=(num_subgrid,) * 3)
+    pos = cell_centres_blocked(g)
+    r = np.sqrt((pos * pos).sum(axis=1))
+    nH = np.where(r < 1.0, 1.0, 0.0)
+    return g, nH, np.ones_like(nH)
+
+
 def stromgren_profile(alpha=4.0e-19, nH=1.0e8, Q=4.26e49, sigma=6.3e-22,
                       reemission_probability=0.0, samples=1200):
     """Semi-analytic x_H(r) and R_S (scripts/plot_neutral_fraction_profile.py:60-82)."""

@@ -15,6 +15,15 @@ inputs and stores inputs + reference outputs as compressed .npz files:
   transport.npz    interact + neighbour routing through a lattice of subgrids
   stromgren_ensemble.npz  64^3 Stromgren runs (reference code, 8 seeds):
                    radial x_H profiles and ionized radii
+  dust_walks.npz   DensitySubGrid::propagate and compute_optical_depth on the
+                   packet lists of walk_interior16 / walk_entries8 /
+                   walk_noncubic (propagate only where the target depth is > 0:
+                   the reference asserts that)
+  dust_image.npz   image.dat of the reference's dust driver
+                   (oracle/_ref/testDensitySubGrid_omp_dust: forced first
+                   scattering, peel-off image) for a unit-density sphere of
+                   radius 1 in a [-1, 1]^3 box, albedo 0.5, 1e6 packets; the
+                   second iteration's image (x_H = 1 after the first balance)
   outputs.npz      the result files of the reference's own driver
                    (oracle/_ref/testDensitySubGrid_omp_files, -DMM_FILE
                    -DBIN_FILE): neutral_fractions.dat and .bin of a small
@@ -265,6 +274,56 @@ def gen_ensemble(seeds=8, packets=1_000_000, iterations=10):
          radii=np.array(radii), packets=packets, iterations=iterations)
 
 
+DUST_CASES = ("interior16", "entries8", "noncubic")
+
+
+def gen_dust_walks():
+    arrays = {}
+    for case in DUST_CASES:
+        g = np.load(os.path.join(OUT, f"walk_{case}.npz"))
+        ph, dirs = g["photons"], g["in_dirs"]
+        keep = ph["tau"] > 0
+        out, res = O.ref_dust_walk(g["box"], g["ncell"], g["nH"], g["xH"], ph[keep], dirs[keep])
+        arrays[f"{case}_keep"] = keep
+        arrays[f"{case}_prop_out"] = out
+        arrays[f"{case}_prop_res"] = res
+        out, res = O.ref_dust_walk(g["box"], g["ncell"], g["nH"], g["xH"], ph, dirs, depth=True)
+        arrays[f"{case}_depth_out"] = out
+        arrays[f"{case}_depth_res"] = res
+    save("dust_walks.npz", **arrays)
+
+
+DUST_IMAGE_CASE = {"ncell": 32, "num_subgrid": 4, "num_photon": 1000000, "albedo": 0.5,
+                   "threads": 4}
+
+
+def gen_dust_image():
+    """Runs the reference's dust driver (params with the keys of
+    params_single_uniform.txt; box in metres) and stores its image.dat."""
+    import subprocess
+    import tempfile
+    b = O.ref_binary("testDensitySubGrid_omp_dust")
+    if b is None:
+        sys.exit("oracle/_ref/testDensitySubGrid_omp_dust missing: run oracle/build_ref.sh")
+    c = DUST_IMAGE_CASE
+    params = "\n".join([
+        "box:", "  anchor: [-1. m, -1. m, -1. m]", "  sides: [2. m, 2. m, 2. m]",
+        f"ncell: [{c['ncell']}, {c['ncell']}, {c['ncell']}]", f"num_photon: {c['num_photon']}",
+        "number_of_iterations: 2", f"reemission_probability: {c['albedo']}",
+        "number_of_sources: 1", "random_density: false",
+        f"num_subgrid: [{c['num_subgrid']}, {c['num_subgrid']}, {c['num_subgrid']}]",
+        "queue_size_per_thread: 1000", "memoryspace_size: 500000", "number_of_tasks: 5000000",
+        "MPI_buffer_size: 1000", "cost_copy_factor: 10", "edge_copy_factor: 0.01",
+        "general_queue_size: 100000", ""])
+    with tempfile.TemporaryDirectory() as td:
+        with open(os.path.join(td, "params.txt"), "w") as f:
+            f.write(params)
+        subprocess.run([b, "-p", "params.txt", "-t", str(c["threads"])], cwd=td, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        img = np.fromfile(os.path.join(td, "image.dat"), dtype=np.float64).reshape(101, 101)
+    save("dust_image.npz", image=img, **{k: np.array(v) for k, v in c.items()})
+
+
 OUTPUT_CASE = {"ncell": (16, 16, 8), "num_subgrid": (2, 2, 1),
                "anchor_pc": (-5.0, -4.0, -3.0), "sides_pc": (10.0, 8.0, 6.0),
                "num_photon": 20000, "iterations": 2}
@@ -307,9 +366,15 @@ def main():
     ap.add_argument("--skip-ensemble", action="store_true")
     ap.add_argument("--only-outputs", action="store_true",
                     help="regenerate outputs.npz only")
+    ap.add_argument("--only-dust", action="store_true",
+                    help="regenerate dust_walks.npz only (from the walk fixtures)")
     args = ap.parse_args()
     if args.only_outputs:
         gen_outputs()
+        return
+    if args.only_dust:
+        gen_dust_walks()
+        gen_dust_image()
         return
     if O.ref_binary() is None:
         sys.exit("oracle/_ref/ref_harness_exact missing: run oracle/build_ref.sh first")
@@ -319,6 +384,8 @@ def main():
     gen_walks()
     gen_balance()
     gen_transport()
+    gen_dust_walks()
+    gen_dust_image()
     gen_outputs()
     if not args.skip_ensemble:
         gen_ensemble()
