@@ -318,7 +318,9 @@ int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
  * `image` (host, npix_x * npix_y) receives the sums divided by num_photon, as
  * the driver writes image.dat.  FP64 throughout, the reference's walk
  * arithmetic; counter-based draws (seed, iteration) replace the reference's
- * per-thread generators.  albedo in [0, 1); num_photon <= 2^30. */
+ * per-thread generators.  albedo in [0, 1); num_photon <= 2^30.  The packet
+ * buffers (about 290 bytes per packet) grow to the largest call and stay with
+ * the context until cmi_destroy. */
 typedef struct cmi_dust_stats {
   uint64_t emitted;            /* source packets */
   uint64_t scatterings;        /* scattered packets (= peel-off packets) */

@@ -86,6 +86,9 @@ void dev_free(T *&p) {
 
 }  // namespace
 
+struct DustBuffers;
+void free_dust_buffers(DustBuffers *b);
+
 struct cmi_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -148,6 +151,11 @@ struct cmi_context {
   };
   std::vector<Timed> timed;
   std::vector<cudaEvent_t> event_pool;
+
+  // cmi_dust_run's packet buffers, grown to the largest call and kept
+  DustBuffers *dust = nullptr;
+  uint64_t dust_capacity = 0;  // packets
+  size_t dust_pixels = 0;
 
   bool fp32() const { return opt.transport_precision == CMI_TRANSPORT_FP32; }
   size_t packet_bytes() const { return fp32() ? sizeof(Packet32) : sizeof(Packet64); }
@@ -951,6 +959,8 @@ int cmi_destroy(cmi_context *c) {
   dev_free(c->d_keys);
   dev_free(c->d_ranks);
   dev_free(c->d_stage);
+  free_dust_buffers(c->dust);
+  c->dust = nullptr;
   if (c->h_stats) cudaFreeHost(c->h_stats);
   for (auto &t : c->timed) {
     cudaEventDestroy(t.start);
@@ -1469,9 +1479,7 @@ int cmi_last_launch_count(cmi_context *c, uint64_t *launches) {
 // ===========================================================================
 // Dust scattering with peel-off image (cmi_dust_run; cmi_dust.cuh)
 // ===========================================================================
-namespace {
-
-// device buffers of one cmi_dust_run call, freed on every exit
+// device buffers of cmi_dust_run, kept by the context between calls
 struct DustBuffers {
   Packet64 *pk[2] = {nullptr, nullptr}, *peel = nullptr;
   uint32_t *sub[2] = {nullptr, nullptr}, *id[2] = {nullptr, nullptr}, *gen[2] = {nullptr, nullptr};
@@ -1494,6 +1502,10 @@ struct DustBuffers {
     cudaFree(image);
   }
 };
+
+void free_dust_buffers(DustBuffers *b) { delete b; }
+
+namespace {
 
 unsigned dust_blocks(uint64_t n, int threads) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + threads - 1) / threads, 148 * 32));
@@ -1526,20 +1538,40 @@ extern "C" int cmi_dust_run(cmi_context *c, int32_t instance, uint64_t num_photo
     si[a] = std::min(si[a], I.desc.num_subgrid[a] - 1);
   }
   const uint32_t n = (uint32_t)num_photon;
-  DustBuffers B;
-  for (int k = 0; k < 2; ++k) {
-    CMI_TRY(dev_alloc(&B.pk[k], n));
-    CMI_TRY(dev_alloc(&B.sub[k], n));
-    CMI_TRY(dev_alloc(&B.id[k], n));
-    CMI_TRY(dev_alloc(&B.gen[k], n));
-  }
-  CMI_TRY(dev_alloc(&B.peel, n));
-  CMI_TRY(dev_alloc(&B.peel_sub, n));
-  CMI_TRY(dev_alloc(&B.status, n));
-  CMI_TRY(dev_alloc(&B.counts, 4));
-  CMI_TRY(dev_alloc(&B.counters, 8));
   const size_t npix = (size_t)npix_x * npix_y;
-  CMI_TRY(dev_alloc(&B.image, npix));
+  // the buffers grow to the largest call and stay with the context (about
+  // 290 bytes per packet); a failed allocation leaves no buffers behind
+  if (!c->dust || c->dust_capacity < n || c->dust_pixels < npix) {
+    CMI_CUDA(cudaStreamSynchronize(c->stream));
+    free_dust_buffers(c->dust);
+    c->dust = nullptr;
+    c->dust_capacity = 0;
+    c->dust_pixels = 0;
+    DustBuffers *nb = new DustBuffers();
+    const uint64_t cap = std::max<uint64_t>(n, 1024);
+    const size_t pix = std::max<size_t>(npix, 101 * 101);
+    int rc = CMI_OK;
+    for (int k = 0; k < 2; ++k) {
+      if (rc == CMI_OK) rc = dev_alloc(&nb->pk[k], cap);
+      if (rc == CMI_OK) rc = dev_alloc(&nb->sub[k], cap);
+      if (rc == CMI_OK) rc = dev_alloc(&nb->id[k], cap);
+      if (rc == CMI_OK) rc = dev_alloc(&nb->gen[k], cap);
+    }
+    if (rc == CMI_OK) rc = dev_alloc(&nb->peel, cap);
+    if (rc == CMI_OK) rc = dev_alloc(&nb->peel_sub, cap);
+    if (rc == CMI_OK) rc = dev_alloc(&nb->status, cap);
+    if (rc == CMI_OK) rc = dev_alloc(&nb->counts, 4);
+    if (rc == CMI_OK) rc = dev_alloc(&nb->counters, 8);
+    if (rc == CMI_OK) rc = dev_alloc(&nb->image, pix);
+    if (rc != CMI_OK) {
+      free_dust_buffers(nb);
+      return rc;
+    }
+    c->dust = nb;
+    c->dust_capacity = cap;
+    c->dust_pixels = pix;
+  }
+  DustBuffers &B = *c->dust;
   cudaStream_t st = c->stream;
   CMI_CUDA(cudaMemsetAsync(B.counters, 0, sizeof(unsigned long long) * 8, st));
   CMI_CUDA(cudaMemsetAsync(B.image, 0, sizeof(double) * npix, st));
