@@ -117,6 +117,7 @@ struct cmi_context {
   uint32_t *d_hist = nullptr, *d_bucket_off = nullptr;
   uint32_t *d_tile_pk = nullptr, *d_tile_ch = nullptr, *d_tile_pk_off = nullptr,
            *d_tile_ch_off = nullptr;
+  uint32_t *d_plan_choff = nullptr, *d_plan_pkoff = nullptr;  // kPlanTile + 1 each
   uint32_t ntiles = 0;
   Chunk *d_chunks = nullptr;
   uint64_t chunk_capacity = 0;
@@ -336,8 +337,11 @@ int refresh_kappa(cmi_context *c, int32_t i) {
 int launch_plan(cmi_context *c, bool scatter) {
   if (c->ntiles == 1) {
     k_plan_fused<<<1, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk, c->d_bucket_off,
-                                                    c->d_chunks, c->d_state);
-    c->enqueued += 1;
+                                                    c->d_chunks, c->d_state, c->d_plan_choff,
+                                                    c->d_plan_pkoff);
+    k_plan_chunks<<<c->num_sms * 2, 256, 0, c->stream>>>(c->d_plan_choff, c->d_plan_pkoff,
+                                                         c->chunk, c->d_chunks, c->d_state);
+    c->enqueued += 2;
   } else {
     k_plan_count<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
                                                             c->d_tile_pk, c->d_tile_ch);
@@ -901,7 +905,9 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
       (rc = dev_alloc(&c->d_hist, c->S)) || (rc = dev_alloc(&c->d_bucket_off, c->S)) ||
       (rc = dev_alloc(&c->d_tile_pk, c->ntiles)) || (rc = dev_alloc(&c->d_tile_ch, c->ntiles)) ||
       (rc = dev_alloc(&c->d_tile_pk_off, c->ntiles)) ||
-      (rc = dev_alloc(&c->d_tile_ch_off, c->ntiles)))
+      (rc = dev_alloc(&c->d_tile_ch_off, c->ntiles)) ||
+      (rc = dev_alloc(&c->d_plan_choff, kPlanTile + 1)) ||
+      (rc = dev_alloc(&c->d_plan_pkoff, kPlanTile + 1)))
     return bail(rc);
   if (cudaMemcpyAsync(c->d_sub, c->h_sub.data(), sizeof(DevSubgrid) * c->S,
                       cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
@@ -953,6 +959,8 @@ int cmi_destroy(cmi_context *c) {
   dev_free(c->d_tile_ch);
   dev_free(c->d_tile_pk_off);
   dev_free(c->d_tile_ch_off);
+  dev_free(c->d_plan_choff);
+  dev_free(c->d_plan_pkoff);
   dev_free(c->d_chunks);
   dev_free(c->d_arena_in);
   dev_free(c->d_arena_out);

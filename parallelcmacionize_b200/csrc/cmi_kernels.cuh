@@ -524,10 +524,34 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan_write(uint32_t *hist, uin
 
 // Whole plan in one block when every subgrid fits one tile (S <= 4096):
 // counts -> bucket offsets -> chunk list, and the round-state update.
+// The chunk q of subgrid lo (by binary search over the first chunk of each
+// subgrid): begin, count and the chunks left in its subgrid.
+__device__ __forceinline__ Chunk plan_chunk(const uint32_t *choff, const uint32_t *pkoff,
+                                            uint32_t q, uint32_t chunk) {
+  int lo = 0, hi = kPlanTile - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (choff[mid] <= q) lo = mid; else hi = mid - 1;
+  }
+  const uint32_t j = q - choff[lo];
+  Chunk cc;
+  cc.subgrid = (uint32_t)lo;
+  cc.begin = pkoff[lo] + j * chunk;
+  cc.count = min(chunk, (pkoff[lo + 1] - pkoff[lo]) - j * chunk);
+  cc.rem = (choff[lo + 1] - choff[lo]) - j;
+  return cc;
+}
+
+// Rounds with more chunks than this have their chunk list written by
+// k_plan_chunks across the GPU instead of by the plan's single block.
+constexpr uint32_t kPlanChunksInBlock = 8192;
+
 __global__ void __launch_bounds__(kPlanThreads) k_plan_fused(uint32_t *hist, uint32_t S,
                                                              uint32_t chunk,
                                                              uint32_t *bucket_off,
-                                                             Chunk *chunks, RoundState *st) {
+                                                             Chunk *chunks, RoundState *st,
+                                                             uint32_t *choff_out,
+                                                             uint32_t *pkoff_out) {
   __shared__ uint32_t ws[32];
   __shared__ uint32_t s_choff[kPlanTile + 1];  // first chunk of each subgrid
   __shared__ uint32_t s_pkoff[kPlanTile + 1];  // first packet of each subgrid
@@ -561,20 +585,16 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan_fused(uint32_t *hist, uin
     s_pkoff[kPlanTile] = tpk;
   }
   __syncthreads();
-  // every thread writes chunks; the subgrid of chunk q by binary search
-  for (uint32_t q = threadIdx.x; q < tch; q += kPlanThreads) {
-    int lo = 0, hi = kPlanTile - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (s_choff[mid] <= q) lo = mid; else hi = mid - 1;
+  if (tch <= kPlanChunksInBlock) {
+    // few chunks: every thread writes some
+    for (uint32_t q = threadIdx.x; q < tch; q += kPlanThreads)
+      chunks[q] = plan_chunk(s_choff, s_pkoff, q, chunk);
+  } else {
+    // many chunks: the offsets go to k_plan_chunks
+    for (int i = threadIdx.x; i <= kPlanTile; i += kPlanThreads) {
+      choff_out[i] = s_choff[i];
+      pkoff_out[i] = s_pkoff[i];
     }
-    const uint32_t j = q - s_choff[lo];
-    Chunk cc;
-    cc.subgrid = (uint32_t)lo;
-    cc.begin = s_pkoff[lo] + j * chunk;
-    cc.count = min(chunk, (s_pkoff[lo + 1] - s_pkoff[lo]) - j * chunk);
-    cc.rem = (s_choff[lo + 1] - s_choff[lo]) - j;
-    chunks[q] = cc;
   }
   if (threadIdx.x == 0) {
     st->total_in = tpk;
@@ -583,6 +603,25 @@ __global__ void __launch_bounds__(kPlanThreads) k_plan_fused(uint32_t *hist, uin
     st->arena_count = 0;
     if (tpk > 0) st->rounds_active += 1;
   }
+}
+
+// Chunk list of a round with many chunks (after k_plan_fused), written by
+// the whole GPU: each block copies the per-subgrid offsets to shared memory
+// and writes chunks q in a grid-stride loop.
+__global__ void __launch_bounds__(256) k_plan_chunks(const uint32_t *choff, const uint32_t *pkoff,
+                                                     uint32_t chunk, Chunk *chunks,
+                                                     const RoundState *st) {
+  __shared__ uint32_t s_choff[kPlanTile + 1];
+  __shared__ uint32_t s_pkoff[kPlanTile + 1];
+  const uint32_t tch = st->num_chunks;
+  if (tch <= kPlanChunksInBlock) return;  // written by k_plan_fused (whole block returns)
+  for (int i = threadIdx.x; i <= kPlanTile; i += blockDim.x) {
+    s_choff[i] = choff[i];
+    s_pkoff[i] = pkoff[i];
+  }
+  __syncthreads();
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < tch; q += gridDim.x * blockDim.x)
+    chunks[q] = plan_chunk(s_choff, s_pkoff, q, chunk);
 }
 
 template <class P>
