@@ -441,12 +441,13 @@ def train(net, feats, labels, ncell, epochs=10, batch=8, lr=2e-3, lr_final=2e-4,
 
 
 def generate_large_runs(net, seeds, iterations=24, average=6, ratio_factor=4, device=0,
-                        log=None):
+                        log=None, num_photon=100_000_000):
     """Runs of the large generator (256^3 as 16^3 subgrids of 16^3, sigma_ln =
-    1.5, 16 sources, 1e8 packets per iteration; problems.large_config), kept on
-    the device: raw features [N, cells, 3] (channel 2 from the grid coarser by
-    ``ratio_factor``) and labels log10 x_H [N, cells] of the long plain run
-    (``iterations`` from x_H = 1e-6, the last ``average`` averaged)."""
+    1.5, 16 sources; problems.large_config) with ``num_photon`` packets per
+    iteration, kept on the device: raw features [N, cells, 3] (channel 2 from
+    the grid coarser by ``ratio_factor``) and labels log10 x_H [N, cells] of the
+    long plain run (``iterations`` from x_H = 1e-6, the last ``average``
+    averaged)."""
     import torch
     from .engine import blocked_to_cube
     from .problems import large_config
@@ -454,7 +455,7 @@ def generate_large_runs(net, seeds, iterations=24, average=6, ratio_factor=4, de
     feats, labels, grids = None, None, []
     t0 = time.perf_counter()
     for i, sd in enumerate(seeds):
-        g, nH = large_config(seed=int(sd))
+        g, nH = large_config(seed=int(sd), num_photon=int(num_photon))
         ncell = int(np.prod(g.ncell))
         if feats is None:
             feats = torch.empty((len(seeds), ncell, NUM_FEATURES), dtype=torch.float32,
