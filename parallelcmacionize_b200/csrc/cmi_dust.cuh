@@ -135,6 +135,11 @@ struct DustParams {
   unsigned long long *counters;  // [crossings, transits, walk-bound hits]
 };
 
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+  return v;
+}
+
 // 1. source packets: TAU type, weight 1, cross section 1, depth 0
 __global__ void k_dust_emit(DustParams p, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -211,9 +216,14 @@ __global__ void __launch_bounds__(128) k_dust_walk(DustParams p) {
     p.sub[i] = s;
     p.status[i] = result;
   }
-  if (cross) atomicAdd(&p.counters[0], cross);
-  if (trans) atomicAdd(&p.counters[1], trans);
-  if (bound_hits) atomicAdd(&p.counters[2], bound_hits);
+  // one atomic per warp and counter (every lane of the warp gets here)
+  const unsigned long long wc = warp_sum64(cross), wt = warp_sum64(trans),
+                           wb = warp_sum64(bound_hits);
+  if ((threadIdx.x & 31) == 0) {
+    if (wc) atomicAdd(&p.counters[0], wc);
+    if (wt) atomicAdd(&p.counters[1], wt);
+    if (wb) atomicAdd(&p.counters[2], wb);
+  }
 }
 
 // 2. relaunch of the TAU packets as DIRECT packets with forced scattering
@@ -255,12 +265,12 @@ __global__ void k_dust_scatter(DustScatterParams p) {
   for (uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < n;
        b += gridDim.x * blockDim.x) {
     const uint32_t i = b + (uint32_t)lane;
-    bool scatter = false;
+    bool scatter = false, escaped = false, dropped = false;
     Packet64 q{};
     uint32_t g = 0;
     if (i < n) {
       const int32_t st = p.status[i];
-      if (st == kDustEscaped) atomicAdd(&p.counters[4], 1ull);
+      escaped = st == kDustEscaped;
       if (st == kDustAbsorbed) {
         q = p.pk[i];
         g = p.gen[i] + 1u;
@@ -276,9 +286,15 @@ __global__ void k_dust_scatter(DustScatterParams p) {
           q.type = kDustDirect;
           q.meta = 0u;
         } else {
-          atomicAdd(&p.counters[3], 1ull);
+          dropped = true;
         }
       }
+    }
+    const unsigned me = __ballot_sync(0xFFFFFFFFu, escaped);
+    const unsigned md = __ballot_sync(0xFFFFFFFFu, dropped);
+    if (lane == 0) {
+      if (me) atomicAdd(&p.counters[4], (unsigned long long)__popc(me));
+      if (md) atomicAdd(&p.counters[3], (unsigned long long)__popc(md));
     }
     const unsigned m = __ballot_sync(0xFFFFFFFFu, scatter);
     const int leader = m ? __ffs(m) - 1 : 0;
