@@ -244,6 +244,16 @@ class DensitySubGrid {
     return out;
   }
 
+  // DensitySubGrid.hpp:1333-1472 (interact without the J tally) and :1482-1604
+  // (the optical depth of the crossing added to the photon's target depth), on
+  // the GPU; the dust driver's per-photon calls
+  int propagate(Photon &photon, int input_direction) {
+    return walk(photon, input_direction, CMI_WALK_PROPAGATE);
+  }
+  int compute_optical_depth(Photon &photon, int input_direction) {
+    return walk(photon, input_direction, CMI_WALK_OPTICAL_DEPTH);
+  }
+
   // DensitySubGrid.hpp:1628-1658, this subgrid only
   void compute_neutral_fraction(double luminosity, unsigned int num_photon) {
     _grid->push();
@@ -282,6 +292,15 @@ class DensitySubGrid {
 
   unsigned int index() const { return _index; }
   DensityGrid *grid() { return _grid; }
+
+ private:
+  int walk(Photon &photon, int input_direction, int mode) {
+    _grid->push();
+    const int32_t in_dir = input_direction;
+    int32_t out = -1;
+    cmi_check(cmi_walk_photons(_grid->context(), 0, _index, mode, photon.raw(), &in_dir, 1, &out));
+    return out;
+  }
 };
 
 // The reference driver's result files (testDensitySubGrid_omp.cpp:394-521):

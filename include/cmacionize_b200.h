@@ -321,6 +321,23 @@ int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
  * per-thread generators.  albedo in [0, 1); num_photon <= 2^30.  The packet
  * buffers (about 290 bytes per packet) grow to the largest call and stay with
  * the context until cmi_destroy. */
+/* The dust driver's per-buffer walks through one subgrid (do_photon_traversal,
+ * testDensitySubGrid_omp_dust.cpp:646-652), FP64 with the reference's
+ * arithmetic, on the instance's current fields:
+ *   CMI_WALK_PROPAGATE      DensitySubGrid::propagate (DensitySubGrid.hpp:
+ *                           1333-1472): interact without the J tally
+ *   CMI_WALK_OPTICAL_DEPTH  DensitySubGrid::compute_optical_depth (:1482-1604):
+ *                           no target; the crossing's optical depth is added
+ *                           to target_optical_depth
+ * photons (host, n) are updated in place; output_directions[i] receives the
+ * TravelDirection photon i leaves by (TRAVELDIRECTION_INSIDE: it reached its
+ * target).  input_directions: one per photon. */
+#define CMI_WALK_PROPAGATE 1
+#define CMI_WALK_OPTICAL_DEPTH 2
+int cmi_walk_photons(cmi_context *ctx, int32_t instance, uint32_t subgrid, int32_t mode,
+                     cmi_photon *photons, const int32_t *input_directions, uint32_t n,
+                     int32_t *output_directions);
+
 typedef struct cmi_dust_stats {
   uint64_t emitted;            /* source packets */
   uint64_t scatterings;        /* scattered packets (= peel-off packets) */

@@ -340,4 +340,49 @@ __global__ void k_dust_image(const Packet64 *pk, const int32_t *status, const ui
   }
 }
 
+// DensitySubGrid::propagate / compute_optical_depth of single photons through
+// one subgrid (the per-buffer calls of the dust driver's do_photon_traversal,
+// :646-652): out_dir = the TravelDirection the photon leaves by (INSIDE: it
+// reached its target depth), -1 if the walk bound was hit.
+template <int kMode>
+__global__ void __launch_bounds__(128) k_walk_photons(const DevSubgrid *subs, uint32_t sub,
+                                                       const double *nH, const double *xH,
+                                                       DirectionTables tables, Packet64 *pk,
+                                                       const int32_t *in_dir, uint32_t n,
+                                                       int32_t *out_dir) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DevSubgrid &S = subs[sub];
+  View64 v;
+  v.nH = nH + S.field_offset;
+  v.xH = xH + S.field_offset;
+  v.J = nullptr;
+  for (int a = 0; a < 3; ++a) {
+    v.n[a] = S.ncell[a];
+    v.anchor[a] = S.anchor[a];
+    v.cs[a] = S.cell_size[a];
+    v.inv_cs[a] = S.inv_cell_size[a];
+  }
+  v.nyz = S.ncell[1] * S.ncell[2];
+  Packet64 q = pk[i];
+  const uint32_t meta0 = q.meta;
+  q.meta = (uint32_t)in_dir[i];
+  Walk64 w;
+  int st = (kMode == kDepth) ? w.begin_depth(q, v, tables.sign_code)
+                             : w.begin(q, v, tables.sign_code);
+  const int limit = S.ncell[0] + S.ncell[1] + S.ncell[2] + 3;
+  while (st == kRun && w.steps <= limit) st = w.step<kMode>(v);
+  int32_t res = -1;
+  if (st == kAbsorbed) {
+    res = 0;  // TRAVELDIRECTION_INSIDE
+  } else if (st == kExited) {
+    const int od = tables.mask_dir[w.exit_mask(v)];
+    res = od < kNumDirections ? od : -1;
+  }
+  Packet64 r = w.packet(v, meta0);
+  if (kMode == kDepth) r.tau = w.tau_target + w.tau_done;
+  pk[i] = r;
+  out_dir[i] = res;
+}
+
 }  // namespace cmi

@@ -1521,6 +1521,54 @@ unsigned dust_blocks(uint64_t n, int threads) {
 
 }  // namespace
 
+extern "C" int cmi_walk_photons(cmi_context *c, int32_t instance, uint32_t subgrid,
+                                int32_t mode, cmi_photon *photons,
+                                const int32_t *input_directions, uint32_t n,
+                                int32_t *output_directions) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  const HostInstance &I = c->inst[instance];
+  if (subgrid >= I.nsub)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "subgrid %u out of range [0, %u)", subgrid, I.nsub);
+  if (mode != CMI_WALK_PROPAGATE && mode != CMI_WALK_OPTICAL_DEPTH)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "mode must be CMI_WALK_PROPAGATE or "
+                                          "CMI_WALK_OPTICAL_DEPTH");
+  if (n == 0) return CMI_OK;
+  if (!photons || !input_directions || !output_directions)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  for (uint32_t i = 0; i < n; ++i)
+    if (input_directions[i] < 0 || input_directions[i] >= kNumDirections)
+      return fail(CMI_ERR_INVALID_ARGUMENT, "input direction %d out of range",
+                  input_directions[i]);
+  const size_t pk_bytes = (sizeof(Packet64) * (size_t)n + 255) & ~(size_t)255;
+  CMI_TRY(ensure_stage(c, pk_bytes + 2 * sizeof(int32_t) * (size_t)n + 256));
+  char *base = reinterpret_cast<char *>(c->d_stage);
+  Packet64 *d_pk = reinterpret_cast<Packet64 *>(base);
+  int32_t *d_in = reinterpret_cast<int32_t *>(base + pk_bytes);
+  int32_t *d_out = d_in + n;
+  CMI_CUDA(cudaMemcpyAsync(d_pk, photons, sizeof(Packet64) * n, cudaMemcpyHostToDevice,
+                           c->stream));
+  CMI_CUDA(cudaMemcpyAsync(d_in, input_directions, sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                           c->stream));
+  const unsigned grid = (n + 127) / 128;
+  if (mode == CMI_WALK_PROPAGATE)
+    k_walk_photons<kPropagate><<<grid, 128, 0, c->stream>>>(
+        c->d_sub, I.first_sub + subgrid, c->d_nH, c->d_xH, c->tables, d_pk, d_in, n, d_out);
+  else
+    k_walk_photons<kDepth><<<grid, 128, 0, c->stream>>>(
+        c->d_sub, I.first_sub + subgrid, c->d_nH, c->d_xH, c->tables, d_pk, d_in, n, d_out);
+  CMI_CUDA(cudaGetLastError());
+  CMI_CUDA(cudaMemcpyAsync(photons, d_pk, sizeof(Packet64) * n, cudaMemcpyDeviceToHost,
+                           c->stream));
+  CMI_CUDA(cudaMemcpyAsync(output_directions, d_out, sizeof(int32_t) * n,
+                           cudaMemcpyDeviceToHost, c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  for (uint32_t i = 0; i < n; ++i)
+    if (output_directions[i] < 0)
+      return fail(CMI_ERR_INVARIANT, "photon %u: walk step bound exceeded", i);
+  return CMI_OK;
+}
+
 extern "C" int cmi_dust_run(cmi_context *c, int32_t instance, uint64_t num_photon, uint64_t seed,
                             uint32_t iteration, double albedo, const double source[3],
                             int32_t npix_x, int32_t npix_y, double *image,

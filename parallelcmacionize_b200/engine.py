@@ -205,6 +205,19 @@ class TransportEngine:
                  for it in range(done.value)]
         return stats, list(at)
 
+    def walk_photons(self, instance, subgrid, photons, input_directions, depth=False):
+        """DensitySubGrid::propagate (or, with depth, compute_optical_depth) of
+        each photon (PHOTON_DTYPE records, copied) through one subgrid.
+        Returns (photons out, output TravelDirections)."""
+        ph = np.ascontiguousarray(photons, dtype=PHOTON_DTYPE).copy()
+        dirs = np.ascontiguousarray(np.broadcast_to(input_directions, ph.shape), dtype=np.int32)
+        out = np.zeros(ph.size, dtype=np.int32)
+        mode = _lib.WALK_OPTICAL_DEPTH if depth else _lib.WALK_PROPAGATE
+        check(self._L.cmi_walk_photons(self._h, int(instance), int(subgrid), mode,
+                                       ph.ctypes.data, dirs.ctypes.data, ph.size,
+                                       out.ctypes.data))
+        return ph, out
+
     def dust_image(self, instance, num_photon, albedo, source=(0.0, 0.0, 0.0), npix=(101, 101),
                    seed=42, iteration=0):
         """The reference dust driver's photon loop on this instance's n_H and x_H
