@@ -43,6 +43,7 @@ def test_struct_layouts_match_header():
     assert C.sizeof(_lib.Options) == 16 * 4
     assert C.sizeof(_lib.Stats) == 6 * 8 + 2 * 4 + 8
     assert _lib.PHOTON_DTYPE.itemsize == 80
+    assert C.sizeof(_lib.DustStats) == 7 * 8 + 2 * 4
 
 
 def test_null_arguments_fail_cleanly():
@@ -51,3 +52,6 @@ def test_null_arguments_fail_cleanly():
     assert L.cmi_synchronize(None) == _lib.ERR_INVALID_ARGUMENT
     assert b"null" in L.cmi_last_error_string()
     assert L.cmi_destroy(None) == _lib.OK
+    assert L.cmi_dust_run(None, 0, 10, 1, 0, 0.5, None, 4, 4, None, None) == \
+        _lib.ERR_INVALID_ARGUMENT
+    assert L.cmi_walk_photons(None, 0, 0, 1, None, None, 1, None) == _lib.ERR_INVALID_ARGUMENT
