@@ -154,6 +154,18 @@ int cmi_destroy(cmi_context *context);
 /* Copy n_H (m^-3) and/or x_H into an instance; either pointer may be NULL. */
 int cmi_set_fields(cmi_context *context, int32_t instance, int32_t layout, int32_t memory,
                    const double *number_density, const double *neutral_fraction);
+/* Overlapped input for callers that send fields every iteration: the n_H
+ * copy from pinned host memory runs on a side stream, so it can proceed while
+ * the previous iteration's x_H comes back (cmi_get_fields), and
+ * cmi_set_fields_prefetched then takes it together with x_H (host or device,
+ * `memory`) in the prefetch's layout.  The host array must stay unchanged
+ * until cmi_set_fields_prefetched returns; one prefetch per instance may be
+ * pending.  No reference counterpart (the reference keeps its fields in host
+ * memory). */
+int cmi_prefetch_number_density(cmi_context *ctx, int32_t instance, int32_t layout,
+                                const double *nH);
+int cmi_set_fields_prefetched(cmi_context *ctx, int32_t instance, int32_t memory,
+                              const double *xH);
 /* Read x_H and/or the intensity integral J (m^3); either pointer may be NULL. */
 int cmi_get_fields(cmi_context *context, int32_t instance, int32_t layout, int32_t memory,
                    double *neutral_fraction, double *intensity_integral);

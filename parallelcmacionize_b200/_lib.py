@@ -47,6 +47,7 @@ EXPORTED = [
     "cmi_destroy", "cmi_set_fields", "cmi_get_fields", "cmi_set_intensity", "cmi_set_sources",
     "cmi_set_packet_budget", "cmi_set_reemission_probability", "cmi_run_iterations",
     "cmi_run_until_converged", "cmi_dust_run", "cmi_walk_photons",
+    "cmi_prefetch_number_density", "cmi_set_fields_prefetched",
     "cmi_shoot_packets",
     "cmi_transport_packets", "cmi_traverse_buffer", "cmi_trace_packet",
     "cmi_compute_neutral_fraction", "cmi_device_field", "cmi_get_stream", "cmi_synchronize",
@@ -181,6 +182,8 @@ def load():
     L.cmi_run_until_converged.argtypes = [ctx, i32, i32, d, u64, vp, vp, vp]
     L.cmi_dust_run.argtypes = [ctx, i32, u64, u64, u32, d, vp, i32, i32, vp, vp]
     L.cmi_walk_photons.argtypes = [ctx, i32, u32, i32, vp, vp, u32, vp]
+    L.cmi_prefetch_number_density.argtypes = [ctx, i32, i32, vp]
+    L.cmi_set_fields_prefetched.argtypes = [ctx, i32, i32, vp]
     L.cmi_shoot_packets.argtypes = [ctx, u64, u32, vp]
     L.cmi_transport_packets.argtypes = [ctx, i32, vp, vp, u64, vp]
     L.cmi_traverse_buffer.argtypes = [ctx, i32, u32, i32, vp, u32, vp, vp, vp, vp]

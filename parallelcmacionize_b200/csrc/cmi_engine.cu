@@ -153,6 +153,13 @@ struct cmi_context {
   std::vector<Timed> timed;
   std::vector<cudaEvent_t> event_pool;
 
+  // cmi_prefetch_number_density: n_H copied on a side stream into its own
+  // staging (the padded layout's offsets), one event per instance
+  cudaStream_t copy_stream = nullptr;
+  double *d_nh_stage = nullptr;
+  std::vector<cudaEvent_t> nh_event;
+  std::vector<int32_t> nh_layout;  // -1: nothing prefetched for the instance
+
   // cmi_dust_run's packet buffers, grown to the largest call and kept
   DustBuffers *dust = nullptr;
   uint64_t dust_capacity = 0;  // packets
@@ -975,6 +982,9 @@ int cmi_destroy(cmi_context *c) {
     cudaEventDestroy(t.stop);
   }
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->nh_event) cudaEventDestroy(e);
+  dev_free(c->d_nh_stage);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->body_stream) cudaStreamDestroy(c->body_stream);
   delete c;
@@ -1039,6 +1049,50 @@ int cmi_set_fields(cmi_context *c, int32_t instance, int32_t layout, int32_t mem
   CMI_TRY(check_instance(c, instance));
   CMI_TRY(check_layout(layout, memory));
   if (nH) CMI_TRY(copy_field_in(c, instance, layout, memory, nH, c->d_nH));
+  if (xH) CMI_TRY(copy_field_in(c, instance, layout, memory, xH, c->d_xH));
+  CMI_TRY(refresh_kappa(c, instance));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return CMI_OK;
+}
+
+int cmi_prefetch_number_density(cmi_context *c, int32_t instance, int32_t layout,
+                                const double *nH) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  CMI_TRY(check_layout(layout, CMI_MEMORY_HOST));
+  if (!nH) return fail(CMI_ERR_INVALID_ARGUMENT, "null density array");
+  if (!c->copy_stream) {
+    CMI_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    CMI_TRY(dev_alloc(&c->d_nh_stage, (size_t)c->total_padded));
+    c->nh_event.assign(c->inst.size(), nullptr);
+    c->nh_layout.assign(c->inst.size(), -1);
+    for (auto &e : c->nh_event) CMI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  if (c->nh_layout[instance] >= 0)
+    return fail(CMI_ERR_INVALID_ARGUMENT,
+                "instance %d: a prefetched density has not been consumed yet", instance);
+  const HostInstance &I = c->inst[instance];
+  CMI_CUDA(cudaMemcpyAsync(c->d_nh_stage + I.first_cell, nH, sizeof(double) * I.ncells,
+                           cudaMemcpyHostToDevice, c->copy_stream));
+  CMI_CUDA(cudaEventRecord(c->nh_event[instance], c->copy_stream));
+  c->nh_layout[instance] = layout;
+  return CMI_OK;
+}
+
+int cmi_set_fields_prefetched(cmi_context *c, int32_t instance, int32_t memory,
+                              const double *xH) {
+  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_instance(c, instance));
+  if (c->nh_layout.empty() || c->nh_layout[instance] < 0)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "instance %d: no prefetched density", instance);
+  const int32_t layout = c->nh_layout[instance];
+  CMI_TRY(check_layout(layout, memory));
+  const HostInstance &I = c->inst[instance];
+  // n_H: the staged copy, once it has landed
+  CMI_CUDA(cudaStreamWaitEvent(c->stream, c->nh_event[instance], 0));
+  CMI_TRY(copy_field_in(c, instance, layout, CMI_MEMORY_DEVICE, c->d_nh_stage + I.first_cell,
+                        c->d_nH));
+  c->nh_layout[instance] = -1;
   if (xH) CMI_TRY(copy_field_in(c, instance, layout, memory, xH, c->d_xH));
   CMI_TRY(refresh_kappa(c, instance));
   CMI_CUDA(cudaStreamSynchronize(c->stream));

@@ -148,6 +148,27 @@ class TransportEngine:
                 raise ValueError("field size does not match the grid")
         check(self._L.cmi_set_fields(self._h, instance, lay, _lib.MEMORY_HOST, ptr(n), ptr(x)))
 
+    def prefetch_number_density(self, instance, number_density, layout="blocked"):
+        """Start copying n_H (a pinned host array, left unchanged until
+        set_fields_prefetched returns) on a side stream."""
+        lay = {"blocked": _lib.LAYOUT_BLOCKED, "cube": _lib.LAYOUT_CUBE}[layout]
+        n = np.asarray(number_density)
+        if n.dtype != np.float64 or not n.flags.c_contiguous or \
+                n.size != self.grids[instance].num_cells:
+            raise ValueError("n_H must be a contiguous float64 array of the grid's size")
+        self._prefetched = getattr(self, "_prefetched", {})
+        self._prefetched[instance] = n  # keep the array alive until it is consumed
+        check(self._L.cmi_prefetch_number_density(self._h, instance, lay, ptr(n)))
+
+    def set_fields_prefetched(self, instance, neutral_fraction=None):
+        """n_H from the last prefetch of the instance, x_H from the host."""
+        x = None if neutral_fraction is None else np.ascontiguousarray(neutral_fraction,
+                                                                       np.float64)
+        if x is not None and x.size != self.grids[instance].num_cells:
+            raise ValueError("field size does not match the grid")
+        check(self._L.cmi_set_fields_prefetched(self._h, instance, _lib.MEMORY_HOST, ptr(x)))
+        getattr(self, "_prefetched", {}).pop(instance, None)
+
     def set_fields_device(self, instance, number_density_ptr=0, neutral_fraction_ptr=0,
                           layout="blocked"):
         lay = {"blocked": _lib.LAYOUT_BLOCKED, "cube": _lib.LAYOUT_CUBE}[layout]

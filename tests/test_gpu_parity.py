@@ -445,3 +445,28 @@ def test_result_files_from_the_engine(tmp_path):
     _, _, Rs = stromgren_profile()
     r, prof = radial_profile(rec, bins=16, r_max=1.5 * Rs)
     assert np.nanmax(prof[r < 0.7 * Rs]) < 0.1 and np.nanmin(prof[r > 1.3 * Rs]) > 0.5
+
+
+def test_prefetched_density_equals_set_fields():
+    """cmi_prefetch_number_density + cmi_set_fields_prefetched load the same
+    fields as cmi_set_fields: one iteration from them gives the same x_H."""
+    import torch
+    spec, nH = lognormal_config(ncell=32, num_subgrid=2, num_photon=50_000, num_sources=2)
+    x0 = np.full(nH.size, 1e-3)
+    res = []
+    for prefetch in (False, True):
+        eng = TransportEngine(spec)
+        if prefetch:
+            pin = torch.from_numpy(nH.copy()).pin_memory()
+            eng.prefetch_number_density(0, pin.numpy())
+            with pytest.raises(CMIError):  # one pending prefetch per instance
+                eng.prefetch_number_density(0, pin.numpy())
+            eng.set_fields_prefetched(0, x0)
+            with pytest.raises(CMIError):  # consumed
+                eng.set_fields_prefetched(0, x0)
+        else:
+            eng.set_fields(0, nH, x0)
+        eng.run_iterations(1, seed=3)
+        res.append(eng.get_fields(0, intensity=False)[0])
+        eng.close()
+    assert np.array_equal(res[0], res[1])
