@@ -449,11 +449,14 @@ def test_result_files_from_the_engine(tmp_path):
 
 def test_prefetched_density_equals_set_fields():
     """cmi_prefetch_number_density + cmi_set_fields_prefetched load the same
-    fields as cmi_set_fields: one iteration from them gives the same x_H."""
+    n_H (the device array, bit for bit) as cmi_set_fields, twice in a row, and
+    an iteration from them gives the same x_H (FP64 tally merges in another
+    order: within 1e-12)."""
     import torch
+    from parallelcmacionize_b200.distributed import _CudaArray
     spec, nH = lognormal_config(ncell=32, num_subgrid=2, num_photon=50_000, num_sources=2)
     x0 = np.full(nH.size, 1e-3)
-    res = []
+    res, dev_n = [], []
     for prefetch in (False, True):
         eng = TransportEngine(spec)
         if prefetch:
@@ -464,9 +467,18 @@ def test_prefetched_density_equals_set_fields():
             eng.set_fields_prefetched(0, x0)
             with pytest.raises(CMIError):  # consumed
                 eng.set_fields_prefetched(0, x0)
+            # a second round with another density, then the first again
+            pin2 = torch.from_numpy(nH * 2.0).pin_memory()
+            eng.prefetch_number_density(0, pin2.numpy())
+            eng.set_fields_prefetched(0, x0)
+            eng.prefetch_number_density(0, pin.numpy())
+            eng.set_fields_prefetched(0, x0)
         else:
             eng.set_fields(0, nH, x0)
+        ptr, count = eng.device_field(0, "n")
+        dev_n.append(torch.as_tensor(_CudaArray(ptr, count), device="cuda").cpu().numpy())
         eng.run_iterations(1, seed=3)
         res.append(eng.get_fields(0, intensity=False)[0])
         eng.close()
-    assert np.array_equal(res[0], res[1])
+    assert np.array_equal(dev_n[0], dev_n[1])
+    np.testing.assert_allclose(res[1], res[0], rtol=1e-12, atol=0)
