@@ -947,6 +947,7 @@ int cmi_destroy(cmi_context *c) {
   if (!c) return CMI_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);  // a prefetch in flight
   free_graph(c);
   dev_free(c->d_sub);
   dev_free(c->d_inst);
