@@ -346,9 +346,14 @@ int launch_plan(cmi_context *c, bool scatter) {
     k_plan_fused<<<1, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk, c->d_bucket_off,
                                                     c->d_chunks, c->d_state, c->d_plan_choff,
                                                     c->d_plan_pkoff);
-    k_plan_chunks<<<c->num_sms * 2, 256, 0, c->stream>>>(c->d_plan_choff, c->d_plan_pkoff,
-                                                         c->chunk, c->d_chunks, c->d_state);
-    c->enqueued += 2;
+    c->enqueued += 1;
+    // a round has at most capacity / chunk + S chunks; below the in-block
+    // limit k_plan_fused writes every list itself and the launch is left out
+    if (c->capacity / c->chunk + c->S + 1 > kPlanChunksInBlock) {
+      k_plan_chunks<<<c->num_sms * 2, 256, 0, c->stream>>>(c->d_plan_choff, c->d_plan_pkoff,
+                                                           c->chunk, c->d_chunks, c->d_state);
+      c->enqueued += 1;
+    }
   } else {
     k_plan_count<<<c->ntiles, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk,
                                                             c->d_tile_pk, c->d_tile_ch);

@@ -543,8 +543,9 @@ __device__ __forceinline__ Chunk plan_chunk(const uint32_t *choff, const uint32_
 }
 
 // Rounds with more chunks than this have their chunk list written by
-// k_plan_chunks across the GPU instead of by the plan's single block.
-constexpr uint32_t kPlanChunksInBlock = 8192;
+// k_plan_chunks across the GPU instead of by the plan's single block (16 per
+// thread cost about as much as the extra launch).
+constexpr uint32_t kPlanChunksInBlock = 16384;
 
 __global__ void __launch_bounds__(kPlanThreads) k_plan_fused(uint32_t *hist, uint32_t S,
                                                              uint32_t chunk,
