@@ -341,7 +341,10 @@ int refresh_kappa(cmi_context *c, int32_t i) {
 // ---------------------------------------------------------------------------
 // Plan of a round from the bucket histogram; with scatter, the packets the
 // previous step appended are moved into their buckets.
-int launch_plan(cmi_context *c, bool scatter) {
+// gate: inside the captured round loop, the scatter also sets the loop's
+// condition (handle h)
+int launch_plan(cmi_context *c, bool scatter, bool gate = false,
+                cudaGraphConditionalHandle h = 0) {
   if (c->ntiles == 1) {
     k_plan_fused<<<1, kPlanThreads, 0, c->stream>>>(c->d_hist, c->S, c->chunk, c->d_bucket_off,
                                                     c->d_chunks, c->d_state, c->d_plan_choff,
@@ -370,11 +373,13 @@ int launch_plan(cmi_context *c, bool scatter) {
     if (c->fp32()) {
       k_scatter<Packet32><<<grid, 256, 0, c->stream>>>(
           (const Packet32 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
-          (Packet32 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
+          (Packet32 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity, gate, h,
+          (uint32_t)c->round_cap);
     } else {
       k_scatter<Packet64><<<grid, 256, 0, c->stream>>>(
           (const Packet64 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
-          (Packet64 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity);
+          (Packet64 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity, gate, h,
+          (uint32_t)c->round_cap);
     }
     c->enqueued += 1;
   }
@@ -544,8 +549,9 @@ int enqueue_rounds(cmi_context *c) {
 }
 
 // The rounds inside a captured iteration: a WHILE conditional node runs
-// (walk -> plan -> gate) while packets remain, so an iteration stops after the
-// rounds it needs instead of the worst-case count (k_round_gate).
+// (walk -> plan -> scatter, whose first thread sets the condition) while
+// packets remain, so an iteration stops after the rounds it needs instead of
+// the worst-case count.  k_round_gate decides whether the first round runs.
 int enqueue_rounds_graph(cmi_context *c) {
   cudaStreamCaptureStatus cs;
   cudaGraph_t g = nullptr;
@@ -576,12 +582,7 @@ int enqueue_rounds_graph(cmi_context *c) {
   const uint64_t before = c->enqueued;
   c->stream = c->body_stream;
   int rc = launch_walk(c);
-  if (rc == CMI_OK) rc = launch_plan(c, true);
-  if (rc == CMI_OK) {
-    k_round_gate<<<1, 32, 0, c->stream>>>(c->d_state, h, (uint32_t)c->round_cap);
-    c->enqueued += 1;
-    if (cudaGetLastError() != cudaSuccess) rc = fail(CMI_ERR_CUDA, "round gate launch");
-  }
+  if (rc == CMI_OK) rc = launch_plan(c, true, true, h);
   c->stream = outer;
   cudaGraph_t captured = nullptr;
   const cudaError_t ee = cudaStreamEndCapture(c->body_stream, &captured);

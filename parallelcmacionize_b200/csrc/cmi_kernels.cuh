@@ -625,11 +625,21 @@ __global__ void __launch_bounds__(256) k_plan_chunks(const uint32_t *choff, cons
     chunks[q] = plan_chunk(s_choff, s_pkoff, q, chunk);
 }
 
+// Scatter of the round's packets into their buckets.  Inside the captured
+// round loop it also decides whether another round follows (gate: the plan
+// before it has set num_chunks), which saves the loop a separate launch.
 template <class P>
 __global__ void __launch_bounds__(256) k_scatter(const P *out, const uint32_t *keys,
                                                  const uint32_t *ranks,
                                                  const uint32_t *bucket_off, P *in,
-                                                 const RoundState *st, uint32_t capacity) {
+                                                 RoundState *st, uint32_t capacity,
+                                                 bool gate, cudaGraphConditionalHandle h,
+                                                 uint32_t max_rounds) {
+  if (gate && blockIdx.x == 0 && threadIdx.x == 0) {
+    const bool more = st->num_chunks > 0u && st->round_index < max_rounds;
+    if (more) st->round_index += 1u;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+  }
   const uint32_t n = min(st->total_in, capacity);
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
