@@ -230,7 +230,11 @@ class ClockSampler:
         self.dev = device_index
         self.proc = None
         self.window = None  # (start, end) of the timed region, host clock
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        # the samples go to CMI_CLOCKS_DIR when set (to keep them), else to a
+        # temporary directory
+        import tempfile
+        out = os.environ.get("CMI_CLOCKS_DIR") or tempfile.mkdtemp(prefix="cmi_clocks_")
+        self.path = os.path.join(out, f"clocks_rank{device_index}.csv")
 
     def __enter__(self):
         try:
