@@ -22,6 +22,7 @@
 
 #include "cmacionize/DensityGrid.hpp"
 #include "cmacionize/Parameters.hpp"
+#include "cmacionize/RandomDensity.hpp"
 #include "cmacionize/RandomGenerator.hpp"
 
 int main(int argc, char **argv) {
@@ -43,37 +44,18 @@ int main(int argc, char **argv) {
     RandomGenerator rng(42 + threads);
 
     if (p.random_density) {
-      // 10-mode cosine field, testDensitySubGrid_omp.cpp:1881-1936
-      const unsigned int nk = 10;
-      std::vector<double> k(3 * nk), phase(3 * nk);
-      for (unsigned int i = 0; i < nk; ++i) {
-        double u[4];
-        for (double &x : u) x = rng.get_uniform_random_double();
-        const double kx = std::sqrt(-2. * std::log(u[0])) * std::cos(2. * M_PI * u[1]);
-        const double ky = std::sqrt(-2. * std::log(u[0])) * std::sin(2. * M_PI * u[1]);
-        const double kz = std::sqrt(-2. * std::log(u[2])) * std::cos(2. * M_PI * u[3]);
-        k[3 * i] = 4. * M_PI * kx / p.box[3];
-        k[3 * i + 1] = 4. * M_PI * ky / p.box[4];
-        k[3 * i + 2] = 4. * M_PI * kz / p.box[5];
-        for (int a = 0; a < 3; ++a) phase[3 * i + a] = 2. * M_PI * rng.get_uniform_random_double();
-      }
+      // 10-mode cosine field, testDensitySubGrid_omp.cpp:1880-1934
+      const CosineDensityField field(rng, p.box);
+      const int *n = grid.subgrid_cells();
       for (unsigned int s = 0; s < grid.number_of_subgrids(); ++s) {
         DensitySubGrid sg = grid.subgrid(s);
         double box[6];
         sg.get_grid_box(box);
-        const int *n = grid.subgrid_cells();
         for (unsigned int c = 0; c < sg.get_number_of_cells(); ++c) {
           const int i3[3] = {(int)(c / (n[1] * n[2])), (int)((c / n[2]) % n[1]), (int)(c % n[2])};
           double mid[3];
-          for (int a = 0; a < 3; ++a) mid[a] = box[a] + (i3[a] + 0.5) * (box[3 + a] / n[a]);
-          double nd = 0.;
-          for (unsigned int q = 0; q < nk; ++q) {
-            nd += 1.e8 * (std::cos(k[3 * q] * mid[0] + phase[3 * q]) *
-                              std::cos(k[3 * q + 1] * mid[1] + phase[3 * q + 1]) *
-                              std::cos(k[3 * q + 2] * mid[2] + phase[3 * q + 2]) +
-                          1.);
-          }
-          sg.set_number_density(c, nd / nk);
+          CosineDensityField::cell_midpoint(box, n, i3, mid);
+          sg.set_number_density(c, field(mid));
         }
       }
     }

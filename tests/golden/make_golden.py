@@ -24,6 +24,8 @@ inputs and stores inputs + reference outputs as compressed .npz files:
                    scattering, peel-off image) for a unit-density sphere of
                    radius 1 in a [-1, 1]^3 box, albedo 0.5, 1e6 packets; the
                    second iteration's image (x_H = 1 after the first balance)
+  outputs_random.npz  the same driver's files for its random density field
+                   (10 cosine modes), one thread
   outputs.npz      the result files of the reference's own driver
                    (oracle/_ref/testDensitySubGrid_omp_files, -DMM_FILE
                    -DBIN_FILE): neutral_fractions.dat and .bin of a small
@@ -329,10 +331,11 @@ OUTPUT_CASE = {"ncell": (16, 16, 8), "num_subgrid": (2, 2, 1),
                "num_photon": 20000, "iterations": 2}
 
 
-def gen_outputs():
+def _files_run(random_density=False, number_of_sources=1):
     """Runs the reference driver with its file output switched on in a
     temporary directory (params written here: the keys of
-    params_single_uniform.txt) and stores both files byte for byte."""
+    params_single_uniform.txt), one thread; returns the .dat bytes, the .bin
+    values and the params text."""
     import subprocess
     import tempfile
     b = O.ref_binary("testDensitySubGrid_omp_files")
@@ -345,7 +348,9 @@ def gen_outputs():
         "box:", f"  anchor: {pcs(c['anchor_pc'])}", f"  sides: {pcs(c['sides_pc'])}",
         f"ncell: {v(c['ncell'])}", f"num_photon: {c['num_photon']}",
         f"number_of_iterations: {c['iterations']}", "reemission_probability: 0.",
-        "number_of_sources: 1", "random_density: false", f"num_subgrid: {v(c['num_subgrid'])}",
+        f"number_of_sources: {number_of_sources}",
+        f"random_density: {'true' if random_density else 'false'}",
+        f"num_subgrid: {v(c['num_subgrid'])}",
         "queue_size_per_thread: 100", "memoryspace_size: 50000", "number_of_tasks: 500000",
         "MPI_buffer_size: 1000", "cost_copy_factor: 10", "edge_copy_factor: 0.01",
         "general_queue_size: 100000", ""])
@@ -356,9 +361,23 @@ def gen_outputs():
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         dat = np.fromfile(os.path.join(td, "neutral_fractions.dat"), dtype=np.uint8)
         binf = np.fromfile(os.path.join(td, "neutral_fractions.bin"), dtype=np.float64)
-    save("outputs.npz", dat=dat, bin=binf, ncell=np.array(c["ncell"]),
-         num_subgrid=np.array(c["num_subgrid"]), anchor_pc=np.array(c["anchor_pc"]),
-         sides_pc=np.array(c["sides_pc"]))
+    return dat, binf, params
+
+
+def gen_outputs():
+    """outputs.npz: uniform density; outputs_random.npz: the driver's random
+    density field (10 cosine modes), for the C++ surface's set-up of the same
+    run (seeded 42 + threads).  One source each: with several sources whose
+    packet counts are not multiples of the buffer size, the driver does not
+    finish (the emitted count differs from num_photon)."""
+    c = OUTPUT_CASE
+    geo = dict(ncell=np.array(c["ncell"]), num_subgrid=np.array(c["num_subgrid"]),
+               anchor_pc=np.array(c["anchor_pc"]), sides_pc=np.array(c["sides_pc"]))
+    dat, binf, _ = _files_run()
+    save("outputs.npz", dat=dat, bin=binf, **geo)
+    dat, binf, params = _files_run(random_density=True, number_of_sources=1)
+    save("outputs_random.npz", dat=dat, bin=binf, params=np.array(params), threads=np.array(1),
+         **geo)
 
 
 def main():

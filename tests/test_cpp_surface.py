@@ -68,6 +68,77 @@ def test_ranlxd_header_matches_reference_stream(tmp_path):
         assert np.array_equal(np.array([float.fromhex(x) for x in out]), ref)
 
 
+def _random_case():
+    from conftest import golden
+    g = golden("outputs_random.npz")
+    from parallelcmacionize_b200.outputs import DAT_RECORD
+    return g, g["dat"].view(DAT_RECORD)
+
+
+def test_random_density_header_matches_reference_files(tmp_path):
+    """CosineDensityField (the driver's random_density set-up) gives the n_H
+    the reference driver wrote to its .dat file, bit for bit, when seeded as
+    the reference seeds its host generator (42 + threads)."""
+    g, rec = _random_case()
+    pc = 3.086e16
+    box = [float(v) * pc for v in g["anchor_pc"]] + [float(v) * pc for v in g["sides_pc"]]
+    src = tmp_path / "d.cpp"
+    src.write_text(
+        '#include "cmacionize/RandomDensity.hpp"\n#include <cstdio>\n#include <cstdlib>\n'
+        "int main(int c, char **v) {\n"
+        "  double box[6]; for (int a = 0; a < 6; ++a) box[a] = strtod(v[1 + a], nullptr);\n"
+        "  int ns[3], n[3]; for (int a = 0; a < 3; ++a) { ns[a] = atoi(v[7 + a]);"
+        " n[a] = atoi(v[10 + a]) / ns[a]; }\n"
+        "  RandomGenerator rng(42 + atoi(v[13])); const CosineDensityField f(rng, box);\n"
+        "  for (int s = 0; s < ns[0] * ns[1] * ns[2]; ++s) {\n"
+        "    const int si[3] = {s / (ns[1] * ns[2]), (s / ns[2]) % ns[1], s % ns[2]};\n"
+        "    double sb[6]; for (int a = 0; a < 3; ++a) { sb[3 + a] = box[3 + a] / ns[a];"
+        " sb[a] = box[a] + si[a] * sb[3 + a]; }\n"
+        "    for (int q = 0; q < n[0] * n[1] * n[2]; ++q) {\n"
+        "      const int i3[3] = {q / (n[1] * n[2]), (q / n[2]) % n[1], q % n[2]};\n"
+        "      double m[3]; CosineDensityField::cell_midpoint(sb, n, i3, m);\n"
+        '      printf("%a %a %a %a\\n", m[0], m[1], m[2], f(m));\n'
+        "    }\n  }\n}\n")
+    exe = tmp_path / "d"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    args = [repr(float(b)) for b in box] + [str(int(v)) for v in g["num_subgrid"]] + \
+        [str(int(v)) for v in g["ncell"]] + [str(int(g["threads"]))]
+    out = subprocess.run([str(exe)] + args, check=True, capture_output=True, text=True).stdout
+    got = np.array([[float.fromhex(x) for x in line.split()] for line in out.splitlines()])
+    assert got.shape == (rec.size, 4)
+    assert np.array_equal(got[:, :3], rec["pos"])
+    assert np.array_equal(got[:, 3], rec["nH"])
+    # a field with structure, not the uniform 1e8
+    assert rec["nH"].std() > 0.05 * rec["nH"].mean()
+
+
+@pytest.mark.gpu
+def test_stromgren_driver_random_density(tmp_path):
+    """The driver with random_density: true and the reference's command line
+    writes the reference's cell centres and n_H bit for bit; x_H comes from
+    a different (device) packet stream and is compared statistically."""
+    if not os.path.exists(DRIVER):
+        pytest.fail("stromgren_driver not built (make -C parallelcmacionize_b200/csrc)")
+    g, rec = _random_case()
+    p = tmp_path / "params.txt"
+    p.write_text(str(g["params"]))
+    r = subprocess.run([DRIVER, "-t", str(int(g["threads"])), "-p", str(p)], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    from parallelcmacionize_b200.outputs import read_neutral_fractions_dat
+    ours = read_neutral_fractions_dat(tmp_path / "neutral_fractions.dat")
+    assert ours.size == rec.size
+    assert np.array_equal(ours["pos"], rec["pos"])
+    assert np.array_equal(ours["nH"], rec["nH"])
+    assert np.array_equal(ours["hydro"], rec["hydro"])
+    x = np.fromfile(tmp_path / "neutral_fractions.bin", dtype=np.float64)
+    assert np.array_equal(x, ours["xH"])
+    assert np.all((x > 0) & (x <= 1))
+    # 2e4 packets over 2048 cells: cell values are noisy, the mean is not
+    assert abs(x.mean() - rec["xH"].mean()) < 0.05 * rec["xH"].mean() + 0.01
+
+
 @pytest.mark.gpu
 def test_stromgren_driver_runs(tmp_path):
     """The reference's command line and params.txt, on the GPU path."""
