@@ -310,7 +310,6 @@ int upload_tables(cmi_context *c) {
   dev_free(c->d_src_first);
   dev_free(c->d_src_rank0);
   dev_free(c->d_buf_first);
-  dev_free(c->d_src_rank0);
   c->nsrc_total = (int)ds.size();
   CMI_TRY(dev_alloc(&c->d_src, ds.size()));
   CMI_TRY(dev_alloc(&c->d_src_count, ds.size() + 1));
