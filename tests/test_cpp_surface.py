@@ -68,6 +68,25 @@ def test_ranlxd_header_matches_reference_stream(tmp_path):
         assert np.array_equal(np.array([float.fromhex(x) for x in out]), ref)
 
 
+def test_stromgren_driver_rejects_bad_input(tmp_path):
+    """Command-line and params.txt errors end the driver with a message and a
+    non-zero status before any device work.  The reference stops on the same
+    inputs through cmac_error (a missing key: YAMLDictionary.hpp:562)."""
+    if not os.path.exists(DRIVER):
+        pytest.fail("stromgren_driver not built (make -C parallelcmacionize_b200/csrc)")
+    r = subprocess.run([DRIVER], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "usage" in r.stderr
+    r = subprocess.run([DRIVER, "-t", "1", "-p", str(tmp_path / "absent.txt")],
+                       cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "unable to open" in r.stderr
+    p = tmp_path / "params.txt"
+    p.write_text("box:\n  anchor: [-5. pc, -5. pc, -5. pc]\n")
+    r = subprocess.run([DRIVER, "-t", "1", "-p", str(p)], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=60)
+    assert r.returncode == 1 and 'missing parameter "box:sides"' in r.stderr
+    assert not (tmp_path / "neutral_fractions.bin").exists()
+
+
 def _random_case():
     from conftest import golden
     g = golden("outputs_random.npz")
