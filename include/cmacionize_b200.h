@@ -158,10 +158,14 @@ int cmi_set_fields(cmi_context *context, int32_t instance, int32_t layout, int32
  * copy from pinned host memory runs on a side stream, so it can proceed while
  * the previous iteration's x_H comes back (cmi_get_fields), and
  * cmi_set_fields_prefetched then takes it together with x_H (host or device,
- * `memory`) in the prefetch's layout.  The host array must stay unchanged
- * until cmi_set_fields_prefetched returns; one prefetch per instance may be
- * pending.  No reference counterpart (the reference keeps its fields in host
- * memory). */
+ * `memory`) in the prefetch's layout.  cmi_set_fields_prefetched returns
+ * without waiting: its copies run on the side stream while the next
+ * iteration emits its packets, and the iteration's first transport round
+ * waits for them.  Both input arrays must stay unchanged until the next
+ * cmi_run_iterations, cmi_run_until_converged, cmi_shoot_packets,
+ * cmi_get_fields or cmi_synchronize returns; every other entry point orders
+ * its own work after the copies.  One prefetch per instance may be pending.
+ * No reference counterpart (the reference keeps its fields in host memory). */
 int cmi_prefetch_number_density(cmi_context *ctx, int32_t instance, int32_t layout,
                                 const double *nH);
 int cmi_set_fields_prefetched(cmi_context *ctx, int32_t instance, int32_t memory,

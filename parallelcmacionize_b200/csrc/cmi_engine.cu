@@ -159,6 +159,14 @@ struct cmi_context {
   double *d_nh_stage = nullptr;
   std::vector<cudaEvent_t> nh_event;
   std::vector<int32_t> nh_layout;  // -1: nothing prefetched for the instance
+  // cmi_set_fields_prefetched issues its copies and the kappa refresh on
+  // copy_stream (after main_mark, the main stream's work so far) and records
+  // fields_ready.  An iteration waits for it after the emission, which reads
+  // no field, so the copies overlap the emission; every other entry point
+  // waits before its first use (fields_pending)
+  cudaEvent_t fields_ready = nullptr;
+  cudaEvent_t main_mark = nullptr;
+  bool fields_pending = false;
 
   // cmi_dust_run's packet buffers, grown to the largest call and kept
   DustBuffers *dust = nullptr;
@@ -171,9 +179,16 @@ struct cmi_context {
 
 namespace {
 
-int check_ctx(cmi_context *c) {
+// await_fields: order the main stream after fields still being copied in by
+// cmi_set_fields_prefetched (the iteration entry points pass false: their
+// iteration waits inside, after the emission)
+int check_ctx(cmi_context *c, bool await_fields = true) {
   if (!c) return fail(CMI_ERR_INVALID_ARGUMENT, "null context");
   CMI_CUDA(cudaSetDevice(c->device));
+  if (await_fields && c->fields_pending) {
+    CMI_CUDA(cudaStreamWaitEvent(c->stream, c->fields_ready, 0));
+    c->fields_pending = false;
+  }
   return CMI_OK;
 }
 
@@ -326,11 +341,11 @@ int upload_tables(cmi_context *c) {
   return CMI_OK;
 }
 
-int refresh_kappa(cmi_context *c, int32_t i) {
+int refresh_kappa(cmi_context *c, int32_t i, cudaStream_t s = nullptr) {
   if (!c->fp32()) return CMI_OK;
   const HostInstance &I = c->inst[i];
-  k_kappa<<<I.nsub, 256, 0, c->stream>>>(c->d_sub, c->d_inst, I.first_sub, c->d_nH, c->d_xH,
-                                         c->d_kappa);
+  k_kappa<<<I.nsub, 256, 0, s ? s : c->stream>>>(c->d_sub, c->d_inst, I.first_sub, c->d_nH,
+                                                 c->d_xH, c->d_kappa);
   CMI_CUDA(cudaGetLastError());
   return CMI_OK;
 }
@@ -620,6 +635,11 @@ int enqueue_iteration(cmi_context *c, bool balance) {
   c->enqueued += 1;
   CMI_CUDA(cudaGetLastError());
   if (!direct) CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c, true); }));
+  // fields sent by cmi_set_fields_prefetched arrive on the copy stream: the
+  // walk waits for them here, so their copy overlaps the emission above (a
+  // graph holds this as an event-wait node on the latest record)
+  CMI_CUDA(cudaStreamWaitEvent(c->stream, c->fields_ready,
+                               c->capturing ? cudaEventWaitExternal : cudaEventWaitDefault));
   CMI_TRY(c->capturing ? enqueue_rounds_graph(c) : enqueue_rounds(c));
   if (balance) {
     BalanceParams b{};
@@ -722,6 +742,7 @@ int run(cmi_context *c, int32_t iterations, uint64_t seed, uint32_t first_iterat
     }
     CMI_CUDA(cudaMemcpyAsync(c->h_stats + (size_t)it * ninst, c->d_stats,
                              sizeof(DevStats) * ninst, cudaMemcpyDeviceToHost, c->stream));
+    c->fields_pending = false;  // the iteration waited for the fields
   }
   CMI_CUDA(cudaStreamSynchronize(c->stream));
   uint32_t flags_any = 0;
@@ -830,7 +851,11 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
     return fail(CMI_ERR_CUDA, "cudaSetDevice failed");
   }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->fields_ready, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->main_mark, cudaEventDisableTiming) != cudaSuccess) {
+    if (c->fields_ready) cudaEventDestroy(c->fields_ready);
+    if (c->body_stream) cudaStreamDestroy(c->body_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return fail(CMI_ERR_CUDA, "stream creation failed");
@@ -989,6 +1014,8 @@ int cmi_destroy(cmi_context *c) {
   }
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   for (cudaEvent_t e : c->nh_event) cudaEventDestroy(e);
+  if (c->fields_ready) cudaEventDestroy(c->fields_ready);
+  if (c->main_mark) cudaEventDestroy(c->main_mark);
   dev_free(c->d_nh_stage);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -998,12 +1025,13 @@ int cmi_destroy(cmi_context *c) {
 }
 
 static int copy_field_in(cmi_context *c, int32_t instance, int32_t layout, int32_t memory,
-                         const double *src, double *dst) {
+                         const double *src, double *dst, cudaStream_t s = nullptr) {
   const HostInstance &I = c->inst[instance];
+  if (!s) s = c->stream;
   const double *dsrc = src;
   if (memory == CMI_MEMORY_HOST) {
     CMI_CUDA(cudaMemcpyAsync(c->d_stage, src, sizeof(double) * I.ncells, cudaMemcpyHostToDevice,
-                             c->stream));
+                             s));
     dsrc = c->d_stage;
   }
   LayoutParams lp{};
@@ -1014,7 +1042,7 @@ static int copy_field_in(cmi_context *c, int32_t instance, int32_t layout, int32
     lp.ncell[a] = I.desc.ncell[a];
   }
   lp.layout = layout;
-  k_fields_in<<<I.nsub, 256, 0, c->stream>>>(lp, dsrc, dst);
+  k_fields_in<<<I.nsub, 256, 0, s>>>(lp, dsrc, dst);
   CMI_CUDA(cudaGetLastError());
   return CMI_OK;
 }
@@ -1094,14 +1122,17 @@ int cmi_set_fields_prefetched(cmi_context *c, int32_t instance, int32_t memory,
   const int32_t layout = c->nh_layout[instance];
   CMI_TRY(check_layout(layout, memory));
   const HostInstance &I = c->inst[instance];
-  // n_H: the staged copy, once it has landed
-  CMI_CUDA(cudaStreamWaitEvent(c->stream, c->nh_event[instance], 0));
+  // on the copy stream, after the main stream's work so far (which may still
+  // read the fields and the staging buffer) and after the n_H copy (FIFO)
+  CMI_CUDA(cudaEventRecord(c->main_mark, c->stream));
+  CMI_CUDA(cudaStreamWaitEvent(c->copy_stream, c->main_mark, 0));
   CMI_TRY(copy_field_in(c, instance, layout, CMI_MEMORY_DEVICE, c->d_nh_stage + I.first_cell,
-                        c->d_nH));
+                        c->d_nH, c->copy_stream));
   c->nh_layout[instance] = -1;
-  if (xH) CMI_TRY(copy_field_in(c, instance, layout, memory, xH, c->d_xH));
-  CMI_TRY(refresh_kappa(c, instance));
-  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  if (xH) CMI_TRY(copy_field_in(c, instance, layout, memory, xH, c->d_xH, c->copy_stream));
+  CMI_TRY(refresh_kappa(c, instance, c->copy_stream));
+  CMI_CUDA(cudaEventRecord(c->fields_ready, c->copy_stream));
+  c->fields_pending = true;
   return CMI_OK;
 }
 
@@ -1167,7 +1198,7 @@ int cmi_set_reemission_probability(cmi_context *c, int32_t instance, double prob
 }
 
 int cmi_run_iterations(cmi_context *c, int32_t iterations, uint64_t seed, cmi_stats *stats) {
-  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_ctx(c, false));
   if (iterations <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "iterations must be > 0");
   CMI_TRY(clear_flags(c));
   // the first iteration index of this call continues from the previous call
@@ -1187,7 +1218,7 @@ static int set_frozen(cmi_context *c, int32_t i, uint32_t v) {
 int cmi_run_until_converged(cmi_context *c, int32_t max_iterations, int32_t min_iterations,
                             double tolerance, uint64_t seed, cmi_stats *stats,
                             int32_t *iterations_done, int32_t *converged_at) {
-  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_ctx(c, false));
   if (max_iterations <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "max_iterations must be > 0");
   if (min_iterations < 1 || min_iterations > max_iterations)
     return fail(CMI_ERR_INVALID_ARGUMENT, "min_iterations must be in [1, max_iterations]");
@@ -1233,7 +1264,7 @@ int cmi_run_until_converged(cmi_context *c, int32_t max_iterations, int32_t min_
 }
 
 int cmi_shoot_packets(cmi_context *c, uint64_t seed, uint32_t iteration, cmi_stats *stats) {
-  CMI_TRY(check_ctx(c));
+  CMI_TRY(check_ctx(c, false));
   CMI_TRY(clear_flags(c));
   return run(c, 1, seed, iteration, false, stats);
 }
@@ -1492,13 +1523,16 @@ int cmi_device_field(cmi_context *c, int32_t instance, int32_t which, double **p
   const HostInstance &I = c->inst[instance];
   double *base = (which == 0) ? c->d_J : (which == 1) ? c->d_xH : (which == 2) ? c->d_nH : nullptr;
   if (!base) return fail(CMI_ERR_INVALID_ARGUMENT, "which must be 0 (J), 1 (x_H) or 2 (n_H)");
+  // the caller may read the array on any stream: the fields are settled first
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
   *ptr = base + I.first_cell;
   *count = (uint64_t)I.nsub * (uint64_t)I.padded_per_sub;
   return CMI_OK;
 }
 
 int cmi_get_stream(cmi_context *c, void **s) {
-  if (!c || !s) return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  if (!s) return fail(CMI_ERR_INVALID_ARGUMENT, "null argument");
+  CMI_TRY(check_ctx(c));  // work queued on the stream comes after the fields
   *s = (void *)c->stream;
   return CMI_OK;
 }

@@ -149,8 +149,9 @@ class TransportEngine:
         check(self._L.cmi_set_fields(self._h, instance, lay, _lib.MEMORY_HOST, ptr(n), ptr(x)))
 
     def prefetch_number_density(self, instance, number_density, layout="blocked"):
-        """Start copying n_H (a pinned host array, left unchanged until
-        set_fields_prefetched returns) on a side stream."""
+        """Start copying n_H (a pinned host array) on a side stream.  The array
+        must stay unchanged until the next run_iterations, run_until_converged,
+        shoot_packets, get_fields or synchronize returns."""
         lay = {"blocked": _lib.LAYOUT_BLOCKED, "cube": _lib.LAYOUT_CUBE}[layout]
         n = np.asarray(number_density)
         if n.dtype != np.float64 or not n.flags.c_contiguous or \
@@ -161,13 +162,24 @@ class TransportEngine:
         check(self._L.cmi_prefetch_number_density(self._h, instance, lay, ptr(n)))
 
     def set_fields_prefetched(self, instance, neutral_fraction=None):
-        """n_H from the last prefetch of the instance, x_H from the host."""
+        """n_H from the last prefetch of the instance, x_H from the host.  The
+        copies run on the side stream and the next iteration waits for them
+        after its emission; x_H (pinned or not) must stay unchanged until the
+        next run_iterations, run_until_converged, shoot_packets, get_fields or
+        synchronize returns."""
         x = None if neutral_fraction is None else np.ascontiguousarray(neutral_fraction,
                                                                        np.float64)
         if x is not None and x.size != self.grids[instance].num_cells:
             raise ValueError("field size does not match the grid")
         check(self._L.cmi_set_fields_prefetched(self._h, instance, _lib.MEMORY_HOST, ptr(x)))
-        getattr(self, "_prefetched", {}).pop(instance, None)
+        # both host arrays may still be read by the side stream
+        self._in_flight = getattr(self, "_in_flight", [])
+        self._in_flight.append(getattr(self, "_prefetched", {}).pop(instance, None))
+        self._in_flight.append(x)
+
+    def _settled(self):
+        """The side stream's copies are complete: release their arrays."""
+        self._in_flight = []
 
     def set_fields_device(self, instance, number_density_ptr=0, neutral_fraction_ptr=0,
                           layout="blocked"):
@@ -182,6 +194,7 @@ class TransportEngine:
         x = (out_x if out_x is not None else np.empty(n)) if neutral_fraction else None
         j = (out_j if out_j is not None else np.empty(n)) if intensity else None
         check(self._L.cmi_get_fields(self._h, instance, lay, _lib.MEMORY_HOST, ptr(x), ptr(j)))
+        self._settled()
         return x, j
 
     def set_intensity(self, instance, J, layout="blocked"):
@@ -208,6 +221,7 @@ class TransportEngine:
         ninst = len(self.grids)
         st = (_lib.Stats * (iterations * ninst))()
         check(self._L.cmi_run_iterations(self._h, iterations, int(seed), st))
+        self._settled()
         return [[st[it * ninst + i].as_dict() for i in range(ninst)] for it in range(iterations)]
 
     def run_until_converged(self, tolerance, max_iterations=100, min_iterations=2, seed=42):
@@ -222,6 +236,7 @@ class TransportEngine:
         check(self._L.cmi_run_until_converged(self._h, int(max_iterations), int(min_iterations),
                                               float(tolerance), int(seed), st, C.byref(done),
                                               at))
+        self._settled()
         stats = [[st[it * ninst + i].as_dict() for i in range(ninst)]
                  for it in range(done.value)]
         return stats, list(at)
@@ -257,6 +272,7 @@ class TransportEngine:
         ninst = len(self.grids)
         st = (_lib.Stats * ninst)()
         check(self._L.cmi_shoot_packets(self._h, int(seed), int(iteration), st))
+        self._settled()
         return [st[i].as_dict() for i in range(ninst)]
 
     def transport_packets(self, instance, photons, start_subgrid):
@@ -313,6 +329,7 @@ class TransportEngine:
 
     def synchronize(self):
         check(self._L.cmi_synchronize(self._h))
+        self._settled()
 
     KERNEL_CLASSES = ("walk", "plan_scatter", "emission", "balance")
 
