@@ -154,10 +154,10 @@ struct cmi_context {
   std::vector<cudaEvent_t> event_pool;
 
   // cmi_prefetch_number_density: n_H copied on a side stream into its own
-  // staging (the padded layout's offsets), one event per instance
+  // staging (the padded layout's offsets); cmi_set_fields_prefetched takes it
+  // up on the same stream, after the copy
   cudaStream_t copy_stream = nullptr;
   double *d_nh_stage = nullptr;
-  std::vector<cudaEvent_t> nh_event;
   std::vector<int32_t> nh_layout;  // -1: nothing prefetched for the instance
   // cmi_set_fields_prefetched issues its copies and the kappa refresh on
   // copy_stream (after main_mark, the main stream's work so far) and records
@@ -1013,7 +1013,6 @@ int cmi_destroy(cmi_context *c) {
     cudaEventDestroy(t.stop);
   }
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
-  for (cudaEvent_t e : c->nh_event) cudaEventDestroy(e);
   if (c->fields_ready) cudaEventDestroy(c->fields_ready);
   if (c->main_mark) cudaEventDestroy(c->main_mark);
   dev_free(c->d_nh_stage);
@@ -1098,9 +1097,7 @@ int cmi_prefetch_number_density(cmi_context *c, int32_t instance, int32_t layout
   if (!c->copy_stream) {
     CMI_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     CMI_TRY(dev_alloc(&c->d_nh_stage, (size_t)c->total_padded));
-    c->nh_event.assign(c->inst.size(), nullptr);
     c->nh_layout.assign(c->inst.size(), -1);
-    for (auto &e : c->nh_event) CMI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   if (c->nh_layout[instance] >= 0)
     return fail(CMI_ERR_INVALID_ARGUMENT,
@@ -1108,7 +1105,6 @@ int cmi_prefetch_number_density(cmi_context *c, int32_t instance, int32_t layout
   const HostInstance &I = c->inst[instance];
   CMI_CUDA(cudaMemcpyAsync(c->d_nh_stage + I.first_cell, nH, sizeof(double) * I.ncells,
                            cudaMemcpyHostToDevice, c->copy_stream));
-  CMI_CUDA(cudaEventRecord(c->nh_event[instance], c->copy_stream));
   c->nh_layout[instance] = layout;
   return CMI_OK;
 }
