@@ -484,6 +484,33 @@ def test_prefetched_density_equals_set_fields():
     np.testing.assert_allclose(res[1], res[0], rtol=1e-12, atol=0)
 
 
+def test_prefetched_fields_are_awaited():
+    """cmi_set_fields_prefetched returns before its side-stream copies are
+    done; the entry points that read the fields wait for them: get_fields
+    returns the x_H just sent (pinned, 2 MB) bit for bit, device_field the
+    n_H, and a second set in a row replaces the first."""
+    import torch
+    from parallelcmacionize_b200.distributed import _CudaArray
+    spec, nH = lognormal_config(ncell=64, num_subgrid=4, num_photon=10_000, num_sources=1)
+    with TransportEngine(spec) as eng:
+        eng.set_fields(0, np.full(nH.size, 1e8), np.full(nH.size, 1e-6))
+        pin_n = torch.from_numpy(nH.copy()).pin_memory()
+        for k in range(2):
+            pin_x = torch.from_numpy(np.linspace(1e-4, 0.9, nH.size) * (k + 1) / 2).pin_memory()
+            eng.prefetch_number_density(0, pin_n.numpy())
+            eng.set_fields_prefetched(0, pin_x.numpy())
+            x = eng.get_fields(0, intensity=False)[0]
+            assert np.array_equal(x, pin_x.numpy())
+        ptr, count = eng.device_field(0, "n")
+        dev = torch.as_tensor(_CudaArray(ptr, count), device="cuda").cpu().numpy()
+        ref = TransportEngine(spec)
+        ref.set_fields(0, nH, np.full(nH.size, 1e-6))
+        p2, c2 = ref.device_field(0, "n")
+        want = torch.as_tensor(_CudaArray(p2, c2), device="cuda").cpu().numpy()
+        ref.close()
+        assert np.array_equal(dev, want)
+
+
 @pytest.mark.parametrize("workload", ["lognormal128", "large256"])
 def test_full_size_conservation_and_fp32_vs_fp64(workload):
     """At the full benchmark sizes (128^3 with 1e7 packets; 256^3 with 1e8):
