@@ -478,7 +478,8 @@ def ours(args):
                  for i in range(len(wl.fields))]
         ncells = sum(n.size for n in wl.fields)
         # n_H of step k + 1 is copied on a side stream while x_H of step k comes
-        # back (the two directions of the link run at once)
+        # back (the two directions of the link run at once); x_H of step k + 1
+        # goes up on the side stream while the step emits its packets
         runner.barrier()
         t0 = time.perf_counter()
         e2e_cross = 0
