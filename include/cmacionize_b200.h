@@ -259,7 +259,10 @@ int cmi_compute_neutral_fraction_subgrids(cmi_context *context, int32_t instance
 
 /* Device-side access for interop (zero-copy views, NCCL reductions): the
  * instance's J (which = 0), x_H (1) or n_H (2) array in BLOCKED layout, and
- * the CUDA stream every kernel of the context runs on. */
+ * the CUDA stream every kernel of the context runs on.  cmi_device_field
+ * returns once the context's queued work (field copies included) is done, so
+ * the array may be read on any stream; work queued on the stream from
+ * cmi_get_stream runs after the field copies. */
 int cmi_device_field(cmi_context *context, int32_t instance, int32_t which, double **device_ptr,
                      uint64_t *count);
 int cmi_get_stream(cmi_context *context, void **cuda_stream);
