@@ -368,8 +368,10 @@ def gen_outputs():
     """outputs.npz: uniform density; outputs_random.npz: the driver's random
     density field (10 cosine modes), for the C++ surface's set-up of the same
     run (seeded 42 + threads).  One source each: with several sources whose
-    packet counts are not multiples of the buffer size, the driver does not
-    finish (the emitted count differs from num_photon)."""
+    packet counts are not multiples of 100, the driver does not finish (its
+    last task of a source emits 200 - n % 200 packets instead of n % 200,
+    testDensitySubGrid_omp.cpp:2266-2270, so the emitted count never reaches
+    num_photon)."""
     c = OUTPUT_CASE
     geo = dict(ncell=np.array(c["ncell"]), num_subgrid=np.array(c["num_subgrid"]),
                anchor_pc=np.array(c["anchor_pc"]), sides_pc=np.array(c["sides_pc"]))
