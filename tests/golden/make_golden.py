@@ -370,8 +370,8 @@ def gen_outputs():
     run (seeded 42 + threads).  One source each: with several sources whose
     packet counts are not multiples of 100, the driver does not finish (its
     last task of a source emits 200 - n % 200 packets instead of n % 200,
-    testDensitySubGrid_omp.cpp:2266-2270, so the emitted count never reaches
-    num_photon)."""
+    testDensitySubGrid_omp.cpp:2266-2270, so the count of finished packets
+    never equals num_photon, its stop test at :2390)."""
     c = OUTPUT_CASE
     geo = dict(ncell=np.array(c["ncell"]), num_subgrid=np.array(c["num_subgrid"]),
                anchor_pc=np.array(c["anchor_pc"]), sides_pc=np.array(c["sides_pc"]))
