@@ -66,3 +66,38 @@ def test_booleans(value, expected):
 def test_errors(edit, message):
     with pytest.raises(ParameterError, match=message):
         Parameters.from_text(TEXT.replace(*edit))
+
+
+def test_cpp_surface_reads_the_same_values(tmp_path):
+    """include/cmacionize/Parameters.hpp (the C++ surface) and this reader
+    agree on every plain-method value of the same file, bit for bit."""
+    import os
+    import subprocess
+
+    from conftest import ROOT
+    src = tmp_path / "p.cpp"
+    src.write_text(
+        '#include "cmacionize/Parameters.hpp"\n#include <cstdio>\n'
+        "int main(int c, char **v) {\n"
+        "  const PlainMethodParameters p(Parameters::from_file(v[1]));\n"
+        '  for (double b : p.box) printf("%a\\n", b);\n'
+        '  printf("%a\\n", p.reemission_probability);\n'
+        '  for (int a = 0; a < 3; ++a) printf("%d %d\\n", p.ncell[a], p.num_subgrid[a]);\n'
+        '  printf("%u %u %u %d\\n", p.num_photon, p.number_of_iterations,'
+        " p.number_of_sources, (int)p.random_density);\n}\n")
+    exe = tmp_path / "p"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    for text in (TEXT, TEXT.replace("random_density: false", "random_density: yes")
+                 .replace("number_of_sources: 1", "number_of_sources: 3")):
+        f = tmp_path / "params.txt"
+        f.write_text(text)
+        out = subprocess.run([str(exe), str(f)], check=True, capture_output=True,
+                             text=True).stdout.split("\n")
+        p = Parameters.from_text(text)
+        assert [float.fromhex(v) for v in out[:6]] == list(p.box)
+        assert float.fromhex(out[6]) == p.reemission_probability
+        assert [tuple(map(int, out[7 + a].split())) for a in range(3)] == \
+            list(zip(p.ncell, p.num_subgrid))
+        assert list(map(int, out[10].split())) == [p.num_photon, p.number_of_iterations,
+                                                   p.number_of_sources, int(p.random_density)]
