@@ -77,7 +77,11 @@ typedef struct {
 
 enum cmi_precision {
   CMI_TRANSPORT_FP64 = 0, /* the reference's FP64 walk, operation for operation */
-  CMI_TRANSPORT_FP32 = 1  /* FP32 cell-unit walk, shared-memory tallies (cmi_tally) merged into FP64 */
+  CMI_TRANSPORT_FP32 = 1, /* FP32 cell-unit walk, shared-memory tallies (cmi_tally) merged into FP64 */
+  CMI_TRANSPORT_MIXED = 2 /* the reference's FP64 geometry operation for operation (cell
+                             sequences and path lengths equal DensitySubGrid::interact's),
+                             FP32 opacity sigma*n*x, optical depths and tallies (cmi_tally);
+                             the target optical depth is held in FP32 */
 };
 enum cmi_balance_form {
   CMI_BALANCE_REFERENCE = 0, /* x = 1 + a(1 - sqrt(2/a + 1)), DensitySubGrid.hpp:1650 */
@@ -91,7 +95,12 @@ enum cmi_tally {
 };
 enum cmi_rng {
   CMI_RNG_PHILOX = 0, /* counter-based Philox4x32-10 per packet */
-  CMI_RNG_RANLUX = 1  /* the reference's ranlxd, one stream per 200-packet buffer */
+  CMI_RNG_RANLUX = 1  /* the reference's ranlxd, one stream per 200-packet buffer: buffer b
+                         (counted over all sources of the context, 0-based) of iteration i
+                         draws from ranlxd(seed + b + i * buffers), first one draw for the
+                         subgrid-copy pick (Source.hpp:94-99), then per packet cos(theta),
+                         phi and the optical depth (testDensitySubGrid_omp.cpp:529-597);
+                         sin, cos and log are correctly rounded */
 };
 enum cmi_layout {
   CMI_LAYOUT_BLOCKED = 0, /* subgrid after subgrid, each in DensitySubGrid order (reference output order) */
@@ -110,11 +119,11 @@ typedef struct {
   int32_t threads_per_cta;     /* 0 = library default (256) */
   int32_t ctas_per_sm;         /* 0 = as many as fit */
   int32_t packets_per_chunk;   /* 0 = library default (128); power of two in [32, 4096] */
-  int32_t tally_mode;          /* FP32 transport: cmi_tally (default CMI_TALLY_FIXED64) */
+  int32_t tally_mode;          /* FP32 and mixed transports: cmi_tally (default CMI_TALLY_FIXED64) */
   int32_t use_graph;           /* 1 = capture each iteration as a CUDA graph (default) */
   int32_t max_run_chunks;      /* most chunks a CTA claims at once (0 = 64): how long a CTA
                                   stays on one subgrid before flushing its tallies */
-  int32_t refill_lanes;        /* FP32 walk: a warp routes finished packets and refills its
+  int32_t refill_lanes;        /* FP32 and mixed walks: a warp routes finished packets and refills its
                                   lanes once this many lanes are not walking (0 = 16; 1..32) */
   int32_t reserved[5];
 } cmi_options;
@@ -214,6 +223,19 @@ int cmi_run_iterations(cmi_context *context, int32_t num_iterations, uint64_t se
 int cmi_run_until_converged(cmi_context *context, int32_t max_iterations, int32_t min_iterations,
                             double tolerance, uint64_t seed, cmi_stats *stats,
                             int32_t *iterations_done, int32_t *converged_at);
+/* fill_buffer (testDensitySubGrid_omp.cpp:556-597) for every source of the
+ * context: the photons one iteration with this seed and iteration index
+ * emits (cmi_run_iterations, cmi_shoot_packets), without transporting them,
+ * in the reference Photon layout (source position, isotropic direction,
+ * target optical depth, the instance's cross section, weight 1).  Order:
+ * instance after instance, source after source, and within a source the
+ * emission order (CMI_RNG_RANLUX: buffer after buffer of 200, each drawn from
+ * the reference's ranlxd seeded as described under cmi_rng, with correctly
+ * rounded sin, cos and log).  *count receives the number of photons; with
+ * out NULL or capacity below it the call fails with CMI_ERR_CAPACITY after
+ * setting *count. */
+int cmi_emit_photons(cmi_context *context, uint64_t seed, uint32_t iteration, cmi_photon *out,
+                     uint64_t capacity, uint64_t *count);
 /* Transport phase only (no balance); J keeps accumulating. */
 int cmi_shoot_packets(cmi_context *context, uint64_t seed, uint32_t iteration, cmi_stats *stats);
 
@@ -307,8 +329,10 @@ int cmi_kernel_timing(cmi_context *context, double milliseconds[CMI_KERNEL_CLASS
  * Runs the reference FP64 walk on the calling thread's current device and
  * returns when the stream has finished it.  The first call on a device looks
  * up the array's device address (once per device), so make the first call
- * before any stream capture.  Calls that overlap on the GPU (other host
- * threads, other streams) share the array and race: serialise them. */
+ * before any stream capture.  A cudaDeviceReset discards the array and makes
+ * that address stale: do not call this entry point on a device after
+ * resetting it in the same process.  Calls that overlap on the GPU (other
+ * host threads, other streams) share the array and race: serialise them. */
 #define CMI_NOALLOC_MAX_PHOTONS 4096
 int cmi_traverse_buffer_noalloc(const double box[6], const int32_t ncell[3],
                                 const double *d_nH, const double *d_xH, double *d_J,
@@ -391,8 +415,8 @@ int cmi_dust_run(cmi_context *ctx, int32_t instance, uint64_t num_photon, uint64
  * Parameters (FP32 master copy, in this order per convolution): W[co][tap][ci]
  * with tap = (dz * 3 + dy) * 3 + dx, then b[co]; last the head's w[c1], b.
  * Weights and activations are BF16, accumulation FP32; the 3x3x3
- * convolutions and their input gradients run on the tensor cores (tcgen05),
- * the weight gradients on CUDA cores.  Training minimises the mean squared
+ * convolutions, their input gradients and their weight gradients run on the
+ * tensor cores (tcgen05).  Training minimises the mean squared
  * error of log10 x_H with Adam.
  *
  * Tensors handed to the network live in device memory, FP32, one sample
@@ -461,7 +485,8 @@ int cmi_unet_upsample_nearest(cmi_unet *net, const float *src, const int32_t dim
 /* x_H = 10^clamp(prediction, log10_min, 0) as FP64 (device), n values */
 int cmi_unet_to_neutral_fraction(cmi_unet *net, const float *prediction, double *xH, int64_t n,
                                  float log10_min);
-/* Building blocks, exposed for testing: one 3x3x3 convolution on the tensor
+/* Building blocks, exposed for testing (grids: X and Y multiples of 8, Z of 2,
+ * the convolution tile of 8 x 8 x 2 voxels): one 3x3x3 convolution on the tensor
  * cores (BF16 channels-last device tensors, channel counts multiples of 16,
  * weights packed by cmi_unet_pack_weights, bias FP32 or NULL, activation 1 =
  * leaky ReLU); packing of FP32 W[cout][27][cin] (flip = 1: the input-gradient

@@ -42,6 +42,14 @@ PACKET32_DTYPE = np.dtype(
 )
 assert PACKET32_DTYPE.itemsize == 32
 
+# mixed-precision packet (cmio_packetm): absolute FP64 position and direction,
+# FP32 remaining optical depth
+PACKETM_DTYPE = np.dtype(
+    [("pos", "<f8", (3,)), ("dir", "<f8", (3,)), ("tau", "<f4"), ("meta", "<u4"),
+     ("pad", "<u4", (2,))]
+)
+assert PACKETM_DTYPE.itemsize == 64
+
 _DIRECTION_NAMES = [
     "INSIDE",
     "CORNER_PPP", "CORNER_PPN", "CORNER_PNP", "CORNER_PNN",
@@ -144,6 +152,10 @@ def lib():
                                     pi32, pd, i32, pi32]
         L.cmio_interact32.argtypes = [pi32, pf, pf, pf, pd, C.POINTER(u64), C.c_float,
                                       C.c_void_p, pi32, pf, i32, pi32]
+        L.cmio_interact_mixed.argtypes = [C.POINTER(Subgrid), pf, pd, C.POINTER(u64),
+                                          C.c_float, C.c_void_p, pi32, pd, i32, pi32]
+        L.cmio_transportm_r.argtypes = [C.POINTER(Lattice), pf, pd, C.POINTER(u64),
+                                        C.c_void_p, pu32, i64, C.POINTER(Counts), C.c_void_p]
         L.cmio_fixed_scale.argtypes = [C.POINTER(Subgrid)]
         L.cmio_fixed_scale.restype = C.c_float
         L.cmio_jfac.argtypes = [d, d, pd]
@@ -153,6 +165,10 @@ def lib():
         L.cmio_ranlux_uniform.argtypes = [C.POINTER(Ranlux)]
         L.cmio_ranlux_uniform.restype = d
         L.cmio_fill_buffer_stream.argtypes = [i32, pd, C.c_void_p, i32, d]
+        L.cmio_fill_buffer_stream_cr.argtypes = [i32, pd, C.c_void_p, i32, d]
+        L.cmio_cr_sincos.argtypes = [d, pd, pd]
+        L.cmio_cr_neg_log.argtypes = [d]
+        L.cmio_cr_neg_log.restype = d
         L.cmio_source_numbers.argtypes = [i32, pd, u32, pu32]
         L.cmio_distribute.argtypes = [i32, i32, C.POINTER(Ranlux), pu32]
         L.cmio_philox4x32.argtypes = [pu32, pu32, pu32]
@@ -283,6 +299,45 @@ def interact32(ncell, cell_size, kappa, tally, packet, max_steps: int = 0,
     return res, cells[:n].copy(), lengths[:n].copy(), nsteps.value
 
 
+def tau32(tau):
+    """FP32 optical depth of the mixed walk: round to nearest, and a positive
+    depth below the FP32 range becomes the smallest subnormal (not 0), so a
+    packet the reference walks is walked."""
+    t = np.asarray(tau, np.float64)
+    f = t.astype(np.float32)
+    tiny = np.frombuffer(np.uint32(1).tobytes(), np.float32)[0]
+    return np.where((f == 0) & (t > 0), tiny, f).astype(np.float32)
+
+
+def packets_mixed(photons, input_directions=None):
+    """PACKETM_DTYPE records of PHOTON_DTYPE photons (tau as tau32)."""
+    q = np.zeros(photons.size, PACKETM_DTYPE)
+    q["pos"] = photons["position"]
+    q["dir"] = photons["direction"]
+    q["tau"] = tau32(photons["tau"])
+    if input_directions is not None:
+        q["meta"] = np.asarray(input_directions, np.uint32)
+    return q
+
+
+def interact_mixed(sg: Subgrid, kappa, packet, max_steps: int = 0, tally=None, fixed=None):
+    """Mixed-precision walk of one PACKETM_DTYPE record (modified in place).
+
+    Returns (result_direction, trace_cells, trace_lengths (FP64), steps)."""
+    cells = np.zeros(max(max_steps, 1), dtype=np.int32)
+    lengths = np.zeros(max(max_steps, 1), dtype=np.float64)
+    nsteps = C.c_int32(0)
+    res = lib().cmio_interact_mixed(
+        C.byref(sg), _ptr(kappa, C.c_float),
+        _ptr(tally, C.c_double) if tally is not None else None,
+        _ptr(fixed, C.c_uint64) if fixed is not None else None,
+        lib().cmio_fixed_scale(C.byref(sg)), packet.ctypes.data,
+        _ptr(cells, C.c_int32) if max_steps else None,
+        _ptr(lengths, C.c_double) if max_steps else None, max_steps, C.byref(nsteps))
+    n = min(nsteps.value, max_steps)
+    return res, cells[:n].copy(), lengths[:n].copy(), nsteps.value
+
+
 def jfac(luminosity, num_photon, inv_cell_size):
     v = np.ascontiguousarray(inv_cell_size, dtype=np.float64)
     return lib().cmio_jfac(float(luminosity), float(num_photon), _ptr(v, C.c_double))
@@ -313,6 +368,28 @@ def fill_buffer_stream(seed, source_position, n, cross_section=6.3e-22):
     lib().cmio_fill_buffer_stream(int(seed), _ptr(p, C.c_double), out.ctypes.data, n,
                                   cross_section)
     return out
+
+
+def fill_buffer_stream_cr(seed, source_position, n, cross_section=6.3e-22):
+    """fill_buffer_stream with correctly rounded sin, cos and log (the CUDA
+    library's replay of the reference stream)."""
+    out = np.zeros(n, dtype=PHOTON_DTYPE)
+    p = np.ascontiguousarray(source_position, dtype=np.float64)
+    lib().cmio_fill_buffer_stream_cr(int(seed), _ptr(p, C.c_double), out.ctypes.data, n,
+                                     cross_section)
+    return out
+
+
+def cr_sincos(x):
+    """Correctly rounded (sin x, cos x) for x in [0, 8)."""
+    s, c = C.c_double(0.), C.c_double(0.)
+    lib().cmio_cr_sincos(float(x), C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
+def cr_neg_log(u):
+    """Correctly rounded -ln(u) for u in [0, 1)."""
+    return lib().cmio_cr_neg_log(float(u))
 
 
 def philox4x32(counter, key):
@@ -402,6 +479,19 @@ class LatticeGrid:
                                  _ptr(fixed, C.c_uint64) if fixed is not None else None,
                                  packets.ctypes.data, _ptr(s, C.c_uint32), packets.size,
                                  C.byref(counts), C.byref(r) if r else None)
+        return counts.as_dict()
+
+    def transport_mixed(self, kappa, tally, packets, start_subgrid, fixed=None,
+                        reemission=None):
+        """Mixed-precision transport (PACKETM_DTYPE packets, modified in place)."""
+        counts = Counts()
+        s = np.ascontiguousarray(start_subgrid, dtype=np.uint32)
+        r = Reemission(*reemission) if reemission else None
+        lib().cmio_transportm_r(C.byref(self.lat), _ptr(kappa, C.c_float),
+                                _ptr(tally, C.c_double) if tally is not None else None,
+                                _ptr(fixed, C.c_uint64) if fixed is not None else None,
+                                packets.ctypes.data, _ptr(s, C.c_uint32), packets.size,
+                                C.byref(counts), C.byref(r) if r else None)
         return counts.as_dict()
 
     def fixed_unit(self, s=0):
@@ -545,8 +635,9 @@ def ref_balance(box, ncell, nH, J, luminosity, num_photon):
 
 def ref_iterations(box, ncell, num_subgrid, nH_blocked, xH_blocked, src_pos, src_lum,
                    packets, iterations, threads=0, seed=42, count=False,
-                   binary="ref_harness_fast", timeout=None):
-    """Whole plain-method iterations with the reference code on the host cores.
+                   binary="ref_harness_fast", timeout=None, reemission=0.0):
+    """Whole plain-method iterations with the reference code on the host cores
+    (reemission: do_reemission's probability, testDensitySubGrid_omp.cpp:675-702).
 
     Returns (xH_final_blocked, per_iteration list of dicts)."""
     ncells = int(np.prod(ncell))
@@ -561,8 +652,11 @@ def ref_iterations(box, ncell, num_subgrid, nH_blocked, xH_blocked, src_pos, src
             f.write(np.asarray(xH_blocked, "<f8").tobytes())
             for p, L in zip(np.asarray(src_pos).reshape(-1, 3), src_lum):
                 f.write(np.asarray(list(p) + [L], "<f8").tobytes())
-        ref_run(["run", inp, out, int(packets), int(iterations), int(threads), int(seed),
-                 int(bool(count))], binary=binary, timeout=timeout)
+        args = ["run", inp, out, int(packets), int(iterations), int(threads), int(seed),
+                int(bool(count))]
+        if reemission > 0.0:
+            args.append(repr(float(reemission)))
+        ref_run(args, binary=binary, timeout=timeout)
         raw = open(out, "rb").read()
     x = np.frombuffer(raw, "<f8", ncells).copy()
     it_dt = np.dtype([("t", "<f8"), ("cross", "<u8"), ("abs", "<u8"), ("esc", "<u8")])

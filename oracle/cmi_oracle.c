@@ -343,6 +343,96 @@ int cmio_interact32(const int32_t ncell[3], const float cell_size[3],
   return out;
 }
 
+/* FP32 optical depth of a mixed-precision packet: round to nearest; a
+ * positive depth below the FP32 range becomes the smallest subnormal. */
+static float tau32(double tau) {
+  const float f = (float)tau;
+  return (f == 0.f && tau > 0.) ? 1.40129846e-45f : f;
+}
+
+/* Mixed-precision walk: interact's loop (DensitySubGrid.hpp:1186-1305) with
+ * the geometry of walk_mode above, operation for operation, and the optical
+ * depth of each crossing in FP32 from the cell's FP32 opacity. */
+int cmio_interact_mixed(const cmio_subgrid *sg, const float *kappa, double *tally,
+                        uint64_t *fixed, float scale, cmio_packetm *packet,
+                        int32_t *trace_cells, double *trace_lengths, int32_t max_steps,
+                        int32_t *nsteps) {
+  const int in_dir = (int)(packet->meta & 31u);
+  const double *d = packet->dir;
+  const double inv[3] = {1. / d[0], 1. / d[1], 1. / d[2]};
+  double pos[3] = {packet->pos[0] - sg->anchor[0], packet->pos[1] - sg->anchor[1],
+                   packet->pos[2] - sg->anchor[2]};
+  float tau_done = 0.f;
+  const float tau_target = packet->tau_left;
+  int32_t idx[3];
+  int cell = cmio_get_start_index(sg, pos, in_dir, idx);
+  int32_t steps = 0;
+  while (tau_done < tau_target && is_inside3(idx, sg->ncell)) {
+    const double lo[3] = {idx[0] * sg->cell_size[0], idx[1] * sg->cell_size[1],
+                          idx[2] * sg->cell_size[2]};
+    const double hi[3] = {(idx[0] + 1.) * sg->cell_size[0], (idx[1] + 1.) * sg->cell_size[1],
+                          (idx[2] + 1.) * sg->cell_size[2]};
+    double l[3];
+    for (int a = 0; a < 3; ++a) {
+      if (d[a] > 0.) {
+        l[a] = (hi[a] - pos[a]) * inv[a];
+      } else if (d[a] < 0.) {
+        l[a] = (lo[a] - pos[a]) * inv[a];
+      } else {
+        l[a] = DBL_MAX;
+      }
+    }
+    double lmin = min_d(l[0], min_d(l[1], l[2]));
+    float lf = (float)lmin;
+    const float tau = lf * kappa[cell];
+    const float tau_before = tau_done;
+    tau_done += tau;
+    if (tau_done >= tau_target) {
+      /* the absorbed fraction 1 - (tau_done - tau_target) / tau of the
+       * reference, as (tau_target - tau_before) / tau: no cancellation when
+       * the packet stops early in the cell */
+      float fraction = (tau_target - tau_before) / tau;
+      fraction = (fraction < 1.f) ? fraction : 1.f;
+      lmin *= (double)fraction;
+      lf = (float)lmin;
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        if (l[a] == lmin) {
+          idx[a] += (d[a] > 0.) ? 1 : -1;
+        }
+      }
+    }
+    if (tally != NULL) {
+      tally[cell] += (double)lf;
+    }
+    if (fixed != NULL) {
+      /* round half to even of lf * scale (< 2^23), clamped at 0 */
+      const float q = lf * scale;
+      fixed[cell] += (q > 0.f) ? (uint64_t)nearbyintf(q) : 0u;
+    }
+    if (trace_cells != NULL && steps < max_steps) {
+      trace_cells[steps] = cell;
+      trace_lengths[steps] = lmin;
+    }
+    ++steps;
+    for (int a = 0; a < 3; ++a) {
+      pos[a] = (l[a] == lmin) ? ((d[a] > 0.) ? hi[a] : lo[a]) : pos[a] + lmin * d[a];
+    }
+    cell = idx[0] * sg->ncell[3] + idx[1] * sg->ncell[2] + idx[2];
+  }
+  packet->tau_left = tau_target - tau_done;
+  for (int a = 0; a < 3; ++a) {
+    packet->pos[a] = pos[a] + sg->anchor[a];
+  }
+  if (nsteps != NULL) {
+    *nsteps = steps;
+  }
+  if (tau_done >= tau_target) {
+    return CMIO_INSIDE;
+  }
+  return cmio_get_output_direction(sg, idx);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Ionization balance, DensitySubGrid.hpp:1628-1658.                         */
 /* ------------------------------------------------------------------------ */
@@ -496,6 +586,130 @@ void cmio_fill_buffer_stream(int32_t seed, const double source_position[3], cmio
   cmio_ranlux_seed(&rng, seed);
   (void)cmio_ranlux_uniform(&rng); /* Source::get_subgrid_index draw */
   cmio_fill_packets(&rng, source_position, out, n, cross_section);
+}
+
+/* Correctly rounded sin, cos and -log of the CUDA library's replay of the
+ * reference emission streams (restated: double-double arithmetic after
+ * Dekker and Knuth, Cody-Waite reduction by pi/2 in three parts, Taylor
+ * series of sin and cos to x^29 / 29!, -ln u = -(e ln 2 + 2 atanh s) with the
+ * atanh series to s^45 / 45).  Every operation is a correctly rounded IEEE
+ * operation or an fma, so host and device give the same bits. */
+typedef struct {
+  double hi, lo;
+} cmio_dd;
+static cmio_dd dd_two_sum(double a, double b) {
+  const double s = a + b, bb = s - a;
+  const cmio_dd r = {s, (a - (s - bb)) + (b - bb)};
+  return r;
+}
+static cmio_dd dd_fast_two_sum(double a, double b) {
+  const double s = a + b;
+  const cmio_dd r = {s, b - (s - a)};
+  return r;
+}
+static cmio_dd dd_two_prod(double a, double b) {
+  const double p = a * b;
+  const cmio_dd r = {p, fma(a, b, -p)};
+  return r;
+}
+static cmio_dd dd_add(cmio_dd a, cmio_dd b) {
+  cmio_dd s = dd_two_sum(a.hi, b.hi);
+  const cmio_dd t = dd_two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = dd_fast_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return dd_fast_two_sum(s.hi, s.lo);
+}
+static cmio_dd dd_mul(cmio_dd a, cmio_dd b) {
+  cmio_dd p = dd_two_prod(a.hi, b.hi);
+  p.lo += a.hi * b.lo + a.lo * b.hi;
+  return dd_fast_two_sum(p.hi, p.lo);
+}
+static cmio_dd dd_div_d(cmio_dd a, double b) {
+  const double q1 = a.hi / b;
+  const cmio_dd p = dd_two_prod(q1, b);
+  cmio_dd s = dd_two_sum(a.hi, -p.hi);
+  s.lo = (s.lo - p.lo) + a.lo;
+  return dd_fast_two_sum(q1, (s.hi + s.lo) / b);
+}
+static cmio_dd dd_div(cmio_dd a, cmio_dd b) {
+  const double q1 = a.hi / b.hi;
+  const cmio_dd m1 = {-q1, 0.};
+  cmio_dd r = dd_add(a, dd_mul(m1, b));
+  const double q2 = r.hi / b.hi;
+  const cmio_dd m2 = {-q2, 0.};
+  r = dd_add(r, dd_mul(m2, b));
+  const cmio_dd q3 = {r.hi / b.hi, 0.};
+  return dd_add(dd_fast_two_sum(q1, q2), q3);
+}
+
+void cmio_cr_sincos(double x, double *sn, double *cs) {
+  const double P1 = 0x1.921fb54442d18p+0, P2 = 0x1.1a62633145c07p-54,
+               P3 = -0x1.f1976b7ed8fbcp-110;
+  const double k = nearbyint(x * (1. / P1));
+  cmio_dd r = {x - k * P1, 0.};
+  r = dd_add(r, dd_two_prod(-k, P2));
+  const cmio_dd r3 = {-k * P3, 0.};
+  r = dd_add(r, r3);
+  const cmio_dd r2 = dd_mul(r, r);
+  const cmio_dd one = {1., 0.};
+  cmio_dd ts = one, tc = one;
+  for (int n = 14; n >= 1; --n) {
+    ts = dd_add(one, dd_div_d(dd_mul(r2, ts), -(double)((2 * n) * (2 * n + 1))));
+    tc = dd_add(one, dd_div_d(dd_mul(r2, tc), -(double)((2 * n - 1) * (2 * n))));
+  }
+  const cmio_dd s = dd_mul(r, ts);
+  const double sv = s.hi + s.lo, cv = tc.hi + tc.lo;
+  const int q = ((int)k) & 3;
+  *sn = (q == 0) ? sv : (q == 1) ? cv : (q == 2) ? -sv : -cv;
+  *cs = (q == 0) ? cv : (q == 1) ? -sv : (q == 2) ? -cv : sv;
+}
+
+double cmio_cr_neg_log(double u) {
+  if (u == 0.) return INFINITY;
+  int e;
+  double m = frexp(u, &e);
+  if (m < 0.70710678118654752440) {
+    m *= 2.;
+    e -= 1;
+  }
+  const cmio_dd one = {1., 0.}, num = {m - 1., 0.}, two = {2., 0.};
+  const cmio_dd s = dd_div(num, dd_two_sum(m, 1.));
+  const cmio_dd s2 = dd_mul(s, s);
+  cmio_dd t = {0., 0.};
+  for (int k = 22; k >= 0; --k) t = dd_add(dd_div_d(one, (double)(2 * k + 1)), dd_mul(s2, t));
+  const cmio_dd lm = dd_mul(dd_mul(two, s), t);
+  const double L2H = 0x1.62e42fefa39efp-1, L2L = 0x1.abc9e3b39803fp-56;
+  const cmio_dd el0 = {L2L * (double)e, 0.};
+  const cmio_dd el = dd_add(dd_two_prod(L2H, (double)e), el0);
+  const cmio_dd l = dd_add(el, lm);
+  return -(l.hi + l.lo);
+}
+
+/* The reference's fill_buffer stream (testDensitySubGrid_omp.cpp:529-597)
+ * with the correctly rounded functions above in place of cos, sin and log. */
+void cmio_fill_buffer_stream_cr(int32_t seed, const double source_position[3],
+                                cmio_photon *out, int32_t n, double cross_section) {
+  cmio_ranlux rng;
+  cmio_ranlux_seed(&rng, seed);
+  (void)cmio_ranlux_uniform(&rng); /* Source::get_subgrid_index draw */
+  for (int32_t i = 0; i < n; ++i) {
+    cmio_photon *p = &out[i];
+    memset(p, 0, sizeof(*p));
+    for (int a = 0; a < 3; ++a) p->position[a] = source_position[a];
+    const double cost = 2. * cmio_ranlux_uniform(&rng) - 1.;
+    const double phi = 2. * M_PI * cmio_ranlux_uniform(&rng);
+    const double s2 = 1. - cost * cost;
+    const double sint = sqrt((s2 < 0.) ? 0. : s2);
+    double sinp, cosp;
+    cmio_cr_sincos(phi, &sinp, &cosp);
+    p->direction[0] = sint * cosp;
+    p->direction[1] = sint * sinp;
+    p->direction[2] = cost;
+    p->weight = 1.;
+    p->target_optical_depth = cmio_cr_neg_log(cmio_ranlux_uniform(&rng));
+    p->cross_section = cross_section;
+  }
 }
 
 /* testDensitySubGrid_omp.cpp:2199-2208: packets proportional to luminosity. */
@@ -816,6 +1030,49 @@ void cmio_transport32(const cmio_lattice *lat, const float *kappa, double *tally
                       uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
                       int64_t n, cmio_counts *counts) {
   cmio_transport32_r(lat, kappa, tally, fixed, packets, start_subgrid, n, counts, NULL);
+}
+
+void cmio_transportm_r(const cmio_lattice *lat, const float *kappa, double *tally,
+                       uint64_t *fixed, cmio_packetm *packets, const uint32_t *start_subgrid,
+                       int64_t n, cmio_counts *counts, const cmio_reemission *r) {
+  const int64_t C = lat->cells_per_subgrid;
+  for (int64_t i = 0; i < n; ++i) {
+    uint32_t s = start_subgrid[i];
+    uint32_t rcount = 0; /* reemissions in this subgrid visit */
+    for (;;) {
+      const cmio_subgrid *sg = &lat->sub[s];
+      int32_t steps = 0;
+      const int out = cmio_interact_mixed(sg, kappa + s * C, tally ? tally + s * C : NULL,
+                                          fixed ? fixed + s * C : NULL, cmio_fixed_scale(sg),
+                                          &packets[i], NULL, NULL, 0, &steps);
+      counts->crossings += (uint64_t)steps;
+      counts->transits += 1;
+      if (out == CMIO_INSIDE) {
+        double d[3], tau;
+        cmio_packetm *pk = &packets[i];
+        if (r && r->probability > 0. &&
+            cmio_reemit_draw(r, cmio_reemit_hash(pk->pos[0]), cmio_reemit_hash(pk->pos[1]),
+                             cmio_reemit_hash(pk->pos[2]), rcount, d, &tau)) {
+          counts->reemitted += 1;
+          rcount += 1;
+          for (int a = 0; a < 3; ++a) pk->dir[a] = d[a];
+          pk->tau_left = tau32(tau);
+          pk->meta = (pk->meta & ~31u) | (uint32_t)CMIO_INSIDE;
+          continue;
+        }
+        counts->absorbed += 1;
+        break;
+      }
+      const uint32_t ngb = lat->ngb[s * CMIO_NUM_DIRECTIONS + out];
+      if (ngb == CMIO_NEIGHBOUR_OUTSIDE) {
+        counts->escaped += 1;
+        break;
+      }
+      s = ngb;
+      packets[i].meta = (packets[i].meta & ~31u) | (uint32_t)cmio_output_to_input_direction(out);
+      rcount = 0;
+    }
+  }
 }
 
 

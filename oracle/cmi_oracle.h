@@ -102,6 +102,34 @@ int cmio_interact32(const int32_t ncell[3], const float cell_size[3],
                     int32_t *trace_cells, float *trace_lengths, int32_t max_steps,
                     int32_t *nsteps);
 
+/* Mixed-precision walk of the CUDA default transport (the project's own
+ * formulation, restated so the GPU kernel can be checked bit for bit).  The
+ * geometry is interact's (DensitySubGrid.hpp:1186-1305) in FP64 with the
+ * reference's operations in the reference's order: position relative to the
+ * anchor, faces idx * cs and (idx + 1.) * cs, l = (face - pos) * (1. / d),
+ * crossed coordinates snapped to their face, pos + lmin * d for the others.
+ * So every cell crossed and every path length up to the last one equal the
+ * reference's.  The opacity kappa = (float)(sigma n x), the optical depths
+ * and the tallies are FP32: tau = (float)lmin * kappa, accumulated in FP32;
+ * the absorbed cell's fraction min(1, (tau_target - tau_before) / tau) (FP32,
+ * tau_before the depth before the cell; the reference's 1 - (tau_done -
+ * tau_target) / tau without its cancellation) scales the last length in
+ * FP64.  pos is absolute (m), as in Photon. */
+typedef struct {
+  double pos[3];
+  double dir[3];
+  float tau_left;
+  uint32_t meta; /* low 5 bits: input TravelDirection */
+  uint32_t pad[2];
+} cmio_packetm;
+
+/* tally / fixed as for cmio_interact32 (FP32 lengths (float)lmin);
+ * trace_lengths receives the FP64 lengths. */
+int cmio_interact_mixed(const cmio_subgrid *sg, const float *kappa, double *tally,
+                        uint64_t *fixed, float scale, cmio_packetm *packet,
+                        int32_t *trace_cells, double *trace_lengths, int32_t max_steps,
+                        int32_t *nsteps);
+
 /* compute_neutral_fraction (DensitySubGrid.hpp:1628-1658).
  * form 0: the reference expression 1 + a(1 - sqrt(2/a + 1));
  * form 1: the cancellation-free equivalent 1/(1 + a + sqrt(a(a+2))). */
@@ -127,6 +155,15 @@ void cmio_fill_packets(cmio_ranlux *rng, const double source_position[3],
  * (Source.hpp:94-99) and is consumed, then the packets follow. */
 void cmio_fill_buffer_stream(int32_t seed, const double source_position[3],
                              cmio_photon *out, int32_t n, double cross_section);
+
+/* Correctly rounded sin / cos (x in [0, 8)) and -log (u in [0, 1)) of the
+ * CUDA library's replay of the reference emission streams, and that replay:
+ * cmio_fill_buffer_stream with them in place of the C library's cos, sin
+ * and log. */
+void cmio_cr_sincos(double x, double *sn, double *cs);
+double cmio_cr_neg_log(double u);
+void cmio_fill_buffer_stream_cr(int32_t seed, const double source_position[3],
+                                cmio_photon *out, int32_t n, double cross_section);
 
 /* Photon split over sources (testDensitySubGrid_omp.cpp:2199-2208, 1650-1677). */
 void cmio_source_numbers(int32_t nsrc, const double *luminosity, uint32_t num_photon,
@@ -197,6 +234,12 @@ void cmio_transport_r(const cmio_lattice *lat, const double *nH, const double *x
 void cmio_transport32_r(const cmio_lattice *lat, const float *kappa, double *tally,
                         uint64_t *fixed, cmio_packet32 *packets, const uint32_t *start_subgrid,
                         int64_t n, cmio_counts *counts, const cmio_reemission *r);
+/* Mixed-precision counterpart (cmio_interact_mixed): same routing; the
+ * reemission counter is the FP64 one (cmio_reemit_hash of the absolute
+ * absorption position per axis), the drawn optical depth rounded to FP32. */
+void cmio_transportm_r(const cmio_lattice *lat, const float *kappa, double *tally,
+                       uint64_t *fixed, cmio_packetm *packets, const uint32_t *start_subgrid,
+                       int64_t n, cmio_counts *counts, const cmio_reemission *r);
 /* scale of the fixed-point tally of a subgrid: 2^24 / max float cell size */
 float cmio_fixed_scale(const cmio_subgrid *sg);
 

@@ -12,9 +12,9 @@
  *     compute_neutral_fraction and its subgrid-copy merge
  *     (update_intensities / update_neutral_fractions).
  *
- * Only get_random_direction (testDensitySubGrid_omp.cpp:529-545) and the
- * luminosity split (:2199-2208) live next to main() in the reference driver;
- * they are restated below with citations.
+ * Only get_random_direction (testDensitySubGrid_omp.cpp:529-545), the
+ * luminosity split (:2199-2208) and do_reemission (:675-702) live next to
+ * main() in the reference driver; they are restated below with citations.
  *
  * All binary I/O is little-endian, fixed-width.
  */
@@ -135,6 +135,16 @@ void emit_photon(RandomGenerator &rng, const double *src, Photon &photon) {
   photon.set_target_optical_depth(-std::log(rng.get_uniform_random_double()));
   photon.set_photoionization_cross_section(6.3e-22);
   photon.set_type(PHOTONPACKETTYPE_DIRECT);
+}
+
+/* do_reemission (testDensitySubGrid_omp.cpp:675-702, restated) for one
+ * absorbed photon: with probability p a new isotropic direction and target
+ * optical depth; returns whether it was re-emitted. */
+bool reemit_photon(RandomGenerator &rng, double p, Photon &photon) {
+  if (!(rng.get_uniform_random_double() < p)) return false;
+  random_direction(rng, photon.get_direction());
+  photon.set_target_optical_depth(-std::log(rng.get_uniform_random_double()));
+  return true;
 }
 
 /* ---- directions: testDensitySubGridDirections.cpp fixtures + sweeps ---- */
@@ -406,7 +416,7 @@ int cmd_transport(const char *in_path, const char *out_path) {
 /* ---- run: whole plain-method iterations on the host cores ----
  * in:  box[6] ncell[3] nsub[3] nsrc(int32) pad nH[cells, subgrid-blocked]
  *      xH[cells] {pos[3], L}*nsrc
- * args: packets iterations threads seed count(0/1)
+ * args: packets iterations threads seed count(0/1) [reemission_probability]
  * out: xH[cells] after the last iteration, then per iteration
  *      {double mc_seconds, uint64 crossings, uint64 absorbed, uint64 escaped}
  *
@@ -416,9 +426,17 @@ int cmd_transport(const char *in_path, const char *out_path) {
  * update_neutral_fractions exactly as testDensitySubGrid_omp.cpp:2403-2434.
  * Buffer b (200 packets) of an iteration draws from RandomGenerator(seed +
  * b); count=1 replays every buffer through the C oracle walk (untimed) to
- * count cell crossings, which the reference walk does not report. */
+ * count cell crossings, which the reference walk does not report (without
+ * reemission only).  With reemission probability p > 0 an absorbed photon is
+ * re-emitted in place (do_reemission, :675-702; the reemit task :1348-1395
+ * walks it on through the same subgrid), drawing from its buffer's
+ * generator. */
 int cmd_run(const char *in_path, const char *out_path, long packets, int iterations,
-            int threads, int seed, int count) {
+            int threads, int seed, int count, double reemission) {
+  if (count && reemission > 0.) {
+    std::fprintf(stderr, "run: crossing counts need reemission 0\n");
+    return 2;
+  }
   Reader r(in_path);
   double box[6];
   r.get(box, 6);
@@ -506,6 +524,10 @@ int cmd_run(const char *in_path, const char *out_path, long packets, int iterati
           for (;;) {
             const int res = mine[s]->interact(photon, in_dir);
             if (res == TRAVELDIRECTION_INSIDE) {
+              if (reemission > 0. && reemit_photon(rng, reemission, photon)) {
+                in_dir = TRAVELDIRECTION_INSIDE;
+                continue;
+              }
               ++n_abs;
               break;
             }
@@ -635,9 +657,9 @@ int main(int argc, char **argv) {
   if (cmd == "depth" && argc == 4) return cmd_dust_walk(argv[2], argv[3], true);
   if (cmd == "balance" && argc == 4) return cmd_balance(argv[2], argv[3]);
   if (cmd == "transport" && argc == 4) return cmd_transport(argv[2], argv[3]);
-  if (cmd == "run" && argc == 9)
+  if (cmd == "run" && (argc == 9 || argc == 10))
     return cmd_run(argv[2], argv[3], std::atol(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]),
-                   std::atoi(argv[7]), std::atoi(argv[8]));
+                   std::atoi(argv[7]), std::atoi(argv[8]), argc == 10 ? std::atof(argv[9]) : 0.);
   std::fprintf(stderr, "bad arguments\n");
   return 2;
 }

@@ -25,6 +25,7 @@ ERR_NOT_SUPPORTED = 7
 
 TRANSPORT_FP64 = 0
 TRANSPORT_FP32 = 1
+TRANSPORT_MIXED = 2
 BALANCE_REFERENCE = 0
 BALANCE_STABLE = 1
 TALLY_FP32 = 0
@@ -48,7 +49,7 @@ EXPORTED = [
     "cmi_set_packet_budget", "cmi_set_reemission_probability", "cmi_run_iterations",
     "cmi_run_until_converged", "cmi_dust_run", "cmi_walk_photons",
     "cmi_prefetch_number_density", "cmi_set_fields_prefetched",
-    "cmi_shoot_packets",
+    "cmi_shoot_packets", "cmi_emit_photons",
     "cmi_transport_packets", "cmi_traverse_buffer", "cmi_trace_packet",
     "cmi_compute_neutral_fraction", "cmi_device_field", "cmi_get_stream", "cmi_synchronize",
     "cmi_last_launch_count", "cmi_set_kernel_timing", "cmi_kernel_timing",
@@ -185,6 +186,7 @@ def load():
     L.cmi_prefetch_number_density.argtypes = [ctx, i32, i32, vp]
     L.cmi_set_fields_prefetched.argtypes = [ctx, i32, i32, vp]
     L.cmi_shoot_packets.argtypes = [ctx, u64, u32, vp]
+    L.cmi_emit_photons.argtypes = [ctx, u64, u32, vp, u64, C.POINTER(u64)]
     L.cmi_transport_packets.argtypes = [ctx, i32, vp, vp, u64, vp]
     L.cmi_traverse_buffer.argtypes = [ctx, i32, u32, i32, vp, u32, vp, vp, vp, vp]
     L.cmi_trace_packet.argtypes = [ctx, i32, u32, i32, vp, i32, vp, vp, vp, vp]

@@ -23,6 +23,12 @@ A candidate (``WalkConfig``) chooses:
 The subgrid decomposition changes where the FP32 walk re-anchors its
 positions, so results of two candidates agree to FP32 rounding, not bit for
 bit; every candidate is a correct transport.
+
+A batch of independent instances of uneven size (one context, one launch per
+kernel; ``Autotuner.tune_batch``) is tuned as a whole, since an instance's
+rate alone says little about the batch: the subgrid side of each size class
+first (greedy, class by class, largest first), then the chunking shared by
+the context (``BatchConfig``).
 """
 from __future__ import annotations
 
@@ -31,11 +37,12 @@ import math
 import os
 import tempfile
 import time
-from dataclasses import asdict, dataclass
+from collections import Counter
+from dataclasses import asdict, dataclass, replace
 
 import numpy as np
 
-from .engine import GridSpec, TransportEngine, cube_to_blocked
+from .engine import GridSpec, TransportEngine, blocked_to_cube, cube_to_blocked
 
 
 @dataclass(frozen=True)
@@ -60,6 +67,39 @@ class WalkConfig:
         return dict(packets_per_chunk=self.packets_per_chunk, tally=self.tally,
                     ctas_per_sm=self.ctas_per_sm, max_run_chunks=self.max_run_chunks,
                     refill_lanes=self.refill_lanes)
+
+
+@dataclass(frozen=True)
+class BatchConfig:
+    """Launch shape of a batch: ``sides`` maps each size class (cells per axis,
+    "NxNxN") to its subgrid side; the rest is shared by the context."""
+    sides: tuple = ()  # (("32x32x32", 16), ...)
+    packets_per_chunk: int = 128
+    max_run_chunks: int = 64
+    tally: str = "fixed64"
+    ctas_per_sm: int = 0
+    refill_lanes: int = 16
+
+    def side_of(self, grid: GridSpec) -> int:
+        return dict(self.sides).get(_class_name(grid), 16)
+
+    def grids(self, base_grids):
+        return [WalkConfig(sub_side=self.side_of(g)).grid(g) for g in base_grids]
+
+    def engine_options(self) -> dict:
+        return dict(packets_per_chunk=self.packets_per_chunk, tally=self.tally,
+                    ctas_per_sm=self.ctas_per_sm, max_run_chunks=self.max_run_chunks,
+                    refill_lanes=self.refill_lanes)
+
+
+def _class_name(grid: GridSpec) -> str:
+    return "x".join(str(int(v)) for v in grid.ncell)
+
+
+def reblock(nH_blocked, old: GridSpec, new: GridSpec):
+    """A blocked field of ``old`` in the subgrid decomposition of ``new``."""
+    cube = blocked_to_cube(nH_blocked, old.ncell, old.num_subgrid)
+    return cube_to_blocked(cube, new.ncell, new.num_subgrid)
 
 
 def candidates(ncell, precision="fp32", sides=(8, 16), chunks=(64, 128, 256),
@@ -93,6 +133,15 @@ def cache_key(device_name: str, grid: GridSpec, precision: str) -> str:
     bucket = int(round(math.log2(max(1, int(grid.num_photon)))))
     n = "x".join(str(int(v)) for v in grid.ncell)
     return f"{device_name}|{n}|src{len(grid.sources)}|pk2^{bucket}|{precision}"
+
+
+def batch_cache_key(device_name: str, grids, precision: str) -> str:
+    """Size classes with their counts, total packets to the nearest power of two."""
+    classes = sorted(Counter(_class_name(g) for g in grids).items())
+    total = sum(int(g.num_photon) for g in grids)
+    bucket = int(round(math.log2(max(1, total))))
+    cls = ",".join(f"{n}*{k}" for n, k in classes)
+    return f"{device_name}|batch|{cls}|pk2^{bucket}|{precision}"
 
 
 def _device_name(device: int) -> str:
@@ -194,6 +243,71 @@ class Autotuner:
         self.last_table = table
         self._store(key, {"config": asdict(best), "crossings_per_s": rate,
                           "searched": len(table)})
+        return best
+
+    # ---- batches ----
+    def _measure_batch(self, cfg: BatchConfig, grids, fields) -> float:
+        gs = cfg.grids(grids)
+        with TransportEngine(gs, precision=self.precision, device=self.device,
+                             **cfg.engine_options()) as eng:
+            for i, (g0, g, n) in enumerate(zip(grids, gs, fields)):
+                eng.set_fields(i, reblock(n, g0, g), np.full(n.size, 1.0e-6))
+            if self.warmup:
+                eng.run_iterations(self.warmup, seed=self.seed)
+            for i, n in enumerate(fields):
+                eng.set_fields(i, None, np.full(n.size, 1.0e-6))
+            eng.synchronize()
+            t0 = time.perf_counter()
+            st = eng.run_iterations(self.iterations, seed=self.seed + 1)
+            eng.synchronize()
+            dt = time.perf_counter() - t0
+        return sum(s["cell_crossings"] for it in st for s in it) / dt
+
+    def tune_batch(self, grids, fields, sides=(8, 16), chunks=(64, 128, 256), runs=(16, 64),
+                   force=False, measure=None):
+        """Best ``BatchConfig`` for a batch of ``grids`` with blocked n_H ``fields``
+        (in the grids' own decomposition), from the cache unless ``force``.
+        ``self.last_table`` lists every measured (config, crossings/s); its first
+        entry is the untuned start: every class in 16^3 subgrids, 128-packet
+        chunks, 64-chunk claims."""
+        measure = measure or self._measure_batch
+        key = batch_cache_key(_device_name(self.device), grids, self.precision)
+        if not force:
+            hit = self._load().get(key)
+            if hit:
+                self.last_table = []
+                c = hit["config"]
+                return BatchConfig(**dict(c, sides=tuple(tuple(x) for x in c["sides"])))
+        classes = sorted({_class_name(g) for g in grids},
+                         key=lambda n: -int(n.split("x")[0]))
+        ok = {c: [s for s in sides if all(int(v) % s == 0 for v in c.split("x"))]
+              for c in classes}
+        table = []
+        rates = {}
+
+        def rate_of(cand):
+            if cand not in rates:
+                rates[cand] = float(measure(cand, grids, fields))
+                table.append((cand, rates[cand]))
+            return rates[cand]
+
+        best = BatchConfig(sides=tuple((c, 16 if 16 in ok[c] else ok[c][0]) for c in classes))
+        rate = rate_of(best)
+        for c in classes:  # the subgrid side, one size class at a time
+            for s in ok[c]:
+                cand = replace(best, sides=tuple((k, s if k == c else v) for k, v in best.sides))
+                r = rate_of(cand)
+                if r > rate:
+                    best, rate = cand, r
+        for ch in chunks:  # then the chunking shared by the context
+            for ru in runs:
+                cand = replace(best, packets_per_chunk=ch, max_run_chunks=ru)
+                r = rate_of(cand)
+                if r > rate:
+                    best, rate = cand, r
+        self.last_table = table
+        self._store(key, {"config": asdict(best), "crossings_per_s": rate,
+                          "untuned_crossings_per_s": table[0][1], "searched": len(table)})
         return best
 
     def engine(self, grid: GridSpec, nH_cube, xH_cube=None, **engine_kw):

@@ -160,6 +160,39 @@ struct alignas(16) Packet32 {
 };
 static_assert(sizeof(Packet32) == 32, "Packet32 is one 32-byte sector");
 
+// Mixed-precision packet (64 B, two sectors): the reference's absolute FP64
+// position and direction, the remaining target optical depth in FP32.
+struct alignas(16) PacketM {
+  double pos[3];
+  double dir[3];
+  float tau;
+  uint32_t meta;  // low 5 bits: input TravelDirection
+  uint32_t pad[2];
+};
+static_assert(sizeof(PacketM) == 64, "PacketM is two 32-byte sectors");
+
+// The three packet records, as a template argument of the kernels that
+// create or move packets.
+enum PacketKind : int { kPk64 = 0, kPk32 = 1, kPkM = 2 };
+template <int K> struct PacketOf { using type = Packet64; };
+template <> struct PacketOf<kPk32> { using type = Packet32; };
+template <> struct PacketOf<kPkM> { using type = PacketM; };
+
+// FP32 target optical depth of a mixed-precision packet: round to nearest;
+// a positive depth below the FP32 range becomes the smallest subnormal, not
+// 0, so every packet the reference walks is walked.
+__host__ __device__ __forceinline__ float tau32(double tau) {
+  const float f = (float)tau;
+  if (f == 0.f && tau > 0.) {
+#ifdef __CUDA_ARCH__
+    return __int_as_float(1);
+#else
+    return 1.40129846e-45f;
+#endif
+  }
+  return f;
+}
+
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy
 // as 1, 2, 3", SC'11).
@@ -319,5 +352,112 @@ __device__ __noinline__ bool reemit_draw_call(uint64_t seed, uint32_t instance,
 
 // ranlxd, the reference's generator (shared with the host C++ surface)
 using Ranlux = cmi_ranlxd::Ranlxd;
+
+// ---------------------------------------------------------------------------
+// Correctly rounded sin, cos and -log for the replay of the reference's
+// emission streams (get_random_direction and fill_buffer,
+// testDensitySubGrid_omp.cpp:529-597): the same uniform draws give the same
+// directions and optical depths on every machine, independent of any math
+// library's last-bit behaviour.
+//
+// Double-double arithmetic (Dekker 1971; Knuth's TwoSum): a value is hi + lo
+// with |lo| <= ulp(hi) / 2; products are split exactly with a fused
+// multiply-add.  sin / cos: Cody-Waite reduction of x in [0, 8) by pi/2 held
+// in three parts (P1 has three trailing zero bits, so k * P1 is exact for
+// k <= 4 and x - k * P1 is exact by Sterbenz's lemma), then the Taylor
+// series of sin and cos to x^29 / 29! in Horner form on |r| <= pi/4.  -log u:
+// u = m 2^e with m in [sqrt(1/2), sqrt(2)), ln m = 2 atanh(s), s = (m - 1) /
+// (m + 1), series to s^45 / 45, plus e ln 2 (ln 2 as a double-double).  The
+// evaluation error is about 1e-30 relative, so rounding hi + lo to a double
+// gives the correctly rounded result except when the exact value lies within
+// about 1e-14 ulp of a rounding midpoint.
+// ---------------------------------------------------------------------------
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ DD dd_two_sum(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  return {s, __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb))};
+}
+__device__ __forceinline__ DD dd_fast_two_sum(double a, double b) {  // |a| >= |b|
+  const double s = __dadd_rn(a, b);
+  return {s, __dsub_rn(b, __dsub_rn(s, a))};
+}
+__device__ __forceinline__ DD dd_two_prod(double a, double b) {
+  const double p = __dmul_rn(a, b);
+  return {p, __fma_rn(a, b, -p)};
+}
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+  DD s = dd_two_sum(a.hi, b.hi);
+  const DD t = dd_two_sum(a.lo, b.lo);
+  s.lo = __dadd_rn(s.lo, t.hi);
+  s = dd_fast_two_sum(s.hi, s.lo);
+  s.lo = __dadd_rn(s.lo, t.lo);
+  return dd_fast_two_sum(s.hi, s.lo);
+}
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+  DD p = dd_two_prod(a.hi, b.hi);
+  p.lo = __dadd_rn(p.lo, __dadd_rn(__dmul_rn(a.hi, b.lo), __dmul_rn(a.lo, b.hi)));
+  return dd_fast_two_sum(p.hi, p.lo);
+}
+__device__ __forceinline__ DD dd_div_d(DD a, double b) {
+  const double q1 = __ddiv_rn(a.hi, b);
+  const DD p = dd_two_prod(q1, b);
+  DD s = dd_two_sum(a.hi, -p.hi);
+  s.lo = __dadd_rn(__dsub_rn(s.lo, p.lo), a.lo);
+  return dd_fast_two_sum(q1, __ddiv_rn(__dadd_rn(s.hi, s.lo), b));
+}
+__device__ __forceinline__ DD dd_div(DD a, DD b) {
+  const double q1 = __ddiv_rn(a.hi, b.hi);
+  DD r = dd_add(a, dd_mul({-q1, 0.}, b));
+  const double q2 = __ddiv_rn(r.hi, b.hi);
+  r = dd_add(r, dd_mul({-q2, 0.}, b));
+  const double q3 = __ddiv_rn(r.hi, b.hi);
+  return dd_add(dd_fast_two_sum(q1, q2), {q3, 0.});
+}
+
+// sin and cos of x in [0, 8)
+__device__ __noinline__ void cr_sincos(double x, double *sn, double *cs) {
+  const double P1 = 0x1.921fb54442d18p+0, P2 = 0x1.1a62633145c07p-54,
+               P3 = -0x1.f1976b7ed8fbcp-110;
+  const double k = rint(__dmul_rn(x, __drcp_rn(P1)));
+  DD r = {__dsub_rn(x, __dmul_rn(k, P1)), 0.};
+  r = dd_add(r, dd_two_prod(-k, P2));
+  r = dd_add(r, {__dmul_rn(-k, P3), 0.});
+  const DD r2 = dd_mul(r, r);
+  const DD one = {1., 0.};
+  DD ts = one, tc = one;
+  for (int n = 14; n >= 1; --n) {
+    ts = dd_add(one, dd_div_d(dd_mul(r2, ts), -(double)((2 * n) * (2 * n + 1))));
+    tc = dd_add(one, dd_div_d(dd_mul(r2, tc), -(double)((2 * n - 1) * (2 * n))));
+  }
+  const DD s = dd_mul(r, ts);
+  const double sv = __dadd_rn(s.hi, s.lo), cv = __dadd_rn(tc.hi, tc.lo);
+  const int q = ((int)k) & 3;
+  *sn = (q == 0) ? sv : (q == 1) ? cv : (q == 2) ? -sv : -cv;
+  *cs = (q == 0) ? cv : (q == 1) ? -sv : (q == 2) ? -cv : sv;
+}
+
+// -ln(u) for u in [0, 1) (+inf at 0)
+__device__ __noinline__ double cr_neg_log(double u) {
+  if (u == 0.) return __longlong_as_double(0x7ff0000000000000ll);
+  int e;
+  double m = frexp(u, &e);
+  if (m < 0.70710678118654752440) {
+    m = __dmul_rn(m, 2.);
+    e -= 1;
+  }
+  const DD one = {1., 0.};
+  const DD s = dd_div({__dsub_rn(m, 1.), 0.}, dd_two_sum(m, 1.));
+  const DD s2 = dd_mul(s, s);
+  DD t = {0., 0.};
+  for (int k = 22; k >= 0; --k) t = dd_add(dd_div_d(one, (double)(2 * k + 1)), dd_mul(s2, t));
+  const DD lm = dd_mul(dd_mul({2., 0.}, s), t);
+  const double L2H = 0x1.62e42fefa39efp-1, L2L = 0x1.abc9e3b39803fp-56;
+  const DD el = dd_add(dd_two_prod(L2H, (double)e), {__dmul_rn(L2L, (double)e), 0.});
+  const DD l = dd_add(el, lm);
+  return -__dadd_rn(l.hi, l.lo);
+}
 
 }  // namespace cmi

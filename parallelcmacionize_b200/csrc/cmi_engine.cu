@@ -99,6 +99,7 @@ struct cmi_context {
   uint32_t S = 0;
   int64_t total_padded = 0;
   int32_t max_padded = 0;
+  int32_t max_faces = 0;  // largest nx + ny + nz + 3 of a subgrid (the mixed walk's face table)
   int rounds = 1;     // straight-line bound + spares
   int round_cap = 1;  // rounds an iteration may run (rounds, or more with reemission)
   bool reemission = false;  // some instance re-emits absorbed packets
@@ -133,11 +134,12 @@ struct cmi_context {
   uint32_t chunk = 4096;
 
   // graph of one iteration
-  cudaGraphExec_t graph_exec = nullptr;
+  // captured iterations: [0] transport only (cmi_shoot_packets), [1] with the balance
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
   bool graph_dirty = true;
   bool capturing = false;        // enqueue_iteration is being captured
   cudaStream_t body_stream = nullptr;  // captures the round loop's body
-  uint64_t graph_kernels = 0;    // kernels per iteration outside the round loop
+  uint64_t graph_kernels[2] = {0, 0};  // kernels per iteration outside the round loop
   uint64_t graph_body_kernels = 0;  // kernels per round of the loop
   uint64_t last_launches = 0;
   uint64_t enqueued = 0;  // kernel launches of the current enqueue
@@ -174,7 +176,14 @@ struct cmi_context {
   size_t dust_pixels = 0;
 
   bool fp32() const { return opt.transport_precision == CMI_TRANSPORT_FP32; }
-  size_t packet_bytes() const { return fp32() ? sizeof(Packet32) : sizeof(Packet64); }
+  bool mixed() const { return opt.transport_precision == CMI_TRANSPORT_MIXED; }
+  // the FP32 and mixed walks read the FP32 opacity field kappa = sigma n x
+  bool uses_kappa() const { return fp32() || mixed(); }
+  int kind() const { return fp32() ? kPk32 : (mixed() ? kPkM : kPk64); }
+  size_t packet_bytes() const {
+    return fp32() ? sizeof(Packet32) : (mixed() ? sizeof(PacketM) : sizeof(Packet64));
+  }
+  const char *precision_name() const { return fp32() ? "FP32" : (mixed() ? "mixed" : "FP64"); }
 };
 
 namespace {
@@ -199,8 +208,10 @@ int check_instance(cmi_context *c, int32_t i) {
 }
 
 void free_graph(cmi_context *c) {
-  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-  c->graph_exec = nullptr;
+  for (cudaGraphExec_t &g : c->graph_exec) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
   c->graph_dirty = true;
 }
 
@@ -342,7 +353,7 @@ int upload_tables(cmi_context *c) {
 }
 
 int refresh_kappa(cmi_context *c, int32_t i, cudaStream_t s = nullptr) {
-  if (!c->fp32()) return CMI_OK;
+  if (!c->uses_kappa()) return CMI_OK;
   const HostInstance &I = c->inst[i];
   k_kappa<<<I.nsub, 256, 0, s ? s : c->stream>>>(c->d_sub, c->d_inst, I.first_sub, c->d_nH,
                                                  c->d_xH, c->d_kappa);
@@ -389,6 +400,11 @@ int launch_plan(cmi_context *c, bool scatter, bool gate = false,
           (const Packet32 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
           (Packet32 *)c->d_arena_in, c->d_state, (uint32_t)c->capacity, gate, h,
           (uint32_t)c->round_cap);
+    } else if (c->mixed()) {
+      k_scatter<PacketM><<<grid, 256, 0, c->stream>>>(
+          (const PacketM *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
+          (PacketM *)c->d_arena_in, c->d_state, (uint32_t)c->capacity, gate, h,
+          (uint32_t)c->round_cap);
     } else {
       k_scatter<Packet64><<<grid, 256, 0, c->stream>>>(
           (const Packet64 *)c->d_arena_out, c->d_keys, c->d_ranks, c->d_bucket_off,
@@ -418,6 +434,7 @@ WalkParams walk_params(cmi_context *c) {
   p.hist = c->d_hist;
   p.capacity = (uint32_t)c->capacity;
   p.max_padded = c->max_padded;
+  p.max_faces = c->mixed() ? c->max_faces : 0;
   p.kappa = c->d_kappa;
   p.nH = c->d_nH;
   p.xH = c->d_xH;
@@ -435,9 +452,17 @@ bool walk32_three_per_sm(const cmi_context *c) {
   return c->opt.tally_mode == CMI_TALLY_FIXED64 && c->opt.ctas_per_sm == 3;
 }
 
+// the mixed-precision walk: 64-byte packets, FP64 geometry in registers; built
+// for 3 resident CTAs per SM (<= 85 registers)
+template <int kTally>
+constexpr int walkm_min_blocks() { return kTally == 2 ? 3 : 1; }
+
 template <int kTally, bool kReemit>
 void launch_walk32_r(cmi_context *c, const WalkParams &p) {
-  if (kTally == 2 && walk32_three_per_sm(c))
+  if (c->mixed())
+    k_walkm<kWalkThreads, kTally, walkm_min_blocks<kTally>(), kReemit>
+        <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
+  else if (kTally == 2 && walk32_three_per_sm(c))
     k_walk32<kWalkThreads, 2, 3, kReemit>
         <<<c->walk_grid, kWalkThreads, c->walk_smem, c->stream>>>(p);
   else
@@ -453,7 +478,7 @@ void launch_walk32_t(cmi_context *c, const WalkParams &p) {
 
 int launch_walk(cmi_context *c) {
   const WalkParams p = walk_params(c);
-  if (c->fp32()) {
+  if (c->uses_kappa()) {
     switch (c->opt.tally_mode) {
       case 0: launch_walk32_t<0>(c, p); break;
       case 1: launch_walk32_t<1>(c, p); break;
@@ -476,8 +501,8 @@ int config_kernel(cmi_context *c, F fn) {
     return fail(CMI_ERR_NOT_SUPPORTED,
                 "the %s walk needs %zu B of shared memory per CTA (largest subgrid %d cells%s), "
                 "the device allows %d B",
-                c->fp32() ? "FP32" : "FP64", c->walk_smem, (int)c->max_padded,
-                c->fp32() ? ", two packet-ring chunks: lower packets_per_chunk" : "", optin);
+                c->precision_name(), c->walk_smem, (int)c->max_padded,
+                c->uses_kappa() ? ", two packet-ring chunks: lower packets_per_chunk" : "", optin);
   CMI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)c->walk_smem));
   int per_sm = 0;
@@ -492,13 +517,30 @@ int config_kernel(cmi_context *c, F fn) {
 }
 
 int config_walk(cmi_context *c) {
-  if (c->fp32()) {
+  if (c->uses_kappa()) {
     const size_t head = (sizeof(Walk32Shared) + 15) & ~(size_t)15;
     const int tm = c->opt.tally_mode;
     const size_t tally_bytes = (tm == 0 || tm == 2 ? 4 : 8) * (size_t)c->max_padded + 16;
-    c->walk_smem = head + 4 * (size_t)c->max_padded + tally_bytes +
-                   sizeof(Packet32) * 2 * (size_t)c->chunk +
-                   (sizeof(Packet32) + 4) * (kWalkThreads / 32) * kStage;
+    const size_t pb = c->packet_bytes();
+    const size_t faces = c->mixed() ? (((size_t)c->max_faces * 8 + 15) & ~(size_t)15) : 0;
+    c->walk_smem = head + faces + 4 * (size_t)c->max_padded + tally_bytes +
+                   pb * 2 * (size_t)c->chunk + (pb + 4) * (kWalkThreads / 32) * kStage;
+    if (c->mixed()) {
+      switch (tm) {
+        case 0:
+          CMI_TRY(config_kernel(c, k_walkm<kWalkThreads, 0, walkm_min_blocks<0>(), true>));
+          return config_kernel(c, k_walkm<kWalkThreads, 0, walkm_min_blocks<0>(), false>);
+        case 1:
+          CMI_TRY(config_kernel(c, k_walkm<kWalkThreads, 1, walkm_min_blocks<1>(), true>));
+          return config_kernel(c, k_walkm<kWalkThreads, 1, walkm_min_blocks<1>(), false>);
+        case 2:
+          CMI_TRY(config_kernel(c, k_walkm<kWalkThreads, 2, walkm_min_blocks<2>(), true>));
+          return config_kernel(c, k_walkm<kWalkThreads, 2, walkm_min_blocks<2>(), false>);
+        default:
+          CMI_TRY(config_kernel(c, k_walkm<kWalkThreads, 3, walkm_min_blocks<3>(), true>));
+          return config_kernel(c, k_walkm<kWalkThreads, 3, walkm_min_blocks<3>(), false>);
+      }
+    }
     // both builds (with and without reemission) get the attribute; the grid
     // comes from the build without (the same 64-register occupancy bound)
     switch (tm) {
@@ -624,11 +666,13 @@ int enqueue_iteration(cmi_context *c, bool balance) {
   if (direct) CMI_TRY(timed_launch(c, 1, [&] { return launch_plan(c, false); }));
   CMI_TRY(timed_launch(c, 2, [&] {
     if (c->opt.rng == CMI_RNG_RANLUX) {
-      if (c->fp32()) k_emit_ranlux<true><<<egrid, 128, 0, c->stream>>>(e);
-      else k_emit_ranlux<false><<<egrid, 128, 0, c->stream>>>(e);
+      if (c->fp32()) k_emit_ranlux<kPk32><<<egrid, 128, 0, c->stream>>>(e);
+      else if (c->mixed()) k_emit_ranlux<kPkM><<<egrid, 128, 0, c->stream>>>(e);
+      else k_emit_ranlux<kPk64><<<egrid, 128, 0, c->stream>>>(e);
     } else {
-      if (c->fp32()) k_emit_philox_direct<true><<<egrid, 256, 0, c->stream>>>(e);
-      else k_emit_philox_direct<false><<<egrid, 256, 0, c->stream>>>(e);
+      if (c->fp32()) k_emit_philox_direct<kPk32><<<egrid, 256, 0, c->stream>>>(e);
+      else if (c->mixed()) k_emit_philox_direct<kPkM><<<egrid, 256, 0, c->stream>>>(e);
+      else k_emit_philox_direct<kPk64><<<egrid, 256, 0, c->stream>>>(e);
     }
     return CMI_OK;
   }));
@@ -648,7 +692,7 @@ int enqueue_iteration(cmi_context *c, bool balance) {
     b.nH = c->d_nH;
     b.xH = c->d_xH;
     b.J = c->d_J;
-    b.kappa = c->fp32() ? c->d_kappa : nullptr;
+    b.kappa = c->uses_kappa() ? c->d_kappa : nullptr;
     b.stats = c->d_stats;
     b.first_sub = 0;
     b.num_subs = c->S;
@@ -708,15 +752,15 @@ int run(cmi_context *c, int32_t iterations, uint64_t seed, uint32_t first_iterat
   CMI_CUDA(cudaMemcpyAsync(&c->d_state->iteration, &first_iteration, sizeof(uint32_t),
                            cudaMemcpyHostToDevice, c->stream));
   c->last_launches = 0;
-  const bool use_graph = c->opt.use_graph != 0 && balance && !c->timing;
-  if (use_graph && (c->graph_dirty || !c->graph_exec)) {
-    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
+  const bool use_graph = c->opt.use_graph != 0 && !c->timing;
+  const int gi = balance ? 1 : 0;
+  if (use_graph && c->graph_dirty) free_graph(c);
+  if (use_graph && !c->graph_exec[gi]) {
     cudaGraph_t g = nullptr;
     CMI_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     c->enqueued = 0;
     c->capturing = true;
-    const int rc = enqueue_iteration(c, true);
+    const int rc = enqueue_iteration(c, balance);
     c->capturing = false;
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     if (rc != CMI_OK) {
@@ -724,17 +768,17 @@ int run(cmi_context *c, int32_t iterations, uint64_t seed, uint32_t first_iterat
       return rc;
     }
     if (ec != cudaSuccess) return fail(CMI_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
-    const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec, g, 0);
+    const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec[gi], g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess)
       return fail(CMI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
-    c->graph_kernels = c->enqueued;
+    c->graph_kernels[gi] = c->enqueued;
     c->graph_dirty = false;
   }
   for (int32_t it = 0; it < iterations; ++it) {
     if (use_graph) {
-      CMI_CUDA(cudaGraphLaunch(c->graph_exec, c->stream));
-      c->last_launches += c->graph_kernels;
+      CMI_CUDA(cudaGraphLaunch(c->graph_exec[gi], c->stream));
+      c->last_launches += c->graph_kernels[gi];
     } else {
       c->enqueued = 0;
       CMI_TRY(enqueue_iteration(c, balance));
@@ -789,7 +833,7 @@ const char *cmi_last_error_string(void) { return g_last_error.c_str(); }
 void cmi_default_options(cmi_options *o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
-  o->transport_precision = CMI_TRANSPORT_FP32;
+  o->transport_precision = CMI_TRANSPORT_MIXED;
   o->balance_form = CMI_BALANCE_STABLE;
   o->rng = CMI_RNG_PHILOX;
   o->device = 0;
@@ -807,7 +851,8 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
   if (!grids || num_instances <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "no grid given");
   cmi_options opt;
   if (options) opt = *options; else cmi_default_options(&opt);
-  if (opt.transport_precision != CMI_TRANSPORT_FP32 && opt.transport_precision != CMI_TRANSPORT_FP64)
+  if (opt.transport_precision != CMI_TRANSPORT_FP32 && opt.transport_precision != CMI_TRANSPORT_FP64 &&
+      opt.transport_precision != CMI_TRANSPORT_MIXED)
     return fail(CMI_ERR_INVALID_ARGUMENT, "unknown transport precision %d", opt.transport_precision);
   if (opt.balance_form != CMI_BALANCE_REFERENCE && opt.balance_form != CMI_BALANCE_STABLE)
     return fail(CMI_ERR_INVALID_ARGUMENT, "unknown balance form %d", opt.balance_form);
@@ -884,7 +929,7 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
     if (I.padded_per_sub > 8192 || (opt.transport_precision == CMI_TRANSPORT_FP64 && I.padded_per_sub > 4096))
       return bail(fail(CMI_ERR_NOT_SUPPORTED,
                        "instance %d: %d cells per subgrid exceed the shared-memory limit "
-                       "(4096 in FP64, 8192 in FP32)",
+                       "(4096 in FP64, 8192 in FP32 and mixed)",
                        i, I.cells_per_sub));
     I.first_sub = (uint32_t)c->h_sub.size();
     I.nsub = (uint32_t)g.num_subgrid[0] * g.num_subgrid[1] * g.num_subgrid[2];
@@ -923,6 +968,7 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
       c->h_sub.push_back(S);
     }
     c->max_padded = std::max(c->max_padded, I.padded_per_sub);
+    c->max_faces = std::max(c->max_faces, I.sub_ncell[0] + I.sub_ncell[1] + I.sub_ncell[2] + 3);
     // a straight path visits at most ns[0] + ns[1] + ns[2] - 2 subgrids; a
     // packet whose position rounds exactly onto a face of a neighbouring
     // subgrid makes one extra transit that crosses no cell, hence the spares
@@ -937,7 +983,7 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
   if ((rc = dev_alloc(&c->d_sub, c->S)) || (rc = dev_alloc(&c->d_inst, c->inst.size())) ||
       (rc = dev_alloc(&c->d_nH, c->total_padded)) || (rc = dev_alloc(&c->d_xH, c->total_padded)) ||
       (rc = dev_alloc(&c->d_J, c->total_padded)) ||
-      (rc = dev_alloc(&c->d_kappa, c->fp32() ? c->total_padded : 1)) ||
+      (rc = dev_alloc(&c->d_kappa, c->uses_kappa() ? c->total_padded : 1)) ||
       (rc = dev_alloc(&c->d_state, 1)) || (rc = dev_alloc(&c->d_stats, c->inst.size())) ||
       (rc = dev_alloc(&c->d_hist, c->S)) || (rc = dev_alloc(&c->d_bucket_off, c->S)) ||
       (rc = dev_alloc(&c->d_tile_pk, c->ntiles)) || (rc = dev_alloc(&c->d_tile_ch, c->ntiles)) ||
@@ -1259,6 +1305,52 @@ int cmi_run_until_converged(cmi_context *c, int32_t max_iterations, int32_t min_
   return rc;
 }
 
+int cmi_emit_photons(cmi_context *c, uint64_t seed, uint32_t iteration, cmi_photon *out,
+                     uint64_t capacity, uint64_t *count) {
+  CMI_TRY(check_ctx(c));
+  if (!count) return fail(CMI_ERR_INVALID_ARGUMENT, "null count");
+  *count = 0;
+  for (size_t i = 0; i < c->inst.size(); ++i) {
+    if (c->inst[i].num_photon > 0 && c->inst[i].src_lum.empty())
+      return fail(CMI_ERR_INVALID_ARGUMENT, "instance %zu has a packet budget but no sources", i);
+  }
+  const uint64_t budget = total_budget(c);
+  if (budget > 0xF0000000ull)
+    return fail(CMI_ERR_CAPACITY, "%llu packets exceed the 32-bit packet index",
+                (unsigned long long)budget);
+  const uint64_t hs[2] = {seed, 0};
+  CMI_CUDA(cudaMemcpyAsync(&c->d_state->seed, hs, sizeof(uint64_t), cudaMemcpyHostToDevice,
+                           c->stream));
+  CMI_CUDA(cudaMemcpyAsync(&c->d_state->iteration, &iteration, sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, c->stream));
+  const int ninst = (int)c->inst.size();
+  k_begin_iteration<<<1, 128, 0, c->stream>>>(c->d_state, c->d_stats, ninst);
+  k_emission_plan<<<1, 128, 0, c->stream>>>(c->d_inst, ninst, c->d_src, c->nsrc_total,
+                                            c->d_state, c->d_src_count, c->d_src_first,
+                                            c->d_buf_first, c->d_stats, nullptr, c->d_hist);
+  CMI_CUDA(cudaGetLastError());
+  uint32_t emitted = 0;
+  CMI_CUDA(cudaMemcpyAsync(&emitted, &c->d_state->emit_total, sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  *count = emitted;
+  if (emitted == 0) return CMI_OK;
+  if (!out || capacity < emitted)
+    return fail(CMI_ERR_CAPACITY, "%u photons emitted, room for %llu", emitted,
+                (unsigned long long)(out ? capacity : 0));
+  CMI_TRY(ensure_stage(c, sizeof(Packet64) * (size_t)emitted));
+  EmitParams e = emit_params(c);
+  e.photons_out = reinterpret_cast<Packet64 *>(c->d_stage);
+  const int egrid = c->num_sms * 8;
+  if (c->opt.rng == CMI_RNG_RANLUX) k_emit_ranlux<kPk64, true><<<egrid, 128, 0, c->stream>>>(e);
+  else k_emit_philox_direct<kPk64, true><<<egrid, 256, 0, c->stream>>>(e);
+  CMI_CUDA(cudaGetLastError());
+  CMI_CUDA(cudaMemcpyAsync(out, c->d_stage, sizeof(Packet64) * (size_t)emitted,
+                           cudaMemcpyDeviceToHost, c->stream));
+  CMI_CUDA(cudaStreamSynchronize(c->stream));
+  return CMI_OK;
+}
+
 int cmi_shoot_packets(cmi_context *c, uint64_t seed, uint32_t iteration, cmi_stats *stats) {
   CMI_TRY(check_ctx(c, false));
   CMI_TRY(clear_flags(c));
@@ -1301,8 +1393,9 @@ int cmi_transport_packets(cmi_context *c, int32_t instance, const cmi_photon *pa
   u.hist = c->d_hist;
   u.capacity = (uint32_t)c->capacity;
   const int grid = c->num_sms * 8;
-  if (c->fp32()) k_upload<true><<<grid, 256, 0, c->stream>>>(u);
-  else k_upload<false><<<grid, 256, 0, c->stream>>>(u);
+  if (c->fp32()) k_upload<kPk32><<<grid, 256, 0, c->stream>>>(u);
+  else if (c->mixed()) k_upload<kPkM><<<grid, 256, 0, c->stream>>>(u);
+  else k_upload<kPk64><<<grid, 256, 0, c->stream>>>(u);
   CMI_CUDA(cudaGetLastError());
   c->enqueued = 0;
   CMI_TRY(launch_plan(c, true));
@@ -1379,17 +1472,22 @@ static int traverse(cmi_context *c, int32_t instance, uint32_t subgrid, int32_t 
   t.trace_steps = num_steps ? d_steps : nullptr;
   t.st = c->d_state;
   t.tables = c->tables;
-  const size_t smem = (c->fp32() ? 12 : 24) * (size_t)c->max_padded;
+  const size_t smem = (c->fp32() ? 12 : 24) * (size_t)c->max_padded +
+                     (c->mixed() ? 8 * (size_t)c->max_faces : 0);
   if (n > 0) {
     const int grid = (int)((n + 255) / 256);
     if (c->fp32()) {
-      CMI_CUDA(cudaFuncSetAttribute(k_traverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-      k_traverse<true><<<grid, 256, smem, c->stream>>>(t);
-    } else {
-      CMI_CUDA(cudaFuncSetAttribute(k_traverse<false>,
+      CMI_CUDA(cudaFuncSetAttribute(k_traverse<kPk32>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_traverse<false><<<grid, 256, smem, c->stream>>>(t);
+      k_traverse<kPk32><<<grid, 256, smem, c->stream>>>(t);
+    } else if (c->mixed()) {
+      CMI_CUDA(cudaFuncSetAttribute(k_traverse<kPkM>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_traverse<kPkM><<<grid, 256, smem, c->stream>>>(t);
+    } else {
+      CMI_CUDA(cudaFuncSetAttribute(k_traverse<kPk64>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_traverse<kPk64><<<grid, 256, smem, c->stream>>>(t);
     }
     CMI_CUDA(cudaGetLastError());
   }
@@ -1485,7 +1583,7 @@ int cmi_compute_neutral_fraction_subgrids(cmi_context *c, int32_t instance,
   b.nH = c->d_nH;
   b.xH = c->d_xH;
   b.J = c->d_J;
-  b.kappa = c->fp32() ? c->d_kappa : nullptr;
+  b.kappa = c->uses_kappa() ? c->d_kappa : nullptr;
   b.stats = c->d_stats;
   b.first_sub = I.first_sub + first_subgrid;
   b.num_subs = count;

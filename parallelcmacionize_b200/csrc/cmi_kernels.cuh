@@ -259,32 +259,47 @@ struct EmitParams {
   void *arena;
   uint32_t *keys, *ranks, *hist;
   uint32_t capacity;
+  // export (cmi_emit_photons): every packet as a reference Photon at its
+  // index in the iteration (source after source, packet order within one)
+  Packet64 *photons_out;
 };
 
-template <bool kF32>
-__device__ __forceinline__ void make_emitted(const DevSource &S, const DevInstance &I,
-                                             const double dir[3], double tau, Packet32 &p32,
-                                             Packet64 &p64) {
-  if (kF32) {
+// A packet leaving source S (testDensitySubGrid_omp.cpp:580-592) in the
+// record of the transport: FP32 (cell units relative to the source's
+// subgrid), mixed (absolute FP64 position, FP32 optical depth) or FP64.
+__device__ __forceinline__ void make_emitted(const DevSource &S, const DevInstance &,
+                                             const double dir[3], double tau, Packet32 &p) {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      p32.pos[a] = S.pos_cell[a];
-      p32.dir[a] = (float)dir[a];
-    }
-    p32.tau = (float)tau;
-    p32.meta = (uint32_t)kInside;
-  } else {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      p64.pos[a] = S.position[a];
-      p64.dir[a] = dir[a];
-    }
-    p64.tau = tau;
-    p64.sigma = I.sigma;
-    p64.weight = 1.;
-    p64.type = 0;
-    p64.meta = (uint32_t)kInside;
+  for (int a = 0; a < 3; ++a) {
+    p.pos[a] = S.pos_cell[a];
+    p.dir[a] = (float)dir[a];
   }
+  p.tau = (float)tau;
+  p.meta = (uint32_t)kInside;
+}
+__device__ __forceinline__ void make_emitted(const DevSource &S, const DevInstance &,
+                                             const double dir[3], double tau, PacketM &p) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    p.pos[a] = S.position[a];
+    p.dir[a] = dir[a];
+  }
+  p.tau = tau32(tau);
+  p.meta = (uint32_t)kInside;
+  p.pad[0] = p.pad[1] = 0u;
+}
+__device__ __forceinline__ void make_emitted(const DevSource &S, const DevInstance &I,
+                                             const double dir[3], double tau, Packet64 &p) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    p.pos[a] = S.position[a];
+    p.dir[a] = dir[a];
+  }
+  p.tau = tau;
+  p.sigma = I.sigma;
+  p.weight = 1.;
+  p.type = 0;
+  p.meta = (uint32_t)kInside;
 }
 
 // Philox emission straight into the sorted arena.  Packet g of the iteration
@@ -292,8 +307,10 @@ __device__ __forceinline__ void make_emitted(const DevSource &S, const DevInstan
 // in the instance's Philox stream; it goes to bucket_off[subgrid of s] +
 // src_rank0[s] + (g - src_first[s]) (the plan ran on the histogram
 // k_emission_plan filled), so no append atomics and no scatter are needed.
-template <bool kF32>
+// kExport: write the photons to prm.photons_out (index g) instead.
+template <int K, bool kExport = false>
 __global__ void __launch_bounds__(256) k_emit_philox_direct(EmitParams prm) {
+  using Pk = typename PacketOf<K>::type;
   const RoundState *st = prm.st;
   const uint64_t N = st->emit_total;
   const uint64_t seed = st->seed;
@@ -306,26 +323,34 @@ __global__ void __launch_bounds__(256) k_emit_philox_direct(EmitParams prm) {
     const uint64_t id = g - prm.src_first[I.first_source];
     double dir[3], tau;
     philox_packet(seed, S.instance, it, id, dir, tau);
-    Packet32 p32{};
-    Packet64 p64{};
-    make_emitted<kF32>(S, I, dir, tau, p32, p64);
+    if (kExport) {
+      Packet64 ph{};
+      make_emitted(S, I, dir, tau, ph);
+      ph.meta = 0u;
+      prm.photons_out[g] = ph;
+      continue;
+    }
+    Pk pk{};
+    make_emitted(S, I, dir, tau, pk);
     const uint64_t dst = (uint64_t)prm.bucket_off[S.subgrid] + prm.src_rank0[s] +
                          (g - prm.src_first[s]);
     if (dst >= prm.capacity) {
       atomicOr(&prm.st->flags, kFlagArenaOverflow);
       continue;
     }
-    if (kF32) store_packet((Packet32 *)prm.arena_sorted + dst, p32);
-    else store_packet((Packet64 *)prm.arena_sorted + dst, p64);
+    store_packet((Pk *)prm.arena_sorted + dst, pk);
   }
 }
 
 // Emission replaying the reference generator: buffer b of 200 packets (global
 // order over sources) draws from ranlxd(seed + b + iteration * buffers), one
 // draw for the subgrid-copy pick (Source.hpp:94-99), then per packet cos(theta),
-// phi and the optical depth (testDensitySubGrid_omp.cpp:529-597).
-template <bool kF32>
+// phi and the optical depth (testDensitySubGrid_omp.cpp:529-597), with
+// correctly rounded sin, cos and log.  kExport: write the photons to
+// prm.photons_out at their index in the iteration instead of appending.
+template <int K, bool kExport = false>
 __global__ void __launch_bounds__(128) k_emit_ranlux(EmitParams prm) {
+  using Pk = typename PacketOf<K>::type;
   const RoundState *st = prm.st;
   const uint64_t nbuf = prm.buf_first[prm.nsrc_total];
   const uint64_t seed = st->seed;
@@ -349,25 +374,32 @@ __global__ void __launch_bounds__(128) k_emit_ranlux(EmitParams prm) {
     const DevInstance I = prm.inst[S.instance];
     for (uint32_t k = 0; k < 200u; ++k) {
       const bool live = valid && k < n_b;
-      Packet32 p32{};
-      Packet64 p64{};
+      Pk pk{};
       if (live) {
         const double cost = 2. * rng.uniform() - 1.;
         const double phi = 2. * 3.14159265358979323846 * rng.uniform();
         const double s2 = 1. - cost * cost;
         const double sint = sqrt((s2 < 0.) ? 0. : s2);
-        const double dir[3] = {sint * cos(phi), sint * sin(phi), cost};
-        const double tau = -log(rng.uniform());
-        make_emitted<kF32>(S, I, dir, tau, p32, p64);
+        double sinp, cosp;
+        cr_sincos(phi, &sinp, &cosp);
+        const double dir[3] = {sint * cosp, sint * sinp, cost};
+        const double tau = cr_neg_log(rng.uniform());
+        if (kExport) {
+          Packet64 ph{};
+          make_emitted(S, I, dir, tau, ph);
+          ph.meta = 0u;
+          prm.photons_out[prm.src_first[s] + (b - prm.buf_first[s]) * 200u + k] = ph;
+        } else {
+          make_emitted(S, I, dir, tau, pk);
+        }
+      }
+      if (kExport) {
+        if (!__any_sync(kFull, live)) break;
+        continue;
       }
       if (!__any_sync(kFull, live)) break;
-      if (kF32) {
-        warp_append(live, S.subgrid, p32, (Packet32 *)prm.arena, prm.keys, prm.ranks, prm.hist,
-                    prm.st, prm.capacity);
-      } else {
-        warp_append(live, S.subgrid, p64, (Packet64 *)prm.arena, prm.keys, prm.ranks, prm.hist,
-                    prm.st, prm.capacity);
-      }
+      warp_append(live, S.subgrid, pk, (Pk *)prm.arena, prm.keys, prm.ranks, prm.hist, prm.st,
+                  prm.capacity);
     }
   }
 }
@@ -386,7 +418,7 @@ struct UploadParams {
   uint32_t capacity;
 };
 
-template <bool kF32>
+template <int K>
 __global__ void __launch_bounds__(256) k_upload(UploadParams prm) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < prm.n; base += stride) {
@@ -395,6 +427,7 @@ __global__ void __launch_bounds__(256) k_upload(UploadParams prm) {
     uint32_t key = 0;
     Packet32 p32{};
     Packet64 p64{};
+    PacketM pm{};
     if (valid) {
       const uint32_t ls = prm.start[g];
       if (ls >= prm.nsub) {
@@ -404,7 +437,15 @@ __global__ void __launch_bounds__(256) k_upload(UploadParams prm) {
         key = prm.first_sub + ls;
         p64 = prm.photons[g];
         p64.meta = (uint32_t)kInside;
-        if (kF32) {
+        if (K == kPkM) {
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            pm.pos[a] = p64.pos[a];
+            pm.dir[a] = p64.dir[a];
+          }
+          pm.tau = tau32(p64.tau);
+          pm.meta = (uint32_t)kInside;
+        } else if (K == kPk32) {
           const DevSubgrid &S = prm.subs[key];
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
@@ -416,8 +457,11 @@ __global__ void __launch_bounds__(256) k_upload(UploadParams prm) {
         }
       }
     }
-    if (kF32) {
+    if (K == kPk32) {
       warp_append(valid, key, p32, (Packet32 *)prm.arena, prm.keys, prm.ranks, prm.hist,
+                  prm.st, prm.capacity);
+    } else if (K == kPkM) {
+      warp_append(valid, key, pm, (PacketM *)prm.arena, prm.keys, prm.ranks, prm.hist,
                   prm.st, prm.capacity);
     } else {
       warp_append(valid, key, p64, (Packet64 *)prm.arena, prm.keys, prm.ranks, prm.hist,
@@ -665,6 +709,7 @@ struct WalkParams {
   uint32_t *keys, *ranks, *hist;
   uint32_t capacity;
   int32_t max_padded;     // largest padded cell count of any subgrid
+  int32_t max_faces;      // mixed walk: largest nx + ny + nz + 3 of any subgrid
   const float *kappa;     // FP32 mode
   const double *nH, *xH;  // FP64 mode
   double *J;
@@ -701,6 +746,7 @@ struct Walk32Shared {
   float inv_cs_f[3];
   float tally_scale;   // 2^22 / lref
   double tally_unit;   // lref / 2^22 (m)
+  double anchor[3], cs[3], inv_cs[3];  // FP64 geometry (mixed-precision walk)
   int64_t field_offset;
   double sigma;
   double reemission;
@@ -745,6 +791,9 @@ __device__ __forceinline__ void load_subgrid32(Walk32Shared &sh, const DevSubgri
     sh.n[a] = S.ncell[a];
     sh.cs_f[a] = S.cell_size_f[a];
     sh.inv_cs_f[a] = (float)S.inv_cell_size[a];
+    sh.anchor[a] = S.anchor[a];
+    sh.cs[a] = S.cell_size[a];
+    sh.inv_cs[a] = S.inv_cell_size[a];
     lref = fmaxf(lref, S.cell_size_f[a]);
   }
   sh.tally_scale = 4194304.f / lref;
@@ -756,6 +805,35 @@ __device__ __forceinline__ void load_subgrid32(Walk32Shared &sh, const DevSubgri
   sh.instance = S.instance;
   sh.sigma = prm.inst[S.instance].sigma;
   sh.reemission = prm.inst[S.instance].reemission;
+}
+
+// The walk's view of the subgrid staged in shared memory.
+__device__ __forceinline__ void make_view(const Walk32Shared &sh, const float *kappa,
+                                          View32 &v) {
+  v.kappa = kappa;
+  for (int a = 0; a < 3; ++a) {
+    v.n[a] = sh.n[a];
+    v.cs[a] = sh.cs_f[a];
+    v.inv_cs[a] = sh.inv_cs_f[a];
+  }
+  v.nyz = sh.nyz;
+}
+__device__ __forceinline__ void make_view(const Walk32Shared &sh, const float *kappa,
+                                          const double *faces, ViewM &v) {
+  v.kappa = kappa;
+  v.anchor = sh.anchor;
+  v.cs = sh.cs;
+  v.inv_cs = sh.inv_cs;
+  v.faces = faces;
+  for (int a = 0; a < 3; ++a) v.n[a] = sh.n[a];
+  v.face_off[0] = 0;
+  v.face_off[1] = sh.n[0] + 1;
+  v.face_off[2] = sh.n[0] + sh.n[1] + 2;
+  v.nyz = sh.nyz;
+}
+__device__ __forceinline__ void make_view(const Walk32Shared &sh, const float *kappa,
+                                          const double *, View32 &v) {
+  make_view(sh, kappa, v);
 }
 
 // per-thread counters -> instance statistics (one atomic per warp and counter)
@@ -1086,10 +1164,14 @@ constexpr uint32_t kStageFlush = 16;
 // log-normal workload)
 constexpr int kStepsPerCheck = 8;
 
-// kReemit: the build with reemission (any instance with p > 0); without it
-// the absorbed-packet path carries no reemission code.
-template <int kThreads, int kTally, int kMinBlocks, bool kReemit>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm) {
+// One wavefront round of the FP32 opacity walks: W = Walk32 (cell-unit FP32
+// geometry, 32-byte packets) or WalkM (the reference's FP64 geometry, 64-byte
+// packets).  kReemit: the build with reemission (any instance with p > 0);
+// without it the absorbed-packet path carries no reemission code.
+template <class W, int kThreads, int kTally, bool kReemit>
+__device__ __forceinline__ void walk_round(const WalkParams &prm) {
+  using Pk = typename WalkTraits<W>::Packet;
+  using View = typename WalkTraits<W>::View;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Walk32Shared &sh = *reinterpret_cast<Walk32Shared *>(smem_raw);
   constexpr int kWarps = kThreads / 32;
@@ -1097,6 +1179,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
   const uint32_t CH = prm.chunk;
   const uint32_t ch_shift = (uint32_t)(__ffs(CH) - 1);  // CH is a power of two
   unsigned char *cur_ptr = smem_raw + ((sizeof(Walk32Shared) + 15) & ~(size_t)15);
+  double *s_faces = reinterpret_cast<double *>(cur_ptr);  // mixed walk: face table
+  cur_ptr += ((size_t)prm.max_faces * 8 + 15) & ~(size_t)15;
   float *s_kappa = reinterpret_cast<float *>(cur_ptr);
   cur_ptr += (size_t)P * 4;
   Tally32<kTally> tally;
@@ -1117,10 +1201,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
   }
   tally.carry_J = nullptr;
   tally.carry_value = 0.;
-  Packet32 *s_pk = reinterpret_cast<Packet32 *>(cur_ptr);  // [2][CH]
-  cur_ptr += sizeof(Packet32) * 2 * (size_t)CH;
-  Packet32 *s_stage = reinterpret_cast<Packet32 *>(cur_ptr);  // [kWarps][kStage]
-  cur_ptr += sizeof(Packet32) * kWarps * kStage;
+  Pk *s_pk = reinterpret_cast<Pk *>(cur_ptr);  // [2][CH]
+  cur_ptr += sizeof(Pk) * 2 * (size_t)CH;
+  Pk *s_stage = reinterpret_cast<Pk *>(cur_ptr);  // [kWarps][kStage]
+  cur_ptr += sizeof(Pk) * kWarps * kStage;
   uint32_t *s_skey = reinterpret_cast<uint32_t *>(cur_ptr);  // [kWarps][kStage]
 
   RoundState *st = prm.st;
@@ -1145,12 +1229,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
   auto issue = [&](uint32_t k) {
     const uint32_t slot = k & 1u;
     const uint32_t cnt = (k + 1u < sh.seg_chunks) ? CH : sh.seg_n - (k << ch_shift);
-    const uint32_t bytes = cnt * (uint32_t)sizeof(Packet32);
+    const uint32_t bytes = cnt * (uint32_t)sizeof(Pk);
     *(volatile uint32_t *)&sh.uses[slot] = sh.uses[slot] + 1u;
     fence_proxy_async();
     mbar_expect_tx(&sh.mbar_pk[slot], bytes);
     tma_load_1d(s_pk + (size_t)slot * CH,
-                ((const Packet32 *)prm.arena_in) + sh.seg_begin + (k << ch_shift), bytes,
+                ((const Pk *)prm.arena_in) + sh.seg_begin + (k << ch_shift), bytes,
                 &sh.mbar_pk[slot]);
   };
   // packets of chunk k copied out of the ring by this warp (lane 0): the copy
@@ -1186,7 +1270,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
   const uint64_t rseed = st->seed;
   const uint32_t riter = st->iteration;
   uint32_t nstage = 0;  // warp-uniform
-  Packet32 *my_stage = s_stage + warp * kStage;
+  Pk *my_stage = s_stage + warp * kStage;
   uint32_t *my_skey = s_skey + warp * kStage;
 
   auto flush = [&]() {
@@ -1203,13 +1287,13 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
   auto flush_stage = [&](uint32_t n) {
     __syncwarp();
     const bool valid = (uint32_t)lane < n;
-    Packet32 rec{};
+    Pk rec{};
     uint32_t key = 0;
     if (valid) {
       rec = my_stage[lane];
       key = my_skey[lane];
     }
-    warp_append(valid, key, rec, (Packet32 *)prm.arena_out, prm.keys, prm.ranks, prm.hist, st,
+    warp_append(valid, key, rec, (Pk *)prm.arena_out, prm.keys, prm.ranks, prm.hist, st,
                 prm.capacity);
     __syncwarp();
     if ((uint32_t)lane + n < nstage) {
@@ -1263,6 +1347,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
         mbar_wait_bounded(&sh.mbar_field, phase_field, &st->flags);
         phase_field ^= 1u;
         staged = sub;
+        // the mbarrier wait acquires thread 0's writes of the subgrid's geometry
+        if (prm.max_faces > 0) fill_faces(s_faces, sh.n, sh.cs, tid, kThreads);
       }
       if (tid == 0) {
         sh.claim = 0u;
@@ -1275,18 +1361,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
       __syncthreads();
 
       const int limit = sh.n[0] + sh.n[1] + sh.n[2] + 3;
-      View32 v;
-      v.kappa = s_kappa;
-      for (int ax = 0; ax < 3; ++ax) {
-        v.n[ax] = sh.n[ax];
-        v.cs[ax] = sh.cs_f[ax];
-        v.inv_cs[ax] = sh.inv_cs_f[ax];
-      }
-      v.nyz = sh.nyz;
+      View v;
+      make_view(sh, s_kappa, s_faces, v);
       tally.scale = sh.tally_scale;
       tally.carry_J = prm.J + sh.field_offset;
       tally.carry_value = 4294967296.0 * sh.tally_unit * sh.sigma;
-      Walk32 w;
+      W w;
       // lane states: active (walking), pending (finished, not yet routed), free
       bool exhausted = false, active = false, pending = false;
       int pstatus = kRun;
@@ -1306,21 +1386,15 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
               ++c_trans;
               c_cross += (uint32_t)w.steps;  // one step per crossed cell
               double rd[4];
+              uint32_t h[3] = {0u, 0u, 0u};
+              if (kReemit && pstatus == kAbsorbed) w.reemit_counter(v, staged, h);
               if (kReemit && pstatus == kAbsorbed && sh.reemission > 0. &&
-                  reemit_draw_call(rseed, sh.instance, riter, __float_as_uint(w.p[0]) ^ staged,
-                                   __float_as_uint(w.p[1]) ^ (staged * 0x9E3779B9u),
-                                   __float_as_uint(w.p[2]), rcount, sh.reemission, rd)) {
+                  reemit_draw_call(rseed, sh.instance, riter, h[0], h[1], h[2], rcount,
+                                   sh.reemission, rd)) {
                 // re-emitted in place: the lane walks on from the absorption point
                 ++c_reem;
                 ++rcount;
-                Packet32 rp;
-                for (int a = 0; a < 3; ++a) {
-                  rp.pos[a] = w.p[a];
-                  rp.dir[a] = (float)rd[a];
-                }
-                rp.tau = (float)rd[3];
-                rp.meta = (uint32_t)kInside;
-                pstatus = w.begin(rp, v, sh.tab.sign_code);
+                pstatus = w.begin(w.reemitted(v, rd), v, sh.tab.sign_code);
                 route = false;
                 if (pstatus == kRun) {
                   active = true;
@@ -1348,7 +1422,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
             const unsigned am = __ballot_sync(kFull, append);
             if (append) {
               const uint32_t slot = nstage + (uint32_t)__popc(am & lt);
-              my_stage[slot] = w.packet(meta);
+              my_stage[slot] = w.packet(v, meta);
               my_skey[slot] = key;
             }
             nstage += (uint32_t)__popc(am);
@@ -1375,7 +1449,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
               if (((idle >> lane) & 1u) && r < take) {
                 const uint32_t vi = base + r;
                 const uint32_t k = vi >> ch_shift;
-                const Packet32 pk = s_pk[(size_t)(k & 1u) * CH + (vi - (k << ch_shift))];
+                const Pk pk = s_pk[(size_t)(k & 1u) * CH + (vi - (k << ch_shift))];
                 const int entry = w.begin(pk, v, sh.tab.sign_code);
                 rcount = 0u;
                 if (entry == kRun) {
@@ -1403,7 +1477,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
           // up to kStepsPerCheck crossings per lane between two looks at the
           // warp (ballot, batch test, reconvergence), which cost more than the
           // idle lanes the longer stretch leaves
-#pragma unroll
+#pragma unroll(WalkTraits<W>::kUnroll)
           for (int u = 1; u < kStepsPerCheck; ++u) {
             if (status != kRun) break;
             status = w.step(v, tcell, len);
@@ -1429,6 +1503,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm)
     for (int s = 0; s < 2; ++s)
       if (sh.uses[s] != 0u) mbar_wait_bounded(&sh.mbar_pk[s], (sh.uses[s] - 1u) & 1u, &st->flags);
   }
+}
+
+// FP32 walk (cell-unit geometry, 32-byte packets)
+template <int kThreads, int kTally, int kMinBlocks, bool kReemit>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_walk32(WalkParams prm) {
+  walk_round<Walk32, kThreads, kTally, kReemit>(prm);
+}
+
+// Mixed-precision walk (the reference's FP64 geometry, FP32 optical depths
+// and tallies, 64-byte packets)
+template <int kThreads, int kTally, int kMinBlocks, bool kReemit>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_walkm(WalkParams prm) {
+  walk_round<WalkM, kThreads, kTally, kReemit>(prm);
 }
 
 // ---------------------------------------------------------------------------
@@ -1571,8 +1658,13 @@ struct TraverseParams {
   DirectionTables tables;
 };
 
-template <bool kF32>
+// K: the transport's packet record.  The mixed-precision walk takes each
+// photon's own cross section: its cell opacity is (float)(sigma n x) of the
+// photon's sigma (the production kappa when sigma is the instance's), and it
+// tallies (lmin sigma) weight into J as the reference does.
+template <int K>
 __global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
+  constexpr bool kF32 = K == kPk32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ DirectionTables tab;
   const DevSubgrid &S = prm.subs[prm.sub];
@@ -1583,6 +1675,7 @@ __global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
   double *s_n = reinterpret_cast<double *>(smem_raw);
   double *s_x = s_n + P;
   double *s_J = s_x + P;
+  double *s_faces = s_J + P;  // mixed walk: face table (nx + ny + nz + 3 entries)
   if (threadIdx.x < sizeof(DirectionTables) / 4) {
     reinterpret_cast<uint32_t *>(&tab)[threadIdx.x] =
         reinterpret_cast<const uint32_t *>(&prm.tables)[threadIdx.x];
@@ -1598,6 +1691,7 @@ __global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
       s_J[c] = 0.;
     }
   }
+  if (K == kPkM) fill_faces(s_faces, S.ncell, S.cell_size, threadIdx.x, blockDim.x);
   __syncthreads();
   View32 v32;
   View64 v64;
@@ -1653,6 +1747,47 @@ __global__ void __launch_bounds__(256) k_traverse(TraverseParams prm) {
       for (int a = 0; a < 3; ++a) ph.pos[a] = S.anchor[a] + (double)w.p[a] * S.cell_size[a];
       ph.tau = (double)__fsub_rn(w.tau_target, w.tau_done);
       if (status == kExited) result = tab.mask_dir[w.exit_mask(v32, false)];
+    } else if (K == kPkM) {
+      ViewM vm;
+      vm.kappa = nullptr;
+      vm.anchor = S.anchor;
+      vm.cs = S.cell_size;
+      vm.inv_cs = S.inv_cell_size;
+      vm.faces = s_faces;
+      for (int a = 0; a < 3; ++a) vm.n[a] = S.ncell[a];
+      vm.face_off[0] = 0;
+      vm.face_off[1] = S.ncell[0] + 1;
+      vm.face_off[2] = S.ncell[0] + S.ncell[1] + 2;
+      vm.nyz = v64.nyz;
+      PacketM pk;
+      for (int a = 0; a < 3; ++a) {
+        pk.pos[a] = ph.pos[a];
+        pk.dir[a] = ph.dir[a];
+      }
+      pk.tau = tau32(ph.tau);
+      pk.meta = ph.meta;
+      const double sg = ph.sigma, wt = ph.weight;
+      WalkM w;
+      status = w.begin(pk, vm, tab.sign_code);
+      while (status == kRun) {
+        const int c = w.cell;
+        const float k = (float)(sg * s_n[c] * s_x[c]);
+        int cell;
+        float lf;
+        double len;
+        status = w.step_k(vm, k, cell, lf, &len);
+        atomicAdd(&s_J[cell], len * sg * wt);
+        if (tracing && nsteps < prm.max_steps) {
+          prm.trace_cells[nsteps] = cell;
+          prm.trace_len[nsteps] = len;
+        }
+        ++nsteps;
+        if (status == kRun && w.steps > limit) status = kDrop;
+      }
+      const PacketM o = w.packet(vm, 0u);
+      for (int a = 0; a < 3; ++a) ph.pos[a] = o.pos[a];
+      ph.tau = (double)o.tau;
+      if (status == kExited) result = tab.mask_dir[w.exit_mask(vm)];
     } else {
       Walk64 w;
       status = w.begin(ph, v64, tab.sign_code);

@@ -2,14 +2,19 @@
 // (DensitySubGrid.hpp:1180-1323) split into entry + one-crossing steps, so a
 // warp can advance 32 packets one crossing at a time.
 //
-// Two precisions:
+// Three precisions:
 //  * Walk64 -- the reference's FP64 arithmetic, operation for operation.  The
 //    translation unit is compiled with --fmad=false, so no multiply-add is
 //    contracted and every result rounds exactly as on the host.
+//  * WalkM -- mixed: Walk64's geometry (positions, face distances, path
+//    lengths) operation for operation, the cell opacity sigma n x, optical
+//    depths and tallies in FP32.  Cell sequences and path lengths equal the
+//    reference's; only the absorbing cell's length carries FP32 error.
 //  * Walk32 -- FP32 in cell units: the position is kept relative to the
 //    subgrid in units of cells, so cell faces are exact small integers; path
-//    lengths stay in metres, l = (face - p) * (cell_size / d).  Path lengths
-//    go to shared-memory tallies (Tally32) merged into FP64 J.
+//    lengths stay in metres, l = (face - p) * (cell_size / d).
+// Walk32 and WalkM path lengths go to shared-memory tallies (Tally32) merged
+// into FP64 J.
 #pragma once
 
 #include "cmi_device.cuh"
@@ -259,6 +264,207 @@ struct Walk32 {
     pk.meta = meta;
     return pk;
   }
+  __device__ __forceinline__ Packet32 packet(const View32 &, uint32_t meta) const {
+    return packet(meta);
+  }
+
+  // Reemission counter of an absorbed packet in subgrid `sub`: the cell-unit
+  // position bits mixed with the subgrid index.
+  __device__ __forceinline__ void reemit_counter(const View32 &, uint32_t sub,
+                                                 uint32_t h[3]) const {
+    h[0] = __float_as_uint(p[0]) ^ sub;
+    h[1] = __float_as_uint(p[1]) ^ (sub * 0x9E3779B9u);
+    h[2] = __float_as_uint(p[2]);
+  }
+  // The re-emitted packet: same position, drawn direction rd[0..2] and
+  // optical depth rd[3].
+  __device__ __forceinline__ Packet32 reemitted(const View32 &, const double rd[4]) const {
+    Packet32 rp;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      rp.pos[a] = p[a];
+      rp.dir[a] = (float)rd[a];
+    }
+    rp.tau = (float)rd[3];
+    rp.meta = (uint32_t)kInside;
+    return rp;
+  }
+};
+
+// ----------------------------------------------------------------------------
+// Mixed-precision walk: the reference's FP64 geometry, FP32 optical depths
+// ----------------------------------------------------------------------------
+// View of the staged subgrid: FP32 opacity kappa = sigma n x per cell, the
+// subgrid's FP64 anchor, cell size and inverse cell size (shared memory, read
+// where they are needed instead of being held in registers), and its cell
+// faces: faces[face_off[a] + i] = i * cs[a], i = 0..n[a], the reference's
+// idx * cs and (idx + 1.) * cs, computed once per subgrid.
+struct ViewM {
+  const float *kappa;
+  const double *anchor, *cs, *inv_cs;
+  const double *faces;
+  int face_off[3];
+  int n[3];
+  int nyz;
+};
+
+// Fill the face table of a subgrid (threads t = 0, stride of the CTA).
+__device__ __forceinline__ void fill_faces(double *faces, const int n[3], const double cs[3],
+                                           int t, int stride) {
+  const int o1 = n[0] + 1, o2 = o1 + n[1] + 1, total = o2 + n[2] + 1;
+  for (int i = t; i < total; i += stride) {
+    const int a = (i < o1) ? 0 : ((i < o2) ? 1 : 2);
+    const int k = i - ((a == 0) ? 0 : ((a == 1) ? o1 : o2));
+    faces[i] = __dmul_rn((double)k, cs[a]);
+  }
+}
+
+// The geometry of interact (DensitySubGrid.hpp:1186-1305) in FP64, operation
+// for operation: position relative to the anchor, face ahead (idx + 1) * cs
+// or idx * cs, l = (face - pos) * (1 / d), crossed coordinates snapped to
+// their face, pos + lmin * d for the others.  Every cell crossed and every
+// path length up to the last one therefore equal the reference's bit for
+// bit.  The optical depth of a crossing is (float)lmin * kappa, accumulated
+// in FP32; in the absorbing cell the FP32 fraction (tau_target - tau_before) /
+// tau (at most 1; tau_before the depth before the cell) scales the FP64
+// length.  Path lengths reach the tallies as FP32.
+struct WalkM {
+  double pos[3], d[3];
+  double inv[3];   // 1 / d, correctly rounded; +inf when d == 0
+  double face[3];  // the face ahead; +inf when d == 0 (l = +inf)
+  int idx[3];
+  float tau_done, tau_target;
+  int cell;
+  int steps;
+
+  // Entry: DensitySubGrid.hpp:1186-1219 and get_start_index (:428-469).
+  __device__ __forceinline__ int begin(const PacketM &pk, const ViewM &v,
+                                      const uint8_t *sign_code) {
+    const uint8_t code = sign_code[pk.meta & 31u];
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      d[a] = pk.dir[a];
+      pos[a] = __dsub_rn(pk.pos[a], v.anchor[a]);
+      const int s = sign_of(code, a);
+      idx[a] = (s == 0) ? __double2int_rz(__dmul_rn(pos[a], v.inv_cs[a]))
+                        : ((s < 0) ? 0 : v.n[a] - 1);
+      inside = inside && idx[a] >= 0 && idx[a] < v.n[a];
+      const bool moving = d[a] > 0. || d[a] < 0.;
+      inv[a] = moving ? __drcp_rn(d[a]) : __longlong_as_double(0x7ff0000000000000ll);
+    }
+    cell = idx[0] * v.nyz + idx[1] * v.n[2] + idx[2];
+    tau_done = 0.f;
+    tau_target = pk.tau;
+    steps = 0;
+    if (!(tau_done < tau_target)) return kAbsorbed;
+    if (!inside) return kExited;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const bool up = d[a] > 0.;
+      face[a] = (up || d[a] < 0.) ? v.faces[v.face_off[a] + idx[a] + (up ? 1 : 0)]
+                                  : __longlong_as_double(0x7ff0000000000000ll);
+    }
+    return kRun;
+  }
+
+  // One iteration of the loop at DensitySubGrid.hpp:1221-1305; the FP32
+  // path length of the crossed cell `tally_cell` is returned for the tally.
+  __device__ __forceinline__ int step(const ViewM &v, int &tally_cell, float &lmin_out) {
+    return step_k(v, v.kappa[cell], tally_cell, lmin_out, nullptr);
+  }
+
+  // The same with the cell's opacity k given; trace (may be null) receives
+  // the FP64 length.
+  __device__ __forceinline__ int step_k(const ViewM &v, float k, int &tally_cell,
+                                        float &lmin_out, double *trace) {
+    double l[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) l[a] = __dmul_rn(__dsub_rn(face[a], pos[a]), inv[a]);
+    double lmin = min_ref(l[0], min_ref(l[1], l[2]));
+    const float lf = __double2float_rn(lmin);
+    const float tau = __fmul_rn(lf, k);
+    const float tau_before = tau_done;
+    tau_done = __fadd_rn(tau_done, tau);
+    tally_cell = cell;
+    ++steps;
+    if (tau_done >= tau_target) {
+      // the reference's 1 - (tau_done - tau_target) / tau as (tau_target -
+      // tau_before) / tau: no cancellation when the packet stops early in the cell
+      const float frac = fminf(__fdiv_rn(__fsub_rn(tau_target, tau_before), tau), 1.f);
+      lmin = __dmul_rn(lmin, (double)frac);
+      lmin_out = __double2float_rn(lmin);
+      if (trace) *trace = lmin;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        pos[a] = (l[a] == lmin) ? face[a] : __dadd_rn(pos[a], __dmul_rn(lmin, d[a]));
+      return kAbsorbed;
+    }
+    lmin_out = lf;
+    if (trace) *trace = lmin;
+    const int stride[3] = {v.nyz, v.n[2], 1};
+    int out = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const bool cross = l[a] == lmin;
+      pos[a] = cross ? face[a] : __dadd_rn(pos[a], __dmul_rn(lmin, d[a]));
+      if (cross) {
+        const bool up = d[a] > 0.;
+        idx[a] += up ? 1 : -1;
+        cell += up ? stride[a] : -stride[a];
+        if ((unsigned)idx[a] < (unsigned)v.n[a])
+          face[a] = v.faces[v.face_off[a] + idx[a] + (up ? 1 : 0)];
+        else
+          out |= 1 << a;
+      }
+    }
+    return out ? kExited : kRun;
+  }
+
+  // Exit: 6-bit mask from the out-of-range indices (DensitySubGrid.hpp:483-506).
+  __device__ __forceinline__ int exit_mask(const ViewM &v) const {
+    int mask = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mask |= ((idx[a] >= v.n[a]) ? (1 << (5 - 2 * a)) : 0) | ((idx[a] < 0) ? (1 << (4 - 2 * a)) : 0);
+    }
+    return mask;
+  }
+
+  // The packet as the reference leaves it (DensitySubGrid.hpp:1307-1309):
+  // absolute position, remaining optical depth.
+  __device__ __forceinline__ PacketM packet(const ViewM &v, uint32_t meta) const {
+    PacketM pk;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      pk.pos[a] = __dadd_rn(pos[a], v.anchor[a]);
+      pk.dir[a] = d[a];
+    }
+    pk.tau = __fsub_rn(tau_target, tau_done);
+    pk.meta = meta;
+    pk.pad[0] = pk.pad[1] = 0u;
+    return pk;
+  }
+
+  // Reemission counter: the FP64 one of the reference walk (hash of each
+  // absolute coordinate of the absorption point).
+  __device__ __forceinline__ void reemit_counter(const ViewM &v, uint32_t,
+                                                 uint32_t h[3]) const {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) h[a] = reemit_hash(__dadd_rn(pos[a], v.anchor[a]));
+  }
+  __device__ __forceinline__ PacketM reemitted(const ViewM &v, const double rd[4]) const {
+    PacketM rp;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      rp.pos[a] = __dadd_rn(pos[a], v.anchor[a]);
+      rp.dir[a] = rd[a];
+    }
+    rp.tau = tau32(rd[3]);
+    rp.meta = (uint32_t)kInside;
+    rp.pad[0] = rp.pad[1] = 0u;
+    return rp;
+  }
 };
 
 // ----------------------------------------------------------------------------
@@ -381,6 +587,22 @@ struct Walk64 {
     pk.meta = meta;
     return pk;
   }
+};
+
+// Packet record and subgrid view of each walk that runs in the wavefront.
+template <class W> struct WalkTraits;
+// kUnroll: crossings of a stretch unrolled in the walk loop (the mixed walk's
+// FP64 step is long; on the 128^3 log-normal workload its walk took 3.45 /
+// 3.26 / 3.49 ms per iteration unrolled 1 / 4 / 8 times).
+template <> struct WalkTraits<Walk32> {
+  using Packet = Packet32;
+  using View = View32;
+  static constexpr int kUnroll = 8;
+};
+template <> struct WalkTraits<WalkM> {
+  using Packet = PacketM;
+  using View = ViewM;
+  static constexpr int kUnroll = 4;
 };
 
 }  // namespace cmi

@@ -113,18 +113,30 @@ class ReplicaRunner:
 
     # ---- iterations ----
     def run(self, iterations, seed=42):
-        """Returns one summed stats dict per iteration (this rank's packets)."""
-        if self.world == 1 or self.mode == "shards":
+        """Returns one summed stats dict per iteration (this rank's packets).
+
+        One rank without a custom all-reduce, or shards: the engine's own
+        iterations.  Replicas: per iteration the engine's captured transport
+        graph (cmi_shoot_packets), the all-reduce of J ordered on the engine's
+        stream (the collective waits for the transport on the device, and the
+        balance launched after it on the same stream waits for the collective),
+        then the balance for the packets of all ranks."""
+        if self.mode == "shards" or (self.world == 1 and self._allreduce is None):
             out = []
             for it in self.eng.run_iterations(iterations, seed):
                 out.append(_sum_stats(it))
             self.launches = self.eng.last_launch_count()
             self.iteration += iterations
             return out
+        import contextlib
+
         import torch
         import torch.distributed as dist
         grid = self.eng.grids[self.instance]
         lum = float(np.sum(np.asarray(grid.sources, dtype=np.float64).reshape(-1, 4)[:, 3]))
+        engine_stream = None
+        if torch.cuda.is_available() and hasattr(self.eng, "stream"):
+            engine_stream = torch.cuda.ExternalStream(self.eng.stream())
         out = []
         launches = 0
         for _ in range(iterations):
@@ -132,9 +144,9 @@ class ReplicaRunner:
                                         iteration=self.iteration)
             launches += self.eng.last_launch_count()
             J = self._intensity()
-            self._reduce(J, dist.ReduceOp.SUM)
-            if torch.cuda.is_available():
-                torch.cuda.synchronize()
+            with (torch.cuda.stream(engine_stream) if engine_stream is not None
+                  else contextlib.nullcontext()):
+                self._reduce(J, dist.ReduceOp.SUM)
             dx = self.eng.compute_neutral_fraction(self.instance, lum,
                                                    int(grid.num_photon) * self.world)
             launches += 2

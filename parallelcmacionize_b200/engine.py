@@ -35,7 +35,13 @@ TRAVEL_DIRECTIONS = [
 ]
 TravelDirection = {name: i for i, name in enumerate(TRAVEL_DIRECTIONS)}
 
-# shared-memory path-length tallies of the FP32 transport (cmi_tally)
+# transport precisions (cmi_precision): "fp64" the reference's walk operation for
+# operation; "mixed" its FP64 geometry with FP32 opacity, optical depths and
+# tallies; "fp32" the FP32 cell-unit walk
+PRECISIONS = {"fp64": _lib.TRANSPORT_FP64, "fp32": _lib.TRANSPORT_FP32,
+              "mixed": _lib.TRANSPORT_MIXED}
+
+# shared-memory path-length tallies of the FP32 and mixed transports (cmi_tally)
 TALLY_MODES = {"fp32": _lib.TALLY_FP32, "fp32_compensated": _lib.TALLY_FP32_COMPENSATED,
                "fixed64": _lib.TALLY_FIXED64, "fixed64_atomic64": _lib.TALLY_FIXED64_ATOMIC64}
 
@@ -91,7 +97,7 @@ def cube_to_blocked(a, ncell, num_subgrid):
 class TransportEngine:
     """A library context holding one or more grid instances on one GPU."""
 
-    def __init__(self, grids, precision="fp32", balance="stable", rng="philox", device=0,
+    def __init__(self, grids, precision="mixed", balance="stable", rng="philox", device=0,
                  packets_per_chunk=0, tally="fixed64", use_graph=True, ctas_per_sm=0,
                  max_run_chunks=0, refill_lanes=0):
         if isinstance(grids, GridSpec):
@@ -99,7 +105,7 @@ class TransportEngine:
         self.grids = list(grids)
         self._L = _lib.load()
         opts = _lib.default_options(
-            transport_precision={"fp64": _lib.TRANSPORT_FP64, "fp32": _lib.TRANSPORT_FP32}[precision],
+            transport_precision=PRECISIONS[precision],
             balance_form={"reference": _lib.BALANCE_REFERENCE, "stable": _lib.BALANCE_STABLE}[balance],
             rng={"philox": _lib.RNG_PHILOX, "ranlux": _lib.RNG_RANLUX}[rng],
             device=device, packets_per_chunk=packets_per_chunk,
@@ -274,6 +280,19 @@ class TransportEngine:
         check(self._L.cmi_shoot_packets(self._h, int(seed), int(iteration), st))
         self._settled()
         return [st[i].as_dict() for i in range(ninst)]
+
+    def emit_photons(self, seed=42, iteration=0):
+        """fill_buffer for every source: the photons an iteration with this seed
+        and iteration index emits (PHOTON_DTYPE, instance, source, emission order)."""
+        n = C.c_uint64(0)
+        rc = self._L.cmi_emit_photons(self._h, int(seed), int(iteration), None, 0, C.byref(n))
+        if rc not in (_lib.OK, _lib.ERR_CAPACITY):
+            check(rc)
+        out = np.zeros(n.value, PHOTON_DTYPE)
+        if n.value:
+            check(self._L.cmi_emit_photons(self._h, int(seed), int(iteration), ptr(out),
+                                           out.size, C.byref(n)))
+        return out
 
     def transport_packets(self, instance, photons, start_subgrid):
         ph = np.ascontiguousarray(photons, dtype=PHOTON_DTYPE)

@@ -15,6 +15,12 @@ inputs and stores inputs + reference outputs as compressed .npz files:
   transport.npz    interact + neighbour routing through a lattice of subgrids
   stromgren_ensemble.npz  64^3 Stromgren runs (reference code, 8 seeds):
                    radial x_H profiles and ionized radii
+  stromgren_reemission_ensemble.npz  the same with do_reemission's
+                   probability 0.364 (testDensitySubGrid_omp.cpp:675-702)
+  lognormal_ensemble.npz  the 128^3 log-normal workload (8^3 subgrids of 16^3,
+                   sigma_ln = 1, 4 sources, 1e7 packets x 20 iterations from
+                   x_H = 1e-6; reference code, 8 seeds): x_H means over
+                   blocks of 8^3 cells
   dust_walks.npz   DensitySubGrid::propagate and compute_optical_depth on the
                    packet lists of walk_interior16 / walk_entries8 /
                    walk_noncubic (propagate only where the target depth is > 0:
@@ -31,7 +37,7 @@ inputs and stores inputs + reference outputs as compressed .npz files:
                    -DBIN_FILE): neutral_fractions.dat and .bin of a small
                    non-cubic run, one thread (files written in subgrid order)
 
-Usage: python tests/golden/make_golden.py [--skip-ensemble]
+Usage: python tests/golden/make_golden.py [--skip-ensemble | --only-ensembles]
 """
 from __future__ import annotations
 
@@ -276,6 +282,57 @@ def gen_ensemble(seeds=8, packets=1_000_000, iterations=10):
          radii=np.array(radii), packets=packets, iterations=iterations)
 
 
+def gen_ensemble_reemission(seeds=8, packets=1_000_000, iterations=10, probability=0.364):
+    """gen_ensemble's Stromgren sphere with reemission: an absorbed packet is
+    re-emitted in place with probability 0.364 (params.txt:12, the value the
+    reference calls realistic), drawing from its buffer's generator."""
+    box = np.array([-5 * PC, -5 * PC, -5 * PC, 10 * PC, 10 * PC, 10 * PC])
+    ncell, nsub = (64, 64, 64), (8, 8, 8)
+    cells = 64 ** 3
+    nH = np.full(cells, 1e8)
+    xH0 = np.full(cells, 1e-6)
+    from parallelcmacionize_b200.engine import blocked_to_cube
+    from parallelcmacionize_b200.problems import GridSpec, cell_radii, ionized_radius
+    g = GridSpec(box=tuple(box), ncell=ncell, num_subgrid=nsub)
+    r = cell_radii(g).reshape(-1)
+    edges = np.linspace(0, 6.0 * PC, 49)
+    which = np.digitize(r, edges) - 1
+    profiles, radii = [], []
+    for k in range(seeds):
+        x, _ = O.ref_iterations(box, ncell, nsub, nH, xH0, [0.0, 0.0, 0.0], [4.26e49], packets,
+                                iterations, seed=3000 + 10_000_000 * k,
+                                binary="ref_harness_exact", reemission=probability)
+        cube = blocked_to_cube(x, ncell, nsub).reshape(-1)
+        profiles.append(np.array([cube[which == b].mean() for b in range(len(edges) - 1)]))
+        radii.append(ionized_radius(blocked_to_cube(x, ncell, nsub), g))
+        print(f"  reemission ensemble seed {k}: R_ion = {radii[-1] / PC:.4f} pc")
+    save("stromgren_reemission_ensemble.npz", edges=edges, profiles=np.array(profiles),
+         radii=np.array(radii), packets=packets, iterations=iterations,
+         probability=probability)
+
+
+def gen_ensemble_lognormal(seeds=8, packets=10_000_000, iterations=20, block=8):
+    """The 128^3 log-normal workload with the reference code: member k draws
+    buffer b of iteration i from ranlxd(2000 + 10^7 k + b + i * 50000)."""
+    from parallelcmacionize_b200.engine import blocked_to_cube
+    from parallelcmacionize_b200.problems import lognormal_config
+    g, nH = lognormal_config(ncell=128, num_subgrid=8, num_photon=packets, num_sources=4,
+                             sigma_ln=1.0, seed=42)
+    src = np.asarray(g.sources, np.float64)
+    m = 128 // block
+    blocks = []
+    for k in range(seeds):
+        x, its = O.ref_iterations(g.box, g.ncell, g.num_subgrid, nH, np.full(nH.size, 1e-6),
+                                  src[:, :3], src[:, 3], packets, iterations,
+                                  seed=2000 + 10_000_000 * k, binary="ref_harness_exact")
+        cube = blocked_to_cube(x, g.ncell, g.num_subgrid)
+        blocks.append(cube.reshape(m, block, m, block, m, block).mean(axis=(1, 3, 5)))
+        print(f"  log-normal ensemble seed {k}: mean x_H = {x.mean():.6f}, "
+              f"{sum(r['seconds'] for r in its):.1f} s")
+    save("lognormal_ensemble.npz", blocks=np.array(blocks), block=np.array(block),
+         packets=np.array(packets), iterations=np.array(iterations))
+
+
 DUST_CASES = ("interior16", "entries8", "noncubic")
 
 
@@ -385,6 +442,8 @@ def gen_outputs():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-ensemble", action="store_true")
+    ap.add_argument("--only-ensembles", action="store_true",
+                    help="regenerate the reemission and log-normal ensembles only")
     ap.add_argument("--only-outputs", action="store_true",
                     help="regenerate outputs.npz only")
     ap.add_argument("--only-dust", action="store_true",
@@ -392,6 +451,10 @@ def main():
     args = ap.parse_args()
     if args.only_outputs:
         gen_outputs()
+        return
+    if args.only_ensembles:
+        gen_ensemble_reemission()
+        gen_ensemble_lognormal()
         return
     if args.only_dust:
         gen_dust_walks()
@@ -410,6 +473,8 @@ def main():
     gen_outputs()
     if not args.skip_ensemble:
         gen_ensemble()
+        gen_ensemble_reemission()
+        gen_ensemble_lognormal()
 
 
 if __name__ == "__main__":

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_default_options():
     o = _lib.default_options()
-    assert o.transport_precision == _lib.TRANSPORT_FP32
+    assert o.transport_precision == _lib.TRANSPORT_MIXED
     assert o.balance_form == _lib.BALANCE_STABLE
     assert o.tally_mode == _lib.TALLY_FIXED64 and o.use_graph == 1
     with pytest.raises(TypeError):

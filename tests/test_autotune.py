@@ -89,3 +89,50 @@ def test_autotune_on_gpu(tmp_path):
     st = eng.run_iterations(2, seed=3)
     assert all(s[0]["error_flags"] == 0 for s in st)
     eng.close()
+
+
+def test_tune_batch_by_class_then_chunking(tmp_path):
+    """The batch search: the untuned start first, then the subgrid side of
+    each size class (largest class first), then the context's chunking; every
+    step keeps the best so far; the result is cached by the batch's classes."""
+    from parallelcmacionize_b200.autotune import BatchConfig, batch_cache_key
+    from parallelcmacionize_b200.problems import batch_configs
+    cfgs = batch_configs(count=6, select=set())
+    grids = [g for g, _ in cfgs]
+    fields = [None] * len(grids)
+    classes = sorted({"x".join(map(str, g.ncell)) for g in grids},
+                     key=lambda n: -int(n.split("x")[0]))
+
+    def model(cfg, gs, fs):
+        # 8^3 subgrids win for grids of 64 cells or fewer per axis, 16^3 above;
+        # 64-packet chunks and 16-chunk claims win
+        r = 1e10
+        for name, side in cfg.sides:
+            small = int(name.split("x")[0]) <= 64
+            r *= 1.1 if (side == 8) == small else 1.0
+        r /= 1 + abs(np.log2(cfg.packets_per_chunk / 64))
+        r /= 1 + 0.1 * abs(np.log2(cfg.max_run_chunks / 16))
+        return r
+
+    calls = []
+
+    def measure(cfg, gs, fs):
+        calls.append(cfg)
+        assert gs is grids and fs is fields
+        return model(cfg, gs, fs)
+
+    t = Autotuner(cache_path=str(tmp_path / "t.json"), measure=None)
+    best = t.tune_batch(grids, fields, measure=measure)
+    assert calls[0] == BatchConfig(sides=tuple((c, 16) for c in classes))
+    assert dict(best.sides) == {c: (8 if int(c.split("x")[0]) <= 64 else 16) for c in classes}
+    assert (best.packets_per_chunk, best.max_run_chunks) == (64, 16)
+    assert len(t.last_table) == len(calls) == 1 + len(classes) + 3 * 2 - 1
+    n = len(calls)
+    assert t.tune_batch(grids, fields, measure=measure) == best and len(calls) == n
+    key = batch_cache_key("cuda0", grids, "fp32")
+    assert "|batch|" in key and all(c in key for c in classes)
+    # regridding keeps every instance's box, sources and budget
+    for g0, g in zip(grids, best.grids(grids)):
+        assert g.ncell == g0.ncell and g.sources == g0.sources
+        assert g.num_photon == g0.num_photon
+        assert g.sub_ncell[0] == best.side_of(g0)

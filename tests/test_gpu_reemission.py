@@ -114,3 +114,37 @@ def test_stromgren_radius_with_reemission(precision):
     assert abs(radii[0.0] / Rs0 - 1) < 0.02
     assert abs(radii[p] / Rsp - 1) < 0.02
     assert abs(radii[p] / radii[0.0] / (1 - p) ** (-1 / 3) - 1) < 0.02
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp32", "fp64"])
+def test_stromgren_reemission_within_reference_ensemble(precision):
+    """64^3 Stromgren sphere with reemission probability 0.364, 1e6 packets x
+    10 iterations: ionized radius within 3 sigma of the reference's own
+    8-seed ensemble (its interact + the driver's do_reemission,
+    tests/golden/stromgren_reemission_ensemble.npz) and the radial profile
+    bin by bin."""
+    from parallelcmacionize_b200.problems import cell_radii
+    ens = golden("stromgren_reemission_ensemble.npz")
+    spec, nH = stromgren(ncell=64, num_subgrid=8, num_photon=int(ens["packets"]))
+    spec.reemission_probability = float(ens["probability"])
+    eng = TransportEngine(spec, precision=precision, balance="reference")
+    eng.set_fields(0, nH)
+    stats = eng.run_iterations(int(ens["iterations"]), seed=4048)
+    x, _ = eng.get_fields(0, layout="cube")
+    eng.close()
+    for it in stats:
+        assert it[0]["error_flags"] == 0
+    R = ionized_radius(x.reshape(spec.ncell), spec)
+    mu, sd = ens["radii"].mean(), ens["radii"].std(ddof=1)
+    n = ens["radii"].size
+    assert abs(R - mu) < 3 * sd * np.sqrt(1 + 1 / n) + 1e-4 * mu
+    r = cell_radii(spec).reshape(-1)
+    edges = ens["edges"]
+    which = np.digitize(r, edges) - 1
+    prof = np.array([x[which == b].mean() if np.any(which == b) else np.nan
+                     for b in range(len(edges) - 1)])
+    m = np.nanmean(ens["profiles"], axis=0)
+    s = np.nanstd(ens["profiles"], axis=0, ddof=1)
+    ok = np.isfinite(m) & (s > 0)
+    z = np.abs(prof[ok] - m[ok]) / (s[ok] * np.sqrt(1 + 1 / n))
+    assert np.mean(z > 3) <= 0.1 and np.median(z) < 2.0

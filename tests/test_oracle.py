@@ -208,34 +208,79 @@ def test_neighbour_table(oracle_mod):
     assert ngb[0, D["CORNER_PPP"]] == 7 and ngb[7, D["CORNER_NNN"]] == 0
 
 
-def test_fp32_walk_tracks_fp64(oracle_mod):
-    """The FP32 cell-unit walk (the GPU single-precision spec) follows the FP64 walk."""
-    g = golden("walk_interior16.npz")
+WALK_SETS = ["interior16", "entries8", "edges16", "noncubic"]
+
+
+def _reference_walk(g, sg, i):
+    p = g["photons"][i: i + 1].copy()
+    return O.interact(sg, g["nH"], g["xH"], np.zeros_like(g["nH"]), p, int(g["in_dirs"][i]),
+                      max_steps=4096) + (p,)
+
+
+@pytest.mark.parametrize("name", WALK_SETS)
+def test_mixed_walk_reproduces_reference_geometry(oracle_mod, name):
+    """The mixed-precision walk (the GPU default, FP64 geometry and FP32
+    optical depths) on every golden packet: the reference's cell sequence and
+    exit direction, every path length but the absorbing cell's bit for bit,
+    and an exiting packet's position bit for bit.  The absorbing cell's
+    length carries the FP32 error of the accumulated optical depth: at most
+    5.6e-5 relative on these sets (packets whose target depth is below the
+    FP32 range, tau = 1e-300, stop with a length of ~0 in both walks)."""
+    g = golden(f"walk_{name}.npz")
     sg = O.subgrid(g["box"], g["ncell"])
-    kappa = O.kappa32(g["nH"], g["xH"])
-    cs = np.array(sg.cell_size, dtype=np.float32)
-    same_seq = 0
     for i in range(g["photons"].size):
-        p = g["photons"][i: i + 1].copy()
-        _, cells64, len64, _ = O.interact(sg, g["nH"], g["xH"], np.zeros_like(g["nH"]), p, 0,
-                                          max_steps=4096)
+        res, cells, lens, n, p = _reference_walk(g, sg, i)
+        kappa = O.kappa32(g["nH"], g["xH"], float(g["photons"]["sigma"][i]))
+        q = O.packets_mixed(g["photons"][i: i + 1], [int(g["in_dirs"][i])])
+        mres, mcells, mlens, mn = O.interact_mixed(sg, kappa, q, max_steps=4096)
+        assert (mres, mn) == (res, n) and np.array_equal(mcells, cells), i
+        full = n if res != 0 else n - 1
+        assert mlens[:full].tobytes() == lens[:full].tobytes(), i
+        if res != 0:
+            assert q["pos"][0].tobytes() == p["position"][0].tobytes(), i
+        elif n > 0 and g["photons"]["tau"][i] > 1e-30:
+            assert abs(mlens[-1] - lens[-1]) <= 1e-4 * abs(lens[-1]), i
+
+
+# FP32 walk against the reference, measured on the golden sets (non-final
+# path lengths; cs = smallest cell side):
+#   set         worst |dl| / cs   relative: median   p90      max     share > 1e-6
+#   interior16  1.35e-5           1.9e-6            2.2e-5   1.5e-3  0.62
+#   entries8    2.25e-5           4.7e-6            2.9e-5   9.2e-3  0.78
+#   edges16     6.8e-6            0                 6.4e-8   2.7e-5  0.01
+#   noncubic    2.7e-6            8.8e-7            1.0e-5   1.9e-4  0.47
+# Cell sequences are identical on every packet but edges16 #80, whose target
+# optical depth 1e-300 rounds to 0 in FP32 (the FP32 walk stops at entry).
+FP32_SEQUENCE_EXCEPTIONS = {"edges16": {80}}
+
+
+@pytest.mark.parametrize("name", WALK_SETS)
+def test_fp32_walk_error_against_reference(oracle_mod, name):
+    """The FP32 cell-unit walk does NOT meet 1e-6 relative path lengths (a
+    short crossing inherits the absolute FP32 error of its position); its
+    errors stay within 3e-5 of a cell side."""
+    g = golden(f"walk_{name}.npz")
+    sg = O.subgrid(g["box"], g["ncell"])
+    cs = np.array(sg.cell_size, dtype=np.float32)
+    cmin = float(min(sg.cell_size))
+    differ = set()
+    for i in range(g["photons"].size):
+        res, cells, lens, n, _ = _reference_walk(g, sg, i)
+        kappa = O.kappa32(g["nH"], g["xH"], float(g["photons"]["sigma"][i]))
         q = np.zeros(1, O.PACKET32_DTYPE)
-        q["pos"] = ((g["photons"]["position"][i] - g["box"][:3]) * np.array(sg.inv_cell_size))
+        q["pos"] = (g["photons"]["position"][i] - g["box"][:3]) * np.array(sg.inv_cell_size)
         q["dir"] = g["photons"]["direction"][i]
         q["tau"] = g["photons"]["tau"][i]
-        _, cells32, len32, _ = O.interact32(g["ncell"], cs, kappa, None, q, max_steps=4096,
-                                            inv_cell_size=np.array(sg.inv_cell_size))
-        if np.array_equal(cells32, cells64):
-            same_seq += 1
-            # FP32 positions in cell units of a 16-cell subgrid: absolute error
-            # ~ 16 * 2^-24 cells, so the bound is on |dl| / cell size.  The
-            # last segment of an absorbed packet also carries the FP32 error of
-            # the accumulated optical depth, (tau_done - tau_target) / tau.
-            cs0 = float(sg.cell_size[0])
-            err = np.abs(len32.astype(np.float64) - len64) / cs0
-            assert np.all(err[:-1] <= 2e-5)
-            assert err[-1] <= 1e-3
-    assert same_seq >= 0.97 * g["photons"].size
+        q["meta"] = int(g["in_dirs"][i])
+        r32, c32, l32, _ = O.interact32(g["ncell"], cs, kappa, None, q, max_steps=4096,
+                                        inv_cell_size=np.array(sg.inv_cell_size))
+        if r32 != res or not np.array_equal(c32, cells):
+            differ.add(i)
+            continue
+        full = n if res != 0 else n - 1
+        err = np.abs(l32[:full].astype(np.float64) - lens[:full]) / cmin
+        assert np.all(err <= 3e-5), i
+    assert differ == FP32_SEQUENCE_EXCEPTIONS.get(name, set())
 
 
 def test_philox_known_answer(oracle_mod):

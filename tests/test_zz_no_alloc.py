@@ -89,3 +89,55 @@ def test_noalloc_rejects_oversized_buffers():
            t.data_ptr(), 4097, None, t.data_ptr(), t.data_ptr(), t.data_ptr(), None)
     assert rc == _lib.ERR_CAPACITY
     assert b"4096" in _lib.load().cmi_last_error_string()
+
+
+def test_noalloc_reproduces_reference_photons_all_entry_directions():
+    """Straight against the reference's own interact (golden photons of
+    walk_entries8: every one of the 27 entry directions), grouped as
+    do_photon_traversal groups them, with unchanged free device memory once
+    the entry point has been called (no allocation)."""
+    torch = pytest.importorskip("torch")
+    f = _bind()
+    g = golden("walk_entries8.npz")
+    box, ncell = g["box"], g["ncell"]
+    nH_t = torch.from_numpy(g["nH"].copy()).cuda()
+    xH_t = torch.from_numpy(g["xH"].copy()).cuda()
+    J_t = torch.zeros_like(nH_t)
+    seen = set()
+    for d in np.unique(g["in_dirs"]):
+        sel = np.nonzero(g["in_dirs"] == d)[0]
+        _noalloc(f, torch, box, ncell, nH_t, xH_t, J_t, int(d), g["photons"][sel], None)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        out, counts, done = _noalloc(f, torch, box, ncell, nH_t, xH_t, J_t, int(d),
+                                     g["photons"][sel], None)
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+        res = g["result"][sel]
+        expect = np.concatenate([g["out"][sel][res == k] for k in range(27)])
+        assert done == 0
+        assert np.array_equal(counts, np.bincount(res, minlength=27))
+        assert out.tobytes() == expect.tobytes()
+        seen.add(int(d))
+    assert seen == set(range(27))
+
+
+def test_noalloc_empty_buffer_and_oversized_subgrid():
+    torch = pytest.importorskip("torch")
+    f = _bind()
+    t = torch.zeros(4096 * 2, dtype=torch.float64, device="cuda")
+    cnt = torch.full((27,), 7, dtype=torch.int32, device="cuda")
+    done = torch.full((1,), 7, dtype=torch.int32, device="cuda")
+    box = np.array([0, 0, 0, 1, 1, 1], np.float64)
+    nc = np.array([2, 2, 2], np.int32)
+    # n = 0 with no photon buffers: nothing walks, every group is empty
+    rc = f(box.ctypes.data, nc.ctypes.data, t.data_ptr(), t.data_ptr(), t.data_ptr(), 0,
+           None, 0, None, None, cnt.data_ptr(), done.data_ptr(), None)
+    assert rc == _lib.OK
+    assert int(cnt.sum().item()) == 0 and int(done.item()) == 0
+    # more than 4096 cells per subgrid: refused before any launch
+    big = np.array([16, 16, 17], np.int32)
+    rc = f(box.ctypes.data, big.ctypes.data, t.data_ptr(), t.data_ptr(), t.data_ptr(), 0,
+           t.data_ptr(), 1, None, t.data_ptr(), cnt.data_ptr(), done.data_ptr(), None)
+    assert rc == _lib.ERR_NOT_SUPPORTED
+    assert b"4096" in _lib.load().cmi_last_error_string()
