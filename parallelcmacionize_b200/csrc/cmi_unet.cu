@@ -11,21 +11,32 @@
 //
 // Kernels
 //  * k_conv3_tc: 3x3x3 convolution, zero padding, as an implicit GEMM on the
-//    5th-generation tensor cores.  A CTA owns 128 voxels (an 8x4x4 box of one
-//    sample) = the 128 TMEM lanes of an M=128 tcgen05.mma; N = output
-//    channels; one K step = one kernel tap x 16 input channels.  Per step a
-//    TMA tiled load brings the box shifted by the tap (out-of-range voxels
-//    read as zero: the padding) and a bulk copy brings the step's weights,
-//    both into a 4-stage ring in shared memory (32-byte swizzled K-major
-//    operands).  One thread issues the MMAs; tcgen05.commit frees a stage
-//    when its MMA has read it.  The epilogue reads the accumulator with
-//    tcgen05.ld, adds bias, applies leaky ReLU and stores BF16.
+//    5th-generation tensor cores.  A CTA owns 128 voxels (an 8x16x1 box of
+//    one sample) = the 128 TMEM lanes of an M=128 tcgen05.mma; N = output
+//    channels; one K step = one kernel tap x 16 input channels.  The CTA
+//    loads its input box with a one-voxel halo once, by TMA (out-of-range
+//    voxels read as zero: the padding), each 16-channel chunk as two 8-channel
+//    halves, unswizzled, and each half as three copies of 10 x 8 x 4 voxels
+//    shifted by -1, 0, +1 in y, so that within a copy the 8-voxel rows of both
+//    z slices lie one 160-byte stride apart.  The A operand of a tap is the
+//    copy of its y offset addressed at its x and z offsets (K-major, 16-byte
+//    rows, 8-row groups 160 bytes apart, the two channel halves one
+//    half-region apart).  A bulk
+//    copy brings each step's weights (32-byte swizzled K-major) into a 4-stage
+//    ring.  One thread issues the MMAs; tcgen05.commit frees a stage when its
+//    MMA has read it.  The epilogue reads the accumulator with tcgen05.ld,
+//    adds bias, applies leaky ReLU and stores BF16.
 //    The input gradient of a convolution is the same kernel run on dy with
 //    the weights flipped in space and transposed in channels.
-//  * k_conv3_wgrad: weight gradient dW[co][tap][ci] = sum_v dy[v][co] *
-//    x[v + tap][ci]: a reduction over all voxels into a few thousand outputs,
-//    on CUDA cores (FP32 FMA, 4x4 register tiles), one CTA per (tap, voxel
-//    range), FP32 atomics into the gradient.
+//  * k_conv3_wgrad_tc: weight gradient dW[co][tap][ci] = sum_v dy[v][co] *
+//    x[v + tap][ci], a reduction over all voxels, on the tensor cores: per tap
+//    a GEMM with M = 128 output-channel rows (rows past the real count read
+//    zeros), N = input channels and K = voxels, both operands MN-major
+//    (channels contiguous).  A CTA owns a group of taps, one TMEM accumulator
+//    each, and a range of 8x8x2 voxel tiles; per tile it loads dy and the
+//    input with its halo by TMA (the input box of the forward kernel), and
+//    every tap's B operand is that halo at the tap's offset.  At the end the
+//    accumulators are read with tcgen05.ld and added to dW with FP32 atomics.
 //  * pooling, upsampling, activation backward, the 1x1 output head fused
 //    with the MSE loss and its gradient, Adam, weight packing, features.
 #include <cuda.h>
@@ -49,8 +60,13 @@ using bf16 = __nv_bfloat16;
 
 constexpr int kConvThreads = 128;
 constexpr int kStages = 4;
-constexpr int kTileX = 8, kTileY = 4, kTileZ = 4;  // 128 voxels
-constexpr int kABytes = 128 * 32;                  // one K step of the A operand
+constexpr int kTileX = 8, kTileY = 8, kTileZ = 2;  // 128 voxels, row r = x + 8 y + 64 z
+// the input box with its one-voxel halo, per 8-channel half: three copies
+// (y offsets -1, 0, +1) of 10 x 8 x 4 voxels of 16 bytes
+constexpr int kHaloX = kTileX + 2, kHaloZ = kTileZ + 2;
+constexpr int kCopyBytes = kHaloX * kTileY * kHaloZ * 16;  // 5120 B (a multiple of 128)
+constexpr int kHalfBytes = 3 * kCopyBytes;
+static_assert(kCopyBytes % 128 == 0, "TMA destinations are 128-byte aligned");
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr uint32_t kErrTimeout = 1u;
 constexpr int kFeatures = 3;  // input channels of the network
@@ -159,6 +175,13 @@ __device__ __forceinline__ uint64_t sw32_desc(const void *p) {
   const uint64_t a = (smem_u32(p) & 0x3FFFFu) >> 4;
   return a | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) | (6ull << 61);
 }
+// shared-memory matrix descriptor without swizzle: 8 x 16-byte core matrices;
+// lbo: from one core matrix to the next along K (K-major) or along M/N
+// (MN-major), sbo: along the other dimension
+__device__ __forceinline__ uint64_t plain_desc(const void *p, uint32_t lbo, uint32_t sbo) {
+  const uint64_t a = (smem_u32(p) & 0x3FFFFu) >> 4;
+  return a | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+}
 // instruction descriptor: BF16 x BF16 -> F32, A and B K-major, M = 128
 __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
@@ -184,16 +207,17 @@ struct ConvArgs {
 __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant__ CUtensorMap in,
                                                            ConvArgs a) {
   extern __shared__ __align__(1024) unsigned char sm_raw[];
-  // 1024-aligned base for the swizzled operands
+  // 1024-aligned base for the swizzled weight operands
   unsigned char *sm = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~(uintptr_t)1023);
-  unsigned char *sA = sm;                              // [kStages][4096]
-  unsigned char *sB = sm + kStages * kABytes;          // [kStages][npad * 32]
   const int bbytes = a.npad * 32;
-  uint64_t *full = reinterpret_cast<uint64_t *>(sB + kStages * bbytes);
+  unsigned char *sB = sm;                              // [kStages][npad * 32]
+  unsigned char *sH = sB + kStages * bbytes;           // halo [nchunk][2][kHalfBytes]
+  uint64_t *full = reinterpret_cast<uint64_t *>(sH + (size_t)a.nchunk * 2 * kHalfBytes);
   uint64_t *empty = full + kStages;
   uint64_t *done = empty + kStages;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
+  uint64_t *halo = done + 1;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(halo + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tx = a.dims[0] / kTileX, ty = a.dims[1] / kTileY, tz = a.dims[2] / kTileZ;
@@ -214,6 +238,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
       mbar_init(&empty[s], 1);
     }
     mbar_init(done, 1);
+    mbar_init(halo, 1);
     fence_mbar_init();
   }
   if (warp == 0) {
@@ -231,22 +256,34 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
   bool ok = true;
   if (tid == 0) {
     const uint32_t idesc = idesc_bf16(a.npad);
+    // the input box with its halo, once: chunk c, half h, y offset d at
+    // sH + (2c + h) * kHalfBytes + d * kCopyBytes
+    mbar_expect_tx(halo, (uint32_t)(a.nchunk * 2 * kHalfBytes));
+    for (int c = 0; c < a.nchunk; ++c)
+      for (int h = 0; h < 2; ++h)
+        for (int d = 0; d < 3; ++d)
+          tma_load_5d(sH + (size_t)(2 * c + h) * kHalfBytes + d * kCopyBytes, &in,
+                      c * 16 + h * 8, x0 - 1, y0 - 1 + d, z0 - 1, n, halo);
     auto load = [&](int k) {
       const int s = k % kStages;
-      const int tap = k / a.nchunk, ch = k - tap * a.nchunk;
-      const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-      mbar_expect_tx(&full[s], (uint32_t)(kABytes + bbytes));
-      tma_load_5d(sA + s * kABytes, &in, ch * 16, x0 + dx, y0 + dy, z0 + dz, n, &full[s]);
+      mbar_expect_tx(&full[s], (uint32_t)bbytes);
       bulk_load(sB + s * bbytes, a.wpack + (size_t)k * a.npad * 16, (uint32_t)bbytes, &full[s]);
     };
     for (int k = 0; k < kStages && k < nsteps; ++k) load(k);
+    ok = mbar_wait(halo, 0u, a.err);
     for (int k = 0; k < nsteps && ok; ++k) {
       const int s = k % kStages;
       const uint32_t ph = (uint32_t)(k / kStages) & 1u;
       ok = mbar_wait(&full[s], ph, a.err);
       if (!ok) break;
       tc_fence_after();
-      const uint64_t ad = sw32_desc(sA + s * kABytes);
+      // tap (dz, dy, dx) reads the input at (x + dx, y + dy, z + dz): copy dy + 1
+      // of the halo, shifted by (dx + 1, dz + 1) voxels
+      const int tap = k / a.nchunk, c = k - tap * a.nchunk;
+      const int hz = tap / 9, hy = (tap / 3) % 3, hx = tap % 3;
+      const unsigned char *a0 = sH + (size_t)(2 * c) * kHalfBytes + hy * kCopyBytes +
+                                (hz * kTileY * kHaloX + hx) * 16;
+      const uint64_t ad = plain_desc(a0, (uint32_t)kHalfBytes, (uint32_t)(kHaloX * 16));
       const uint64_t bd = sw32_desc(sB + s * bbytes);
       const uint32_t acc = k > 0 ? 1u : 0u;
       asm volatile(
@@ -276,9 +313,9 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
   const bool done_ok = __all_sync(0xffffffffu, mbar_wait(done, 0u, a.err));
   tc_fence_after();
   if (done_ok) {
-    // row r = voxel (x0 + r % 8, y0 + (r / 8) % 4, z0 + r / 32); warp w owns lanes 32w..
+    // row r = voxel (x0 + r % 8, y0 + (r / 8) % 8, z0 + r / 64); warp w owns lanes 32w..
     const int r = warp * 32 + lane;
-    const int vx = x0 + (r & 7), vy = y0 + ((r >> 3) & 3), vz = z0 + (r >> 5);
+    const int vx = x0 + (r & 7), vy = y0 + ((r >> 3) & 7), vz = z0 + (r >> 6);
     const size_t vox = (((size_t)n * a.dims[2] + vz) * a.dims[1] + vy) * a.dims[0] + vx;
     bf16 *dst = a.out + vox * a.out_ctot + a.out_c0;
     for (int j = 0; j < a.npad; j += 16) {
@@ -315,117 +352,170 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
 }
 
 // ---------------------------------------------------------------------------
-// weight gradient (CUDA cores): dW[co][tap][ci] over all voxels
+// weight gradient on the tensor cores
 // ---------------------------------------------------------------------------
-struct WgradArgs {
-  const bf16 *x;   // layer input
-  int x_ctot, x_c0, cin;     // channels of the input tensor, first input channel, count (x16)
-  const bf16 *dy;  // gradient at the layer output (after the activation derivative)
-  int dy_ctot, dy_c0, cout;  // count multiple of 16
+struct WgradTcArgs {
+  int cout;                  // dy channels (storage, multiple of 16, <= 128)
+  int nchunk;                // 16-channel chunks of the input (N = 16 nchunk <= 256)
   int dims[3];
   int batch;
-  int splits;      // voxel ranges per tap
-  float *dw;       // [cout_real][27][cin_real] (FP32, accumulated)
+  int tap0, taps;            // taps of this launch's CTAs: blockIdx.y selects a group
+  int taps_per_cta;
+  uint32_t tmem_cols;        // power of two >= taps_per_cta * N (<= 256: two CTAs per SM)
+  int tiles_per_cta;         // voxel tiles of one CTA (blockIdx.x)
+  float *dw;                 // [cout_real][27][cin_real] (FP32, accumulated)
   const int *ci_map;         // storage input channel -> real input channel or -1
   int cin_real, cout_real;
+  uint32_t *err;
 };
-// One CTA per (tap, range of x-rows); a row is the X voxels of one (sample,
-// z, y).  Per row the CTA stages dy (cout channels) and the input row shifted
-// by the tap (cin channels, zero outside the grid) as FP32 in shared memory.
-// Threads own 4x4 (co, ci) register tiles; when there are fewer tiles than
-// threads, G = 256 / tiles groups split the row's voxels and are summed in
-// shared memory before the atomics.
-__global__ void __launch_bounds__(256) k_conv3_wgrad(WgradArgs a) {
-  extern __shared__ __align__(16) float wsm[];
-  const int X = a.dims[0], Y = a.dims[1], Z = a.dims[2];
-  float *sdy = wsm;                 // [X][cout]
-  float *sx = wsm + X * a.cout;     // [X][cin]
-  const int tap = blockIdx.x, split = blockIdx.y;
-  const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-  const int rows = a.batch * Z * Y;
-  const int per = (rows + a.splits - 1) / a.splits;
-  const int r0 = split * per, r1 = min(rows, r0 + per);
-  const int tci = a.cin / 4, tiles = (a.cout / 4) * tci;
-  const int groups = max(1, (int)blockDim.x / tiles);
-  const int tile = threadIdx.x % tiles, group = threadIdx.x / tiles;
-  const bool active = group < groups;
-  const int co0 = (tile / tci) * 4, ci0 = (tile % tci) * 4;
-  const int vq = a.cout / 8, xq = a.cin / 8;  // 16-byte chunks per voxel
-  float acc[4][4] = {};
-  for (int row = r0; row < r1; ++row) {
-    const int y = row % Y, z = (row / Y) % Z, s = row / (Y * Z);
-    const int qy = y + dy, qz = z + dz;
-    const bool row_in = qy >= 0 && qy < Y && qz >= 0 && qz < Z;
-    const size_t base = (((size_t)s * Z + z) * Y + y) * X;
-    const size_t qbase = (((size_t)s * Z + qz) * Y + qy) * X;
-    __syncthreads();
-    for (int i = threadIdx.x; i < X * vq; i += blockDim.x) {
-      const int v = i / vq, q = i - v * vq;
-      const uint4 raw = *reinterpret_cast<const uint4 *>(a.dy + (base + v) * a.dy_ctot + a.dy_c0 +
-                                                         q * 8);
-      const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw);
-      const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]),
-                   f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
-      float4 *o = reinterpret_cast<float4 *>(sdy + v * a.cout + q * 8);
-      o[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
-      o[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
-    }
-    for (int i = threadIdx.x; i < X * xq; i += blockDim.x) {
-      const int v = i / xq, q = i - v * xq;
-      const int qx = v + dx;
-      float4 *o = reinterpret_cast<float4 *>(sx + v * a.cin + q * 8);
-      if (row_in && qx >= 0 && qx < X) {
-        const uint4 raw = *reinterpret_cast<const uint4 *>(a.x + (qbase + qx) * a.x_ctot +
-                                                           a.x_c0 + q * 8);
-        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw);
-        const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]),
-                     f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
-        o[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
-        o[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
-      } else {
-        o[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-        o[1] = o[0];
+constexpr int kDyGroupBytes = kTileX * kTileY * kTileZ * 16;  // 8 output channels: 2 KB
+constexpr int kDyBytes = 16 * kDyGroupBytes;          // the 128 A rows (16 groups of 8)
+
+__global__ void __launch_bounds__(kConvThreads) k_conv3_wgrad_tc(
+    const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dymap,
+    WgradTcArgs a) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  unsigned char *sm = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~(uintptr_t)1023);
+  unsigned char *sA = sm;                 // dy: [16 groups of 8 channels][16 y][8 x][8]
+  unsigned char *sH = sA + kDyBytes;      // input halo: [2 nchunk][3 copies][4][8][10][8]
+  uint64_t *loaded = reinterpret_cast<uint64_t *>(sH + (size_t)a.nchunk * 2 * kHalfBytes);
+  uint64_t *mma_done = loaded + 1;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(mma_done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int N = a.nchunk * 16;
+  const int t0 = a.tap0 + blockIdx.y * a.taps_per_cta;
+  const int ntap = min(a.taps_per_cta, a.tap0 + a.taps - t0);
+  const int tx = a.dims[0] / kTileX, ty = a.dims[1] / kTileY, tz = a.dims[2] / kTileZ;
+  const int tiles = a.batch * tx * ty * tz;
+  const int tile0 = blockIdx.x * a.tiles_per_cta, tile1 = min(tiles, tile0 + a.tiles_per_cta);
+
+  // rows of A past the real output channels read zeros
+  for (int i = tid; i < (kDyBytes - (a.cout / 8) * kDyGroupBytes) / 16; i += kConvThreads)
+    reinterpret_cast<uint4 *>(sA + (a.cout / 8) * kDyGroupBytes)[i] = make_uint4(0, 0, 0, 0);
+  if (tid == 0) {
+    mbar_init(loaded, 1);
+    mbar_init(mma_done, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(a.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // the zeros above are generic-proxy writes that the MMAs read through the async proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  bool ok = true;
+  if (tid == 0 && ntap > 0) {
+    // BF16 x BF16 -> F32, A and B MN-major, M = 128, N
+    const uint32_t idesc = idesc_bf16(N) | (1u << 15) | (1u << 16);
+    const uint32_t bytes = (uint32_t)((a.cout / 8) * kDyGroupBytes + a.nchunk * 2 * kHalfBytes);
+    bool first = true;
+    uint32_t phase = 0;
+    for (int t = tile0; t < tile1 && ok; ++t) {
+      int r = t;
+      const int bx = r % tx;
+      r /= tx;
+      const int by = r % ty;
+      r /= ty;
+      const int bz = r % tz;
+      const int n = r / tz;
+      const int x0 = bx * kTileX, y0 = by * kTileY, z0 = bz * kTileZ;
+      if (!first) {  // the previous tile's MMAs have read the buffers
+        ok = mbar_wait(mma_done, phase ^ 1u, a.err);
+        if (!ok) break;
       }
+      mbar_expect_tx(loaded, bytes);
+      for (int g = 0; g < a.cout / 8; ++g)
+        tma_load_5d(sA + g * kDyGroupBytes, &dymap, g * 8, x0, y0, z0, n, loaded);
+      for (int c = 0; c < a.nchunk; ++c)
+        for (int h = 0; h < 2; ++h)
+          for (int d = 0; d < 3; ++d)
+            tma_load_5d(sH + (size_t)(2 * c + h) * kHalfBytes + d * kCopyBytes, &xmap,
+                        c * 16 + h * 8, x0 - 1, y0 - 1 + d, z0 - 1, n, loaded);
+      ok = mbar_wait(loaded, phase, a.err);
+      if (!ok) break;
+      tc_fence_after();
+      for (int j = 0; j < ntap; ++j) {
+        const int tap = t0 + j;
+        const int hz = tap / 9, hy = (tap / 3) % 3, hx = tap % 3;
+        const unsigned char *b0 = sH + hy * kCopyBytes + (hz * kTileY * kHaloX + hx) * 16;
+        // K step k: tile rows q = 2k, 2k + 1 of 8 voxels (q = y + 8 z)
+        for (int k = 0; k < kTileY * kTileZ / 2; ++k) {
+          // A: core matrices of 8 voxels x 8 channels; LBO along K (next row),
+          // SBO along M (next 8 output channels)
+          const uint64_t ad = plain_desc(sA + k * 2 * kTileX * 16, kTileX * 16, kDyGroupBytes);
+          // B: rows 2k, 2k + 1 of the tap's halo copy at its x and z offsets;
+          // SBO along N (next 8 input channels: the next half region)
+          const uint64_t bd =
+              plain_desc(b0 + k * 2 * kHaloX * 16, kHaloX * 16, (uint32_t)kHalfBytes);
+          const uint32_t acc = (first && k == 0) ? 0u : 1u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(
+                  tmem + (uint32_t)(j * N)),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(mma_done))
+          : "memory");
+      first = false;
+      phase ^= 1u;
     }
-    __syncthreads();
-    if (active) {
-      for (int v = group; v < X; v += groups) {
-        const float4 d = *reinterpret_cast<const float4 *>(sdy + v * a.cout + co0);
-        const float4 xx = *reinterpret_cast<const float4 *>(sx + v * a.cin + ci0);
-        const float dv[4] = {d.x, d.y, d.z, d.w}, xv[4] = {xx.x, xx.y, xx.z, xx.w};
+    if (!first && ok) ok = mbar_wait(mma_done, phase ^ 1u, a.err);
+    if (first) ok = false;  // no tile: nothing accumulated
+  }
+  __syncwarp();
+  // thread 0 knows whether the accumulators are complete; share it
+  __shared__ int s_have;
+  if (tid == 0) s_have = ok ? 1 : 0;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (s_have && warp * 32 < a.cout_real) {
+    // lane = output channel (TMEM lane), columns = input channels
+    const int co = warp * 32 + lane;
+    for (int j = 0; j < ntap; ++j) {
+      const int tap = t0 + j;
+      for (int c = 0; c < N; c += 16) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * N + c);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+            "%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (co < a.cout_real) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(dv[i], xv[j], acc[i][j]);
+          for (int e = 0; e < 16; ++e) {
+            const int ci = a.ci_map[c + e];
+            const float f = __uint_as_float(v[e]);
+            if (ci >= 0 && f != 0.f)
+              atomicAdd(&a.dw[((size_t)co * 27 + tap) * a.cin_real + ci], f);
+          }
+        }
       }
     }
   }
-  // sum the groups (reusing the staging area: groups * tiles * 16 floats)
+  tc_fence_before();
   __syncthreads();
-  float *red = wsm;
-  if (active && groups > 1) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) red[(group * tiles + tile) * 16 + i * 4 + j] = acc[i][j];
-  }
-  __syncthreads();
-  if (active && group == 0) {
-    for (int g = 1; g < groups; ++g)
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += red[(g * tiles + tile) * 16 + i * 4 + j];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      if (co0 + i >= a.cout_real) continue;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int ci = a.ci_map[ci0 + j];
-        if (ci >= 0 && acc[i][j] != 0.f)
-          atomicAdd(&a.dw[((size_t)(co0 + i) * 27 + tap) * a.cin_real + ci], acc[i][j]);
-      }
-    }
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(a.tmem_cols)
+                 : "memory");
   }
 }
 
@@ -1018,7 +1108,9 @@ int grid_for(long long n, int threads = 256) {
   return (int)std::min<long long>((n + threads - 1) / threads, 148LL * 16);
 }
 
-// tensor map of an input slice: dims (channels, X, Y, Z, batch), box (16, 8, 4, 4, 1)
+// tensor map of an input slice: dims (channels, X, Y, Z, batch), box (8, 10, 8, 4, 1):
+// one 8-channel half of one y-shifted copy of a convolution tile's input with its
+// x and z halo, unswizzled
 int make_map(CUtensorMap *map, const Slice &s, int batch, const int dims[3]) {
   EncodeTiledFn enc;
   UN_TRY(get_encoder(&enc));
@@ -1027,25 +1119,26 @@ int make_map(CUtensorMap *map, const Slice &s, int batch, const int dims[3]) {
   const cuuint64_t row = (cuuint64_t)s.ctot * sizeof(bf16);
   const cuuint64_t gstride[4] = {row, row * dims[0], row * dims[0] * dims[1],
                                  row * dims[0] * dims[1] * dims[2]};
-  const cuuint32_t box[5] = {16, kTileX, kTileY, kTileZ, 1};
+  const cuuint32_t box[5] = {8, kHaloX, kTileY, kHaloZ, 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void *)(s.base + s.c0), gdim,
                          gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(CMI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return CMI_OK;
 }
 
-size_t conv_smem(int npad) {
-  return 1024 + (size_t)kStages * (kABytes + npad * 32) + (2 * kStages + 1) * 8 + 16;
+size_t conv_smem(int npad, int nchunk) {
+  return 1024 + (size_t)kStages * npad * 32 + (size_t)nchunk * 2 * kHalfBytes +
+         (2 * kStages + 2) * 8 + 16;
 }
 
 // y = act(conv(x) + b) into out slice; wpack rows = out.c
 int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, const Slice &out,
             int act, int batch, const int dims[3]) {
   if (dims[0] % kTileX || dims[1] % kTileY || dims[2] % kTileZ)
-    return fail(CMI_ERR_INVALID_ARGUMENT, "grid %dx%dx%d is not a multiple of the 8x4x4 tile",
+    return fail(CMI_ERR_INVALID_ARGUMENT, "grid %dx%dx%d is not a multiple of the 8x8x2 tile",
                 dims[0], dims[1], dims[2]);
   if (in.c % 16 || out.c % 16 || out.c > 256 || out.c < 16)
     return fail(CMI_ERR_INVALID_ARGUMENT, "channel counts must be multiples of 16 (<= 256)");
@@ -1063,7 +1156,7 @@ int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, 
   a.act = act;
   a.slope = u->slope;
   a.err = u->d_err;
-  const size_t smem = conv_smem(out.c);
+  const size_t smem = conv_smem(out.c, a.nchunk);
   UN_CUDA(cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem));
   const int tiles = batch * (dims[0] / kTileX) * (dims[1] / kTileY) * (dims[2] / kTileZ);
@@ -1072,34 +1165,64 @@ int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, 
   return CMI_OK;
 }
 
+// tensor map of a tile's dy: dims (channels, X, Y, Z, batch), box (8, 8, 8, 2, 1)
+int make_dy_map(CUtensorMap *map, const Slice &s, int batch, const int dims[3]) {
+  EncodeTiledFn enc;
+  UN_TRY(get_encoder(&enc));
+  const cuuint64_t gdim[5] = {(cuuint64_t)s.c, (cuuint64_t)dims[0], (cuuint64_t)dims[1],
+                              (cuuint64_t)dims[2], (cuuint64_t)batch};
+  const cuuint64_t row = (cuuint64_t)s.ctot * sizeof(bf16);
+  const cuuint64_t gstride[4] = {row, row * dims[0], row * dims[0] * dims[1],
+                                 row * dims[0] * dims[1] * dims[2]};
+  const cuuint32_t box[5] = {8, kTileX, kTileY, kTileZ, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void *)(s.base + s.c0), gdim,
+                         gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(CMI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return CMI_OK;
+}
+
 int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *ci_map,
           int cin_real, int cout_real, int batch, const int dims[3]) {
-  WgradArgs a{};
+  if (dims[0] % kTileX || dims[1] % kTileY || dims[2] % kTileZ)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "grid %dx%dx%d is not a multiple of the 8x8x2 tile",
+                dims[0], dims[1], dims[2]);
+  if (x.c % 16 || dy.c % 16 || x.c < 16 || x.c > 256 || dy.c < 16 || dy.c > 128)
+    return fail(CMI_ERR_NOT_SUPPORTED,
+                "weight gradient: input channels must be 16..256, output channels 16..128, "
+                "multiples of 16");
+  CUtensorMap xm, dym;
+  UN_TRY(make_map(&xm, x, batch, dims));
+  UN_TRY(make_dy_map(&dym, dy, batch, dims));
+  WgradTcArgs a{};
+  a.cout = dy.c;
+  a.nchunk = x.c / 16;
+  for (int k = 0; k < 3; ++k) a.dims[k] = dims[k];
+  a.batch = batch;
+  a.tap0 = 0;
+  a.taps = 27;
+  const int N = x.c;
+  a.taps_per_cta = std::min(27, 256 / N);
+  uint32_t cols = 32;
+  while (cols < (uint32_t)(a.taps_per_cta * N)) cols <<= 1;
+  a.tmem_cols = cols;
+  const int groups = (27 + a.taps_per_cta - 1) / a.taps_per_cta;
+  const int tiles = batch * (dims[0] / kTileX) * (dims[1] / kTileY) * (dims[2] / kTileZ);
+  // about two CTAs per SM over all tap groups
+  const int want = std::max(1, 2 * 148 / groups);
+  a.tiles_per_cta = (tiles + want - 1) / want;
+  const int ctas = (tiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
+  a.dw = dw;
   a.ci_map = ci_map;
   a.cin_real = cin_real;
   a.cout_real = cout_real;
-  a.x = x.base;
-  a.x_ctot = x.ctot;
-  a.x_c0 = x.c0;
-  a.cin = x.c;
-  a.dy = dy.base;
-  a.dy_ctot = dy.ctot;
-  a.dy_c0 = dy.c0;
-  a.cout = dy.c;
-  for (int k = 0; k < 3; ++k) a.dims[k] = dims[k];
-  a.batch = batch;
-  const int rows = batch * dims[1] * dims[2];
-  // about 4 waves of (27 taps x splits) CTAs, at least 8 rows each
-  a.splits = std::max(1, std::min(rows / 8, 148 * 8 * 4 / 27));
-  a.dw = dw;
-  const int tiles = (a.cout / 4) * (a.cin / 4);
-  if (tiles > 256) return fail(CMI_ERR_NOT_SUPPORTED, "weight-gradient tile count above 256");
-  const size_t stage = sizeof(float) * (size_t)dims[0] * (a.cout + a.cin);
-  const size_t red = sizeof(float) * (size_t)(256 / tiles) * tiles * 16;
-  const size_t smem = std::max(stage, red);
-  UN_CUDA(cudaFuncSetAttribute(k_conv3_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  a.err = u->d_err;
+  const size_t smem = 1024 + (size_t)kDyBytes + (size_t)a.nchunk * 2 * kHalfBytes + 64;
+  UN_CUDA(cudaFuncSetAttribute(k_conv3_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem));
-  k_conv3_wgrad<<<dim3(27, a.splits), 256, smem, u->stream>>>(a);
+  k_conv3_wgrad_tc<<<dim3(ctas, groups), kConvThreads, smem, u->stream>>>(xm, dym, a);
   UN_CUDA(cudaGetLastError());
   return CMI_OK;
 }

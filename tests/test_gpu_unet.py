@@ -81,7 +81,7 @@ def net():
 @pytest.mark.parametrize("cin,cout", [(16, 16), (32, 48), (80, 32)])
 def test_conv3_forward_matches_oracle(net, cin, cout):
     rng = np.random.default_rng(cin + cout)
-    shape = (2, 8, 8, 16)  # B, Z, Y, X
+    shape = (2, 4, 16, 16)  # B, Z, Y, X
     x = U.bf16_round(rng.normal(size=shape + (cin,)))
     W = rng.normal(0, 0.2, size=(cout, 27, cin))
     bias = rng.normal(0, 0.1, size=cout).astype(np.float32).astype(np.float64)
@@ -104,7 +104,7 @@ def test_conv3_input_gradient_matches_oracle(net):
 def test_conv3_weight_gradient_matches_oracle(net):
     rng = np.random.default_rng(6)
     cin, cout = 32, 16
-    shape = (2, 8, 8, 16)
+    shape = (2, 4, 16, 16)
     x = U.bf16_round(rng.normal(size=shape + (cin,)))
     dy = U.bf16_round(rng.normal(size=shape + (cout,)))
     dw = torch.zeros(cout * 27 * cin, dtype=torch.float32, device="cuda")
@@ -112,7 +112,7 @@ def test_conv3_weight_gradient_matches_oracle(net):
     torch.cuda.synchronize()
     _lib.check_unet(net._L.cmi_unet_conv3_wgrad(net._h, C.c_void_p(xt.data_ptr()), cin,
                                                 C.c_void_p(dyt.data_ptr()), cout, 2,
-                                                _dims(16, 8, 8), C.c_void_p(dw.data_ptr())))
+                                                _dims(16, 16, 4), C.c_void_p(dw.data_ptr())))
     got = dw.cpu().numpy().reshape(cout, 27, cin)
     ref = U.conv3_weight_grad(x, dy)
     # sums of 2048 products in FP32 in another order
