@@ -11,32 +11,36 @@
 //
 // Kernels
 //  * k_conv3_tc: 3x3x3 convolution, zero padding, as an implicit GEMM on the
-//    5th-generation tensor cores.  A CTA owns 128 voxels (an 8x16x1 box of
-//    one sample) = the 128 TMEM lanes of an M=128 tcgen05.mma; N = output
-//    channels; one K step = one kernel tap x 16 input channels.  The CTA
-//    loads its input box with a one-voxel halo once, by TMA (out-of-range
-//    voxels read as zero: the padding), each 16-channel chunk as two 8-channel
-//    halves, unswizzled, and each half as three copies of 10 x 8 x 4 voxels
-//    shifted by -1, 0, +1 in y, so that within a copy the 8-voxel rows of both
-//    z slices lie one 160-byte stride apart.  The A operand of a tap is the
-//    copy of its y offset addressed at its x and z offsets (K-major, 16-byte
-//    rows, 8-row groups 160 bytes apart, the two channel halves one
-//    half-region apart).  A bulk
-//    copy brings each step's weights (32-byte swizzled K-major) into a 4-stage
-//    ring.  One thread issues the MMAs; tcgen05.commit frees a stage when its
-//    MMA has read it.  The epilogue reads the accumulator with tcgen05.ld,
-//    adds bias, applies leaky ReLU and stores BF16.
+//    5th-generation tensor cores.  A tile is 128 voxels of one sample (8x16x1,
+//    or 8x8x2 when Y is not a multiple of 16) = the 128 TMEM lanes of an
+//    M = 128 tcgen05.mma; N = output channels; one K step = one kernel tap x
+//    16 input channels.  The kernel is persistent (one CTA per SM walks the
+//    tiles) and warp-specialised: one thread loads each tile's input box
+//    with a one-voxel halo by TMA (out-of-range voxels read as zero: the
+//    padding), each 16-channel chunk as two 8-channel halves, unswizzled
+//    (8x8x2 tiles: three copies of the halo shifted by -1, 0, +1 in y, so
+//    that the 8-voxel rows of both z slices lie one row stride apart), into
+//    one of two buffers, so that the next tile loads while this one computes.
+//    The A operand of a tap is the halo at its offset (K-major, 16-byte rows,
+//    8-row groups one row stride apart, the two channel halves one
+//    half-region apart).  The weights (32-byte swizzled K-major) are loaded
+//    once per CTA and stay in shared memory when they fit, else they stream
+//    through a ring of whole-tap stages.  One thread issues the MMAs into one
+//    of two TMEM accumulators; four warps read the other one with tcgen05.ld,
+//    add bias, apply leaky ReLU and store BF16.
 //    The input gradient of a convolution is the same kernel run on dy with
 //    the weights flipped in space and transposed in channels.
 //  * k_conv3_wgrad_tc: weight gradient dW[co][tap][ci] = sum_v dy[v][co] *
-//    x[v + tap][ci], a reduction over all voxels, on the tensor cores: per tap
-//    a GEMM with M = 128 output-channel rows (rows past the real count read
-//    zeros), N = input channels and K = voxels, both operands MN-major
-//    (channels contiguous).  A CTA owns a group of taps, one TMEM accumulator
-//    each, and a range of 8x8x2 voxel tiles; per tile it loads dy and the
-//    input with its halo by TMA (the input box of the forward kernel), and
-//    every tap's B operand is that halo at the tap's offset.  At the end the
-//    accumulators are read with tcgen05.ld and added to dW with FP32 atomics.
+//    x[v + tap][ci], a reduction over all voxels, on the tensor cores: GEMMs
+//    with M = 128 output-channel rows, K = voxels and N = 48 = three taps
+//    along x x 16 input channels (the B operand's column groups one voxel
+//    apart).  A CTA owns a group of such units, one TMEM accumulator each,
+//    and walks the tiles; per tile it loads dy and the input with its halo by
+//    TMA (the input box of the forward kernel); four warps move dy into TMEM
+//    transposed (lane = output channel), the A operand that every unit's MMAs
+//    share, and the B operand of a unit is the halo at its offset (MN-major).
+//    At the end the accumulators are read with tcgen05.ld and added to dW
+//    with FP32 atomics.
 //  * pooling, upsampling, activation backward, the 1x1 output head fused
 //    with the MSE loss and its gradient, Adam, weight packing, features.
 #include <cuda.h>
@@ -58,16 +62,7 @@ namespace cmiu {
 
 using bf16 = __nv_bfloat16;
 
-constexpr int kConvThreads = 128;
-constexpr int kStages = 4;
-constexpr int kTileX = 8, kTileY = 8, kTileZ = 2;  // 128 voxels, row r = x + 8 y + 64 z
-// the input box with its one-voxel halo, per 8-channel half: three copies
-// (y offsets -1, 0, +1) of 10 x 8 x 4 voxels of 16 bytes
-constexpr int kHaloX = kTileX + 2, kHaloZ = kTileZ + 2;
-constexpr int kCopyBytes = kHaloX * kTileY * kHaloZ * 16;  // 5120 B (a multiple of 128)
-constexpr int kHalfBytes = 3 * kCopyBytes;
-static_assert(kCopyBytes % 128 == 0, "TMA destinations are 128-byte aligned");
-constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr long long kWaitCycles = 4000000000ll;
 constexpr uint32_t kErrTimeout = 1u;
 constexpr int kFeatures = 3;  // input channels of the network
 
@@ -108,11 +103,6 @@ int fail(int code, const char *fmt, ...) {
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
-__device__ __forceinline__ unsigned long long now_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 __device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
 }
@@ -134,12 +124,13 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait: false (and the error flag) after kWaitNs
+// bounded wait: false (and the error flag) after kWaitCycles SM clock cycles
+// (about 2 s); the SM's own cycle counter is cheap to read in the spin loop
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, uint32_t *err) {
   if (mbar_try(b, parity)) return true;
-  const unsigned long long t0 = now_ns();
+  const long long t0 = clock64();
   while (!mbar_try(b, parity)) {
-    if (now_ns() - t0 > kWaitNs) {
+    if (clock64() - t0 > kWaitCycles) {
       atomicOr(err, kErrTimeout);
       return false;
     }
@@ -175,12 +166,13 @@ __device__ __forceinline__ uint64_t sw32_desc(const void *p) {
   const uint64_t a = (smem_u32(p) & 0x3FFFFu) >> 4;
   return a | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) | (6ull << 61);
 }
-// shared-memory matrix descriptor without swizzle: 8 x 16-byte core matrices;
-// lbo: from one core matrix to the next along K (K-major) or along M/N
-// (MN-major), sbo: along the other dimension
-__device__ __forceinline__ uint64_t plain_desc(const void *p, uint32_t lbo, uint32_t sbo) {
+// shared-memory matrix descriptor, 32-byte swizzle, with the given byte offsets
+// (K-major: sbo between 8-row groups; MN-major: lbo between 16-element column
+// groups, sbo between 8-row K groups)
+__device__ __forceinline__ uint64_t sw32_desc_off(const void *p, uint32_t lbo, uint32_t sbo) {
   const uint64_t a = (smem_u32(p) & 0x3FFFFu) >> 4;
-  return a | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+  return a | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) | (1ull << 46) |
+         (6ull << 61);
 }
 // instruction descriptor: BF16 x BF16 -> F32, A and B K-major, M = 128
 __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
@@ -189,7 +181,83 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
 }
 
 // ---------------------------------------------------------------------------
-// 3x3x3 convolution on tensor cores
+// convolution tiles
+// ---------------------------------------------------------------------------
+// A tile is kMT sub-tiles of 128 voxels, each the M = 128 rows of its own MMAs
+// and TMEM accumulator, row r = x + 8 (y + TY z):
+//  * TY = 16: 8 x 16 x KZ voxels (KZ = kMT z slices of 8 x 16); the input box
+//    with its one-voxel halo is one copy of 10 x 18 x (KZ + 2) voxels, shared by
+//    the sub-tiles (the deeper the tile, the fewer halo voxels per output);
+//  * TY = 8:  8 x 8 x 2 voxels, one sub-tile (grids whose Y is not a multiple
+//    of 16); the halo is three copies of 10 x 8 x 4 voxels shifted by -1, 0, +1
+//    in y, so that in a copy the 8-voxel rows of both z slices lie one row
+//    stride apart.
+// Each 16-channel chunk of the input is stored in its own region, one 32-byte
+// row per voxel (x fastest), with the 32-byte swizzle of the tensor cores
+// (address bit 4 ^= bit 7) that TMA applies as it writes.  An A operand (K-major,
+// SWIZZLE_32B: 8 voxel rows x 16 channels per atom) is then the halo at the tap's
+// offset with its 8-voxel groups kRowBytes apart (SBO): the swizzle is a function
+// of the shared-memory address, so an operand may start at any voxel row.  The
+// weight-gradient kernel reads the same regions as MN-major B operands (16
+// channels per row, 8-voxel K groups kRowBytes apart, chunks kChunkBytes apart).
+template <int TY, int KZ = 1>
+struct ConvTile {
+  static_assert(TY == 16 || KZ == 1, "8 x 8 x 2 tiles have one sub-tile");
+  static constexpr int kMT = KZ;                         // sub-tiles (M = 128 each)
+  static constexpr int kTX = 8, kTY = TY, kTZ = (TY == 16) ? KZ : 2;
+  static constexpr int kHX = kTX + 2, kHZ = kTZ + 2;
+  static constexpr int kCopies = (TY == 16) ? 1 : 3;
+  static constexpr int kCopyRows = (TY == 16) ? kTY + 2 : kTY;  // y rows per z slice
+  static constexpr int kCopyBytes = kHX * kCopyRows * kHZ * 32;
+  static constexpr int kChunkBytes = (kCopies * kCopyBytes + 1023) / 1024 * 1024;
+  static constexpr int kRowBytes = kHX * 32;  // from one 8-voxel row to the next
+  static_assert(kCopies == 1 || kCopyBytes % 1024 == 0, "copies start on 1024-byte boundaries");
+  // A operand of sub-tile st and tap (hz, hy, hx) (halo offsets 0..2), from the
+  // start of a chunk
+  static __host__ __device__ constexpr int tap_offset(int st, int hz, int hy, int hx) {
+    return (kCopies == 1) ? (((hz + st) * kCopyRows + hy) * kHX + hx) * 32
+                          : hy * kCopyBytes + (hz * kCopyRows * kHX + hx) * 32;
+  }
+  // the TMA loads of one 16-channel chunk of the halo (c0: first channel)
+  static __device__ __forceinline__ void load_chunk(unsigned char *dst, const CUtensorMap *map,
+                                                    int c0, int x0, int y0, int z0, int n,
+                                                    uint64_t *bar) {
+#pragma unroll
+    for (int d = 0; d < kCopies; ++d)
+      tma_load_5d(dst + d * kCopyBytes, map, c0, x0 - 1, y0 - 1 + (kCopies == 1 ? 0 : d),
+                  z0 - 1, n, bar);
+  }
+  static __device__ __forceinline__ void tile_origin(int t, const int dims[3], int &x0, int &y0,
+                                                     int &z0, int &n) {
+    const int tx = dims[0] / kTX, ty = dims[1] / kTY, tz = dims[2] / kTZ;
+    const int bx = t % tx;
+    t /= tx;
+    const int by = t % ty;
+    t /= ty;
+    const int bz = t % tz;
+    n = t / tz;
+    x0 = bx * kTX;
+    y0 = by * kTY;
+    z0 = bz * kTZ;
+  }
+  static __host__ __device__ int num_tiles(int batch, const int dims[3]) {
+    return batch * (dims[0] / kTX) * (dims[1] / kTY) * (dims[2] / kTZ);
+  }
+};
+
+// bounded wait that also gives up once another role of the CTA has given up
+__device__ __forceinline__ bool role_wait(uint64_t *b, uint32_t parity, uint32_t *err,
+                                          volatile int *abort) {
+  if (*abort) return false;
+  if (!mbar_wait(b, parity, err)) {
+    *abort = 1;
+    return false;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// 3x3x3 convolution on tensor cores: persistent, warp-specialised
 // ---------------------------------------------------------------------------
 struct ConvArgs {
   const bf16 *wpack;     // [steps][npad][16], 32-byte swizzled rows
@@ -198,53 +266,78 @@ struct ConvArgs {
   int out_ctot, out_c0;  // its channel count and this convolution's first channel
   int npad;              // output channels (multiple of 16, <= 256)
   int nchunk;            // 16-channel chunks of the input
+  int nbuf;              // halo buffers (2: the next tile's halo loads during this one)
+  int wstages;           // weight stages of one tap each; 27: all weights stay resident
   int dims[3];           // X, Y, Z
+  int batch;
   int act;               // 1: leaky ReLU
   float slope;
   uint32_t *err;
 };
+constexpr int kConvWarps = 6;               // 0-3 epilogue, 4 loads, 5 MMAs
+constexpr int kConvThreads = kConvWarps * 32;
+constexpr int kMaxWStages = 27;            // one per tap: resident weights
 
+// A CTA walks tiles blockIdx.x, + gridDim.x, ...: warp 4 loads each tile's halo
+// (into buffer i % nbuf) and the weights, one stage per tap (nchunk K steps);
+// with 27 stages the weights are loaded once and stay for all tiles of the CTA,
+// else they stream through a ring of wstages.  Warp 5 issues the MMAs of tile i
+// into TMEM accumulator set i % 2 (one accumulator per sub-tile); warps 0-3 read
+// set i % 2, add bias, apply the activation and store BF16 while the MMAs of
+// tile i + 1 run.  With resident weights the MMA loop is fully unrolled over the
+// taps and sub-tiles, so that one tcgen05.mma follows the next with only a
+// descriptor add between them.
+template <int TY, int KZ>
 __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant__ CUtensorMap in,
                                                            ConvArgs a) {
+  using T = ConvTile<TY, KZ>;
   extern __shared__ __align__(1024) unsigned char sm_raw[];
-  // 1024-aligned base for the swizzled weight operands
   unsigned char *sm = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~(uintptr_t)1023);
-  const int bbytes = a.npad * 32;
-  unsigned char *sB = sm;                              // [kStages][npad * 32]
-  unsigned char *sH = sB + kStages * bbytes;           // halo [nchunk][2][kHalfBytes]
-  uint64_t *full = reinterpret_cast<uint64_t *>(sH + (size_t)a.nchunk * 2 * kHalfBytes);
-  uint64_t *empty = full + kStages;
-  uint64_t *done = empty + kStages;
-  uint64_t *halo = done + 1;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(halo + 1);
+  const int bbytes = a.npad * 32;                             // one K step's weights
+  const int tbytes = a.nchunk * bbytes;                        // one tap's weights
+  const int S = a.wstages;
+  const bool resident = S == 27;
+  const size_t hbytes = (size_t)a.nchunk * T::kChunkBytes;    // one halo buffer
+  unsigned char *sH = sm;                                      // [nbuf][nchunk][chunk]
+  unsigned char *sB = sH + a.nbuf * hbytes;                    // [S][nchunk][npad * 32]
+  float *sbias = reinterpret_cast<float *>(sB + (size_t)S * tbytes);
+  uint64_t *b_full = reinterpret_cast<uint64_t *>(sbias + a.npad);
+  uint64_t *b_empty = b_full + kMaxWStages;
+  uint64_t *h_full = b_empty + kMaxWStages;  // [2]
+  uint64_t *h_empty = h_full + 2;          // [2]
+  uint64_t *a_full = h_empty + 2;          // [2]
+  uint64_t *a_empty = a_full + 2;          // [2]
+  uint64_t *drain = a_empty + 2;           // the MMAs in flight when the CTA ends
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+  __shared__ int s_abort;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int tx = a.dims[0] / kTileX, ty = a.dims[1] / kTileY, tz = a.dims[2] / kTileZ;
-  int t = blockIdx.x;
-  const int bx = t % tx;
-  t /= tx;
-  const int by = t % ty;
-  t /= ty;
-  const int bz = t % tz;
-  const int n = t / tz;
-  const int x0 = bx * kTileX, y0 = by * kTileY, z0 = bz * kTileZ;
-  const int nsteps = 27 * a.nchunk;
-  const uint32_t ncols = a.npad <= 32 ? 32u : a.npad <= 64 ? 64u : a.npad <= 128 ? 128u : 256u;
+  const int tiles = T::num_tiles(a.batch, a.dims);
+  const int nmine = (blockIdx.x < tiles) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t acols = a.npad <= 32 ? 32u : a.npad <= 64 ? 64u : a.npad <= 128 ? 128u : 256u;
+  const uint32_t scols = T::kMT * acols;  // one accumulator set
 
+  for (int c = tid; c < a.npad; c += kConvThreads) sbias[c] = a.bias ? a.bias[c] : 0.f;
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+    s_abort = 0;
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&b_full[s], 1);
+      mbar_init(&b_empty[s], 1);
     }
-    mbar_init(done, 1);
-    mbar_init(halo, 1);
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&h_full[s], 1);
+      mbar_init(&h_empty[s], 1);
+      mbar_init(&a_full[s], 1);
+      mbar_init(&a_empty[s], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(drain, 1);
     fence_mbar_init();
   }
-  if (warp == 0) {
+  if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tslot)),
-                 "r"(ncols)
+                 "r"(2 * scols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -252,101 +345,209 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
+  volatile int *abort = &s_abort;
 
-  bool ok = true;
-  if (tid == 0) {
+  if (warp == 4 && lane == 0) {
+    // loads: the halo of tile i, then its weights, one stage per tap
+    int tiles_issued = 0, stages_issued = 0;
+    for (int i = 0; i < nmine && !*abort; ++i) {
+      int x0, y0, z0, n;
+      T::tile_origin(blockIdx.x + i * gridDim.x, a.dims, x0, y0, z0, n);
+      const int hb = i % a.nbuf, hu = i / a.nbuf;
+      if (hu > 0 && !role_wait(&h_empty[hb], (uint32_t)(hu - 1) & 1u, a.err, abort)) break;
+      mbar_expect_tx(&h_full[hb], (uint32_t)(a.nchunk * T::kCopies * T::kCopyBytes));
+      unsigned char *h = sH + hb * hbytes;
+      for (int c = 0; c < a.nchunk; ++c)
+        T::load_chunk(h + (size_t)c * T::kChunkBytes, &in, c * 16, x0, y0, z0, n, &h_full[hb]);
+      tiles_issued = i + 1;
+      if (resident && i > 0) continue;
+      for (int tap = 0; tap < 27; ++tap) {
+        const int g = i * 27 + tap, s = g % S, u = g / S;
+        if (u > 0 && !role_wait(&b_empty[s], (uint32_t)(u - 1) & 1u, a.err, abort)) break;
+        mbar_expect_tx(&b_full[s], (uint32_t)tbytes);
+        bulk_load(sB + (size_t)s * tbytes, a.wpack + (size_t)tap * a.nchunk * a.npad * 16,
+                  (uint32_t)tbytes, &b_full[s]);
+        stages_issued = g + 1;
+      }
+    }
+    // the last copy into every buffer has landed before the CTA ends (they have
+    // all been consumed, unless a role gave up)
+    for (int i = max(0, tiles_issued - a.nbuf); i < tiles_issued; ++i)
+      mbar_wait(&h_full[i % a.nbuf], (uint32_t)(i / a.nbuf) & 1u, a.err);
+    for (int g = max(0, stages_issued - S); g < stages_issued; ++g)
+      mbar_wait(&b_full[g % S], (uint32_t)(g / S) & 1u, a.err);
+  } else if (warp == 5 && lane == 0) {
     const uint32_t idesc = idesc_bf16(a.npad);
-    // the input box with its halo, once: chunk c, half h, y offset d at
-    // sH + (2c + h) * kHalfBytes + d * kCopyBytes
-    mbar_expect_tx(halo, (uint32_t)(a.nchunk * 2 * kHalfBytes));
-    for (int c = 0; c < a.nchunk; ++c)
-      for (int h = 0; h < 2; ++h)
-        for (int d = 0; d < 3; ++d)
-          tma_load_5d(sH + (size_t)(2 * c + h) * kHalfBytes + d * kCopyBytes, &in,
-                      c * 16 + h * 8, x0 - 1, y0 - 1 + d, z0 - 1, n, halo);
-    auto load = [&](int k) {
-      const int s = k % kStages;
-      mbar_expect_tx(&full[s], (uint32_t)bbytes);
-      bulk_load(sB + s * bbytes, a.wpack + (size_t)k * a.npad * 16, (uint32_t)bbytes, &full[s]);
-    };
-    for (int k = 0; k < kStages && k < nsteps; ++k) load(k);
-    ok = mbar_wait(halo, 0u, a.err);
-    for (int k = 0; k < nsteps && ok; ++k) {
-      const int s = k % kStages;
-      const uint32_t ph = (uint32_t)(k / kStages) & 1u;
-      ok = mbar_wait(&full[s], ph, a.err);
-      if (!ok) break;
+    // descriptors advance by (byte offset >> 4) in their low 14-bit address
+    // field; every operand lies below 256 KB, so the sums never carry out of it
+    const uint64_t bdesc0 = sw32_desc_off(sB, 16u, 256u);
+    const uint32_t cstep = (uint32_t)T::kChunkBytes >> 4;  // next 16-channel chunk
+    const uint32_t bstep = (uint32_t)bbytes >> 4;           // next K step's weights
+    const int nchunk = a.nchunk;
+    const uint64_t tstep = (uint64_t)nchunk * bstep;        // next tap's weights
+    bool ok = true;
+    if (resident && nmine > 0) {
+      for (int t = 0; t < 27 && ok; ++t) ok = role_wait(&b_full[t], 0u, a.err, abort);
       tc_fence_after();
-      // tap (dz, dy, dx) reads the input at (x + dx, y + dy, z + dz): copy dy + 1
-      // of the halo, shifted by (dx + 1, dz + 1) voxels
-      const int tap = k / a.nchunk, c = k - tap * a.nchunk;
-      const int hz = tap / 9, hy = (tap / 3) % 3, hx = tap % 3;
-      const unsigned char *a0 = sH + (size_t)(2 * c) * kHalfBytes + hy * kCopyBytes +
-                                (hz * kTileY * kHaloX + hx) * 16;
-      const uint64_t ad = plain_desc(a0, (uint32_t)kHalfBytes, (uint32_t)(kHaloX * 16));
-      const uint64_t bd = sw32_desc(sB + s * bbytes);
-      const uint32_t acc = k > 0 ? 1u : 0u;
+    }
+    int s = 0;            // weight stage of the next tap (streaming)
+    uint32_t sphase = 0;  // its parity
+    for (int i = 0; i < nmine && ok && !*abort; ++i) {
+      const int ab = i & 1, au = i >> 1;
+      const int hb = i % a.nbuf, hu = i / a.nbuf;
+      if (au > 0 && !role_wait(&a_empty[ab], (uint32_t)(au - 1) & 1u, a.err, abort)) break;
+      if (!role_wait(&h_full[hb], (uint32_t)hu & 1u, a.err, abort)) break;
+      tc_fence_after();
+      const uint64_t adesc0 = sw32_desc_off(sH + hb * hbytes, 16u, (uint32_t)T::kRowBytes);
+      const uint32_t d0 = tmem + (uint32_t)ab * scols;
+      if (resident) {
+        // registers only in this loop: the MMA statements carry no memory
+        // clobber (they are ordered by being volatile, and the data they read
+        // was published by the barrier waits above)
+        uint64_t bd = bdesc0;
+        const int nch = nchunk;
+        if (nch == 1) {
+          // one 16-channel chunk: one MMA per tap and sub-tile
+          for (int tap = 0; tap < 27; ++tap) {
+            const uint64_t at =
+                adesc0 + ((uint32_t)T::tap_offset(0, tap / 9, (tap / 3) % 3, tap % 3) >> 4);
+            const uint32_t acc = tap > 0 ? 1u : 0u;
+#pragma unroll
+            for (int st = 0; st < T::kMT; ++st)
+              asm volatile(
+                  "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                  " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(
+                      d0 + (uint32_t)st * acols),
+                  "l"(at + (uint32_t)(T::tap_offset(st, 0, 0, 0) >> 4)), "l"(bd), "r"(idesc),
+                  "r"(acc));
+            bd += bstep;
+          }
+        } else {
+          for (int tap = 0; tap < 27; ++tap) {
+            // tap (dz, dy, dx) reads the input at (x + dx, y + dy, z + dz)
+            uint64_t at =
+                adesc0 + ((uint32_t)T::tap_offset(0, tap / 9, (tap / 3) % 3, tap % 3) >> 4);
+            uint64_t bc = bd;
+            for (int c = 0; c < nch; ++c) {
+              const uint32_t acc = (tap > 0 || c > 0) ? 1u : 0u;
+#pragma unroll
+              for (int st = 0; st < T::kMT; ++st)
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(
+                        d0 + (uint32_t)st * acols),
+                    "l"(at + (uint32_t)(T::tap_offset(st, 0, 0, 0) >> 4)), "l"(bc),
+                    "r"(idesc), "r"(acc));
+              at += cstep;
+              bc += bstep;
+            }
+            bd += tstep;
+          }
+        }
+      } else {
+        for (int tap = 0; tap < 27; ++tap) {
+          if (!role_wait(&b_full[s], sphase, a.err, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint64_t bc = bdesc0 + (uint32_t)(s * nchunk) * bstep;
+          uint64_t at =
+              adesc0 + ((uint32_t)T::tap_offset(0, tap / 9, (tap / 3) % 3, tap % 3) >> 4);
+          for (int c = 0; c < nchunk; ++c) {
+            const uint32_t acc = (tap > 0 || c > 0) ? 1u : 0u;
+#pragma unroll
+            for (int st = 0; st < T::kMT; ++st)
+              asm volatile(
+                  "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                  " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(
+                      d0 + (uint32_t)st * acols),
+                  "l"(at + (uint32_t)(T::tap_offset(st, 0, 0, 0) >> 4)), "l"(bc), "r"(idesc),
+                  "r"(acc));
+            at += cstep;
+            bc += bstep;
+          }
+          asm volatile(
+              "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                  smem_u32(&b_empty[s]))
+              : "memory");
+          if (++s == S) {
+            s = 0;
+            sphase ^= 1u;
+          }
+        }
+        if (!ok) break;
+      }
+      // the halo buffer and the accumulators are released once these MMAs complete
       asm volatile(
-          "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-          " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
-          "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(&h_empty[hb]))
           : "memory");
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(&empty[s]))
+              smem_u32(&a_full[ab]))
           : "memory");
-      // refill the stage of the previous MMA (MMA k stays queued meanwhile)
-      const int kp = k - 1;
-      if (kp >= 0 && kp + kStages < nsteps) {
-        const int sp = kp % kStages;
-        ok = mbar_wait(&empty[sp], (uint32_t)(kp / kStages) & 1u, a.err);
-        if (ok) load(kp + kStages);
-      }
     }
+    // every MMA issued has completed before TMEM is released
     asm volatile(
         "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            smem_u32(done))
+            smem_u32(drain))
         : "memory");
-  }
-  __syncwarp();
-  // every thread: the accumulator is complete
-  const bool done_ok = __all_sync(0xffffffffu, mbar_wait(done, 0u, a.err));
-  tc_fence_after();
-  if (done_ok) {
-    // row r = voxel (x0 + r % 8, y0 + (r / 8) % 8, z0 + r / 64); warp w owns lanes 32w..
-    const int r = warp * 32 + lane;
-    const int vx = x0 + (r & 7), vy = y0 + ((r >> 3) & 7), vz = z0 + (r >> 6);
-    const size_t vox = (((size_t)n * a.dims[2] + vz) * a.dims[1] + vy) * a.dims[0] + vx;
-    bf16 *dst = a.out + vox * a.out_ctot + a.out_c0;
-    for (int j = 0; j < a.npad; j += 16) {
-      uint32_t v[16];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-          "%13,%14,%15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-            "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-            "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      __align__(16) bf16 o[16];
+    mbar_wait(drain, 0, a.err);
+  } else if (warp < 4) {
+    for (int i = 0; i < nmine; ++i) {
+      const int ab = i & 1;
+      // one lane waits, then the warp reads its 32 TMEM lanes of every sub-tile
+      bool ok0 = true;
+      if (lane == 0) ok0 = role_wait(&a_full[ab], (uint32_t)(i >> 1) & 1u, a.err, abort);
+      if (!__shfl_sync(0xffffffffu, ok0, 0)) break;
+      tc_fence_after();
+      int x0, y0, z0, n;
+      T::tile_origin(blockIdx.x + i * gridDim.x, a.dims, x0, y0, z0, n);
+      // row r of sub-tile st = voxel (x0 + r % 8, y0 + (r / 8) % TY, z)
+      const int r = warp * 32 + lane;
+      const int vx = x0 + (r & 7), vy = y0 + ((r >> 3) % T::kTY);
 #pragma unroll
-      for (int e = 0; e < 16; ++e) {
-        float f = __uint_as_float(v[e]);
-        if (a.bias) f += a.bias[j + e];
-        if (a.act) f = f > 0.f ? f : f * a.slope;
-        o[e] = __float2bfloat16_rn(f);
+      for (int st = 0; st < T::kMT; ++st) {
+        const int vz = z0 + (T::kCopies == 1 ? st : r / (8 * T::kTY));
+        const size_t vox = (((size_t)n * a.dims[2] + vz) * a.dims[1] + vy) * a.dims[0] + vx;
+        bf16 *dst = a.out + vox * a.out_ctot + a.out_c0;
+        for (int j = 0; j < a.npad; j += 16) {
+          uint32_t v[16];
+          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)ab * scols +
+                                 (uint32_t)st * acols + (uint32_t)j;
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+              "%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+              : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          __align__(16) bf16 o[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            float f = __uint_as_float(v[e]) + sbias[j + e];
+            if (a.act) f = f > 0.f ? f : f * a.slope;
+            o[e] = __float2bfloat16_rn(f);
+          }
+          uint4 *d4 = reinterpret_cast<uint4 *>(dst + j);
+          d4[0] = reinterpret_cast<const uint4 *>(o)[0];
+          d4[1] = reinterpret_cast<const uint4 *>(o)[1];
+        }
       }
-      uint4 *d4 = reinterpret_cast<uint4 *>(dst + j);
-      d4[0] = reinterpret_cast<const uint4 *>(o)[0];
-      d4[1] = reinterpret_cast<const uint4 *>(o)[1];
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                      smem_u32(&a_empty[ab]))
+                                  : "memory");
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 5) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(ncols)
+                 "r"(2 * scols)
                  : "memory");
   }
 }
@@ -356,140 +557,217 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
 // ---------------------------------------------------------------------------
 struct WgradTcArgs {
   int cout;                  // dy channels (storage, multiple of 16, <= 128)
-  int nchunk;                // 16-channel chunks of the input (N = 16 nchunk <= 256)
+  int nchunk;                // 16-channel chunks of the input
+  int nbuf;                  // tile buffers (2: the next tile loads during this one)
   int dims[3];
   int batch;
-  int tap0, taps;            // taps of this launch's CTAs: blockIdx.y selects a group
-  int taps_per_cta;
-  uint32_t tmem_cols;        // power of two >= taps_per_cta * N (<= 256: two CTAs per SM)
-  int tiles_per_cta;         // voxel tiles of one CTA (blockIdx.x)
+  int units_per_cta;         // units (a (dz, dy) tap row x one input chunk) of a CTA;
+                             // blockIdx.y selects a group of units
+  uint32_t tmem_cols;        // power of two >= units_per_cta * kUnitCols + 2 * kDyCols
   float *dw;                 // [cout_real][27][cin_real] (FP32, accumulated)
   const int *ci_map;         // storage input channel -> real input channel or -1
   int cin_real, cout_real;
   uint32_t *err;
 };
-constexpr int kDyGroupBytes = kTileX * kTileY * kTileZ * 16;  // 8 output channels: 2 KB
-constexpr int kDyBytes = 16 * kDyGroupBytes;          // the 128 A rows (16 groups of 8)
+constexpr int kWgradWarps = 6;            // 0-3 dy -> TMEM and readout, 4 loads, 5 MMAs
+constexpr int kWgradThreads = kWgradWarps * 32;
+constexpr int kDyGroupBytes = 128 * 16;   // 8 output channels of one tile: 2 KB
+constexpr int kDyCols = 64;               // one tile of dy in TMEM: 128 voxels, 2 per column
+constexpr int kUnitCols = 48;             // one unit's accumulator: taps dx = -1, 0, 1 x 16
+constexpr int kWgradUnitsPerCta = 8;      // 8 x 48 + 2 x 64 = 512 TMEM columns
 
-__global__ void __launch_bounds__(kConvThreads) k_conv3_wgrad_tc(
+// The work of a tile is 9 x nchunk units: a row of three taps (dz, dy fixed, dx =
+// -1, 0, 1) times one 16-channel input chunk, one MMA of N = 48 per K step: the
+// B operand (MN-major) has its three 16-channel column groups one voxel (32
+// bytes) apart, so that column group g reads the input shifted by dx = g - 1.
+// A CTA owns a group of units (one TMEM accumulator each, M = 128 output-channel
+// lanes) and the tiles blockIdx.x, + gridDim.x, ...: warp 4 loads tile i's dy
+// and input halo into buffer i % nbuf by TMA; warps 0-3 move dy into TMEM buffer
+// i % 2 transposed (lane = output channel, column = two voxels), the A operand
+// of every unit's MMAs, so that the MMAs (warp 5: K = 16 voxels each) read only
+// the input from shared memory; at the end warps 0-3 read their 32 TMEM lanes
+// and add them to dW.  Lanes past the storage output channels are never written
+// or read.
+template <int TY>
+__global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
     const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dymap,
     WgradTcArgs a) {
+  using T = ConvTile<TY>;
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   unsigned char *sm = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~(uintptr_t)1023);
-  unsigned char *sA = sm;                 // dy: [16 groups of 8 channels][16 y][8 x][8]
-  unsigned char *sH = sA + kDyBytes;      // input halo: [2 nchunk][3 copies][4][8][10][8]
-  uint64_t *loaded = reinterpret_cast<uint64_t *>(sH + (size_t)a.nchunk * 2 * kHalfBytes);
-  uint64_t *mma_done = loaded + 1;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(mma_done + 1);
+  const size_t dybytes = (size_t)(a.cout / 8) * kDyGroupBytes;
+  const size_t hbytes = (size_t)a.nchunk * T::kChunkBytes;
+  const size_t bufbytes = dybytes + hbytes;  // [dy groups][input halo] per buffer
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + a.nbuf * bufbytes);  // [2]
+  uint64_t *empty = full + 2;    // [2]: dy moved (4 warps) and the MMAs done (1)
+  uint64_t *a_full = empty + 2;  // [2]: dy in TMEM buffer (4 warps)
+  uint64_t *a_empty = a_full + 2;  // [2]: the MMAs reading it done
+  uint64_t *drain = a_empty + 2;   // the MMAs in flight when the CTA ends
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+  __shared__ int s_abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int N = a.nchunk * 16;
-  const int t0 = a.tap0 + blockIdx.y * a.taps_per_cta;
-  const int ntap = min(a.taps_per_cta, a.tap0 + a.taps - t0);
-  const int tx = a.dims[0] / kTileX, ty = a.dims[1] / kTileY, tz = a.dims[2] / kTileZ;
-  const int tiles = a.batch * tx * ty * tz;
-  const int tile0 = blockIdx.x * a.tiles_per_cta, tile1 = min(tiles, tile0 + a.tiles_per_cta);
+  const int u0 = blockIdx.y * a.units_per_cta;
+  const int nunit = min(a.units_per_cta, 9 * a.nchunk - u0);
+  const int tiles = a.batch * (a.dims[0] / T::kTX) * (a.dims[1] / T::kTY) * (a.dims[2] / T::kTZ);
+  const int nmine = (blockIdx.x < tiles && nunit > 0)
+                        ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // first column of the dy buffers
+  const uint32_t acol0 = (uint32_t)(a.units_per_cta * kUnitCols);
 
-  // rows of A past the real output channels read zeros
-  for (int i = tid; i < (kDyBytes - (a.cout / 8) * kDyGroupBytes) / 16; i += kConvThreads)
-    reinterpret_cast<uint4 *>(sA + (a.cout / 8) * kDyGroupBytes)[i] = make_uint4(0, 0, 0, 0);
   if (tid == 0) {
-    mbar_init(loaded, 1);
-    mbar_init(mma_done, 1);
+    s_abort = 0;
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 5);
+      mbar_init(&a_full[s], 4);
+      mbar_init(&a_empty[s], 1);
+    }
+    mbar_init(drain, 1);
     fence_mbar_init();
   }
-  if (warp == 0) {
+  if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tslot)),
                  "r"(a.tmem_cols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  // the zeros above are generic-proxy writes that the MMAs read through the async proxy
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
+  volatile int *abort = &s_abort;
+  const uint32_t bytes = (uint32_t)(dybytes + (size_t)a.nchunk * T::kCopies * T::kCopyBytes);
 
-  bool ok = true;
-  if (tid == 0 && ntap > 0) {
-    // BF16 x BF16 -> F32, A and B MN-major, M = 128, N
-    const uint32_t idesc = idesc_bf16(N) | (1u << 15) | (1u << 16);
-    const uint32_t bytes = (uint32_t)((a.cout / 8) * kDyGroupBytes + a.nchunk * 2 * kHalfBytes);
-    bool first = true;
-    uint32_t phase = 0;
-    for (int t = tile0; t < tile1 && ok; ++t) {
-      int r = t;
-      const int bx = r % tx;
-      r /= tx;
-      const int by = r % ty;
-      r /= ty;
-      const int bz = r % tz;
-      const int n = r / tz;
-      const int x0 = bx * kTileX, y0 = by * kTileY, z0 = bz * kTileZ;
-      if (!first) {  // the previous tile's MMAs have read the buffers
-        ok = mbar_wait(mma_done, phase ^ 1u, a.err);
-        if (!ok) break;
-      }
-      mbar_expect_tx(loaded, bytes);
+  if (warp == 4 && lane == 0) {
+    int issued = 0;
+    for (int i = 0; i < nmine && !*abort; ++i) {
+      int x0, y0, z0, n;
+      T::tile_origin(blockIdx.x + i * gridDim.x, a.dims, x0, y0, z0, n);
+      const int b = i % a.nbuf, u = i / a.nbuf;
+      if (u > 0 && !role_wait(&empty[b], (uint32_t)(u - 1) & 1u, a.err, abort)) break;
+      unsigned char *buf = sm + b * bufbytes;
+      mbar_expect_tx(&full[b], bytes);
       for (int g = 0; g < a.cout / 8; ++g)
-        tma_load_5d(sA + g * kDyGroupBytes, &dymap, g * 8, x0, y0, z0, n, loaded);
+        tma_load_5d(buf + g * kDyGroupBytes, &dymap, g * 8, x0, y0, z0, n, &full[b]);
       for (int c = 0; c < a.nchunk; ++c)
-        for (int h = 0; h < 2; ++h)
-          for (int d = 0; d < 3; ++d)
-            tma_load_5d(sH + (size_t)(2 * c + h) * kHalfBytes + d * kCopyBytes, &xmap,
-                        c * 16 + h * 8, x0 - 1, y0 - 1 + d, z0 - 1, n, loaded);
-      ok = mbar_wait(loaded, phase, a.err);
-      if (!ok) break;
+        T::load_chunk(buf + dybytes + (size_t)c * T::kChunkBytes, &xmap, c * 16, x0, y0, z0, n,
+                      &full[b]);
+      issued = i + 1;
+    }
+    // the last copy into every buffer has landed before the CTA ends
+    for (int i = max(0, issued - a.nbuf); i < issued; ++i)
+      mbar_wait(&full[i % a.nbuf], (uint32_t)(i / a.nbuf) & 1u, a.err);
+  } else if (warp == 5 && lane == 0) {
+    // BF16 x BF16 -> F32, A (TMEM) K-major, B MN-major, M = 128, N = 48
+    const uint32_t idesc = idesc_bf16(kUnitCols) | (1u << 16);
+    for (int i = 0; i < nmine; ++i) {
+      const int b = i % a.nbuf, ab = i & 1;
+      if (!role_wait(&a_full[ab], (uint32_t)(i >> 1) & 1u, a.err, abort)) break;
+      if (!role_wait(&full[b], (uint32_t)(i / a.nbuf) & 1u, a.err, abort)) break;
       tc_fence_after();
-      for (int j = 0; j < ntap; ++j) {
-        const int tap = t0 + j;
-        const int hz = tap / 9, hy = (tap / 3) % 3, hx = tap % 3;
-        const unsigned char *b0 = sH + hy * kCopyBytes + (hz * kTileY * kHaloX + hx) * 16;
-        // K step k: tile rows q = 2k, 2k + 1 of 8 voxels (q = y + 8 z)
-        for (int k = 0; k < kTileY * kTileZ / 2; ++k) {
-          // A: core matrices of 8 voxels x 8 channels; LBO along K (next row),
-          // SBO along M (next 8 output channels)
-          const uint64_t ad = plain_desc(sA + k * 2 * kTileX * 16, kTileX * 16, kDyGroupBytes);
-          // B: rows 2k, 2k + 1 of the tap's halo copy at its x and z offsets;
-          // SBO along N (next 8 input channels: the next half region)
-          const uint64_t bd =
-              plain_desc(b0 + k * 2 * kHaloX * 16, kHaloX * 16, (uint32_t)kHalfBytes);
-          const uint32_t acc = (first && k == 0) ? 0u : 1u;
+      // B: MN-major, LBO along N (the next 16 columns: the next voxel in x), SBO
+      // along K (the next 8-voxel row)
+      const uint64_t hdesc =
+          sw32_desc_off(sm + b * bufbytes + dybytes, 32u, (uint32_t)T::kRowBytes);
+      const uint32_t adt = tmem + acol0 + (uint32_t)(ab * kDyCols);
+      const uint32_t rstep = (uint32_t)(2 * T::kRowBytes) >> 4;  // the next 16 voxels
+      const uint32_t acc0 = i > 0 ? 1u : 0u;
+      for (int j = 0; j < nunit; ++j) {
+        const int u = u0 + j, row = u / a.nchunk, c = u - row * a.nchunk;
+        // K step k = voxels 16k .. 16k + 15 of the tile
+        uint64_t bd = hdesc + ((uint32_t)(c * T::kChunkBytes +
+                                          T::tap_offset(0, row / 3, row % 3, 0)) >> 4);
+        const uint32_t dt = tmem + (uint32_t)(j * kUnitCols);
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}" ::"r"(dt),
+            "r"(adt), "l"(bd), "r"(idesc), "r"(acc0));
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+          bd += rstep;
           asm volatile(
-              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(
-                  tmem + (uint32_t)(j * N)),
-              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-              : "memory");
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, 1;" ::"r"(dt),
+              "r"(adt + (uint32_t)(8 * k)), "l"(bd), "r"(idesc));
         }
       }
+      // the halo and the TMEM dy buffer are free once these MMAs complete
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(mma_done))
+              smem_u32(&empty[b]))
           : "memory");
-      first = false;
-      phase ^= 1u;
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(&a_empty[ab]))
+          : "memory");
     }
-    if (!first && ok) ok = mbar_wait(mma_done, phase ^ 1u, a.err);
-    if (first) ok = false;  // no tile: nothing accumulated
+    // every MMA issued has completed before the readout and the release of TMEM
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(drain))
+        : "memory");
+    mbar_wait(drain, 0, a.err);
+  } else if (warp < 4) {
+    // dy -> TMEM: lane co, column c = voxels 2c (low half) and 2c + 1
+    const int co = warp * 32 + lane;
+    const bool active = warp * 32 < a.cout;  // warp-uniform
+    for (int i = 0; i < nmine; ++i) {
+      const int b = i % a.nbuf, ab = i & 1;
+      bool ok = role_wait(&full[b], (uint32_t)(i / a.nbuf) & 1u, a.err, abort);
+      if (ok && i >= 2) ok = role_wait(&a_empty[ab], (uint32_t)((i >> 1) - 1) & 1u, a.err, abort);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+      if (active) {
+        const unsigned char *dy = sm + b * bufbytes + (co >> 3) * kDyGroupBytes + (co & 7) * 2;
+        const bool real = co < a.cout;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + acol0 +
+                               (uint32_t)(ab * kDyCols);
+#pragma unroll
+        for (int q = 0; q < kDyCols / 16; ++q) {
+          uint32_t v[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int r = 2 * (16 * q + e);
+            const uint32_t lo = real ? *reinterpret_cast<const unsigned short *>(dy + r * 16) : 0u;
+            const uint32_t hi =
+                real ? *reinterpret_cast<const unsigned short *>(dy + (r + 1) * 16) : 0u;
+            v[e] = lo | (hi << 16);
+          }
+          asm volatile(
+              "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,"
+              "%11,%12,%13,%14,%15,%16};" ::"r"(taddr + (uint32_t)(16 * q)),
+              "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
+              "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]),
+              "r"(v[14]), "r"(v[15])
+              : "memory");
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&a_full[ab]))
+                     : "memory");
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b]))
+                     : "memory");
+      }
+    }
   }
-  __syncwarp();
-  // thread 0 knows whether the accumulators are complete; share it
-  __shared__ int s_have;
-  if (tid == 0) s_have = ok ? 1 : 0;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (s_have && warp * 32 < a.cout_real) {
-    // lane = output channel (TMEM lane), columns = input channels
+  if (nmine > 0 && !*abort && warp < 4 && warp * 32 < a.cout_real) {
+    // lane = output channel (TMEM lane); unit j: columns g * 16 + e = tap
+    // (row, dx = g - 1), input channel 16 c + e
     const int co = warp * 32 + lane;
-    for (int j = 0; j < ntap; ++j) {
-      const int tap = t0 + j;
-      for (int c = 0; c < N; c += 16) {
+    for (int j = 0; j < nunit; ++j) {
+      const int u = u0 + j, row = u / a.nchunk, c = u - row * a.nchunk;
+      for (int g = 0; g < 3; ++g) {
+        const int tap = row * 3 + g;
         uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * N + c);
+        const uint32_t taddr =
+            tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * kUnitCols + g * 16);
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
             "%13,%14,%15}, [%16];"
@@ -501,7 +779,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_wgrad_tc(
         if (co < a.cout_real) {
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
-            const int ci = a.ci_map[c + e];
+            const int ci = a.ci_map[c * 16 + e];
             const float f = __uint_as_float(v[e]);
             if (ci >= 0 && f != 0.f)
               atomicAdd(&a.dw[((size_t)co * 27 + tap) * a.cin_real + ci], f);
@@ -512,7 +790,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_wgrad_tc(
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 5) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(a.tmem_cols)
                  : "memory");
@@ -1108,10 +1386,11 @@ int grid_for(long long n, int threads = 256) {
   return (int)std::min<long long>((n + threads - 1) / threads, 148LL * 16);
 }
 
-// tensor map of an input slice: dims (channels, X, Y, Z, batch), box (8, 10, 8, 4, 1):
-// one 8-channel half of one y-shifted copy of a convolution tile's input with its
-// x and z halo, unswizzled
-int make_map(CUtensorMap *map, const Slice &s, int batch, const int dims[3]) {
+// tensor map of a slice: dims (channels, X, Y, Z, batch); boxes of box_c
+// channels (16: 32-byte voxel rows with the 32-byte swizzle; 8: unswizzled
+// 16-byte rows) x box_x/y/z voxels
+int make_map_box(CUtensorMap *map, const Slice &s, int batch, const int dims[3], int box_c,
+                 int box_x, int box_y, int box_z) {
   EncodeTiledFn enc;
   UN_TRY(get_encoder(&enc));
   const cuuint64_t gdim[5] = {(cuuint64_t)s.c, (cuuint64_t)dims[0], (cuuint64_t)dims[1],
@@ -1119,31 +1398,77 @@ int make_map(CUtensorMap *map, const Slice &s, int batch, const int dims[3]) {
   const cuuint64_t row = (cuuint64_t)s.ctot * sizeof(bf16);
   const cuuint64_t gstride[4] = {row, row * dims[0], row * dims[0] * dims[1],
                                  row * dims[0] * dims[1] * dims[2]};
-  const cuuint32_t box[5] = {8, kHaloX, kTileY, kHaloZ, 1};
+  const cuuint32_t box[5] = {(cuuint32_t)box_c, (cuuint32_t)box_x, (cuuint32_t)box_y,
+                             (cuuint32_t)box_z, 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void *)(s.base + s.c0), gdim,
                          gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         box_c == 16 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(CMI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return CMI_OK;
 }
 
-size_t conv_smem(int npad, int nchunk) {
-  return 1024 + (size_t)kStages * npad * 32 + (size_t)nchunk * 2 * kHalfBytes +
-         (2 * kStages + 2) * 8 + 16;
+// the tile shape of a grid: 8 x 16 x 1 when Y is a multiple of 16, else 8 x 8 x 2
+int tile_y(const int dims[3]) {
+  if (dims[0] % 8 == 0 && dims[1] % 16 == 0) return 16;
+  if (dims[0] % 8 == 0 && dims[1] % 8 == 0 && dims[2] % 2 == 0) return 8;
+  return 0;
 }
 
-// y = act(conv(x) + b) into out slice; wpack rows = out.c
-int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, const Slice &out,
-            int act, int batch, const int dims[3]) {
-  if (dims[0] % kTileX || dims[1] % kTileY || dims[2] % kTileZ)
-    return fail(CMI_ERR_INVALID_ARGUMENT, "grid %dx%dx%d is not a multiple of the 8x8x2 tile",
-                dims[0], dims[1], dims[2]);
-  if (in.c % 16 || out.c % 16 || out.c > 256 || out.c < 16)
-    return fail(CMI_ERR_INVALID_ARGUMENT, "channel counts must be multiples of 16 (<= 256)");
+// one y-copy of the input halo of a tile (box 10 x rows x slices voxels)
+template <int TY, int KZ = 1>
+int make_halo_map(CUtensorMap *map, const Slice &s, int batch, const int dims[3]) {
+  using T = ConvTile<TY, KZ>;
+  return make_map_box(map, s, batch, dims, 16, T::kHX, T::kCopyRows, T::kHZ);
+}
+
+// dynamic shared memory a CTA of kernel f may take (the opt-in limit less the
+// kernel's static shared memory)
+template <typename F>
+int smem_optin(cmi_unet *u, F f, int *bytes) {
+  int dev = 0;
+  UN_CUDA(cudaGetDevice(&dev));
+  UN_CUDA(cudaDeviceGetAttribute(bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  UN_CUDA(cudaFuncGetAttributes(&fa, f));
+  *bytes -= (int)fa.sharedSizeBytes;
+  return CMI_OK;
+}
+
+// shared memory of a convolution CTA: halo buffers, weight stages, bias, barriers
+struct ConvPlan {
+  int nbuf = 0, wstages = 0;
+  size_t smem = 0;
+};
+template <int TY, int KZ>
+ConvPlan conv_plan(int nchunk, int npad, int optin) {
+  using T = ConvTile<TY, KZ>;
+  const size_t tbytes = (size_t)nchunk * npad * 32;
+  auto smem_for = [&](int nbuf, int stages) {
+    return 1024 + (size_t)stages * tbytes + (size_t)nbuf * nchunk * T::kChunkBytes +
+           (size_t)npad * 4 + (2 * kMaxWStages + 9) * 8 + 16;
+  };
+  auto stages_for = [&](int nbuf) {
+    const size_t fixed = smem_for(nbuf, 0);
+    return fixed >= (size_t)optin ? 0 : (int)std::min<size_t>(27, (optin - fixed) / tbytes);
+  };
+  // weights resident (27 stages) when they fit beside two halo buffers, else a
+  // ring of as many tap stages as fit (at least 4), else one halo buffer
+  ConvPlan p;
+  p.nbuf = stages_for(2) >= 4 ? 2 : 1;
+  p.wstages = stages_for(p.nbuf);
+  p.smem = smem_for(p.nbuf, p.wstages);
+  return p;
+}
+
+template <int TY, int KZ>
+int conv_launch(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias,
+                const Slice &out, int act, int batch, const int dims[3], int optin) {
+  using T = ConvTile<TY, KZ>;
   CUtensorMap map;
-  UN_TRY(make_map(&map, in, batch, dims));
+  UN_TRY((make_halo_map<TY, KZ>(&map, in, batch, dims)));
   ConvArgs a{};
   a.wpack = wpack;
   a.bias = bias;
@@ -1153,78 +1478,131 @@ int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, 
   a.npad = out.c;
   a.nchunk = in.c / 16;
   for (int k = 0; k < 3; ++k) a.dims[k] = dims[k];
+  a.batch = batch;
   a.act = act;
   a.slope = u->slope;
   a.err = u->d_err;
-  const size_t smem = conv_smem(out.c, a.nchunk);
-  UN_CUDA(cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
-  const int tiles = batch * (dims[0] / kTileX) * (dims[1] / kTileY) * (dims[2] / kTileZ);
-  k_conv3_tc<<<tiles, kConvThreads, smem, u->stream>>>(map, a);
+  const ConvPlan p = conv_plan<TY, KZ>(a.nchunk, a.npad, optin);
+  if (p.wstages < 2)
+    return fail(CMI_ERR_NOT_SUPPORTED, "convolution: weights of one tap (%d B) do not fit",
+                a.nchunk * a.npad * 32);
+  a.nbuf = p.nbuf;
+  a.wstages = p.wstages;
+  auto kern = k_conv3_tc<TY, KZ>;
+  UN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+  int per_sm = 0;
+  UN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConvThreads, p.smem));
+  // TMEM: two accumulator sets of a CTA, at most 512 columns per SM
+  const int acols = a.npad <= 32 ? 32 : a.npad <= 64 ? 64 : a.npad <= 128 ? 128 : 256;
+  per_sm = std::max(1, std::min(per_sm, 512 / (2 * KZ * acols)));
+  int sms = 0, dev = 0;
+  UN_CUDA(cudaGetDevice(&dev));
+  UN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int tiles = T::num_tiles(batch, dims);
+  const int grid = std::max(1, std::min(tiles, per_sm * sms));
+  kern<<<grid, kConvThreads, p.smem, u->stream>>>(map, a);
   UN_CUDA(cudaGetLastError());
   return CMI_OK;
 }
 
-// tensor map of a tile's dy: dims (channels, X, Y, Z, batch), box (8, 8, 8, 2, 1)
-int make_dy_map(CUtensorMap *map, const Slice &s, int batch, const int dims[3]) {
-  EncodeTiledFn enc;
-  UN_TRY(get_encoder(&enc));
-  const cuuint64_t gdim[5] = {(cuuint64_t)s.c, (cuuint64_t)dims[0], (cuuint64_t)dims[1],
-                              (cuuint64_t)dims[2], (cuuint64_t)batch};
-  const cuuint64_t row = (cuuint64_t)s.ctot * sizeof(bf16);
-  const cuuint64_t gstride[4] = {row, row * dims[0], row * dims[0] * dims[1],
-                                 row * dims[0] * dims[1] * dims[2]};
-  const cuuint32_t box[5] = {8, kTileX, kTileY, kTileZ, 1};
-  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void *)(s.base + s.c0), gdim,
-                         gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(CMI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-  return CMI_OK;
+// the deepest tile (KZ z slices) whose two accumulator sets fit the tensor
+// memory, whose weights stay resident beside two halo buffers and that still
+// gives every SM a tile
+template <int KZ>
+bool conv_deep_ok(const Slice &in, const Slice &out, int batch, const int dims[3], int optin,
+                  int sms) {
+  using T = ConvTile<16, KZ>;
+  const int acols = out.c <= 32 ? 32 : out.c <= 64 ? 64 : out.c <= 128 ? 128 : 256;
+  if (dims[2] % KZ || 2 * KZ * acols > 512) return false;
+  const ConvPlan p = conv_plan<16, KZ>(in.c / 16, out.c, optin);
+  return p.wstages == 27 && p.nbuf == 2 && T::num_tiles(batch, dims) >= sms;
 }
 
-int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *ci_map,
-          int cin_real, int cout_real, int batch, const int dims[3]) {
-  if (dims[0] % kTileX || dims[1] % kTileY || dims[2] % kTileZ)
-    return fail(CMI_ERR_INVALID_ARGUMENT, "grid %dx%dx%d is not a multiple of the 8x8x2 tile",
+// y = act(conv(x) + b) into out slice; wpack rows = out.c
+int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, const Slice &out,
+            int act, int batch, const int dims[3]) {
+  const int ty = tile_y(dims);
+  if (!ty)
+    return fail(CMI_ERR_INVALID_ARGUMENT,
+                "grid %dx%dx%d: X and Y must be multiples of 8, and Y of 16 or Z of 2",
                 dims[0], dims[1], dims[2]);
-  if (x.c % 16 || dy.c % 16 || x.c < 16 || x.c > 256 || dy.c < 16 || dy.c > 128)
-    return fail(CMI_ERR_NOT_SUPPORTED,
-                "weight gradient: input channels must be 16..256, output channels 16..128, "
-                "multiples of 16");
+  if (in.c % 16 || out.c % 16 || out.c > 256 || out.c < 16)
+    return fail(CMI_ERR_INVALID_ARGUMENT, "channel counts must be multiples of 16 (<= 256)");
+  int optin = 0, sms = 0, dev = 0;
+  // the kernels' static shared memory is the same for every instance
+  UN_TRY(smem_optin(u, k_conv3_tc<16, 1>, &optin));
+  UN_CUDA(cudaGetDevice(&dev));
+  UN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (ty == 8) return conv_launch<8, 1>(u, in, wpack, bias, out, act, batch, dims, optin);
+  if (conv_deep_ok<4>(in, out, batch, dims, optin, sms))
+    return conv_launch<16, 4>(u, in, wpack, bias, out, act, batch, dims, optin);
+  if (conv_deep_ok<2>(in, out, batch, dims, optin, sms))
+    return conv_launch<16, 2>(u, in, wpack, bias, out, act, batch, dims, optin);
+  return conv_launch<16, 1>(u, in, wpack, bias, out, act, batch, dims, optin);
+}
+
+template <int TY>
+int wgrad_t(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *ci_map,
+            int cin_real, int cout_real, int batch, const int dims[3]) {
+  using T = ConvTile<TY>;
   CUtensorMap xm, dym;
-  UN_TRY(make_map(&xm, x, batch, dims));
-  UN_TRY(make_dy_map(&dym, dy, batch, dims));
+  UN_TRY(make_halo_map<TY>(&xm, x, batch, dims));
+  UN_TRY(make_map_box(&dym, dy, batch, dims, 8, T::kTX, T::kTY, T::kTZ));
   WgradTcArgs a{};
   a.cout = dy.c;
   a.nchunk = x.c / 16;
   for (int k = 0; k < 3; ++k) a.dims[k] = dims[k];
   a.batch = batch;
-  a.tap0 = 0;
-  a.taps = 27;
-  const int N = x.c;
-  a.taps_per_cta = std::min(27, 256 / N);
+  // units spread evenly over the fewest groups that fit the tensor memory
+  const int units = 9 * a.nchunk;
+  const int groups = (units + kWgradUnitsPerCta - 1) / kWgradUnitsPerCta;
+  a.units_per_cta = (units + groups - 1) / groups;
   uint32_t cols = 32;
-  while (cols < (uint32_t)(a.taps_per_cta * N)) cols <<= 1;
+  while (cols < (uint32_t)(a.units_per_cta * kUnitCols + 2 * kDyCols)) cols <<= 1;
   a.tmem_cols = cols;
-  const int groups = (27 + a.taps_per_cta - 1) / a.taps_per_cta;
-  const int tiles = batch * (dims[0] / kTileX) * (dims[1] / kTileY) * (dims[2] / kTileZ);
-  // about two CTAs per SM over all tap groups
-  const int want = std::max(1, 2 * 148 / groups);
-  a.tiles_per_cta = (tiles + want - 1) / want;
-  const int ctas = (tiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
   a.dw = dw;
   a.ci_map = ci_map;
   a.cin_real = cin_real;
   a.cout_real = cout_real;
   a.err = u->d_err;
-  const size_t smem = 1024 + (size_t)kDyBytes + (size_t)a.nchunk * 2 * kHalfBytes + 64;
-  UN_CUDA(cudaFuncSetAttribute(k_conv3_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  int optin = 0;
+  UN_TRY(smem_optin(u, k_conv3_wgrad_tc<TY>, &optin));
+  const size_t buf = (size_t)(a.cout / 8) * kDyGroupBytes + (size_t)a.nchunk * T::kChunkBytes;
+  auto smem_for = [&](int nbuf) { return 1024 + nbuf * buf + 128; };
+  a.nbuf = smem_for(2) <= (size_t)optin ? 2 : 1;
+  const size_t smem = smem_for(a.nbuf);
+  if (smem > (size_t)optin)
+    return fail(CMI_ERR_NOT_SUPPORTED, "weight gradient needs %zu B of shared memory", smem);
+  UN_CUDA(cudaFuncSetAttribute(k_conv3_wgrad_tc<TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem));
-  k_conv3_wgrad_tc<<<dim3(ctas, groups), kConvThreads, smem, u->stream>>>(xm, dym, a);
+  int per_sm = 0;
+  UN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3_wgrad_tc<TY>,
+                                                        kWgradThreads, smem));
+  // TMEM: at most 512 columns per SM
+  per_sm = std::max(1, std::min(per_sm, (int)(512 / a.tmem_cols)));
+  int sms = 0, dev = 0;
+  UN_CUDA(cudaGetDevice(&dev));
+  UN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int tiles = batch * (dims[0] / T::kTX) * (dims[1] / T::kTY) * (dims[2] / T::kTZ);
+  const int ctas = std::max(1, std::min(tiles, per_sm * sms / groups));
+  k_conv3_wgrad_tc<TY><<<dim3(ctas, groups), kWgradThreads, smem, u->stream>>>(xm, dym, a);
   UN_CUDA(cudaGetLastError());
   return CMI_OK;
+}
+
+int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *ci_map,
+          int cin_real, int cout_real, int batch, const int dims[3]) {
+  const int ty = tile_y(dims);
+  if (!ty)
+    return fail(CMI_ERR_INVALID_ARGUMENT,
+                "grid %dx%dx%d: X and Y must be multiples of 8, and Y of 16 or Z of 2",
+                dims[0], dims[1], dims[2]);
+  if (x.c % 16 || dy.c % 16 || x.c < 16 || x.c > 256 || dy.c < 16 || dy.c > 128)
+    return fail(CMI_ERR_NOT_SUPPORTED,
+                "weight gradient: input channels must be 16..256, output channels 16..128, "
+                "multiples of 16");
+  return ty == 16 ? wgrad_t<16>(u, x, dy, dw, ci_map, cin_real, cout_real, batch, dims)
+                  : wgrad_t<8>(u, x, dy, dw, ci_map, cin_real, cout_real, batch, dims);
 }
 
 // packs every layer's weights from the FP32 master parameters

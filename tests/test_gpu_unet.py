@@ -78,10 +78,17 @@ def net():
     n.close()
 
 
-@pytest.mark.parametrize("cin,cout", [(16, 16), (32, 48), (80, 32)])
-def test_conv3_forward_matches_oracle(net, cin, cout):
+# shapes (B, Z, Y, X): Y = 16 takes 8x16xKZ tiles, Y = 8 the 8x8x2 tiles; grids
+# with at least one tile per SM take 4 (1 x 32 x 64 x 64) or 2 (2 x 16 x 32 x
+# 64) z slices per tile; the weights of (16, 16) and (32, 48) stay resident in
+# shared memory, those of (80, 32) stream through a ring of tap stages, those of
+# (128, 128) through a ring beside a single halo buffer
+@pytest.mark.parametrize("cin,cout,shape", [
+    (16, 16, (2, 4, 16, 16)), (32, 48, (2, 4, 16, 16)), (80, 32, (2, 4, 16, 16)),
+    (16, 32, (1, 6, 8, 16)), (48, 16, (2, 4, 8, 8)), (128, 128, (1, 2, 16, 8)),
+    (16, 16, (1, 32, 64, 64)), (32, 32, (2, 16, 32, 64))])
+def test_conv3_forward_matches_oracle(net, cin, cout, shape):
     rng = np.random.default_rng(cin + cout)
-    shape = (2, 4, 16, 16)  # B, Z, Y, X
     x = U.bf16_round(rng.normal(size=shape + (cin,)))
     W = rng.normal(0, 0.2, size=(cout, 27, cin))
     bias = rng.normal(0, 0.1, size=cout).astype(np.float32).astype(np.float64)
@@ -101,21 +108,25 @@ def test_conv3_input_gradient_matches_oracle(net):
     _assert_bf16_rounded(dx, ref)
 
 
-def test_conv3_weight_gradient_matches_oracle(net):
-    rng = np.random.default_rng(6)
-    cin, cout = 32, 16
-    shape = (2, 4, 16, 16)
+# input channels 16 .. 80 (16 taps per CTA down to 3), output channels 16 ..
+# 128 (one to four warps move dy into the tensor memory), both tile shapes
+@pytest.mark.parametrize("cin,cout,shape", [
+    (32, 16, (2, 4, 16, 16)), (16, 48, (1, 4, 8, 8)), (80, 32, (1, 2, 16, 8)),
+    (48, 128, (1, 2, 8, 8))])
+def test_conv3_weight_gradient_matches_oracle(net, cin, cout, shape):
+    rng = np.random.default_rng(6 + cin + cout)
+    B, Z, Y, X = shape
     x = U.bf16_round(rng.normal(size=shape + (cin,)))
     dy = U.bf16_round(rng.normal(size=shape + (cout,)))
     dw = torch.zeros(cout * 27 * cin, dtype=torch.float32, device="cuda")
     xt, dyt = _bf16_tensor(x), _bf16_tensor(dy)
     torch.cuda.synchronize()
     _lib.check_unet(net._L.cmi_unet_conv3_wgrad(net._h, C.c_void_p(xt.data_ptr()), cin,
-                                                C.c_void_p(dyt.data_ptr()), cout, 2,
-                                                _dims(16, 16, 4), C.c_void_p(dw.data_ptr())))
+                                                C.c_void_p(dyt.data_ptr()), cout, B,
+                                                _dims(X, Y, Z), C.c_void_p(dw.data_ptr())))
     got = dw.cpu().numpy().reshape(cout, 27, cin)
     ref = U.conv3_weight_grad(x, dy)
-    # sums of 2048 products in FP32 in another order
+    # sums of up to 2048 products in FP32 in another order
     np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-3)
 
 
