@@ -256,6 +256,37 @@ __device__ __forceinline__ bool role_wait(uint64_t *b, uint32_t parity, uint32_t
   return true;
 }
 
+// BF16 vectors of 8 channels (16 bytes)
+struct Bf8 {
+  float v[8];
+};
+__device__ __forceinline__ Bf8 load8(const bf16 *p) {
+  const uint4 q = *reinterpret_cast<const uint4 *>(p);
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+  Bf8 r;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float2 f = __bfloat1622float2(h[k]);
+    r.v[2 * k] = f.x;
+    r.v[2 * k + 1] = f.y;
+  }
+  return r;
+}
+__device__ __forceinline__ void store8(bf16 *p, const Bf8 &r) {
+  uint4 q;
+  __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&q);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) h[k] = __floats2bfloat162_rn(r.v[2 * k], r.v[2 * k + 1]);
+  *reinterpret_cast<uint4 *>(p) = q;
+}
+// leaky ReLU derivative from the activation output y (same sign as its input)
+__device__ __forceinline__ void gate8(Bf8 &d, const bf16 *y, float slope) {
+  const Bf8 g = load8(y);
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (!(g.v[k] > 0.f)) d.v[k] *= slope;
+}
+
 // ---------------------------------------------------------------------------
 // 3x3x3 convolution on tensor cores: persistent, warp-specialised
 // ---------------------------------------------------------------------------
@@ -272,6 +303,8 @@ struct ConvArgs {
   int batch;
   int act;               // 1: leaky ReLU
   float slope;
+  const bf16 *gate;      // input-gradient convolutions: out *= leaky'(gate) (may be null)
+  int gate_ctot, gate_c0;
   uint32_t *err;
 };
 constexpr int kConvWarps = 6;               // 0-3 epilogue, 4 loads, 5 MMAs
@@ -525,10 +558,25 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
               : "r"(taddr));
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           __align__(16) bf16 o[16];
+          float gy[16];
+          if (a.gate) {
+            const bf16 *gp = a.gate + vox * a.gate_ctot + a.gate_c0 + j;
+            const Bf8 g0 = load8(gp), g1 = load8(gp + 8);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              gy[e] = g0.v[e];
+              gy[e + 8] = g1.v[e];
+            }
+          }
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
             float f = __uint_as_float(v[e]) + sbias[j + e];
             if (a.act) f = f > 0.f ? f : f * a.slope;
+            if (a.gate) {
+              // the stored BF16 gradient times the activation derivative
+              f = __bfloat162float(__float2bfloat16_rn(f));
+              if (!(gy[e] > 0.f)) f *= a.slope;
+            }
             o[e] = __float2bfloat16_rn(f);
           }
           uint4 *d4 = reinterpret_cast<uint4 *>(dst + j);
@@ -561,67 +609,100 @@ struct WgradTcArgs {
   int nbuf;                  // tile buffers (2: the next tile loads during this one)
   int dims[3];
   int batch;
-  int units_per_cta;         // units (a (dz, dy) tap row x one input chunk) of a CTA;
+  int units_per_cta;         // units (dz x dy chunk x input chunk) of a CTA;
                              // blockIdx.y selects a group of units
-  uint32_t tmem_cols;        // power of two >= units_per_cta * kUnitCols + 2 * kDyCols
+  uint32_t tmem_cols;        // power of two >= units_per_cta * kUnitCols
+  int bar_off;               // bytes from the buffers' start to the barriers (past every
+                             // byte an MMA may read)
   float *dw;                 // [cout_real][27][cin_real] (FP32, accumulated)
+  float *db;                 // [cout_real] bias gradient: sum of dy (accumulated; may be null)
   const int *ci_map;         // storage input channel -> real input channel or -1
   int cin_real, cout_real;
   uint32_t *err;
 };
-constexpr int kWgradWarps = 6;            // 0-3 dy -> TMEM and readout, 4 loads, 5 MMAs
+constexpr int kWgradWarps = 6;            // 0-3 bias sums and readout, 4 loads, 5 MMAs
 constexpr int kWgradThreads = kWgradWarps * 32;
-constexpr int kDyGroupBytes = 128 * 16;   // 8 output channels of one tile: 2 KB
-constexpr int kDyCols = 64;               // one tile of dy in TMEM: 128 voxels, 2 per column
 constexpr int kUnitCols = 48;             // one unit's accumulator: taps dx = -1, 0, 1 x 16
-constexpr int kWgradUnitsPerCta = 8;      // 8 x 48 + 2 x 64 = 512 TMEM columns
+constexpr int kWgradUnitsPerCta = 10;     // 10 x 48 <= 512 TMEM columns
 
-// The work of a tile is 9 x nchunk units: a row of three taps (dz, dy fixed, dx =
-// -1, 0, 1) times one 16-channel input chunk, one MMA of N = 48 per K step: the
-// B operand (MN-major) has its three 16-channel column groups one voxel (32
-// bytes) apart, so that column group g reads the input shifted by dx = g - 1.
-// A CTA owns a group of units (one TMEM accumulator each, M = 128 output-channel
-// lanes) and the tiles blockIdx.x, + gridDim.x, ...: warp 4 loads tile i's dy
-// and input halo into buffer i % nbuf by TMA; warps 0-3 move dy into TMEM buffer
-// i % 2 transposed (lane = output channel, column = two voxels), the A operand
-// of every unit's MMAs, so that the MMAs (warp 5: K = 16 voxels each) read only
-// the input from shared memory; at the end warps 0-3 read their 32 TMEM lanes
-// and add them to dW.  Lanes past the storage output channels are never written
-// or read.
+// dy of a tile with one extra voxel row on either side in y, 16 channels per
+// 32-byte voxel row (32-byte swizzle), x fastest:
+//  * 8 x 16 x 1 tiles: one box of 8 x 18 rows (rows y0 - 1 .. y0 + 16);
+//  * 8 x 8 x 2 tiles: three copies of 8 x 8 x 2 voxels shifted by -1, 0, +1 in y.
+// The voxels of the tile shifted by t - 1 rows in y then start kMStride bytes x t
+// after the start of the first row (copy).
+template <int TY>
+struct DyTile {
+  static constexpr int kCopies = (TY == 16) ? 1 : 3;
+  static constexpr int kRows = (TY == 16) ? TY + 2 : TY;  // y rows of a box
+  static constexpr int kTZ = 128 / (8 * TY);
+  static constexpr int kCopyBytes = 8 * kRows * kTZ * 32;
+  static constexpr int kChunkBytes = (kCopies * kCopyBytes + 1023) / 1024 * 1024;
+  static constexpr int kMStride = (TY == 16) ? 8 * 32 : kCopyBytes;
+  // bytes past a chunk's start that an MMA's A operand may read: M group 7 of the
+  // last K step (voxels 112 .. 127)
+  static constexpr int kReach = 7 * kMStride + 7 * 512 + 512;
+  static __device__ __forceinline__ void load_chunk(unsigned char *dst, const CUtensorMap *map,
+                                                    int c0, int x0, int y0, int z0, int n,
+                                                    uint64_t *bar) {
+#pragma unroll
+    for (int d = 0; d < kCopies; ++d)
+      tma_load_5d(dst + d * kCopyBytes, map, c0, x0, y0 - 1 + (kCopies == 1 ? 0 : d), z0, n, bar);
+  }
+  // byte offset of tile voxel r (r = x + 8 (y + TY z)) in the unshifted rows
+  static __device__ __forceinline__ int own_offset(int r) {
+    return (kCopies == 1) ? (r + 8) * 32 : kCopyBytes + r * 32;
+  }
+};
+
+// The work of a tile is 3 x (cout / 16) x nchunk units: one z tap row (dz) x one
+// 16-output-channel chunk of dy x one 16-channel input chunk, 8 MMAs (K = 16
+// voxels each) that cover all 9 (dy, dx) taps of the row at once:
+//  * B (the input halo at dz and the centre y row, MN-major) has its three
+//    16-channel column groups one voxel (32 bytes) apart: column group g reads
+//    the input shifted by dx = g - 1;
+//  * A (dy, MN-major, M = 128 rows in 8 groups of 16 output channels) has its M
+//    groups kMStride apart: group t reads dy shifted by t - 1 rows in y, which
+//    pairs dy(v) with the input at v + (1 - t) rows.  Groups 3 .. 7 read
+//    whatever follows and feed accumulator rows that are never read.
+// Over all tiles every voxel meets every tap once: the rows a shifted tile
+// misses at the grid's edge pair with input outside the grid (zero).
+// A CTA owns a group of units (one TMEM accumulator each) and the tiles
+// blockIdx.x, + gridDim.x, ...: warp 4 loads tile i's dy and input halo into
+// buffer i % nbuf by TMA; warp 5 issues the MMAs; warps 0-3 sum dy for the bias
+// gradient (the CTAs of the first group) and at the end read the TMEM lanes and
+// add them to dW.
 template <int TY>
 __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
     const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dymap,
     WgradTcArgs a) {
   using T = ConvTile<TY>;
+  using D = DyTile<TY>;
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   unsigned char *sm = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~(uintptr_t)1023);
-  const size_t dybytes = (size_t)(a.cout / 8) * kDyGroupBytes;
+  const int ncc = a.cout / 16;
+  const size_t dybytes = (size_t)ncc * D::kChunkBytes;
   const size_t hbytes = (size_t)a.nchunk * T::kChunkBytes;
-  const size_t bufbytes = dybytes + hbytes;  // [dy groups][input halo] per buffer
-  uint64_t *full = reinterpret_cast<uint64_t *>(sm + a.nbuf * bufbytes);  // [2]
-  uint64_t *empty = full + 2;    // [2]: dy moved (4 warps) and the MMAs done (1)
-  uint64_t *a_full = empty + 2;  // [2]: dy in TMEM buffer (4 warps)
-  uint64_t *a_empty = a_full + 2;  // [2]: the MMAs reading it done
-  uint64_t *drain = a_empty + 2;   // the MMAs in flight when the CTA ends
+  const size_t bufbytes = dybytes + hbytes;  // [dy chunks][input halo] per buffer
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + a.bar_off);  // [2]
+  uint64_t *empty = full + 2;    // [2]: the MMAs done (1) and dy summed (4 warps)
+  uint64_t *drain = empty + 2;   // the MMAs in flight when the CTA ends
   uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
   __shared__ int s_abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nunits = 3 * ncc * a.nchunk;
   const int u0 = blockIdx.y * a.units_per_cta;
-  const int nunit = min(a.units_per_cta, 9 * a.nchunk - u0);
+  const int nunit = min(a.units_per_cta, nunits - u0);
   const int tiles = a.batch * (a.dims[0] / T::kTX) * (a.dims[1] / T::kTY) * (a.dims[2] / T::kTZ);
   const int nmine = (blockIdx.x < tiles && nunit > 0)
                         ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  // first column of the dy buffers
-  const uint32_t acol0 = (uint32_t)(a.units_per_cta * kUnitCols);
 
   if (tid == 0) {
     s_abort = 0;
     for (int s = 0; s < 2; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 5);
-      mbar_init(&a_full[s], 4);
-      mbar_init(&a_empty[s], 1);
     }
     mbar_init(drain, 1);
     fence_mbar_init();
@@ -638,7 +719,8 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
   tc_fence_after();
   const uint32_t tmem = *tslot;
   volatile int *abort = &s_abort;
-  const uint32_t bytes = (uint32_t)(dybytes + (size_t)a.nchunk * T::kCopies * T::kCopyBytes);
+  const uint32_t bytes = (uint32_t)((size_t)ncc * D::kCopies * D::kCopyBytes +
+                                    (size_t)a.nchunk * T::kCopies * T::kCopyBytes);
 
   if (warp == 4 && lane == 0) {
     int issued = 0;
@@ -649,8 +731,8 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
       if (u > 0 && !role_wait(&empty[b], (uint32_t)(u - 1) & 1u, a.err, abort)) break;
       unsigned char *buf = sm + b * bufbytes;
       mbar_expect_tx(&full[b], bytes);
-      for (int g = 0; g < a.cout / 8; ++g)
-        tma_load_5d(buf + g * kDyGroupBytes, &dymap, g * 8, x0, y0, z0, n, &full[b]);
+      for (int g = 0; g < ncc; ++g)
+        D::load_chunk(buf + g * D::kChunkBytes, &dymap, g * 16, x0, y0, z0, n, &full[b]);
       for (int c = 0; c < a.nchunk; ++c)
         T::load_chunk(buf + dybytes + (size_t)c * T::kChunkBytes, &xmap, c * 16, x0, y0, z0, n,
                       &full[b]);
@@ -660,46 +742,43 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
     for (int i = max(0, issued - a.nbuf); i < issued; ++i)
       mbar_wait(&full[i % a.nbuf], (uint32_t)(i / a.nbuf) & 1u, a.err);
   } else if (warp == 5 && lane == 0) {
-    // BF16 x BF16 -> F32, A (TMEM) K-major, B MN-major, M = 128, N = 48
-    const uint32_t idesc = idesc_bf16(kUnitCols) | (1u << 16);
+    // BF16 x BF16 -> F32, A and B MN-major, M = 128, N = 48
+    const uint32_t idesc = idesc_bf16(kUnitCols) | (1u << 15) | (1u << 16);
+    const uint32_t kstep_a = (uint32_t)(16 * 32) >> 4;           // the next 16 voxels of dy
+    const uint32_t kstep_b = (uint32_t)(2 * T::kRowBytes) >> 4;  // ... of the halo
+    const int per_dz = ncc * a.nchunk;
     for (int i = 0; i < nmine; ++i) {
-      const int b = i % a.nbuf, ab = i & 1;
-      if (!role_wait(&a_full[ab], (uint32_t)(i >> 1) & 1u, a.err, abort)) break;
+      const int b = i % a.nbuf;
       if (!role_wait(&full[b], (uint32_t)(i / a.nbuf) & 1u, a.err, abort)) break;
       tc_fence_after();
-      // B: MN-major, LBO along N (the next 16 columns: the next voxel in x), SBO
-      // along K (the next 8-voxel row)
-      const uint64_t hdesc =
-          sw32_desc_off(sm + b * bufbytes + dybytes, 32u, (uint32_t)T::kRowBytes);
-      const uint32_t adt = tmem + acol0 + (uint32_t)(ab * kDyCols);
-      const uint32_t rstep = (uint32_t)(2 * T::kRowBytes) >> 4;  // the next 16 voxels
+      const unsigned char *buf = sm + b * bufbytes;
+      // A: LBO along M (the next 16 rows: dy one voxel row further in y), SBO
+      // along K (the next 8 voxels); B: LBO along N (the next 16 columns: the
+      // next voxel in x), SBO along K (the next 8-voxel row)
+      const uint64_t adesc = sw32_desc_off(buf, (uint32_t)D::kMStride, 256u);
+      const uint64_t hdesc = sw32_desc_off(buf + dybytes, 32u, (uint32_t)T::kRowBytes);
       const uint32_t acc0 = i > 0 ? 1u : 0u;
       for (int j = 0; j < nunit; ++j) {
-        const int u = u0 + j, row = u / a.nchunk, c = u - row * a.nchunk;
-        // K step k = voxels 16k .. 16k + 15 of the tile
-        uint64_t bd = hdesc + ((uint32_t)(c * T::kChunkBytes +
-                                          T::tap_offset(0, row / 3, row % 3, 0)) >> 4);
+        const int u = u0 + j, dz = u / per_dz, rem = u - dz * per_dz;
+        const int cc = rem / a.nchunk, c = rem - cc * a.nchunk;
+        const uint64_t ad = adesc + ((uint32_t)(cc * D::kChunkBytes) >> 4);
+        const uint64_t bd =
+            hdesc + ((uint32_t)(c * T::kChunkBytes + T::tap_offset(0, dz, 1, 0)) >> 4);
         const uint32_t dt = tmem + (uint32_t)(j * kUnitCols);
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}" ::"r"(dt),
-            "r"(adt), "l"(bd), "r"(idesc), "r"(acc0));
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(dt),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc0));
 #pragma unroll
-        for (int k = 1; k < 8; ++k) {
-          bd += rstep;
-          asm volatile(
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, 1;" ::"r"(dt),
-              "r"(adt + (uint32_t)(8 * k)), "l"(bd), "r"(idesc));
-        }
+        for (int k = 1; k < 8; ++k)
+          asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, 1;" ::"r"(dt),
+                       "l"(ad + (uint32_t)k * kstep_a), "l"(bd + (uint32_t)k * kstep_b),
+                       "r"(idesc));
       }
-      // the halo and the TMEM dy buffer are free once these MMAs complete
+      // the buffer is free once these MMAs complete
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
               smem_u32(&empty[b]))
-          : "memory");
-      asm volatile(
-          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(&a_empty[ab]))
           : "memory");
     }
     // every MMA issued has completed before the readout and the release of TMEM
@@ -709,62 +788,50 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
         : "memory");
     mbar_wait(drain, 0, a.err);
   } else if (warp < 4) {
-    // dy -> TMEM: lane co, column c = voxels 2c (low half) and 2c + 1
+    // bias gradient: thread co sums dy[v][co] over the CTA's tiles (the first
+    // group's CTAs; the others only release the buffers)
     const int co = warp * 32 + lane;
-    const bool active = warp * 32 < a.cout;  // warp-uniform
+    const bool sum = a.db && blockIdx.y == 0 && warp * 32 < a.cout_real;  // warp-uniform
+    float bsum = 0.f;
     for (int i = 0; i < nmine; ++i) {
-      const int b = i % a.nbuf, ab = i & 1;
-      bool ok = role_wait(&full[b], (uint32_t)(i / a.nbuf) & 1u, a.err, abort);
-      if (ok && i >= 2) ok = role_wait(&a_empty[ab], (uint32_t)((i >> 1) - 1) & 1u, a.err, abort);
-      if (!__all_sync(0xffffffffu, ok)) break;
-      tc_fence_after();
-      if (active) {
-        const unsigned char *dy = sm + b * bufbytes + (co >> 3) * kDyGroupBytes + (co & 7) * 2;
-        const bool real = co < a.cout;
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + acol0 +
-                               (uint32_t)(ab * kDyCols);
-#pragma unroll
-        for (int q = 0; q < kDyCols / 16; ++q) {
-          uint32_t v[16];
-#pragma unroll
-          for (int e = 0; e < 16; ++e) {
-            const int r = 2 * (16 * q + e);
-            const uint32_t lo = real ? *reinterpret_cast<const unsigned short *>(dy + r * 16) : 0u;
-            const uint32_t hi =
-                real ? *reinterpret_cast<const unsigned short *>(dy + (r + 1) * 16) : 0u;
-            v[e] = lo | (hi << 16);
-          }
-          asm volatile(
-              "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,"
-              "%11,%12,%13,%14,%15,%16};" ::"r"(taddr + (uint32_t)(16 * q)),
-              "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
-              "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]),
-              "r"(v[14]), "r"(v[15])
-              : "memory");
+      const int b = i % a.nbuf;
+      bool ok0 = true;
+      if (lane == 0) ok0 = role_wait(&full[b], (uint32_t)(i / a.nbuf) & 1u, a.err, abort);
+      if (!__shfl_sync(0xffffffffu, ok0, 0)) break;
+      if (sum && co < a.cout_real) {
+        // the 32-byte swizzle: 16-byte half h of the row at byte offset o sits
+        // at half h ^ ((o >> 7) & 1)
+        const unsigned char *dy = sm + b * bufbytes + (co >> 4) * D::kChunkBytes;
+        const int h = (co >> 3) & 1, e = co & 7;
+#pragma unroll 8
+        for (int r = 0; r < 128; ++r) {
+          const int o = D::own_offset(r);
+          bsum += __bfloat162float(
+              *reinterpret_cast<const bf16 *>(dy + o + ((h ^ ((o >> 7) & 1)) << 4) + e * 2));
         }
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       }
-      tc_fence_before();
       __syncwarp();
-      if (lane == 0) {
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&a_full[ab]))
-                     : "memory");
+      if (lane == 0)
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b]))
                      : "memory");
-      }
     }
+    if (sum && co < a.cout_real) atomicAdd(&a.db[co], bsum);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (nmine > 0 && !*abort && warp < 4 && warp * 32 < a.cout_real) {
-    // lane = output channel (TMEM lane); unit j: columns g * 16 + e = tap
-    // (row, dx = g - 1), input channel 16 c + e
-    const int co = warp * 32 + lane;
+  if (nmine > 0 && !*abort && warp < 2) {
+    // TMEM lane 16 t + co (t = 0, 1, 2): dy shifted by t - 1 rows, output
+    // channel 16 cc + co; unit j, column 16 g + e: dx = g - 1, input channel
+    // 16 c + e; the tap's y offset is 1 - t
+    const int lrow = warp * 32 + lane, t = lrow >> 4, col = lrow & 15;
+    const int per_dz = ncc * a.nchunk;
     for (int j = 0; j < nunit; ++j) {
-      const int u = u0 + j, row = u / a.nchunk, c = u - row * a.nchunk;
+      const int u = u0 + j, dz = u / per_dz, rem = u - dz * per_dz;
+      const int cc = rem / a.nchunk, c = rem - cc * a.nchunk;
+      const int co = cc * 16 + col;
       for (int g = 0; g < 3; ++g) {
-        const int tap = row * 3 + g;
+        const int tap = dz * 9 + (2 - t) * 3 + g;
         uint32_t v[16];
         const uint32_t taddr =
             tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * kUnitCols + g * 16);
@@ -776,7 +843,7 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
               "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (co < a.cout_real) {
+        if (t < 3 && co < a.cout_real) {
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
             const int ci = a.ci_map[c * 16 + e];
@@ -797,76 +864,53 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
   }
 }
 
-// bias gradient: db[c] = sum over voxels of dy[v][c]
-__global__ void k_bias_grad(const bf16 *dy, int ctot, int c0, int cout, long long nvox,
-                            float *db) {
-  __shared__ float red[256];
-  const int c = blockIdx.y;
-  float s = 0.f;
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox;
-       v += (long long)gridDim.x * blockDim.x)
-    s += __bfloat162float(dy[v * ctot + c0 + c]);
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0 && c < cout) atomicAdd(&db[c], red[0]);
-}
-
 // ---------------------------------------------------------------------------
-// elementwise and resampling kernels (channel slices of channels-last tensors)
+// elementwise and resampling kernels (channel slices of channels-last tensors).
+// Channel counts and slice offsets are multiples of 16, so a thread moves
+// groups of 8 channels (16 bytes).
 // ---------------------------------------------------------------------------
-// dy *= leaky'(y) (y is the activation output: same sign as its input)
-__global__ void k_act_bwd(bf16 *dy, int dctot, int dc0, const bf16 *y, int yctot, int yc0,
-                          int c, long long nvox, float slope) {
-  const long long n = nvox * c;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long v = i / c;
-    const int k = (int)(i - v * c);
-    const float yy = __bfloat162float(y[v * yctot + yc0 + k]);
-    bf16 &d = dy[v * dctot + dc0 + k];
-    if (!(yy > 0.f)) d = __float2bfloat16_rn(__bfloat162float(d) * slope);
-  }
-}
-
 // 2x2x2 average pooling: out (X/2, Y/2, Z/2) from in (X, Y, Z)
 __global__ void k_pool2(const bf16 *in, int ictot, int ic0, bf16 *out, int octot, int oc0, int c,
                         int batch, int X, int Y, int Z) {
-  const int Xo = X / 2, Yo = Y / 2, Zo = Z / 2;
-  const long long n = (long long)batch * Xo * Yo * Zo * c;
+  const int Xo = X / 2, Yo = Y / 2, Zo = Z / 2, c8 = c / 8;
+  const long long n = (long long)batch * Xo * Yo * Zo * c8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c;
-    const int k = (int)(i - g * c);
+    long long g = i / c8;
+    const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % Xo);
     g /= Xo;
     const int y = (int)(g % Yo);
     g /= Yo;
     const int z = (int)(g % Zo);
     const long long s = g / Zo;
-    float acc = 0.f;
+    Bf8 acc{};
     for (int d = 0; d < 8; ++d) {
       const size_t q = (((size_t)s * Z + 2 * z + (d >> 2)) * Y + 2 * y + ((d >> 1) & 1)) * X +
                        2 * x + (d & 1);
-      acc += __bfloat162float(in[q * ictot + ic0 + k]);
+      const Bf8 t = load8(in + q * ictot + ic0 + k);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) acc.v[e] += t.v[e];
     }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc.v[e] *= 0.125f;
     const size_t o = (((size_t)s * Zo + z) * Yo + y) * Xo + x;
-    out[o * octot + oc0 + k] = __float2bfloat16_rn(acc * 0.125f);
+    store8(out + o * octot + oc0 + k, acc);
   }
 }
 
-// gradient of pooling, added to din: din[child] += dout[parent] / 8
+// gradient of pooling, added to din: din[child] += dout[parent] / 8; then, with
+// a gate y, din *= leaky'(y) (din is complete: the gradient of the activation y)
 __global__ void k_pool2_bwd_add(const bf16 *dout, int octot, int oc0, bf16 *din, int ictot,
-                                int ic0, int c, int batch, int X, int Y, int Z) {
-  const long long n = (long long)batch * X * Y * Z * c;
+                                int ic0, int c, int batch, int X, int Y, int Z, const bf16 *gy,
+                                int gctot, int gc0, float slope) {
+  const int c8 = c / 8;
+  const long long n = (long long)batch * X * Y * Z * c8;
   const int Xo = X / 2, Yo = Y / 2, Zo = Z / 2;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c;
-    const int k = (int)(i - g * c);
+    long long g = i / c8;
+    const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % X);
     g /= X;
     const int y = (int)(g % Y);
@@ -875,21 +919,24 @@ __global__ void k_pool2_bwd_add(const bf16 *dout, int octot, int oc0, bf16 *din,
     const long long s = g / Z;
     const size_t o = (((size_t)s * Zo + z / 2) * Yo + y / 2) * Xo + x / 2;
     const size_t q = (((size_t)s * Z + z) * Y + y) * X + x;
-    bf16 &d = din[q * ictot + ic0 + k];
-    d = __float2bfloat16_rn(__bfloat162float(d) +
-                            0.125f * __bfloat162float(dout[o * octot + oc0 + k]));
+    Bf8 d = load8(din + q * ictot + ic0 + k);
+    const Bf8 t = load8(dout + o * octot + oc0 + k);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) d.v[e] = __bfloat162float(__float2bfloat16_rn(d.v[e] + 0.125f * t.v[e]));
+    if (gy) gate8(d, gy + q * gctot + gc0 + k, slope);
+    store8(din + q * ictot + ic0 + k, d);
   }
 }
 
 // nearest-neighbour upsampling by 2: out (2X, 2Y, 2Z)
 __global__ void k_up2(const bf16 *in, int ictot, int ic0, bf16 *out, int octot, int oc0, int c,
                       int batch, int X, int Y, int Z) {
-  const int X2 = 2 * X, Y2 = 2 * Y, Z2 = 2 * Z;
-  const long long n = (long long)batch * X2 * Y2 * Z2 * c;
+  const int X2 = 2 * X, Y2 = 2 * Y, Z2 = 2 * Z, c8 = c / 8;
+  const long long n = (long long)batch * X2 * Y2 * Z2 * c8;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c;
-    const int k = (int)(i - g * c);
+    long long g = i / c8;
+    const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % X2);
     g /= X2;
     const int y = (int)(g % Y2);
@@ -898,55 +945,76 @@ __global__ void k_up2(const bf16 *in, int ictot, int ic0, bf16 *out, int octot, 
     const long long s = g / Z2;
     const size_t q = (((size_t)s * Z + z / 2) * Y + y / 2) * X + x / 2;
     const size_t o = (((size_t)s * Z2 + z) * Y2 + y) * X2 + x;
-    out[o * octot + oc0 + k] = in[q * ictot + ic0 + k];
+    *reinterpret_cast<uint4 *>(out + o * octot + oc0 + k) =
+        *reinterpret_cast<const uint4 *>(in + q * ictot + ic0 + k);
   }
 }
 
-// gradient of upsampling: dout (X, Y, Z) = sum of the 8 children in din (2X...)
+// gradient of upsampling: dout (X, Y, Z) = sum of the 8 children in din (2X...);
+// with a gate y, dout *= leaky'(y)
 __global__ void k_up2_bwd(const bf16 *din, int ictot, int ic0, bf16 *dout, int octot, int oc0,
-                          int c, int batch, int X, int Y, int Z) {
-  const long long n = (long long)batch * X * Y * Z * c;
+                          int c, int batch, int X, int Y, int Z, const bf16 *gy, int gctot,
+                          int gc0, float slope) {
+  const int c8 = c / 8;
+  const long long n = (long long)batch * X * Y * Z * c8;
   const int X2 = 2 * X, Y2 = 2 * Y;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c;
-    const int k = (int)(i - g * c);
+    long long g = i / c8;
+    const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % X);
     g /= X;
     const int y = (int)(g % Y);
     g /= Y;
     const int z = (int)(g % Z);
     const long long s = g / Z;
-    float acc = 0.f;
+    Bf8 acc{};
     for (int d = 0; d < 8; ++d) {
       const size_t q = (((size_t)s * 2 * Z + 2 * z + (d >> 2)) * Y2 + 2 * y + ((d >> 1) & 1)) *
                            X2 + 2 * x + (d & 1);
-      acc += __bfloat162float(din[q * ictot + ic0 + k]);
+      const Bf8 t = load8(din + q * ictot + ic0 + k);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) acc.v[e] += t.v[e];
     }
     const size_t o = (((size_t)s * Z + z) * Y + y) * X + x;
-    dout[o * octot + oc0 + k] = __float2bfloat16_rn(acc);
+    if (gy) {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) acc.v[e] = __bfloat162float(__float2bfloat16_rn(acc.v[e]));
+      gate8(acc, gy + o * gctot + gc0 + k, slope);
+    }
+    store8(dout + o * octot + oc0 + k, acc);
   }
 }
 
 // 1x1 output head (c -> 1, FP32 weights) fused with the MSE loss and its
 // gradient.  pred = w . h + b; with a target: loss += (pred - t)^2,
-// dpred = 2 (pred - t) / nvox, dh = dpred * w (BF16), dw += dpred * h,
-// db += dpred.
+// dpred = 2 (pred - t) / nvox, dh = dpred * w (BF16) * leaky'(h) (h is the
+// activation output of the last convolution), dw += dpred * h, db += dpred.
+// One thread per voxel; h rows are 16-channel multiples (hctot <= 16 here).
 __global__ void k_head(const bf16 *h, int hctot, int c, const float *w, const float *b,
                        long long nvox, float *pred, const float *target, bf16 *dh,
-                       float *dw, float *db, float *loss, float over_weight) {
+                       float *dw, float *db, float *loss, float over_weight, float slope) {
   __shared__ float red[256];
   __shared__ float redw[16][33];
   float l = 0.f, gb = 0.f;
   float gw[16] = {};
+  float wk[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) wk[k] = k < c ? w[k] : 0.f;
+  const float b0 = b[0];
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox;
        v += (long long)gridDim.x * blockDim.x) {
+    const Bf8 h0 = load8(h + v * hctot), h1 = load8(h + v * hctot + 8);
     float hv[16];
-    float p = b[0];
-    for (int k = 0; k < c; ++k) {
-      hv[k] = __bfloat162float(h[v * hctot + k]);
-      p = fmaf(w[k], hv[k], p);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      hv[k] = h0.v[k];
+      hv[k + 8] = h1.v[k];
     }
+    float p = b0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      if (k < c) p = fmaf(wk[k], hv[k], p);
     if (pred) pred[v] = p;
     if (target) {
       const float diff = p - target[v];
@@ -956,9 +1024,23 @@ __global__ void k_head(const bf16 *h, int hctot, int c, const float *w, const fl
       l += wl * diff * diff;
       const float g = 2.f * wl * diff / (float)nvox;
       gb += g;
-      for (int k = 0; k < hctot; ++k)
-        dh[v * hctot + k] = __float2bfloat16_rn(k < c ? g * w[k] : 0.f);
-      for (int k = 0; k < c; ++k) gw[k] = fmaf(g, hv[k], gw[k]);
+      Bf8 d0, d1;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        // BF16 gradient, then the activation derivative (two roundings, as a
+        // stored gradient followed by the activation backward)
+        float a0 = k < c ? __bfloat162float(__float2bfloat16_rn(g * wk[k])) : 0.f;
+        float a1 = k + 8 < c ? __bfloat162float(__float2bfloat16_rn(g * wk[k + 8])) : 0.f;
+        if (!(hv[k] > 0.f)) a0 *= slope;
+        if (!(hv[k + 8] > 0.f)) a1 *= slope;
+        d0.v[k] = a0;
+        d1.v[k] = a1;
+      }
+      store8(dh + v * hctot, d0);
+      store8(dh + v * hctot + 8, d1);
+#pragma unroll
+      for (int k = 0; k < 16; ++k)
+        if (k < c) gw[k] = fmaf(g, hv[k], gw[k]);
     }
   }
   if (!target) return;
@@ -1465,7 +1547,8 @@ ConvPlan conv_plan(int nchunk, int npad, int optin) {
 
 template <int TY, int KZ>
 int conv_launch(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias,
-                const Slice &out, int act, int batch, const int dims[3], int optin) {
+                const Slice &out, int act, int batch, const int dims[3], int optin,
+                const Slice *gate) {
   using T = ConvTile<TY, KZ>;
   CUtensorMap map;
   UN_TRY((make_halo_map<TY, KZ>(&map, in, batch, dims)));
@@ -1481,6 +1564,11 @@ int conv_launch(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bi
   a.batch = batch;
   a.act = act;
   a.slope = u->slope;
+  if (gate) {
+    a.gate = gate->base;
+    a.gate_ctot = gate->ctot;
+    a.gate_c0 = gate->c0;
+  }
   a.err = u->d_err;
   const ConvPlan p = conv_plan<TY, KZ>(a.nchunk, a.npad, optin);
   if (p.wstages < 2)
@@ -1518,9 +1606,10 @@ bool conv_deep_ok(const Slice &in, const Slice &out, int batch, const int dims[3
   return p.wstages == 27 && p.nbuf == 2 && T::num_tiles(batch, dims) >= sms;
 }
 
-// y = act(conv(x) + b) into out slice; wpack rows = out.c
+// y = act(conv(x) + b) into out slice; wpack rows = out.c; with a gate (an
+// activation output of out's shape), y *= leaky'(gate)
 int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, const Slice &out,
-            int act, int batch, const int dims[3]) {
+            int act, int batch, const int dims[3], const Slice *gate = nullptr) {
   const int ty = tile_y(dims);
   if (!ty)
     return fail(CMI_ERR_INVALID_ARGUMENT,
@@ -1533,43 +1622,55 @@ int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, 
   UN_TRY(smem_optin(u, k_conv3_tc<16, 1>, &optin));
   UN_CUDA(cudaGetDevice(&dev));
   UN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  if (ty == 8) return conv_launch<8, 1>(u, in, wpack, bias, out, act, batch, dims, optin);
+  if (gate && (gate->c != out.c || gate->c0 % 16 || gate->ctot % 16))
+    return fail(CMI_ERR_INVALID_ARGUMENT, "gate slice does not match the output");
+  if (ty == 8) return conv_launch<8, 1>(u, in, wpack, bias, out, act, batch, dims, optin, gate);
   if (conv_deep_ok<4>(in, out, batch, dims, optin, sms))
-    return conv_launch<16, 4>(u, in, wpack, bias, out, act, batch, dims, optin);
+    return conv_launch<16, 4>(u, in, wpack, bias, out, act, batch, dims, optin, gate);
   if (conv_deep_ok<2>(in, out, batch, dims, optin, sms))
-    return conv_launch<16, 2>(u, in, wpack, bias, out, act, batch, dims, optin);
-  return conv_launch<16, 1>(u, in, wpack, bias, out, act, batch, dims, optin);
+    return conv_launch<16, 2>(u, in, wpack, bias, out, act, batch, dims, optin, gate);
+  return conv_launch<16, 1>(u, in, wpack, bias, out, act, batch, dims, optin, gate);
 }
 
 template <int TY>
-int wgrad_t(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *ci_map,
-            int cin_real, int cout_real, int batch, const int dims[3]) {
+int wgrad_t(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, float *db,
+            const int *ci_map, int cin_real, int cout_real, int batch, const int dims[3]) {
   using T = ConvTile<TY>;
   CUtensorMap xm, dym;
   UN_TRY(make_halo_map<TY>(&xm, x, batch, dims));
-  UN_TRY(make_map_box(&dym, dy, batch, dims, 8, T::kTX, T::kTY, T::kTZ));
+  using D = DyTile<TY>;
+  UN_TRY(make_map_box(&dym, dy, batch, dims, 16, T::kTX, D::kRows, D::kTZ));
   WgradTcArgs a{};
   a.cout = dy.c;
   a.nchunk = x.c / 16;
   for (int k = 0; k < 3; ++k) a.dims[k] = dims[k];
   a.batch = batch;
   // units spread evenly over the fewest groups that fit the tensor memory
-  const int units = 9 * a.nchunk;
+  const int units = 3 * (a.cout / 16) * a.nchunk;
   const int groups = (units + kWgradUnitsPerCta - 1) / kWgradUnitsPerCta;
   a.units_per_cta = (units + groups - 1) / groups;
   uint32_t cols = 32;
-  while (cols < (uint32_t)(a.units_per_cta * kUnitCols + 2 * kDyCols)) cols <<= 1;
+  while (cols < (uint32_t)(a.units_per_cta * kUnitCols)) cols <<= 1;
   a.tmem_cols = cols;
   a.dw = dw;
+  a.db = db;
   a.ci_map = ci_map;
   a.cin_real = cin_real;
   a.cout_real = cout_real;
   a.err = u->d_err;
   int optin = 0;
   UN_TRY(smem_optin(u, k_conv3_wgrad_tc<TY>, &optin));
-  const size_t buf = (size_t)(a.cout / 8) * kDyGroupBytes + (size_t)a.nchunk * T::kChunkBytes;
-  auto smem_for = [&](int nbuf) { return 1024 + nbuf * buf + 128; };
+  // buffers [dy chunks][input halo]; the barriers sit past the buffers and past
+  // the furthest byte the last dy chunk's A operands reach
+  const size_t buf = (size_t)(a.cout / 16) * D::kChunkBytes + (size_t)a.nchunk * T::kChunkBytes;
+  auto bars_at = [&](int nbuf) {
+    const size_t reach_end =
+        (size_t)(nbuf - 1) * buf + (size_t)(a.cout / 16 - 1) * D::kChunkBytes + D::kReach;
+    return (std::max(nbuf * buf, reach_end) + 127) / 128 * 128;
+  };
+  auto smem_for = [&](int nbuf) { return 1024 + bars_at(nbuf) + 128; };
   a.nbuf = smem_for(2) <= (size_t)optin ? 2 : 1;
+  a.bar_off = (int)bars_at(a.nbuf);
   const size_t smem = smem_for(a.nbuf);
   if (smem > (size_t)optin)
     return fail(CMI_ERR_NOT_SUPPORTED, "weight gradient needs %zu B of shared memory", smem);
@@ -1590,7 +1691,9 @@ int wgrad_t(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *
   return CMI_OK;
 }
 
-int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *ci_map,
+// dW (and, with db, the bias gradient) of a convolution from its input x and
+// output gradient dy, accumulated
+int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, float *db, const int *ci_map,
           int cin_real, int cout_real, int batch, const int dims[3]) {
   const int ty = tile_y(dims);
   if (!ty)
@@ -1601,8 +1704,8 @@ int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, const int *ci
     return fail(CMI_ERR_NOT_SUPPORTED,
                 "weight gradient: input channels must be 16..256, output channels 16..128, "
                 "multiples of 16");
-  return ty == 16 ? wgrad_t<16>(u, x, dy, dw, ci_map, cin_real, cout_real, batch, dims)
-                  : wgrad_t<8>(u, x, dy, dw, ci_map, cin_real, cout_real, batch, dims);
+  return ty == 16 ? wgrad_t<16>(u, x, dy, dw, db, ci_map, cin_real, cout_real, batch, dims)
+                  : wgrad_t<8>(u, x, dy, dw, db, ci_map, cin_real, cout_real, batch, dims);
 }
 
 // packs every layer's weights from the FP32 master parameters
@@ -1655,14 +1758,14 @@ int forward(cmi_unet *u, int batch, const int d1[3]) {
                  batch, d1));
   UN_TRY(conv_tc(u, S(u->E1A, c.s1, 0, c.s1), L[1].wf, L[1].bias_pad,
                  S(u->CAT1, c.cat1, c.s2, c.s1), 1, batch, d1));
-  k_pool2<<<grid_for(v1 / 8 * c.s1), 256, 0, u->stream>>>(u->CAT1, c.cat1, c.s2, u->P1, c.s1, 0,
+  k_pool2<<<grid_for(v1 / 8 * c.s1 / 8), 256, 0, u->stream>>>(u->CAT1, c.cat1, c.s2, u->P1, c.s1, 0,
                                                            c.s1, batch, d1[0], d1[1], d1[2]);
   // level 2
   UN_TRY(conv_tc(u, S(u->P1, c.s1, 0, c.s1), L[2].wf, L[2].bias_pad, S(u->E2A, c.s2, 0, c.s2), 1,
                  batch, d2));
   UN_TRY(conv_tc(u, S(u->E2A, c.s2, 0, c.s2), L[3].wf, L[3].bias_pad,
                  S(u->CAT2, c.cat2, c.s3, c.s2), 1, batch, d2));
-  k_pool2<<<grid_for(v1 / 64 * c.s2), 256, 0, u->stream>>>(u->CAT2, c.cat2, c.s3, u->P2, c.s2, 0,
+  k_pool2<<<grid_for(v1 / 64 * c.s2 / 8), 256, 0, u->stream>>>(u->CAT2, c.cat2, c.s3, u->P2, c.s2, 0,
                                                             c.s2, batch, d2[0], d2[1], d2[2]);
   // level 3
   UN_TRY(conv_tc(u, S(u->P2, c.s2, 0, c.s2), L[4].wf, L[4].bias_pad, S(u->BA, c.s3, 0, c.s3), 1,
@@ -1670,14 +1773,14 @@ int forward(cmi_unet *u, int batch, const int d1[3]) {
   UN_TRY(conv_tc(u, S(u->BA, c.s3, 0, c.s3), L[5].wf, L[5].bias_pad, S(u->BB, c.s3, 0, c.s3), 1,
                  batch, d3));
   // up to level 2
-  k_up2<<<grid_for(v1 / 8 * c.s3), 256, 0, u->stream>>>(u->BB, c.s3, 0, u->CAT2, c.cat2, 0, c.s3,
+  k_up2<<<grid_for(v1 / 8 * c.s3 / 8), 256, 0, u->stream>>>(u->BB, c.s3, 0, u->CAT2, c.cat2, 0, c.s3,
                                                          batch, d3[0], d3[1], d3[2]);
   UN_TRY(conv_tc(u, S(u->CAT2, c.cat2, 0, c.cat2), L[6].wf, L[6].bias_pad,
                  S(u->D2A, c.s2, 0, c.s2), 1, batch, d2));
   UN_TRY(conv_tc(u, S(u->D2A, c.s2, 0, c.s2), L[7].wf, L[7].bias_pad, S(u->D2B, c.s2, 0, c.s2), 1,
                  batch, d2));
   // up to level 1
-  k_up2<<<grid_for(v1 * c.s2), 256, 0, u->stream>>>(u->D2B, c.s2, 0, u->CAT1, c.cat1, 0, c.s2,
+  k_up2<<<grid_for(v1 * c.s2 / 8), 256, 0, u->stream>>>(u->D2B, c.s2, 0, u->CAT1, c.cat1, 0, c.s2,
                                                      batch, d2[0], d2[1], d2[2]);
   UN_TRY(conv_tc(u, S(u->CAT1, c.cat1, 0, c.cat1), L[8].wf, L[8].bias_pad,
                  S(u->D1A, c.s1, 0, c.s1), 1, batch, d1));
@@ -1698,82 +1801,85 @@ int backward(cmi_unet *u, const float *target, int batch, const int d1[3]) {
   std::vector<Layer> &L = u->L;
   UN_CUDA(cudaMemsetAsync(u->g, 0, sizeof(float) * u->nparams, u->stream));
   UN_CUDA(cudaMemsetAsync(u->d_loss, 0, sizeof(float), u->stream));
+  const float sl = u->slope;
+  // the head writes dy of the last convolution, times its activation derivative
   k_head<<<grid_for(v1), 256, 0, u->stream>>>(u->D1B, c.s1, c.c1, u->p + u->head_w,
                                                u->p + u->head_b, v1, u->pred, target, u->gD1B,
                                                u->g + u->head_w, u->g + u->head_b, u->d_loss,
-                                               u->over_weight);
-  const float sl = u->slope;
-  // one convolution layer backwards: dy (in place) *= act'(y); wgrad; input gradient
-  auto layer_bwd = [&](int li, const Slice &x, const Slice &y, const Slice &dy, const Slice *dx,
-                       int b, const int *dims, long long nv) -> int {
-    k_act_bwd<<<grid_for(nv * dy.c), 256, 0, u->stream>>>(dy.base, dy.ctot, dy.c0, y.base, y.ctot,
-                                                         y.c0, dy.c, nv, sl);
-    UN_TRY(wgrad(u, x, dy, u->g + L[li].w_off, L[li].d_map, L[li].cin_real, L[li].cout, b,
-                 dims));
-    k_bias_grad<<<dim3(64, dy.c), 256, 0, u->stream>>>(dy.base, dy.ctot, dy.c0, L[li].cout, nv,
-                                                       u->g + L[li].b_off);
-    if (dx) UN_TRY(conv_tc(u, dy, L[li].wd, nullptr, *dx, 0, b, dims));
+                                               u->over_weight, sl);
+  // one convolution layer backwards from dy (already times the derivative of
+  // its activation): weight and bias gradients, then the input gradient dx,
+  // with a gate the activation output that dx is the gradient of
+  auto layer_bwd = [&](int li, const Slice &x, const Slice &dy, const Slice *dx,
+                       const Slice *gate, int b, const int *dims) -> int {
+    UN_TRY(wgrad(u, x, dy, u->g + L[li].w_off, u->g + L[li].b_off, L[li].d_map,
+                 L[li].cin_real, L[li].cout, b, dims));
+    if (dx) UN_TRY(conv_tc(u, dy, L[li].wd, nullptr, *dx, 0, b, dims, gate));
     return CMI_OK;
   };
   // level 1 decoder
   {
-    const Slice dx = S(u->gD1A, c.s1, 0, c.s1);
-    UN_TRY(layer_bwd(9, S(u->D1A, c.s1, 0, c.s1), S(u->D1B, c.s1, 0, c.s1),
-                     S(u->gD1B, c.s1, 0, c.s1), &dx, batch, d1, v1));
+    const Slice dx = S(u->gD1A, c.s1, 0, c.s1), gate = S(u->D1A, c.s1, 0, c.s1);
+    UN_TRY(layer_bwd(9, S(u->D1A, c.s1, 0, c.s1), S(u->gD1B, c.s1, 0, c.s1), &dx, &gate, batch,
+                     d1));
   }
   {
     const Slice dx = S(u->gCAT1, c.cat1, 0, c.cat1);
-    UN_TRY(layer_bwd(8, S(u->CAT1, c.cat1, 0, c.cat1), S(u->D1A, c.s1, 0, c.s1),
-                     S(u->gD1A, c.s1, 0, c.s1), &dx, batch, d1, v1));
+    UN_TRY(layer_bwd(8, S(u->CAT1, c.cat1, 0, c.cat1), S(u->gD1A, c.s1, 0, c.s1), &dx, nullptr,
+                     batch, d1));
   }
-  // up1 backward: gD2B = sum of children of gCAT1[0:s2]
-  k_up2_bwd<<<grid_for(v2 * c.s2), 256, 0, u->stream>>>(u->gCAT1, c.cat1, 0, u->gD2B, c.s2, 0,
-                                                         c.s2, batch, d2[0], d2[1], d2[2]);
+  // up1 backward: gD2B = sum of children of gCAT1[0:s2], times leaky'(D2B)
+  k_up2_bwd<<<grid_for(v2 * c.s2 / 8), 256, 0, u->stream>>>(
+      u->gCAT1, c.cat1, 0, u->gD2B, c.s2, 0, c.s2, batch, d2[0], d2[1], d2[2], u->D2B, c.s2, 0,
+      sl);
   {
-    const Slice dx = S(u->gD2A, c.s2, 0, c.s2);
-    UN_TRY(layer_bwd(7, S(u->D2A, c.s2, 0, c.s2), S(u->D2B, c.s2, 0, c.s2),
-                     S(u->gD2B, c.s2, 0, c.s2), &dx, batch, d2, v2));
+    const Slice dx = S(u->gD2A, c.s2, 0, c.s2), gate = S(u->D2A, c.s2, 0, c.s2);
+    UN_TRY(layer_bwd(7, S(u->D2A, c.s2, 0, c.s2), S(u->gD2B, c.s2, 0, c.s2), &dx, &gate, batch,
+                     d2));
   }
   {
     const Slice dx = S(u->gCAT2, c.cat2, 0, c.cat2);
-    UN_TRY(layer_bwd(6, S(u->CAT2, c.cat2, 0, c.cat2), S(u->D2A, c.s2, 0, c.s2),
-                     S(u->gD2A, c.s2, 0, c.s2), &dx, batch, d2, v2));
+    UN_TRY(layer_bwd(6, S(u->CAT2, c.cat2, 0, c.cat2), S(u->gD2A, c.s2, 0, c.s2), &dx, nullptr,
+                     batch, d2));
   }
-  // up2 backward: gBB = sum of children of gCAT2[0:s3]
-  k_up2_bwd<<<grid_for(v3 * c.s3), 256, 0, u->stream>>>(u->gCAT2, c.cat2, 0, u->gBB, c.s3, 0,
-                                                         c.s3, batch, d3[0], d3[1], d3[2]);
+  // up2 backward: gBB = sum of children of gCAT2[0:s3], times leaky'(BB)
+  k_up2_bwd<<<grid_for(v3 * c.s3 / 8), 256, 0, u->stream>>>(
+      u->gCAT2, c.cat2, 0, u->gBB, c.s3, 0, c.s3, batch, d3[0], d3[1], d3[2], u->BB, c.s3, 0, sl);
   {
-    const Slice dx = S(u->gBA, c.s3, 0, c.s3);
-    UN_TRY(layer_bwd(5, S(u->BA, c.s3, 0, c.s3), S(u->BB, c.s3, 0, c.s3),
-                     S(u->gBB, c.s3, 0, c.s3), &dx, batch, d3, v3));
+    const Slice dx = S(u->gBA, c.s3, 0, c.s3), gate = S(u->BA, c.s3, 0, c.s3);
+    UN_TRY(layer_bwd(5, S(u->BA, c.s3, 0, c.s3), S(u->gBB, c.s3, 0, c.s3), &dx, &gate, batch,
+                     d3));
   }
   {
     const Slice dx = S(u->gP2, c.s2, 0, c.s2);
-    UN_TRY(layer_bwd(4, S(u->P2, c.s2, 0, c.s2), S(u->BA, c.s3, 0, c.s3),
-                     S(u->gBA, c.s3, 0, c.s3), &dx, batch, d3, v3));
+    UN_TRY(layer_bwd(4, S(u->P2, c.s2, 0, c.s2), S(u->gBA, c.s3, 0, c.s3), &dx, nullptr, batch,
+                     d3));
   }
-  // pool2 backward, added to the skip gradient gCAT2[s3 : s3 + s2]
-  k_pool2_bwd_add<<<grid_for(v2 * c.s2), 256, 0, u->stream>>>(
-      u->gP2, c.s2, 0, u->gCAT2, c.cat2, c.s3, c.s2, batch, d2[0], d2[1], d2[2]);
+  // pool2 backward, added to the skip gradient gCAT2[s3 : s3 + s2], times the
+  // derivative of that activation (CAT2[s3:])
+  k_pool2_bwd_add<<<grid_for(v2 * c.s2 / 8), 256, 0, u->stream>>>(
+      u->gP2, c.s2, 0, u->gCAT2, c.cat2, c.s3, c.s2, batch, d2[0], d2[1], d2[2], u->CAT2, c.cat2,
+      c.s3, sl);
   {
-    const Slice dx = S(u->gE2A, c.s2, 0, c.s2);
-    UN_TRY(layer_bwd(3, S(u->E2A, c.s2, 0, c.s2), S(u->CAT2, c.cat2, c.s3, c.s2),
-                     S(u->gCAT2, c.cat2, c.s3, c.s2), &dx, batch, d2, v2));
+    const Slice dx = S(u->gE2A, c.s2, 0, c.s2), gate = S(u->E2A, c.s2, 0, c.s2);
+    UN_TRY(layer_bwd(3, S(u->E2A, c.s2, 0, c.s2), S(u->gCAT2, c.cat2, c.s3, c.s2), &dx, &gate,
+                     batch, d2));
   }
   {
     const Slice dx = S(u->gP1, c.s1, 0, c.s1);
-    UN_TRY(layer_bwd(2, S(u->P1, c.s1, 0, c.s1), S(u->E2A, c.s2, 0, c.s2),
-                     S(u->gE2A, c.s2, 0, c.s2), &dx, batch, d2, v2));
+    UN_TRY(layer_bwd(2, S(u->P1, c.s1, 0, c.s1), S(u->gE2A, c.s2, 0, c.s2), &dx, nullptr, batch,
+                     d2));
   }
-  k_pool2_bwd_add<<<grid_for(v1 * c.s1), 256, 0, u->stream>>>(
-      u->gP1, c.s1, 0, u->gCAT1, c.cat1, c.s2, c.s1, batch, d1[0], d1[1], d1[2]);
+  k_pool2_bwd_add<<<grid_for(v1 * c.s1 / 8), 256, 0, u->stream>>>(
+      u->gP1, c.s1, 0, u->gCAT1, c.cat1, c.s2, c.s1, batch, d1[0], d1[1], d1[2], u->CAT1, c.cat1,
+      c.s2, sl);
   {
-    const Slice dx = S(u->gE1A, c.s1, 0, c.s1);
-    UN_TRY(layer_bwd(1, S(u->E1A, c.s1, 0, c.s1), S(u->CAT1, c.cat1, c.s2, c.s1),
-                     S(u->gCAT1, c.cat1, c.s2, c.s1), &dx, batch, d1, v1));
+    const Slice dx = S(u->gE1A, c.s1, 0, c.s1), gate = S(u->E1A, c.s1, 0, c.s1);
+    UN_TRY(layer_bwd(1, S(u->E1A, c.s1, 0, c.s1), S(u->gCAT1, c.cat1, c.s2, c.s1), &dx, &gate,
+                     batch, d1));
   }
-  UN_TRY(layer_bwd(0, S(u->X0, 16, 0, 16), S(u->E1A, c.s1, 0, c.s1), S(u->gE1A, c.s1, 0, c.s1),
-                   nullptr, batch, d1, v1));
+  UN_TRY(layer_bwd(0, S(u->X0, 16, 0, 16), S(u->gE1A, c.s1, 0, c.s1), nullptr, nullptr, batch,
+                   d1));
   UN_CUDA(cudaGetLastError());
   return CMI_OK;
 }
@@ -1984,7 +2090,7 @@ int cmi_unet_forward(cmi_unet *u, const float *features, float *pred, int32_t ba
   const Chans c = chans(u);
   k_head<<<grid_for(v1), 256, 0, u->stream>>>(u->D1B, c.s1, c.c1, u->p + u->head_w,
                                                u->p + u->head_b, v1, pred, nullptr, nullptr,
-                                               nullptr, nullptr, nullptr, 1.f);
+                                               nullptr, nullptr, nullptr, 1.f, u->slope);
   UN_CUDA(cudaGetLastError());
   return check_err(u);
 }
@@ -2243,8 +2349,8 @@ int cmi_unet_conv3_wgrad(cmi_unet *u, const void *x, int32_t cin, const void *dy
   UN_CUDA(cudaMalloc(&map, sizeof(int) * cin));
   UN_CUDA(cudaMemcpy(map, id.data(), sizeof(int) * cin, cudaMemcpyHostToDevice));
   UN_CUDA(cudaMemsetAsync(dw, 0, sizeof(float) * 27 * cin * cout, u->stream));
-  const int rc = wgrad(u, Slice{(bf16 *)x, cin, 0, cin}, Slice{(bf16 *)dy, cout, 0, cout}, dw, map,
-                       cin, cout, batch, d);
+  const int rc = wgrad(u, Slice{(bf16 *)x, cin, 0, cin}, Slice{(bf16 *)dy, cout, 0, cout}, dw,
+                       nullptr, map, cin, cout, batch, d);
   const cudaError_t e = cudaStreamSynchronize(u->stream);
   cudaFree(map);
   if (rc != CMI_OK) return rc;
