@@ -381,8 +381,13 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
   volatile int *abort = &s_abort;
 
   if (warp == 4 && lane == 0) {
-    // loads: the halo of tile i, then its weights, one stage per tap
+    // loads: resident weights once, in one copy; then per tile its halo and,
+    // when the weights stream, one stage per tap
     int tiles_issued = 0, stages_issued = 0;
+    if (resident && nmine > 0) {
+      mbar_expect_tx(&b_full[0], (uint32_t)(27 * tbytes));
+      bulk_load(sB, a.wpack, (uint32_t)(27 * tbytes), &b_full[0]);
+    }
     for (int i = 0; i < nmine && !*abort; ++i) {
       int x0, y0, z0, n;
       T::tile_origin(blockIdx.x + i * gridDim.x, a.dims, x0, y0, z0, n);
@@ -393,7 +398,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
       for (int c = 0; c < a.nchunk; ++c)
         T::load_chunk(h + (size_t)c * T::kChunkBytes, &in, c * 16, x0, y0, z0, n, &h_full[hb]);
       tiles_issued = i + 1;
-      if (resident && i > 0) continue;
+      if (resident) continue;
       for (int tap = 0; tap < 27; ++tap) {
         const int g = i * 27 + tap, s = g % S, u = g / S;
         if (u > 0 && !role_wait(&b_empty[s], (uint32_t)(u - 1) & 1u, a.err, abort)) break;
@@ -409,6 +414,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
       mbar_wait(&h_full[i % a.nbuf], (uint32_t)(i / a.nbuf) & 1u, a.err);
     for (int g = max(0, stages_issued - S); g < stages_issued; ++g)
       mbar_wait(&b_full[g % S], (uint32_t)(g / S) & 1u, a.err);
+    if (resident && nmine > 0) mbar_wait(&b_full[0], 0u, a.err);
   } else if (warp == 5 && lane == 0) {
     const uint32_t idesc = idesc_bf16(a.npad);
     // descriptors advance by (byte offset >> 4) in their low 14-bit address
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
     const uint64_t tstep = (uint64_t)nchunk * bstep;        // next tap's weights
     bool ok = true;
     if (resident && nmine > 0) {
-      for (int t = 0; t < 27 && ok; ++t) ok = role_wait(&b_full[t], 0u, a.err, abort);
+      ok = role_wait(&b_full[0], 0u, a.err, abort);
       tc_fence_after();
     }
     int s = 0;            // weight stage of the next tap (streaming)
