@@ -118,7 +118,8 @@ typedef struct {
   int32_t device;              /* CUDA device ordinal */
   int32_t threads_per_cta;     /* 0 = library default (256) */
   int32_t ctas_per_sm;         /* 0 = as many as fit */
-  int32_t packets_per_chunk;   /* 0 = library default (128); power of two in [32, 4096] */
+  int32_t packets_per_chunk;   /* 0 = library default (128; 256 when subgrids have <= 1024
+                                  cells); power of two in [32, 4096] */
   int32_t tally_mode;          /* FP32 and mixed transports: cmi_tally (default CMI_TALLY_FIXED64) */
   int32_t use_graph;           /* 1 = capture each iteration as a CUDA graph (default) */
   int32_t max_run_chunks;      /* most chunks a CTA claims at once (0 = 64): how long a CTA
@@ -485,9 +486,10 @@ int cmi_unet_upsample_nearest(cmi_unet *net, const float *src, const int32_t dim
 /* x_H = 10^clamp(prediction, log10_min, 0) as FP64 (device), n values */
 int cmi_unet_to_neutral_fraction(cmi_unet *net, const float *prediction, double *xH, int64_t n,
                                  float log10_min);
-/* Building blocks, exposed for testing (grids: X and Y multiples of 8, Z of 2,
- * the convolution tile of 8 x 8 x 2 voxels): one 3x3x3 convolution on the tensor
- * cores (BF16 channels-last device tensors, channel counts multiples of 16,
+/* Building blocks, exposed for testing (grids: X and Y multiples of 8, and Y a
+ * multiple of 16 or Z of 2: tiles of 8 x 16 x KZ or 8 x 8 x 2 voxels): one 3x3x3
+ * convolution on the tensor cores (BF16 channels-last device tensors, channel
+ * counts multiples of 16 (the weight gradient: output channels <= 128),
  * weights packed by cmi_unet_pack_weights, bias FP32 or NULL, activation 1 =
  * leaky ReLU); packing of FP32 W[cout][27][cin] (flip = 1: the input-gradient
  * form); the weight gradient dW[cout][27][cin] (FP32, device) of a

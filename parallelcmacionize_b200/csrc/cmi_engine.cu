@@ -55,7 +55,12 @@ constexpr int kSpareRounds = 3;  // wavefront rounds beyond the straight-line bo
 // have no fixed bound: the round loop runs until no packet is left, capped
 // here only against a runaway loop.
 constexpr int kReemissionRoundCap = 4096;
-constexpr uint32_t kDefaultRefill = 16;  // lanes not walking before a warp routes + refills
+// lanes not walking before a warp routes + refills: FP32 walk 16 (sweep on B200,
+// lognormal128: 12 -> 6.77e10, 16 -> 6.92e10, 24 -> 6.86e10); the mixed walk's
+// longer FP64 steps favour 12 (8 -> 6.05e10, 12 -> 6.07e10, 16 -> 5.98e10,
+// 24 -> 5.69e10)
+constexpr uint32_t kDefaultRefill = 16;
+constexpr uint32_t kDefaultRefillMixed = 12;
 
 struct HostInstance {
   cmi_grid_desc desc;
@@ -421,7 +426,8 @@ WalkParams walk_params(cmi_context *c) {
   WalkParams p{};
   p.chunk = c->chunk;
   p.max_run = c->opt.max_run_chunks > 0 ? (uint32_t)c->opt.max_run_chunks : 64u;
-  p.refill = c->opt.refill_lanes > 0 ? (uint32_t)c->opt.refill_lanes : kDefaultRefill;
+  p.refill = c->opt.refill_lanes > 0 ? (uint32_t)c->opt.refill_lanes
+                                      : (c->mixed() ? kDefaultRefillMixed : kDefaultRefill);
   p.subs = c->d_sub;
   p.inst = c->d_inst;
   p.chunks = c->d_chunks;
@@ -977,6 +983,11 @@ int cmi_create(const cmi_grid_desc *grids, int32_t num_instances, const cmi_opti
   }
   c->S = (uint32_t)c->h_sub.size();
   c->total_padded = cell_off;
+  // default chunk: 256 packets for small subgrids (<= 1024 cells: a visit is a
+  // few crossings, so claims and ring refills are a larger share of a packet's
+  // cost; B200, stromgren64's 8^3 subgrids: 3.20e10 -> 3.63e10 crossings/s),
+  // else 128 (16^3 subgrids: 128 beats 256 by 14% on lognormal128)
+  if (opt.packets_per_chunk == 0 && c->max_padded <= 1024) c->chunk = 256u;
   c->ntiles = (c->S + kPlanTile - 1) / kPlanTile;
 
   int rc = CMI_OK;
