@@ -487,11 +487,12 @@ int cmi_unet_upsample_nearest(cmi_unet *net, const float *src, const int32_t dim
 int cmi_unet_to_neutral_fraction(cmi_unet *net, const float *prediction, double *xH, int64_t n,
                                  float log10_min);
 /* Building blocks, exposed for testing (grids: X and Y multiples of 8, and Y a
- * multiple of 16 or Z of 2: tiles of 8 x 16 x KZ or 8 x 8 x 2 voxels): one 3x3x3
- * convolution on the tensor cores (BF16 channels-last device tensors, channel
- * counts multiples of 16 (the weight gradient: output channels <= 128),
- * weights packed by cmi_unet_pack_weights, bias FP32 or NULL, activation 1 =
- * leaky ReLU); packing of FP32 W[cout][27][cin] (flip = 1: the input-gradient
+ * multiple of 16 or Z of 2): one 3x3x3 convolution on the tensor cores (BF16
+ * channels-last device tensors, channel counts multiples of 16 (the weight
+ * gradient: output channels <= 128); up to 80 output channels the three x taps
+ * share one MMA (tiles of 16 x 8 x KZ voxels), above that tiles of 8 x 16 x KZ or
+ * 8 x 8 x 2 voxels; weights packed by cmi_unet_pack_weights for the same output
+ * channel count, bias FP32 or NULL, activation 1 = leaky ReLU); packing of FP32 W[cout][27][cin] (flip = 1: the input-gradient
  * form); the weight gradient dW[cout][27][cin] (FP32, device) of a
  * convolution from its input x and output gradient dy. */
 int cmi_unet_conv3(cmi_unet *net, const void *in, int32_t in_channels, const void *weights_packed,

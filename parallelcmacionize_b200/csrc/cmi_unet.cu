@@ -299,6 +299,7 @@ struct ConvArgs {
   int nchunk;            // 16-channel chunks of the input
   int nbuf;              // halo buffers (2: the next tile's halo loads during this one)
   int wstages;           // weight stages of one tap each; 27: all weights stay resident
+  int kq;                // k_conv3_xf: K steps per weight stage (divides nchunk)
   int dims[3];           // X, Y, Z
   int batch;
   int act;               // 1: leaky ReLU
@@ -600,6 +601,373 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_tc(const __grid_constant
   tc_fence_before();
   __syncthreads();
   if (warp == 5) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(2 * scols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3x3x3 convolution with the x taps folded into N
+// ---------------------------------------------------------------------------
+// The MMA rows are u = 16 x 8 voxels (x fastest) and N = 3 x npad columns: for
+// a (dz, dy) tap row, column g npad + c of row u accumulates sum over the input
+// channels of x(u + (0, dy, dz)) W(dz, dy, dx = g)[c].  The output at v is then
+// D(v - 1)[0] + D(v)[1] + D(v + 1)[2]: the neighbours along x are the lanes
+// either side in the warp, so the epilogue combines them with two shuffles.  A
+// tile yields the 14 x 8 outputs of its u columns 1 .. 14 (tiles overlap by two
+// columns; the last one along x is cut at the grid's edge).  Each (dz, dy, chunk)
+// is one MMA of N = 3 npad instead of three of N = npad, and the input box needs
+// no halo in x: 16 x 10 x (KZ + 2) voxels.
+template <int KZ>
+struct XTile {
+  static constexpr int kUX = 16, kUY = 8;            // MMA rows: 16 x 8 voxels
+  static constexpr int kOX = 14;                     // outputs per tile along x
+  static constexpr int kHY = kUY + 2, kHZ = KZ + 2;  // input rows, slices
+  static constexpr int kCopyBytes = kUX * kHY * kHZ * 32;
+  static constexpr int kChunkBytes = (kCopyBytes + 1023) / 1024 * 1024;
+  // A operand of sub-tile st and tap row (dz, dy): 128 consecutive voxel rows
+  static __host__ __device__ constexpr int tap_offset(int st, int dz, int dy) {
+    return ((st + dz) * kHY + dy) * kUX * 32;
+  }
+  static __device__ __forceinline__ void origin(int t, const int dims[3], int &x0, int &y0,
+                                                int &z0, int &n) {
+    const int tx = (dims[0] + kOX - 1) / kOX, ty = dims[1] / kUY, tz = dims[2] / KZ;
+    const int bx = t % tx;
+    t /= tx;
+    const int by = t % ty;
+    t /= ty;
+    const int bz = t % tz;
+    n = t / tz;
+    x0 = bx * kOX - 1;
+    y0 = by * kUY;
+    z0 = bz * KZ;
+  }
+  static __host__ __device__ int num_tiles(int batch, const int dims[3]) {
+    return batch * ((dims[0] + kOX - 1) / kOX) * (dims[1] / kUY) * (dims[2] / KZ);
+  }
+};
+
+// The same persistent, warp-specialised structure as k_conv3_tc: warp 4 loads
+// (the weights once when resident, else kq K steps per ring stage; each tile's
+// input box into a ring of up to kMaxInBufs buffers: a tile's MMAs are short,
+// so several input boxes are in flight to cover the load latency), warp 5
+// issues the MMAs, warps 0-3 combine, add bias, apply the activation or the
+// derivative gate and store.
+constexpr int kMaxInBufs = 8;
+constexpr int kXfEpiWarps = 8;                      // two per quarter of the TMEM lanes
+constexpr int kXfThreads = (kXfEpiWarps + 2) * 32;  // + loads + MMAs
+// tcgen05.mma and tcgen05.commit issued by one elected lane of a converged warp:
+// the x-folded kernel's MMA role runs its loops on the whole warp, whose
+// branches are then uniform (a branch inside a one-lane region costs more than
+// an MMA).  elect.sync picks the same lane every time, so the commits track the
+// MMAs that lane issued.  No memory clobber on the MMA: the statements are
+// ordered by being volatile, and their operands were published by the barrier
+// waits before them.
+__device__ __forceinline__ void mma_el(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p, e;\n elect.sync _|e, 0xffffffff;\n setp.ne.b32 p, %4, 0;\n"
+      " @e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void commit_el(uint64_t *bar) {
+  asm volatile(
+      "{\n .reg .pred e;\n elect.sync _|e, 0xffffffff;\n"
+      " @e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n}" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+// bounded wait of a whole warp with one outcome for all its lanes
+__device__ __forceinline__ bool warp_wait(uint64_t *b, uint32_t parity, uint32_t *err,
+                                          volatile int *abort) {
+  return __all_sync(0xffffffffu, role_wait(b, parity, err, abort));
+}
+
+// The MMAs of one tile with resident weights, fully unrolled (NCH input chunks),
+// so that they follow one another with only descriptor adds between them.
+template <int KZ, int NCH>
+__device__ __forceinline__ void xf_mma_tile(uint32_t d0, uint32_t acols, uint64_t adesc0,
+                                            uint64_t bdesc0, uint32_t idesc, uint32_t bstep) {
+  using T = XTile<KZ>;
+  uint64_t bd = bdesc0;
+#pragma unroll
+  for (int t9 = 0; t9 < 9; ++t9)
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) {
+#pragma unroll
+      for (int st = 0; st < KZ; ++st)
+        mma_el(d0 + (uint32_t)st * acols,
+               adesc0 + (uint32_t)((T::tap_offset(st, t9 / 3, t9 % 3) + c * T::kChunkBytes) >> 4),
+               bd, idesc, (t9 > 0 || c > 0) ? 1u : 0u);
+      bd += bstep;
+    }
+}
+
+// NCH > 0: the kernel for NCH input chunks (resident weights fully unrolled);
+// 0: any chunk count
+template <int KZ, int NCH>
+__global__ void __launch_bounds__(kXfThreads, 1) k_conv3_xf(const __grid_constant__ CUtensorMap in,
+                                                           ConvArgs a) {
+  using T = XTile<KZ>;
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  unsigned char *sm = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~(uintptr_t)1023);
+  const int nrow = 3 * a.npad;                                // MMA N
+  const int bbytes = nrow * 32;                               // one K step's weights
+  const int tbytes = a.nchunk * bbytes;                       // one tap row's weights
+  const int qbytes = a.kq * bbytes;                           // one weight stage
+  const int kst = 9 * a.nchunk / a.kq;                        // weight stages per tile
+  const int S = a.wstages;
+  const bool resident = S == kst && a.kq == a.nchunk;
+  const size_t hbytes = (size_t)a.nchunk * T::kChunkBytes;   // one input buffer
+  unsigned char *sH = sm;                                     // [nbuf][nchunk][chunk]
+  unsigned char *sB = sH + a.nbuf * hbytes;                   // [S][kq][3 npad * 32]
+  float *sbias = reinterpret_cast<float *>(sB + (size_t)S * qbytes);
+  uint64_t *b_full = reinterpret_cast<uint64_t *>(sbias + a.npad);
+  uint64_t *b_empty = b_full + kMaxWStages;
+  uint64_t *h_full = b_empty + kMaxWStages;  // [kMaxInBufs]
+  uint64_t *h_empty = h_full + kMaxInBufs;   // [kMaxInBufs]
+  uint64_t *a_full = h_empty + kMaxInBufs;   // [2]
+  uint64_t *a_empty = a_full + 2;            // [2]
+  uint64_t *drain = a_empty + 2;             // the MMAs in flight when the CTA ends
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+  __shared__ int s_abort;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles = T::num_tiles(a.batch, a.dims);
+  const int nmine = (blockIdx.x < tiles) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t acols = nrow <= 64 ? 64u : nrow <= 128 ? 128u : 256u;
+  const uint32_t scols = KZ * acols;  // one accumulator set
+
+  for (int c = tid; c < a.npad; c += kXfThreads) sbias[c] = a.bias ? a.bias[c] : 0.f;
+  if (tid == 0) {
+    s_abort = 0;
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&b_full[s], 1);
+      mbar_init(&b_empty[s], 1);
+    }
+    for (int s = 0; s < a.nbuf; ++s) {
+      mbar_init(&h_full[s], 1);
+      mbar_init(&h_empty[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&a_full[s], 1);
+      mbar_init(&a_empty[s], kXfEpiWarps);  // one arrival per epilogue warp
+    }
+    mbar_init(drain, 1);
+    fence_mbar_init();
+  }
+  if (warp == kXfEpiWarps + 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(2 * scols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  volatile int *abort = &s_abort;
+
+  if (warp == kXfEpiWarps && lane == 0) {
+    int tiles_issued = 0, stages_issued = 0;
+    if (resident && nmine > 0) {
+      mbar_expect_tx(&b_full[0], (uint32_t)(9 * tbytes));
+      bulk_load(sB, a.wpack, (uint32_t)(9 * tbytes), &b_full[0]);
+    }
+    for (int i = 0; i < nmine && !*abort; ++i) {
+      int x0, y0, z0, n;
+      T::origin(blockIdx.x + i * gridDim.x, a.dims, x0, y0, z0, n);
+      const int hb = i % a.nbuf, hu = i / a.nbuf;
+      if (hu > 0 && !role_wait(&h_empty[hb], (uint32_t)(hu - 1) & 1u, a.err, abort)) break;
+      mbar_expect_tx(&h_full[hb], (uint32_t)(a.nchunk * T::kCopyBytes));
+      unsigned char *h = sH + hb * hbytes;
+      for (int c = 0; c < a.nchunk; ++c)
+        tma_load_5d(h + (size_t)c * T::kChunkBytes, &in, c * 16, x0, y0 - 1, z0 - 1, n,
+                    &h_full[hb]);
+      tiles_issued = i + 1;
+      if (resident) continue;
+      for (int k = 0; k < kst; ++k) {
+        const int g = i * kst + k, s = g % S, u = g / S;
+        if (u > 0 && !role_wait(&b_empty[s], (uint32_t)(u - 1) & 1u, a.err, abort)) break;
+        mbar_expect_tx(&b_full[s], (uint32_t)qbytes);
+        bulk_load(sB + (size_t)s * qbytes, a.wpack + (size_t)k * a.kq * nrow * 16,
+                  (uint32_t)qbytes, &b_full[s]);
+        stages_issued = g + 1;
+      }
+    }
+    // the last copy into every buffer has landed before the CTA ends
+    for (int i = max(0, tiles_issued - a.nbuf); i < tiles_issued; ++i)
+      mbar_wait(&h_full[i % a.nbuf], (uint32_t)(i / a.nbuf) & 1u, a.err);
+    for (int g = max(0, stages_issued - S); g < stages_issued; ++g)
+      mbar_wait(&b_full[g % S], (uint32_t)(g / S) & 1u, a.err);
+    if (resident && nmine > 0) mbar_wait(&b_full[0], 0u, a.err);
+  } else if (warp == kXfEpiWarps + 1) {
+    const uint32_t idesc = idesc_bf16(nrow);
+    // descriptors advance by (byte offset >> 4) in their low 14-bit address
+    // field; every operand lies below 256 KB, so the sums never carry out of it
+    const uint64_t bdesc0 = sw32_desc_off(sB, 16u, 256u);
+    const uint32_t cstep = (uint32_t)T::kChunkBytes >> 4;  // next 16-channel chunk
+    const uint32_t bstep = (uint32_t)bbytes >> 4;           // next K step's weights
+    const int nchunk = a.nchunk;
+    bool ok = true;
+    if (resident && nmine > 0) {
+      ok = warp_wait(&b_full[0], 0u, a.err, abort);
+      tc_fence_after();
+    }
+    int s = 0;            // weight stage of the next K steps (streaming)
+    uint32_t sphase = 0;  // its parity
+    int hb = 0;           // input buffer of tile i
+    uint32_t hphase = 0;  // its parity
+    for (int i = 0; i < nmine && ok; ++i) {
+      const int ab = i & 1;
+      if (i >= 2 && !warp_wait(&a_empty[ab], (uint32_t)((i >> 1) - 1) & 1u, a.err, abort)) break;
+      if (!warp_wait(&h_full[hb], hphase, a.err, abort)) break;
+      tc_fence_after();
+      const uint64_t adesc0 = sw32_desc_off(sH + hb * hbytes, 16u, 256u);
+      const uint32_t d0 = tmem + (uint32_t)ab * scols;
+      if (NCH > 0 && resident) {
+        xf_mma_tile<KZ, (NCH > 0 ? NCH : 1)>(d0, acols, adesc0, bdesc0, idesc, bstep);
+      } else if (resident) {
+        // registers only: see xf_mma_tile
+        uint64_t bd = bdesc0;
+        for (int t9 = 0; t9 < 9; ++t9) {
+          uint64_t at = adesc0 + ((uint32_t)T::tap_offset(0, t9 / 3, t9 % 3) >> 4);
+          for (int c = 0; c < nchunk; ++c) {
+            const uint32_t acc = (t9 > 0 || c > 0) ? 1u : 0u;
+#pragma unroll
+            for (int st = 0; st < KZ; ++st)
+              mma_el(d0 + (uint32_t)st * acols, at + (uint32_t)(T::tap_offset(st, 0, 0) >> 4), bd,
+                     idesc, acc);
+            at += cstep;
+            bd += bstep;
+          }
+        }
+      } else {
+        // stage k holds K steps k kq .. k kq + kq - 1 (tap row t9 = step / nchunk)
+        for (int k = 0; k < kst; ++k) {
+          if (!warp_wait(&b_full[s], sphase, a.err, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint64_t bd = bdesc0 + (uint32_t)(s * a.kq) * bstep;
+          const int step0 = k * a.kq, t9 = step0 / nchunk, c0 = step0 - t9 * nchunk;
+          uint64_t at = adesc0 + ((uint32_t)(T::tap_offset(0, t9 / 3, t9 % 3) +
+                                             c0 * T::kChunkBytes) >> 4);
+          for (int c = 0; c < a.kq; ++c) {
+            const uint32_t acc = (step0 + c > 0) ? 1u : 0u;
+#pragma unroll
+            for (int st = 0; st < KZ; ++st)
+              mma_el(d0 + (uint32_t)st * acols, at + (uint32_t)(T::tap_offset(st, 0, 0) >> 4), bd,
+                     idesc, acc);
+            at += cstep;
+            bd += bstep;
+          }
+          commit_el(&b_empty[s]);
+          if (++s == S) {
+            s = 0;
+            sphase ^= 1u;
+          }
+        }
+        if (!ok) break;
+      }
+      // the input buffer and the accumulators are released once these MMAs complete
+      commit_el(&h_empty[hb]);
+      commit_el(&a_full[ab]);
+      if (++hb == a.nbuf) {
+        hb = 0;
+        hphase ^= 1u;
+      }
+    }
+    // every MMA issued has completed before TMEM is released
+    commit_el(drain);
+    mbar_wait(drain, 0, a.err);
+  } else if (warp < kXfEpiWarps) {
+    for (int i = 0; i < nmine; ++i) {
+      const int ab = i & 1;
+      bool ok0 = true;
+      if (lane == 0) ok0 = role_wait(&a_full[ab], (uint32_t)(i >> 1) & 1u, a.err, abort);
+      if (!__shfl_sync(0xffffffffu, ok0, 0)) break;
+      tc_fence_after();
+      int x0, y0, z0, n;
+      T::origin(blockIdx.x + i * gridDim.x, a.dims, x0, y0, z0, n);
+      // row r = u (16 x 8, x fastest); outputs at u columns 1 .. 14 inside the grid.
+      // Warps q and q + 4 read TMEM lanes 32 q .. 32 q + 31 and share the
+      // (sub-tile, 16-channel group) items of the tile between them.
+      const int q = warp & 3, r = q * 32 + lane, ux = r & 15;
+      const int vx = x0 + ux, vy = y0 + (r >> 4);
+      const bool valid = ux >= 1 && ux <= T::kOX && vx < a.dims[0];
+      const int ngrp = a.npad >> 4;
+      for (int item = warp >> 2; item < KZ * ngrp; item += kXfEpiWarps / 4) {
+        const int st = item / ngrp, j = (item - st * ngrp) * 16;
+        const int vz = z0 + st;
+        const size_t vox = (((size_t)n * a.dims[2] + vz) * a.dims[1] + vy) * a.dims[0] + vx;
+        {
+          uint32_t v[3][16];
+#pragma unroll
+          for (int g = 0; g < 3; ++g) {
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)ab * scols +
+                                   (uint32_t)st * acols + (uint32_t)(g * a.npad + j);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+                "%12,%13,%14,%15}, [%16];"
+                : "=r"(v[g][0]), "=r"(v[g][1]), "=r"(v[g][2]), "=r"(v[g][3]), "=r"(v[g][4]),
+                  "=r"(v[g][5]), "=r"(v[g][6]), "=r"(v[g][7]), "=r"(v[g][8]), "=r"(v[g][9]),
+                  "=r"(v[g][10]), "=r"(v[g][11]), "=r"(v[g][12]), "=r"(v[g][13]),
+                  "=r"(v[g][14]), "=r"(v[g][15])
+                : "r"(taddr));
+          }
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          float f[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            // x tap -1 from the lane before, +1 from the lane after
+            const float left = __shfl_up_sync(0xffffffffu, __uint_as_float(v[0][e]), 1);
+            const float right = __shfl_down_sync(0xffffffffu, __uint_as_float(v[2][e]), 1);
+            f[e] = left + __uint_as_float(v[1][e]) + right;
+          }
+          if (valid) {
+            bf16 *dst = a.out + vox * a.out_ctot + a.out_c0 + j;
+            float gy[16];
+            if (a.gate) {
+              const bf16 *gp = a.gate + vox * a.gate_ctot + a.gate_c0 + j;
+              const Bf8 g0 = load8(gp), g1 = load8(gp + 8);
+#pragma unroll
+              for (int e = 0; e < 8; ++e) {
+                gy[e] = g0.v[e];
+                gy[e + 8] = g1.v[e];
+              }
+            }
+            __align__(16) bf16 o[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              float x = f[e] + sbias[j + e];
+              if (a.act) x = x > 0.f ? x : x * a.slope;
+              if (a.gate) {
+                x = __bfloat162float(__float2bfloat16_rn(x));
+                if (!(gy[e] > 0.f)) x *= a.slope;
+              }
+              o[e] = __float2bfloat16_rn(x);
+            }
+            uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+            d4[0] = reinterpret_cast<const uint4 *>(o)[0];
+            d4[1] = reinterpret_cast<const uint4 *>(o)[1];
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                      smem_u32(&a_empty[ab]))
+                                  : "memory");
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kXfEpiWarps + 1) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(2 * scols)
                  : "memory");
@@ -1091,7 +1459,11 @@ struct PackArgs {
   int rows, kchan;      // packed rows and K channels (multiples of 16)
   const int *ci_of_storage;  // storage input channel -> real ci or -1 (length cin storage)
   int flip;
+  int xf;               // x-folded layout of k_conv3_xf: [dz][dy][chunk][dx][row][16]
 };
+
+// k_conv3_xf serves convolutions whose three x taps fit one MMA's N (<= 256)
+__host__ __device__ inline bool conv_xf(int npad) { return 3 * npad <= 256; }
 
 __global__ void k_pack(PackArgs a) {
   const int nchunk = a.kchan / 16;
@@ -1114,9 +1486,17 @@ __global__ void k_pack(PackArgs a) {
       const int co = kc, ci = a.ci_of_storage[r];
       if (co < a.cout && ci >= 0) v = a.w[((size_t)co * 27 + (26 - tap)) * a.cin_real + ci];
     }
-    const size_t step = (size_t)tap * nchunk + ch;
-    const int half = (e >> 3) ^ ((r >> 2) & 1);
-    a.out[(step * a.rows + r) * 16 + half * 8 + (e & 7)] = __float2bfloat16_rn(v);
+    if (a.xf) {
+      // K step (dz, dy, chunk) holds the rows of its three x taps: dx-major
+      const size_t step = (size_t)(tap / 3) * nchunk + ch;
+      const int rr = (tap % 3) * a.rows + r;
+      const int half = (e >> 3) ^ ((rr >> 2) & 1);
+      a.out[(step * 3 * a.rows + rr) * 16 + half * 8 + (e & 7)] = __float2bfloat16_rn(v);
+    } else {
+      const size_t step = (size_t)tap * nchunk + ch;
+      const int half = (e >> 3) ^ ((r >> 2) & 1);
+      a.out[(step * a.rows + r) * 16 + half * 8 + (e & 7)] = __float2bfloat16_rn(v);
+    }
   }
 }
 
@@ -1612,6 +1992,131 @@ bool conv_deep_ok(const Slice &in, const Slice &out, int batch, const int dims[3
   return p.wstages == 27 && p.nbuf == 2 && T::num_tiles(batch, dims) >= sms;
 }
 
+// shared memory of an x-folded convolution CTA: the weights resident (9 tap
+// rows) beside two input buffers when they fit, else a ring of stages of kq K
+// steps (the largest divisor of nchunk that leaves at least 4 stages, or at
+// least 2 with one input buffer)
+struct XfPlan {
+  int nbuf = 0, wstages = 0, kq = 0;
+  size_t smem = 0;
+};
+template <int KZ>
+XfPlan xf_plan(int nchunk, int npad, int optin) {
+  using T = XTile<KZ>;
+  const size_t bbytes = (size_t)3 * npad * 32;
+  auto smem_for = [&](int nbuf, int stages, int kq) {
+    return 1024 + (size_t)stages * kq * bbytes + (size_t)nbuf * nchunk * T::kChunkBytes +
+           (size_t)npad * 4 + (2 * kMaxWStages + 2 * kMaxInBufs + 5) * 8 + 16;
+  };
+  XfPlan p;
+  if (smem_for(2, 9, nchunk) <= (size_t)optin) {
+    // resident weights and as many input buffers as fit
+    p.nbuf = 2;
+    while (p.nbuf < kMaxInBufs && smem_for(p.nbuf + 1, 9, nchunk) <= (size_t)optin) ++p.nbuf;
+    p.wstages = 9;
+    p.kq = nchunk;
+  } else {
+    for (int nbuf = 2; nbuf >= 1 && !p.kq; --nbuf) {
+      const int need = nbuf == 2 ? 4 : 2;
+      for (int kq = nchunk; kq >= 1; --kq) {
+        if (nchunk % kq) continue;
+        const size_t fixed = smem_for(nbuf, 0, kq);
+        if (fixed >= (size_t)optin) break;
+        const int stages = (int)std::min<size_t>(std::min(kMaxWStages, 9 * nchunk / kq),
+                                                 (optin - fixed) / (kq * bbytes));
+        if (stages >= need) {
+          p.nbuf = nbuf;
+          p.wstages = stages;
+          p.kq = kq;
+          break;
+        }
+      }
+    }
+    if (!p.kq) return p;
+  }
+  p.smem = smem_for(p.nbuf, p.wstages, p.kq);
+  return p;
+}
+
+template <int KZ>
+int xf_launch(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias,
+              const Slice &out, int act, int batch, const int dims[3], int optin,
+              const Slice *gate, const XfPlan &p) {
+  using T = XTile<KZ>;
+  CUtensorMap map;
+  UN_TRY(make_map_box(&map, in, batch, dims, 16, T::kUX, T::kHY, T::kHZ));
+  ConvArgs a{};
+  a.wpack = wpack;
+  a.bias = bias;
+  a.out = out.base;
+  a.out_ctot = out.ctot;
+  a.out_c0 = out.c0;
+  a.npad = out.c;
+  a.nchunk = in.c / 16;
+  for (int k = 0; k < 3; ++k) a.dims[k] = dims[k];
+  a.batch = batch;
+  a.act = act;
+  a.slope = u->slope;
+  if (gate) {
+    a.gate = gate->base;
+    a.gate_ctot = gate->ctot;
+    a.gate_c0 = gate->c0;
+  }
+  a.err = u->d_err;
+  a.nbuf = p.nbuf;
+  a.wstages = p.wstages;
+  a.kq = p.kq;
+  // resident weights: the MMA sequence unrolled for the common chunk counts
+  auto kern = k_conv3_xf<KZ, 0>;
+  if (p.wstages == 9 && p.kq == a.nchunk) {
+    if (a.nchunk == 1) kern = k_conv3_xf<KZ, 1>;
+    if (a.nchunk == 2) kern = k_conv3_xf<KZ, 2>;
+    if (a.nchunk == 3) kern = k_conv3_xf<KZ, 3>;
+    if (a.nchunk == 5) kern = k_conv3_xf<KZ, 5>;
+  }
+  UN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+  int per_sm = 0;
+  UN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kXfThreads, p.smem));
+  const int nrow = 3 * a.npad;
+  const int acols = nrow <= 64 ? 64 : nrow <= 128 ? 128 : 256;
+  per_sm = std::max(1, std::min(per_sm, 512 / (2 * KZ * acols)));
+  int sms = 0, dev = 0;
+  UN_CUDA(cudaGetDevice(&dev));
+  UN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int tiles = T::num_tiles(batch, dims);
+  const int grid = std::max(1, std::min(tiles, per_sm * sms));
+  kern<<<grid, kXfThreads, p.smem, u->stream>>>(map, a);
+  UN_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+
+// x-folded convolution (weights packed with conv_xf): the deepest tile whose
+// accumulators fit the tensor memory, whose weights stay resident beside two
+// input buffers and that still gives every SM a tile; else one z slice
+int conv_xf_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias,
+               const Slice &out, int act, int batch, const int dims[3], const Slice *gate,
+               int sms) {
+  int optin = 0;
+  UN_TRY(smem_optin(u, k_conv3_xf<1, 0>, &optin));
+  const int nchunk = in.c / 16, npad = out.c;
+  const int acols = 3 * npad <= 64 ? 64 : 3 * npad <= 128 ? 128 : 256;
+  auto deep = [&](int kz, const XfPlan &p, int tiles) {
+    return dims[2] % kz == 0 && 2 * kz * acols <= 512 && p.kq == nchunk && p.wstages == 9 &&
+           p.nbuf >= 2 && tiles >= sms;
+  };
+  const XfPlan p4 = xf_plan<4>(nchunk, npad, optin);
+  if (deep(4, p4, XTile<4>::num_tiles(batch, dims)))
+    return xf_launch<4>(u, in, wpack, bias, out, act, batch, dims, optin, gate, p4);
+  const XfPlan p2 = xf_plan<2>(nchunk, npad, optin);
+  if (deep(2, p2, XTile<2>::num_tiles(batch, dims)))
+    return xf_launch<2>(u, in, wpack, bias, out, act, batch, dims, optin, gate, p2);
+  const XfPlan p1 = xf_plan<1>(nchunk, npad, optin);
+  if (!p1.kq)
+    return fail(CMI_ERR_NOT_SUPPORTED,
+                "convolution: %d input channels do not fit the shared memory", in.c);
+  return xf_launch<1>(u, in, wpack, bias, out, act, batch, dims, optin, gate, p1);
+}
+
 // y = act(conv(x) + b) into out slice; wpack rows = out.c; with a gate (an
 // activation output of out's shape), y *= leaky'(gate)
 int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, const Slice &out,
@@ -1630,6 +2135,7 @@ int conv_tc(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias, 
   UN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (gate && (gate->c != out.c || gate->c0 % 16 || gate->ctot % 16))
     return fail(CMI_ERR_INVALID_ARGUMENT, "gate slice does not match the output");
+  if (conv_xf(out.c)) return conv_xf_tc(u, in, wpack, bias, out, act, batch, dims, gate, sms);
   if (ty == 8) return conv_launch<8, 1>(u, in, wpack, bias, out, act, batch, dims, optin, gate);
   if (conv_deep_ok<4>(in, out, batch, dims, optin, sms))
     return conv_launch<16, 4>(u, in, wpack, bias, out, act, batch, dims, optin, gate);
@@ -1726,11 +2232,13 @@ int pack_all(cmi_unet *u) {
     a.rows = l.npad;
     a.kchan = l.kin;
     a.flip = 0;
+    a.xf = conv_xf(a.rows);
     k_pack<<<grid_for(27LL * l.kin * l.npad), 256, 0, u->stream>>>(a);
     a.out = l.wd;
     a.rows = l.kin;
     a.kchan = l.npad;
     a.flip = 1;
+    a.xf = conv_xf(a.rows);
     k_pack<<<grid_for(27LL * l.kin * l.npad), 256, 0, u->stream>>>(a);
     // bias padded to npad (zero beyond cout)
     UN_CUDA(cudaMemsetAsync(l.bias_pad, 0, sizeof(float) * l.npad, u->stream));
@@ -2336,6 +2844,7 @@ int cmi_unet_pack_weights(cmi_unet *u, const float *w, int32_t cout, int32_t cin
   a.flip = flip;
   a.rows = flip ? cin : cout;
   a.kchan = flip ? cout : cin;
+  a.xf = conv_xf(a.rows);
   k_pack<<<grid_for(27LL * cin * cout), 256, 0, u->stream>>>(a);
   const cudaError_t e = cudaStreamSynchronize(u->stream);
   cudaFree(map);

@@ -78,15 +78,22 @@ def net():
     n.close()
 
 
-# shapes (B, Z, Y, X): Y = 16 takes 8x16xKZ tiles, Y = 8 the 8x8x2 tiles; grids
-# with at least one tile per SM take 4 (1 x 32 x 64 x 64) or 2 (2 x 16 x 32 x
-# 64) z slices per tile; the weights of (16, 16) and (32, 48) stay resident in
-# shared memory, those of (80, 32) stream through a ring of tap stages, those of
-# (128, 128) through a ring beside a single halo buffer
+# shapes (B, Z, Y, X).  Up to 80 output channels the x taps share one MMA
+# (16 x 8 x KZ tiles, the last one along x cut at the grid's edge): grids with at
+# least one tile per SM take 4 (1 x 32 x 64 x 64) or 2 (2 x 16 x 32 x 64) z
+# slices per tile; the weights of (16, 16) and (32, 48) stay resident in shared
+# memory beside a ring of input boxes that wraps around in (4 x 32 x 64 x 64) and
+# (2 x 16 x 64 x 64); those of (80, 32) stream through a ring of tap rows, those
+# of (128, 80) through a ring of half tap rows beside one input box.  Above 80
+# output channels, 8 x 16 x KZ tiles (Y = 16) or 8 x 8 x 2 (Y = 8): the weights
+# of (64, 128) stream through a ring of tap stages beside two halo buffers,
+# those of (128, 128) beside a single one.
 @pytest.mark.parametrize("cin,cout,shape", [
     (16, 16, (2, 4, 16, 16)), (32, 48, (2, 4, 16, 16)), (80, 32, (2, 4, 16, 16)),
     (16, 32, (1, 6, 8, 16)), (48, 16, (2, 4, 8, 8)), (128, 128, (1, 2, 16, 8)),
-    (16, 16, (1, 32, 64, 64)), (32, 32, (2, 16, 32, 64))])
+    (16, 16, (1, 32, 64, 64)), (32, 32, (2, 16, 32, 64)), (16, 16, (4, 32, 64, 64)),
+    (16, 48, (2, 16, 64, 64)), (128, 80, (1, 4, 16, 24)), (64, 128, (1, 4, 16, 8)),
+    (16, 96, (1, 4, 8, 16)), (32, 64, (1, 2, 8, 40))])
 def test_conv3_forward_matches_oracle(net, cin, cout, shape):
     rng = np.random.default_rng(cin + cout)
     x = U.bf16_round(rng.normal(size=shape + (cin,)))
@@ -216,8 +223,8 @@ def test_training_reduces_loss():
     ft = torch.from_numpy(f.reshape(4, -1, 3).astype(np.float32)).cuda()
     tt = torch.from_numpy(target.reshape(4, -1)).cuda()
     with UNet(seed=1) as n:
-        losses = [n.train_step(ft, tt, (32, 32, 32), 3e-3) for _ in range(60)]
+        losses = [n.train_step(ft, tt, (32, 32, 32), 1e-3) for _ in range(60)]
     assert np.all(np.isfinite(losses))
     # FP32 atomics in the weight gradient make runs differ slightly: a threefold
-    # drop in 60 steps (typically 4-6x)
+    # drop in 60 steps (typically 14x; at 3e-3 the loss spikes now and then)
     assert np.mean(losses[-5:]) < 0.33 * losses[0], losses[::10]
