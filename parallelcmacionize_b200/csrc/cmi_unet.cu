@@ -1115,15 +1115,26 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
     // the last copy into every buffer has landed before the CTA ends
     for (int i = max(0, issued - a.nbuf); i < issued; ++i)
       mbar_wait(&full[i % a.nbuf], (uint32_t)(i / a.nbuf) & 1u, a.err);
-  } else if (warp == 5 && lane == 0) {
+  } else if (warp == 5) {
+    // the whole warp runs the loop (uniform branches), one elected lane issues.
     // BF16 x BF16 -> F32, A and B MN-major, M = 128, N = 48
     const uint32_t idesc = idesc_bf16(kUnitCols) | (1u << 15) | (1u << 16);
     const uint32_t kstep_a = (uint32_t)(16 * 32) >> 4;           // the next 16 voxels of dy
     const uint32_t kstep_b = (uint32_t)(2 * T::kRowBytes) >> 4;  // ... of the halo
+    // descriptor offsets of the CTA's units (dz, dy chunk cc, input chunk c)
     const int per_dz = ncc * a.nchunk;
+    uint32_t aoff[kWgradUnitsPerCta], boff[kWgradUnitsPerCta];
+#pragma unroll
+    for (int j = 0; j < kWgradUnitsPerCta; ++j) {
+      const int u = u0 + min(j, max(nunit - 1, 0)), dz = u / per_dz, rem = u - dz * per_dz;
+      const int cc = rem / a.nchunk, c = rem - cc * a.nchunk;
+      aoff[j] = (uint32_t)(cc * D::kChunkBytes) >> 4;
+      boff[j] = (uint32_t)(c * T::kChunkBytes + T::tap_offset(0, dz, 1, 0)) >> 4;
+    }
+    int b = 0;           // buffer of tile i
+    uint32_t bph = 0;    // its parity
     for (int i = 0; i < nmine; ++i) {
-      const int b = i % a.nbuf;
-      if (!role_wait(&full[b], (uint32_t)(i / a.nbuf) & 1u, a.err, abort)) break;
+      if (!warp_wait(&full[b], bph, a.err, abort)) break;
       tc_fence_after();
       const unsigned char *buf = sm + b * bufbytes;
       // A: LBO along M (the next 16 rows: dy one voxel row further in y), SBO
@@ -1132,34 +1143,26 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
       const uint64_t adesc = sw32_desc_off(buf, (uint32_t)D::kMStride, 256u);
       const uint64_t hdesc = sw32_desc_off(buf + dybytes, 32u, (uint32_t)T::kRowBytes);
       const uint32_t acc0 = i > 0 ? 1u : 0u;
-      for (int j = 0; j < nunit; ++j) {
-        const int u = u0 + j, dz = u / per_dz, rem = u - dz * per_dz;
-        const int cc = rem / a.nchunk, c = rem - cc * a.nchunk;
-        const uint64_t ad = adesc + ((uint32_t)(cc * D::kChunkBytes) >> 4);
-        const uint64_t bd =
-            hdesc + ((uint32_t)(c * T::kChunkBytes + T::tap_offset(0, dz, 1, 0)) >> 4);
-        const uint32_t dt = tmem + (uint32_t)(j * kUnitCols);
-        asm volatile(
-            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(dt),
-            "l"(ad), "l"(bd), "r"(idesc), "r"(acc0));
 #pragma unroll
-        for (int k = 1; k < 8; ++k)
-          asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, 1;" ::"r"(dt),
-                       "l"(ad + (uint32_t)k * kstep_a), "l"(bd + (uint32_t)k * kstep_b),
-                       "r"(idesc));
+      for (int j = 0; j < kWgradUnitsPerCta; ++j) {
+        if (j < nunit) {
+          const uint64_t ad = adesc + aoff[j], bd = hdesc + boff[j];
+          const uint32_t dt = tmem + (uint32_t)(j * kUnitCols);
+          mma_el(dt, ad, bd, idesc, acc0);
+#pragma unroll
+          for (int k = 1; k < 8; ++k)
+            mma_el(dt, ad + (uint32_t)k * kstep_a, bd + (uint32_t)k * kstep_b, idesc, 1u);
+        }
       }
       // the buffer is free once these MMAs complete
-      asm volatile(
-          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              smem_u32(&empty[b]))
-          : "memory");
+      commit_el(&empty[b]);
+      if (++b == a.nbuf) {
+        b = 0;
+        bph ^= 1u;
+      }
     }
     // every MMA issued has completed before the readout and the release of TMEM
-    asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            smem_u32(drain))
-        : "memory");
+    commit_el(drain);
     mbar_wait(drain, 0, a.err);
   } else if (warp < 4) {
     // bias gradient: thread co sums dy[v][co] over the CTA's tiles (the first
@@ -1764,6 +1767,10 @@ struct cmi_unet {
   size_t ratio_cap = 0;
   float over_weight = 1.f;      // loss weight of predictions above the target
   bool packed = false;
+  // CUDA graphs of the launch sequences whose arguments do not change between
+  // calls: the forward layers and the backward layers (for the current
+  // activation buffers), the weight packing (for the life of the network)
+  cudaGraphExec_t gx_fwd = nullptr, gx_bwd = nullptr, gx_pack = nullptr;
 };
 
 namespace cmiu {
@@ -1774,10 +1781,45 @@ int dev_zero_alloc(void **p, size_t bytes) {
   return CMI_OK;
 }
 
+void drop_graph(cudaGraphExec_t *g) {
+  if (*g) cudaGraphExecDestroy(*g);
+  *g = nullptr;
+}
+
+// the graphs that name the activation buffers go with them
 void free_bufs(cmi_unet *u) {
+  drop_graph(&u->gx_fwd);
+  drop_graph(&u->gx_bwd);
   for (void *b : u->bufs) cudaFree(b);
   u->bufs.clear();
   u->batch = 0;
+}
+
+// body() (a sequence of launches on u->stream) is captured into *exec on the
+// first call and replayed from then on: the per-launch host work (tensor maps,
+// attributes, occupancy) is done once
+template <class F>
+int graph_run(cmi_unet *u, cudaGraphExec_t *exec, F &&body) {
+  if (!*exec) {
+    UN_CUDA(cudaStreamBeginCapture(u->stream, cudaStreamCaptureModeRelaxed));
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(u->stream, &g);
+    if (rc != CMI_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess)
+      return fail(CMI_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      *exec = nullptr;
+      return fail(CMI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+    }
+  }
+  UN_CUDA(cudaGraphLaunch(*exec, u->stream));
+  return CMI_OK;
 }
 
 int alloc_t(cmi_unet *u, bf16 **t, long long nvox, int ctot) {
@@ -1963,7 +2005,10 @@ int conv_launch(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bi
   a.nbuf = p.nbuf;
   a.wstages = p.wstages;
   auto kern = k_conv3_tc<TY, KZ>;
-  UN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+  // the kernel's limit is the device's whole opt-in size, the same for every
+  // launch: a launch captured in a graph must stay valid whatever limit a
+  // later launch of the same kernel would otherwise have set
+  UN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   int per_sm = 0;
   UN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConvThreads, p.smem));
   // TMEM: two accumulator sets of a CTA, at most 512 columns per SM
@@ -2074,7 +2119,10 @@ int xf_launch(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias
     if (a.nchunk == 3) kern = k_conv3_xf<KZ, 3>;
     if (a.nchunk == 5) kern = k_conv3_xf<KZ, 5>;
   }
-  UN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+  // the kernel's limit is the device's whole opt-in size, the same for every
+  // launch: a launch captured in a graph must stay valid whatever limit a
+  // later launch of the same kernel would otherwise have set
+  UN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   int per_sm = 0;
   UN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kXfThreads, p.smem));
   const int nrow = 3 * a.npad;
@@ -2186,8 +2234,9 @@ int wgrad_t(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, float *db,
   const size_t smem = smem_for(a.nbuf);
   if (smem > (size_t)optin)
     return fail(CMI_ERR_NOT_SUPPORTED, "weight gradient needs %zu B of shared memory", smem);
+  // the whole opt-in size, the same for every launch (see xf_launch)
   UN_CUDA(cudaFuncSetAttribute(k_conv3_wgrad_tc<TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
+                               optin));
   int per_sm = 0;
   UN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3_wgrad_tc<TY>,
                                                         kWgradThreads, smem));
@@ -2221,7 +2270,7 @@ int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, float *db, co
 }
 
 // packs every layer's weights from the FP32 master parameters
-int pack_all(cmi_unet *u) {
+int pack_launches(cmi_unet *u) {
   for (Layer &l : u->L) {
     PackArgs a{};
     a.w = u->p + l.w_off;
@@ -2246,6 +2295,10 @@ int pack_all(cmi_unet *u) {
                             cudaMemcpyDeviceToDevice, u->stream));
   }
   UN_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+int pack_all(cmi_unet *u) {
+  UN_TRY(graph_run(u, &u->gx_pack, [&] { return pack_launches(u); }));
   u->packed = true;
   return CMI_OK;
 }
@@ -2259,8 +2312,7 @@ int check_dims(const int dims[3]) {
 }
 
 // forward pass from u->X0; writes u->pred
-int forward(cmi_unet *u, int batch, const int d1[3]) {
-  if (!u->packed) UN_TRY(pack_all(u));
+int forward_layers(cmi_unet *u, int batch, const int d1[3]) {
   const Chans c = chans(u);
   const int d2[3] = {d1[0] / 2, d1[1] / 2, d1[2] / 2};
   const int d3[3] = {d1[0] / 4, d1[1] / 4, d1[2] / 4};
@@ -2305,7 +2357,23 @@ int forward(cmi_unet *u, int batch, const int d1[3]) {
 }
 
 // loss + backward from u->D1B etc. (forward must have run); gradients into u->g
-int backward(cmi_unet *u, const float *target, int batch, const int d1[3]) {
+// the loss and the head's gradients from the target; dy of the last convolution
+int backward_head(cmi_unet *u, const float *target, int batch, const int d1[3]) {
+  const Chans c = chans(u);
+  const long long v1 = (long long)batch * d1[0] * d1[1] * d1[2];
+  UN_CUDA(cudaMemsetAsync(u->g, 0, sizeof(float) * u->nparams, u->stream));
+  UN_CUDA(cudaMemsetAsync(u->d_loss, 0, sizeof(float), u->stream));
+  // the head writes dy of the last convolution, times its activation derivative
+  k_head<<<grid_for(v1), 256, 0, u->stream>>>(u->D1B, c.s1, c.c1, u->p + u->head_w,
+                                               u->p + u->head_b, v1, u->pred, target, u->gD1B,
+                                               u->g + u->head_w, u->g + u->head_b, u->d_loss,
+                                               u->over_weight, u->slope);
+  UN_CUDA(cudaGetLastError());
+  return CMI_OK;
+}
+
+// the convolution layers backwards from dy of the last one: gradients into u->g
+int backward_layers(cmi_unet *u, int batch, const int d1[3]) {
   const Chans c = chans(u);
   const int d2[3] = {d1[0] / 2, d1[1] / 2, d1[2] / 2};
   const int d3[3] = {d1[0] / 4, d1[1] / 4, d1[2] / 4};
@@ -2313,14 +2381,7 @@ int backward(cmi_unet *u, const float *target, int batch, const int d1[3]) {
   const long long v2 = v1 / 8, v3 = v1 / 64;
   auto S = [](bf16 *b, int ctot, int c0, int cc) { return Slice{b, ctot, c0, cc}; };
   std::vector<Layer> &L = u->L;
-  UN_CUDA(cudaMemsetAsync(u->g, 0, sizeof(float) * u->nparams, u->stream));
-  UN_CUDA(cudaMemsetAsync(u->d_loss, 0, sizeof(float), u->stream));
   const float sl = u->slope;
-  // the head writes dy of the last convolution, times its activation derivative
-  k_head<<<grid_for(v1), 256, 0, u->stream>>>(u->D1B, c.s1, c.c1, u->p + u->head_w,
-                                               u->p + u->head_b, v1, u->pred, target, u->gD1B,
-                                               u->g + u->head_w, u->g + u->head_b, u->d_loss,
-                                               u->over_weight, sl);
   // one convolution layer backwards from dy (already times the derivative of
   // its activation): weight and bias gradients, then the input gradient dx,
   // with a gate the activation output that dx is the gradient of
@@ -2414,10 +2475,21 @@ int load_input(cmi_unet *u, const float *in, int batch, const int dims[3]) {
   if (batch <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "batch must be > 0");
   UN_CUDA(cudaSetDevice(u->device));
   UN_TRY(ensure_buffers(u, batch, dims));
+  if (!u->packed) UN_TRY(pack_all(u));
   const long long v1 = (long long)batch * dims[0] * dims[1] * dims[2];
   k_input<<<grid_for(v1 * 16), 256, 0, u->stream>>>(in, u->X0, v1);
   UN_CUDA(cudaGetLastError());
   return CMI_OK;
+}
+
+// the layers of a pass, replayed from their graphs (the buffers are those of
+// (batch, dims), which load_input has made current)
+int forward(cmi_unet *u, int batch, const int d[3]) {
+  return graph_run(u, &u->gx_fwd, [&] { return forward_layers(u, batch, d); });
+}
+int backward(cmi_unet *u, const float *target, int batch, const int d[3]) {
+  UN_TRY(backward_head(u, target, batch, d));
+  return graph_run(u, &u->gx_bwd, [&] { return backward_layers(u, batch, d); });
 }
 
 }  // namespace cmiu
@@ -2545,6 +2617,7 @@ int cmi_unet_destroy(cmi_unet *u) {
   cudaSetDevice(u->device);
   if (u->stream) cudaStreamSynchronize(u->stream);
   free_bufs(u);
+  drop_graph(&u->gx_pack);
   for (Layer &l : u->L) {
     cudaFree(l.wf);
     cudaFree(l.wd);
