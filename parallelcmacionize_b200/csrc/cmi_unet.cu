@@ -704,8 +704,25 @@ __device__ __forceinline__ void xf_mma_tile(uint32_t d0, uint32_t acols, uint64_
     }
 }
 
-// NCH > 0: the kernel for NCH input chunks (resident weights fully unrolled);
-// 0: any chunk count
+// The MMAs of one tap row (NCH input chunks) from one weight stage, unrolled;
+// acc0 = 0 starts the accumulators
+template <int KZ, int NCH>
+__device__ __forceinline__ void xf_mma_row(uint32_t d0, uint32_t acols, uint64_t at, uint64_t bd,
+                                           uint32_t idesc, uint32_t bstep, uint32_t acc0) {
+  using T = XTile<KZ>;
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) {
+#pragma unroll
+    for (int st = 0; st < KZ; ++st)
+      mma_el(d0 + (uint32_t)st * acols,
+             at + (uint32_t)((T::tap_offset(st, 0, 0) + c * T::kChunkBytes) >> 4), bd, idesc,
+             c > 0 ? 1u : acc0);
+    bd += bstep;
+  }
+}
+
+// NCH > 0: the kernel for NCH input chunks (resident weights, or a stage per
+// tap row, fully unrolled); 0: any chunk count
 template <int KZ, int NCH>
 __global__ void __launch_bounds__(kXfThreads, 1) k_conv3_xf(const __grid_constant__ CUtensorMap in,
                                                            ConvArgs a) {
@@ -854,6 +871,18 @@ __global__ void __launch_bounds__(kXfThreads, 1) k_conv3_xf(const __grid_constan
           }
           tc_fence_after();
           uint64_t bd = bdesc0 + (uint32_t)(s * a.kq) * bstep;
+          if (NCH > 0 && a.kq == NCH) {
+            // one tap row per stage
+            xf_mma_row<KZ, (NCH > 0 ? NCH : 1)>(
+                d0, acols, adesc0 + ((uint32_t)T::tap_offset(0, k / 3, k % 3) >> 4), bd, idesc,
+                bstep, k > 0 ? 1u : 0u);
+            commit_el(&b_empty[s]);
+            if (++s == S) {
+              s = 0;
+              sphase ^= 1u;
+            }
+            continue;
+          }
           const int step0 = k * a.kq, t9 = step0 / nchunk, c0 = step0 - t9 * nchunk;
           uint64_t at = adesc0 + ((uint32_t)(T::tap_offset(0, t9 / 3, t9 % 3) +
                                              c0 * T::kChunkBytes) >> 4);
@@ -1063,6 +1092,7 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
   uint64_t *empty = full + 2;    // [2]: the MMAs done (1) and dy summed (4 warps)
   uint64_t *drain = empty + 2;   // the MMAs in flight when the CTA ends
   uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+  __shared__ float s_db[128];  // the CTA's bias-gradient sums
   __shared__ int s_abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nunits = 3 * ncc * a.nchunk;
@@ -1072,6 +1102,7 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
   const int nmine = (blockIdx.x < tiles && nunit > 0)
                         ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
+  for (int c = tid; c < 128; c += kWgradThreads) s_db[c] = 0.f;
   if (tid == 0) {
     s_abort = 0;
     for (int s = 0; s < 2; ++s) {
@@ -1165,26 +1196,30 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
     commit_el(drain);
     mbar_wait(drain, 0, a.err);
   } else if (warp < 4) {
-    // bias gradient: thread co sums dy[v][co] over the CTA's tiles (the first
-    // group's CTAs; the others only release the buffers)
-    const int co = warp * 32 + lane;
-    const bool sum = a.db && blockIdx.y == 0 && warp * 32 < a.cout_real;  // warp-uniform
-    float bsum = 0.f;
+    // bias gradient: dy[v][co] summed over the CTA's tiles (the first group's
+    // CTAs; the others only release the buffers).  The 16-byte halves of the
+    // dy rows (8 channels each; 2 per 16-channel chunk) are spread over the
+    // 128 threads: thread t reads half p = t % pairs of rows t / pairs,
+    // + 128 / pairs, ...; its 8 sums go to shared memory at the end.
+    const bool sum = a.db && blockIdx.y == 0;  // CTA-uniform
+    const int pairs = 2 * ncc, tpp = 128 / pairs, p = tid % pairs, r0 = tid / pairs;
+    const bool mine = sum && r0 < tpp;
+    float bsum[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int i = 0; i < nmine; ++i) {
       const int b = i % a.nbuf;
       bool ok0 = true;
       if (lane == 0) ok0 = role_wait(&full[b], (uint32_t)(i / a.nbuf) & 1u, a.err, abort);
       if (!__shfl_sync(0xffffffffu, ok0, 0)) break;
-      if (sum && co < a.cout_real) {
+      if (mine) {
         // the 32-byte swizzle: 16-byte half h of the row at byte offset o sits
         // at half h ^ ((o >> 7) & 1)
-        const unsigned char *dy = sm + b * bufbytes + (co >> 4) * D::kChunkBytes;
-        const int h = (co >> 3) & 1, e = co & 7;
-#pragma unroll 8
-        for (int r = 0; r < 128; ++r) {
+        const unsigned char *dy = sm + b * bufbytes + (p >> 1) * D::kChunkBytes;
+        const int h = p & 1;
+        for (int r = r0; r < 128; r += tpp) {
           const int o = D::own_offset(r);
-          bsum += __bfloat162float(
-              *reinterpret_cast<const bf16 *>(dy + o + ((h ^ ((o >> 7) & 1)) << 4) + e * 2));
+          const Bf8 v = load8(reinterpret_cast<const bf16 *>(dy + o + ((h ^ ((o >> 7) & 1)) << 4)));
+#pragma unroll
+          for (int e = 0; e < 8; ++e) bsum[e] += v.v[e];
         }
       }
       __syncwarp();
@@ -1192,11 +1227,15 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b]))
                      : "memory");
     }
-    if (sum && co < a.cout_real) atomicAdd(&a.db[co], bsum);
+    if (mine) {
+#pragma unroll
+      for (int e = 0; e < 8; ++e) atomicAdd(&s_db[p * 8 + e], bsum[e]);
+    }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  if (a.db && blockIdx.y == 0 && nmine > 0 && tid < a.cout_real) atomicAdd(&a.db[tid], s_db[tid]);
   if (nmine > 0 && !*abort && warp < 2) {
     // TMEM lane 16 t + co (t = 0, 1, 2): dy shifted by t - 1 rows, output
     // channel 16 cc + co; unit j, column 16 g + e: dx = g - 1, input channel
@@ -2111,9 +2150,10 @@ int xf_launch(cmi_unet *u, const Slice &in, const bf16 *wpack, const float *bias
   a.nbuf = p.nbuf;
   a.wstages = p.wstages;
   a.kq = p.kq;
-  // resident weights: the MMA sequence unrolled for the common chunk counts
+  // resident weights or a stage per tap row: the MMA sequence unrolled for the
+  // common chunk counts
   auto kern = k_conv3_xf<KZ, 0>;
-  if (p.wstages == 9 && p.kq == a.nchunk) {
+  if (p.kq == a.nchunk) {
     if (a.nchunk == 1) kern = k_conv3_xf<KZ, 1>;
     if (a.nchunk == 2) kern = k_conv3_xf<KZ, 2>;
     if (a.nchunk == 3) kern = k_conv3_xf<KZ, 3>;
