@@ -404,19 +404,21 @@ struct WalkM {
     if (trace) *trace = lmin;
     const int stride[3] = {v.nyz, v.n[2], 1};
     int out = 0;
+    // branch-free: the lanes of a warp cross different axes, so per-axis
+    // branches would diverge; every axis reads its (clamped) next face and
+    // keeps it only when it crossed into a cell of the subgrid
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const bool cross = l[a] == lmin;
       pos[a] = cross ? face[a] : __dadd_rn(pos[a], __dmul_rn(lmin, d[a]));
-      if (cross) {
-        const bool up = d[a] > 0.;
-        idx[a] += up ? 1 : -1;
-        cell += up ? stride[a] : -stride[a];
-        if ((unsigned)idx[a] < (unsigned)v.n[a])
-          face[a] = v.faces[v.face_off[a] + idx[a] + (up ? 1 : 0)];
-        else
-          out |= 1 << a;
-      }
+      const bool up = d[a] > 0.;
+      const int di = cross ? (up ? 1 : -1) : 0;
+      idx[a] += di;
+      cell += di * stride[a];
+      const bool inside = (unsigned)idx[a] < (unsigned)v.n[a];
+      const double next = v.faces[v.face_off[a] + min(max(idx[a], 0), v.n[a] - 1) + (up ? 1 : 0)];
+      face[a] = (cross && inside) ? next : face[a];
+      out |= (cross && !inside) ? (1 << a) : 0;
     }
     return out ? kExited : kRun;
   }
