@@ -49,7 +49,7 @@ BYTES_PER_CROSSING = 32  # FP64 n, x read + J read-modify-write per crossing
 # of `bench.py --steps 3 --warmup 3` (k_walk32: FP32 walk, k_walkm: mixed walk);
 # other workloads and settings were not captured and report null.
 WALK_TRAFFIC_PER_LAUNCH = {("lognormal128", 1e7, "fp32"): 94.02e6,
-                           ("lognormal128", 1e7, "mixed"): 187.48e6}
+                           ("lognormal128", 1e7, "mixed"): 207.79e6}
 METRIC = "cell-crossings/s"  # plus time to converged x_H, warm start vs plain ("warm_start")
 UNIT = "crossings/s"
 DESCRIPTIONS = {
