@@ -424,7 +424,13 @@ int cmi_dust_run(cmi_context *ctx, int32_t instance, uint64_t num_photon, uint64
  * after another in the engine's cube order (index (ix * ny + iy) * nz + iz):
  * features [batch][cells][3], targets and predictions [batch][cells].  Grid
  * sides must be multiples of 32.  Calls are synchronous.  Errors: the codes
- * above, message in cmi_unet_last_error_string(). */
+ * above, message in cmi_unet_last_error_string().
+ *
+ * The network runs on a stream of its own.  The first forward, gradient or
+ * training call for a (batch, grid) shape records the pass's kernel launches
+ * in CUDA graphs on that stream (and the first call of all, the weight
+ * packing) and later calls replay them; a new shape re-records.  Make such
+ * first calls while no global-mode stream capture is active in the process. */
 typedef struct cmi_unet cmi_unet;
 typedef struct {
   int32_t channels[3];  /* c1 (<= 16), c2, c3 (<= 64); default 12, 24, 48 (~2e5 parameters) */
