@@ -1021,6 +1021,9 @@ struct WgradTcArgs {
   float *db;                 // [cout_real] bias gradient: sum of dy (accumulated; may be null)
   const int *ci_map;         // storage input channel -> real input channel or -1
   int cin_real, cout_real;
+  // the CTAs' sums, reduced into dw by k_wgrad_reduce (null: FP32 atomics into
+  // dw): [group][cta][unit][dx tap g][accumulator row < 48][16 input channels]
+  float *part;
   uint32_t *err;
 };
 constexpr int kWgradWarps = 6;            // 0-3 bias sums and readout, 4 loads, 5 MMAs
@@ -1236,6 +1239,19 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
   __syncthreads();
   tc_fence_after();
   if (a.db && blockIdx.y == 0 && nmine > 0 && tid < a.cout_real) atomicAdd(&a.db[tid], s_db[tid]);
+  if (a.part && warp < 2 && (nmine == 0 || *abort)) {
+    // no tiles: this CTA's share of the sums is zero
+    const int lrow = warp * 32 + lane;
+    if (lrow < 48)
+      for (int j = 0; j < nunit; ++j)
+        for (int g = 0; g < 3; ++g) {
+          float4 *dst = reinterpret_cast<float4 *>(
+              a.part + ((((size_t)blockIdx.y * gridDim.x + blockIdx.x) * a.units_per_cta + j) * 3 +
+                        g) * 768 + lrow * 16);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) dst[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+  }
   if (nmine > 0 && !*abort && warp < 2) {
     // TMEM lane 16 t + co (t = 0, 1, 2): dy shifted by t - 1 rows, output
     // channel 16 cc + co; unit j, column 16 g + e: dx = g - 1, input channel
@@ -1259,7 +1275,18 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
               "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (t < 3 && co < a.cout_real) {
+        if (a.part) {
+          // raw sums, 64 bytes per row: reduced over the CTAs by k_wgrad_reduce
+          if (t < 3) {
+            float4 *dst = reinterpret_cast<float4 *>(
+                a.part + ((((size_t)blockIdx.y * gridDim.x + blockIdx.x) * a.units_per_cta + j) *
+                              3 + g) * 768 + lrow * 16);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                   __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+          }
+        } else if (t < 3 && co < a.cout_real) {
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
             const int ci = a.ci_map[c * 16 + e];
@@ -1277,6 +1304,47 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(a.tmem_cols)
                  : "memory");
+  }
+}
+
+// dw += the sum over a group's CTAs of their raw weight-gradient sums.  A block
+// takes 32 consecutive (unit, dx tap g, accumulator row, input channel)
+// outputs, its 8 warps a slice of the CTAs each (coalesced 128-byte reads); the
+// slices are added in shared memory and every dw element has one writer.
+constexpr int kReduceSlices = 8;
+__global__ void __launch_bounds__(32 * kReduceSlices) k_wgrad_reduce(const float *part, int ctas,
+                                                                     int units, WgradTcArgs a) {
+  __shared__ float s_sum[kReduceSlices][32];
+  const int lane = threadIdx.x & 31, sl = threadIdx.x >> 5;
+  const int ncc = a.cout / 16, per_dz = ncc * a.nchunk;
+  const long long n = (long long)units * 3 * 768;
+  const size_t step = (size_t)a.units_per_cta * 3 * 768;
+  for (long long b0 = (long long)blockIdx.x * 32; b0 < n; b0 += (long long)gridDim.x * 32) {
+    const long long i = b0 + lane;
+    const int e = (int)(i & 15), lrow = (int)((i >> 4) % 48);
+    const long long ug = i / 768;
+    const int g = (int)(ug % 3), u = (int)(ug / 3);
+    float sum = 0.f;
+    if (i < n) {
+      const int y = u / a.units_per_cta, j = u - y * a.units_per_cta;
+      const float *src =
+          part + (((size_t)y * ctas * a.units_per_cta + j) * 3 + g) * 768 + lrow * 16 + e;
+#pragma unroll 4
+      for (int x = sl; x < ctas; x += kReduceSlices) sum += src[(size_t)x * step];
+    }
+    s_sum[sl][lane] = sum;
+    __syncthreads();
+    if (sl == 0 && i < n) {
+      float tot = 0.f;
+#pragma unroll
+      for (int k = 0; k < kReduceSlices; ++k) tot += s_sum[k][lane];
+      const int t = lrow >> 4, dz = u / per_dz, rem = u - dz * per_dz;
+      const int cc = rem / a.nchunk, c = rem - cc * a.nchunk;
+      const int co = cc * 16 + (lrow & 15), ci = a.ci_map[c * 16 + e];
+      const int tap = dz * 9 + (2 - t) * 3 + g;
+      if (co < a.cout_real && ci >= 0) a.dw[((size_t)co * 27 + tap) * a.cin_real + ci] += tot;
+    }
+    __syncthreads();
   }
 }
 
@@ -1785,6 +1853,8 @@ struct cmi_unet {
   long long adam_t = 0;
   uint32_t *d_err = nullptr;
   float *d_loss = nullptr;
+  float *wg_part = nullptr;    // the weight gradient's per-CTA sums (64 MB, allocated once)
+  size_t wg_part_floats = 0;
   // activation buffers for the current (batch, dims)
   int batch = 0, dims[3] = {0, 0, 0};
   std::vector<void *> bufs;
@@ -1886,7 +1956,18 @@ Chans chans(const cmi_unet *u) {
   return c;
 }
 
+// the weight gradient's per-CTA scratch: allocated once, before any graph that
+// names it is recorded (every launch configuration of this network fits)
+int ensure_wg_part(cmi_unet *u) {
+  if (u->wg_part) return CMI_OK;
+  const size_t n = (size_t)16 << 20;
+  UN_CUDA(cudaMalloc(&u->wg_part, n * sizeof(float)));
+  u->wg_part_floats = n;
+  return CMI_OK;
+}
+
 int ensure_buffers(cmi_unet *u, int batch, const int dims[3]) {
+  UN_TRY(ensure_wg_part(u));
   if (u->batch == batch && u->dims[0] == dims[0] && u->dims[1] == dims[1] &&
       u->dims[2] == dims[2])
     return CMI_OK;
@@ -2287,8 +2368,19 @@ int wgrad_t(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, float *db,
   UN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int tiles = batch * (dims[0] / T::kTX) * (dims[1] / T::kTY) * (dims[2] / T::kTZ);
   const int ctas = std::max(1, std::min(tiles, per_sm * sms / groups));
+  // the CTAs' sums go through the network's scratch and one reduction pass when
+  // they fit (without it every CTA adds its sums to the same dw entries with
+  // FP32 atomics, which costs more than the scratch round trip)
+  const size_t part_floats = (size_t)groups * ctas * a.units_per_cta * 3 * 768;
+  if (u->wg_part && part_floats <= u->wg_part_floats) a.part = u->wg_part;
   k_conv3_wgrad_tc<TY><<<dim3(ctas, groups), kWgradThreads, smem, u->stream>>>(xm, dym, a);
   UN_CUDA(cudaGetLastError());
+  if (a.part) {
+    const long long outs = (long long)units * 3 * 768;
+    k_wgrad_reduce<<<(int)std::min<long long>((outs + 31) / 32, 8192), 32 * kReduceSlices, 0,
+                     u->stream>>>(a.part, ctas, units, a);
+    UN_CUDA(cudaGetLastError());
+  }
   return CMI_OK;
 }
 
@@ -2670,6 +2762,7 @@ int cmi_unet_destroy(cmi_unet *u) {
   cudaFree(u->v);
   cudaFree(u->d_err);
   cudaFree(u->d_loss);
+  cudaFree(u->wg_part);
   cudaFree(u->d_src);
   cudaFree(u->d_nrel);
   cudaFree(u->d_ncoarse);
@@ -2977,6 +3070,7 @@ int cmi_unet_conv3_wgrad(cmi_unet *u, const void *x, int32_t cin, const void *dy
   UN_CUDA(cudaMalloc(&map, sizeof(int) * cin));
   UN_CUDA(cudaMemcpy(map, id.data(), sizeof(int) * cin, cudaMemcpyHostToDevice));
   UN_CUDA(cudaMemsetAsync(dw, 0, sizeof(float) * 27 * cin * cout, u->stream));
+  UN_TRY(ensure_wg_part(u));
   const int rc = wgrad(u, Slice{(bf16 *)x, cin, 0, cin}, Slice{(bf16 *)dy, cout, 0, cout}, dw,
                        nullptr, map, cin, cout, batch, d);
   const cudaError_t e = cudaStreamSynchronize(u->stream);
