@@ -1030,6 +1030,7 @@ constexpr int kWgradWarps = 6;            // 0-3 bias sums and readout, 4 loads,
 constexpr int kWgradThreads = kWgradWarps * 32;
 constexpr int kUnitCols = 48;             // one unit's accumulator: taps dx = -1, 0, 1 x 16
 constexpr int kWgradUnitsPerCta = 10;     // 10 x 48 <= 512 TMEM columns
+constexpr int kWgMaxBufs = 4;             // tile buffers in flight at most
 
 // dy of a tile with one extra voxel row on either side in y, 16 channels per
 // 32-byte voxel row (32-byte swizzle), x fastest:
@@ -1091,9 +1092,9 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
   const size_t dybytes = (size_t)ncc * D::kChunkBytes;
   const size_t hbytes = (size_t)a.nchunk * T::kChunkBytes;
   const size_t bufbytes = dybytes + hbytes;  // [dy chunks][input halo] per buffer
-  uint64_t *full = reinterpret_cast<uint64_t *>(sm + a.bar_off);  // [2]
-  uint64_t *empty = full + 2;    // [2]: the MMAs done (1) and dy summed (4 warps)
-  uint64_t *drain = empty + 2;   // the MMAs in flight when the CTA ends
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + a.bar_off);  // [kWgMaxBufs]
+  uint64_t *empty = full + kWgMaxBufs;  // the MMAs done (1) and dy summed (4 warps)
+  uint64_t *drain = empty + kWgMaxBufs;  // the MMAs in flight when the CTA ends
   uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
   __shared__ float s_db[128];  // the CTA's bias-gradient sums
   __shared__ int s_abort;
@@ -1108,7 +1109,7 @@ __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
   for (int c = tid; c < 128; c += kWgradThreads) s_db[c] = 0.f;
   if (tid == 0) {
     s_abort = 0;
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < a.nbuf; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 5);
     }
@@ -2350,7 +2351,16 @@ int wgrad_t(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, float *db,
     return (std::max(nbuf * buf, reach_end) + 127) / 128 * 128;
   };
   auto smem_for = [&](int nbuf) { return 1024 + bars_at(nbuf) + 128; };
-  a.nbuf = smem_for(2) <= (size_t)optin ? 2 : 1;
+  // as many tile buffers (up to kWgMaxBufs) as leave room for the CTAs per SM
+  // that the tensor memory allows
+  const int tmem_ctas = std::max(1, (int)(512 / a.tmem_cols));
+  const size_t cap = std::min<size_t>((size_t)optin, 233472 / tmem_ctas - 2048);
+  a.nbuf = smem_for(2) <= (size_t)optin ? 2 : 1;  // fewer CTAs per SM before one buffer
+  for (int nb = kWgMaxBufs; nb > 2; --nb)
+    if (smem_for(nb) <= cap) {
+      a.nbuf = nb;
+      break;
+    }
   a.bar_off = (int)bars_at(a.nbuf);
   const size_t smem = smem_for(a.nbuf);
   if (smem > (size_t)optin)
