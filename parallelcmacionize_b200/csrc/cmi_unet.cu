@@ -1576,11 +1576,10 @@ struct PackArgs {
 // k_conv3_xf serves convolutions whose three x taps fit one MMA's N (<= 256)
 __host__ __device__ inline bool conv_xf(int npad) { return 3 * npad <= 256; }
 
-__global__ void k_pack(PackArgs a) {
+// element i of a packed operand
+__device__ __forceinline__ void pack_element(const PackArgs &a, long long i) {
   const int nchunk = a.kchan / 16;
-  const long long n = 27LL * nchunk * a.rows * 16;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  {
     long long g = i;
     const int e = (int)(g % 16);
     g /= 16;
@@ -1608,6 +1607,34 @@ __global__ void k_pack(PackArgs a) {
       const int half = (e >> 3) ^ ((r >> 2) & 1);
       a.out[(step * a.rows + r) * 16 + half * 8 + (e & 7)] = __float2bfloat16_rn(v);
     }
+  }
+}
+
+__global__ void k_pack(PackArgs a) {
+  const long long n = 27LL * (a.kchan / 16) * a.rows * 16;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    pack_element(a, i);
+}
+
+// every layer's packing in one launch: job k covers elements [begin, begin +
+// count) of the whole; a job with a bias destination pads the FP32 bias to
+// npad (zero beyond cout), the others pack one operand
+struct PackJob {
+  PackArgs a;
+  long long begin, count;
+  const float *bias;  // null: a weight job
+  float *bias_pad;
+};
+__global__ void k_pack_all(const PackJob *jobs, int njobs, long long total) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    int k = 0;
+    while (k + 1 < njobs && jobs[k + 1].begin <= i) ++k;
+    const PackJob &jb = jobs[k];
+    const long long r = i - jb.begin;
+    if (jb.bias) jb.bias_pad[r] = r < jb.a.cout ? jb.bias[r] : 0.f;
+    else pack_element(jb.a, r);
   }
 }
 
@@ -1881,6 +1908,9 @@ struct cmi_unet {
   // calls: the forward layers and the backward layers (for the current
   // activation buffers), the weight packing (for the life of the network)
   cudaGraphExec_t gx_fwd = nullptr, gx_bwd = nullptr, gx_pack = nullptr;
+  void *d_jobs = nullptr;  // the packing jobs of every layer (k_pack_all)
+  int njobs = 0;
+  long long jobs_total = 0;
 };
 
 namespace cmiu {
@@ -2411,31 +2441,55 @@ int wgrad(cmi_unet *u, const Slice &x, const Slice &dy, float *dw, float *db, co
                   : wgrad_t<8>(u, x, dy, dw, db, ci_map, cin_real, cout_real, batch, dims);
 }
 
-// packs every layer's weights from the FP32 master parameters
-int pack_launches(cmi_unet *u) {
+// the packing jobs of every layer: forward operand, input-gradient operand
+// (flipped, transposed), bias padded to npad; uploaded once
+int make_pack_jobs(cmi_unet *u) {
+  std::vector<PackJob> jobs;
+  long long at = 0;
   for (Layer &l : u->L) {
-    PackArgs a{};
-    a.w = u->p + l.w_off;
-    a.cout = l.cout;
-    a.cin_real = l.cin_real;
-    a.ci_of_storage = l.d_map;
-    a.out = l.wf;
-    a.rows = l.npad;
-    a.kchan = l.kin;
-    a.flip = 0;
-    a.xf = conv_xf(a.rows);
-    k_pack<<<grid_for(27LL * l.kin * l.npad), 256, 0, u->stream>>>(a);
-    a.out = l.wd;
-    a.rows = l.kin;
-    a.kchan = l.npad;
-    a.flip = 1;
-    a.xf = conv_xf(a.rows);
-    k_pack<<<grid_for(27LL * l.kin * l.npad), 256, 0, u->stream>>>(a);
-    // bias padded to npad (zero beyond cout)
-    UN_CUDA(cudaMemsetAsync(l.bias_pad, 0, sizeof(float) * l.npad, u->stream));
-    UN_CUDA(cudaMemcpyAsync(l.bias_pad, u->p + l.b_off, sizeof(float) * l.cout,
-                            cudaMemcpyDeviceToDevice, u->stream));
+    PackJob j{};
+    j.a.w = u->p + l.w_off;
+    j.a.cout = l.cout;
+    j.a.cin_real = l.cin_real;
+    j.a.ci_of_storage = l.d_map;
+    j.a.out = l.wf;
+    j.a.rows = l.npad;
+    j.a.kchan = l.kin;
+    j.a.flip = 0;
+    j.a.xf = conv_xf(j.a.rows);
+    j.begin = at;
+    j.count = 27LL * l.kin * l.npad;
+    at += j.count;
+    jobs.push_back(j);
+    j.a.out = l.wd;
+    j.a.rows = l.kin;
+    j.a.kchan = l.npad;
+    j.a.flip = 1;
+    j.a.xf = conv_xf(j.a.rows);
+    j.begin = at;
+    at += j.count;
+    jobs.push_back(j);
+    PackJob b{};
+    b.a.cout = l.cout;
+    b.bias = u->p + l.b_off;
+    b.bias_pad = l.bias_pad;
+    b.begin = at;
+    b.count = l.npad;
+    at += b.count;
+    jobs.push_back(b);
   }
+  UN_CUDA(cudaMalloc(&u->d_jobs, sizeof(PackJob) * jobs.size()));
+  UN_CUDA(cudaMemcpy(u->d_jobs, jobs.data(), sizeof(PackJob) * jobs.size(),
+                     cudaMemcpyHostToDevice));
+  u->njobs = (int)jobs.size();
+  u->jobs_total = at;
+  return CMI_OK;
+}
+
+// packs every layer's weights from the FP32 master parameters (one launch)
+int pack_launches(cmi_unet *u) {
+  k_pack_all<<<grid_for(u->jobs_total), 256, 0, u->stream>>>(
+      static_cast<const PackJob *>(u->d_jobs), u->njobs, u->jobs_total);
   UN_CUDA(cudaGetLastError());
   return CMI_OK;
 }
@@ -2750,6 +2804,7 @@ int cmi_unet_create(const cmi_unet_config *cfg, cmi_unet **out) {
     if ((rc = dev_zero_alloc(&p, sizeof(float) * l.npad))) return bail(rc);
     l.bias_pad = static_cast<float *>(p);
   }
+  if ((rc = make_pack_jobs(u))) return bail(rc);
   *out = u;
   return CMI_OK;
 }
@@ -2760,6 +2815,7 @@ int cmi_unet_destroy(cmi_unet *u) {
   if (u->stream) cudaStreamSynchronize(u->stream);
   free_bufs(u);
   drop_graph(&u->gx_pack);
+  cudaFree(u->d_jobs);
   for (Layer &l : u->L) {
     cudaFree(l.wf);
     cudaFree(l.wd);
