@@ -1358,17 +1358,16 @@ __global__ void __launch_bounds__(32 * kReduceSlices) k_wgrad_reduce(const float
 __global__ void k_pool2(const bf16 *in, int ictot, int ic0, bf16 *out, int octot, int oc0, int c,
                         int batch, int X, int Y, int Z) {
   const int Xo = X / 2, Yo = Y / 2, Zo = Z / 2, c8 = c / 8;
-  const long long n = (long long)batch * Xo * Yo * Zo * c8;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c8;
+  const unsigned n = (unsigned)batch * Xo * Yo * Zo * c8;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned g = i / c8;
     const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % Xo);
     g /= Xo;
     const int y = (int)(g % Yo);
     g /= Yo;
     const int z = (int)(g % Zo);
-    const long long s = g / Zo;
+    const unsigned s = g / Zo;
     Bf8 acc{};
     for (int d = 0; d < 8; ++d) {
       const size_t q = (((size_t)s * Z + 2 * z + (d >> 2)) * Y + 2 * y + ((d >> 1) & 1)) * X +
@@ -1390,18 +1389,17 @@ __global__ void k_pool2_bwd_add(const bf16 *dout, int octot, int oc0, bf16 *din,
                                 int ic0, int c, int batch, int X, int Y, int Z, const bf16 *gy,
                                 int gctot, int gc0, float slope) {
   const int c8 = c / 8;
-  const long long n = (long long)batch * X * Y * Z * c8;
+  const unsigned n = (unsigned)batch * X * Y * Z * c8;
   const int Xo = X / 2, Yo = Y / 2, Zo = Z / 2;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c8;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned g = i / c8;
     const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % X);
     g /= X;
     const int y = (int)(g % Y);
     g /= Y;
     const int z = (int)(g % Z);
-    const long long s = g / Z;
+    const unsigned s = g / Z;
     const size_t o = (((size_t)s * Zo + z / 2) * Yo + y / 2) * Xo + x / 2;
     const size_t q = (((size_t)s * Z + z) * Y + y) * X + x;
     Bf8 d = load8(din + q * ictot + ic0 + k);
@@ -1417,17 +1415,16 @@ __global__ void k_pool2_bwd_add(const bf16 *dout, int octot, int oc0, bf16 *din,
 __global__ void k_up2(const bf16 *in, int ictot, int ic0, bf16 *out, int octot, int oc0, int c,
                       int batch, int X, int Y, int Z) {
   const int X2 = 2 * X, Y2 = 2 * Y, Z2 = 2 * Z, c8 = c / 8;
-  const long long n = (long long)batch * X2 * Y2 * Z2 * c8;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c8;
+  const unsigned n = (unsigned)batch * X2 * Y2 * Z2 * c8;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned g = i / c8;
     const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % X2);
     g /= X2;
     const int y = (int)(g % Y2);
     g /= Y2;
     const int z = (int)(g % Z2);
-    const long long s = g / Z2;
+    const unsigned s = g / Z2;
     const size_t q = (((size_t)s * Z + z / 2) * Y + y / 2) * X + x / 2;
     const size_t o = (((size_t)s * Z2 + z) * Y2 + y) * X2 + x;
     *reinterpret_cast<uint4 *>(out + o * octot + oc0 + k) =
@@ -1441,18 +1438,17 @@ __global__ void k_up2_bwd(const bf16 *din, int ictot, int ic0, bf16 *dout, int o
                           int c, int batch, int X, int Y, int Z, const bf16 *gy, int gctot,
                           int gc0, float slope) {
   const int c8 = c / 8;
-  const long long n = (long long)batch * X * Y * Z * c8;
+  const unsigned n = (unsigned)batch * X * Y * Z * c8;
   const int X2 = 2 * X, Y2 = 2 * Y;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long g = i / c8;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned g = i / c8;
     const int k = (int)(i - g * c8) * 8;
     const int x = (int)(g % X);
     g /= X;
     const int y = (int)(g % Y);
     g /= Y;
     const int z = (int)(g % Z);
-    const long long s = g / Z;
+    const unsigned s = g / Z;
     Bf8 acc{};
     for (int d = 0; d < 8; ++d) {
       const size_t q = (((size_t)s * 2 * Z + 2 * z + (d >> 2)) * Y2 + 2 * y + ((d >> 1) & 1)) *
@@ -1653,12 +1649,16 @@ __global__ void k_adam(float *p, const float *g, float *m, float *v, long long n
 }
 
 // input features -> the 16-channel BF16 input tensor (channels 3..15 zero)
-__global__ void k_input(const float *f, bf16 *x, long long nvox) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvox * 16;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long v = i / 16;
-    const int k = (int)(i % 16);
-    x[i] = __float2bfloat16_rn(k < kFeatures ? f[v * kFeatures + k] : 0.f);
+__global__ void k_input(const float *f, bf16 *x, unsigned nvox) {
+  // one voxel (16 storage channels, 32 bytes) per thread
+  for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += gridDim.x * blockDim.x) {
+    __align__(16) bf16 o[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      o[k] = __float2bfloat16_rn(k < kFeatures ? f[(size_t)v * kFeatures + k] : 0.f);
+    uint4 *d = reinterpret_cast<uint4 *>(x + (size_t)v * 16);
+    d[0] = reinterpret_cast<const uint4 *>(o)[0];
+    d[1] = reinterpret_cast<const uint4 *>(o)[1];
   }
 }
 
@@ -2507,6 +2507,13 @@ int check_dims(const int dims[3]) {
   return CMI_OK;
 }
 
+// the elementwise kernels index 16-byte groups with 32-bit arithmetic
+int check_size(int batch, const int dims[3]) {
+  if ((long long)batch * dims[0] * dims[1] * dims[2] * 16 > (1LL << 31))
+    return fail(CMI_ERR_NOT_SUPPORTED, "batch x cells must be at most 2^27 (134217728)");
+  return CMI_OK;
+}
+
 // forward pass from u->X0; writes u->pred
 int forward_layers(cmi_unet *u, int batch, const int d1[3]) {
   const Chans c = chans(u);
@@ -2669,11 +2676,12 @@ int check_err(cmi_unet *u) {
 int load_input(cmi_unet *u, const float *in, int batch, const int dims[3]) {
   UN_TRY(check_dims(dims));
   if (batch <= 0) return fail(CMI_ERR_INVALID_ARGUMENT, "batch must be > 0");
+  UN_TRY(check_size(batch, dims));
   UN_CUDA(cudaSetDevice(u->device));
   UN_TRY(ensure_buffers(u, batch, dims));
   if (!u->packed) UN_TRY(pack_all(u));
   const long long v1 = (long long)batch * dims[0] * dims[1] * dims[2];
-  k_input<<<grid_for(v1 * 16), 256, 0, u->stream>>>(in, u->X0, v1);
+  k_input<<<grid_for(v1), 256, 0, u->stream>>>(in, u->X0, (unsigned)v1);
   UN_CUDA(cudaGetLastError());
   return CMI_OK;
 }
