@@ -423,7 +423,8 @@ int cmi_dust_run(cmi_context *ctx, int32_t instance, uint64_t num_photon, uint64
  * Tensors handed to the network live in device memory, FP32, one sample
  * after another in the engine's cube order (index (ix * ny + iy) * nz + iz):
  * features [batch][cells][3], targets and predictions [batch][cells].  Grid
- * sides must be multiples of 32.  Calls are synchronous.  Errors: the codes
+ * sides must be multiples of 32, and batch x cells at most 2^27 (134217728;
+ * CMI_ERR_NOT_SUPPORTED beyond).  Calls are synchronous.  Errors: the codes
  * above, message in cmi_unet_last_error_string().
  *
  * The network runs on a stream of its own.  The first forward, gradient or
