@@ -648,12 +648,13 @@ struct XTile {
   }
 };
 
-// The same persistent, warp-specialised structure as k_conv3_tc: warp 4 loads
-// (the weights once when resident, else kq K steps per ring stage; each tile's
-// input box into a ring of up to kMaxInBufs buffers: a tile's MMAs are short,
-// so several input boxes are in flight to cover the load latency), warp 5
-// issues the MMAs, warps 0-3 combine, add bias, apply the activation or the
-// derivative gate and store.
+// A persistent, warp-specialised CTA like k_conv3_tc's, with kXfEpiWarps + 2
+// warps: warp kXfEpiWarps loads (the weights once when resident, else kq K
+// steps per ring stage; each tile's input box into a ring of up to kMaxInBufs
+// buffers, as many as shared memory holds), warp kXfEpiWarps + 1 issues the
+// MMAs (the whole warp, one elected lane issuing), warps 0 .. kXfEpiWarps - 1
+// combine the x taps, add bias, apply the activation or the derivative gate
+// and store.
 constexpr int kMaxInBufs = 8;
 constexpr int kXfEpiWarps = 8;                      // two per quarter of the TMEM lanes
 constexpr int kXfThreads = (kXfEpiWarps + 2) * 32;  // + loads + MMAs
@@ -1076,9 +1077,11 @@ struct DyTile {
 // misses at the grid's edge pair with input outside the grid (zero).
 // A CTA owns a group of units (one TMEM accumulator each) and the tiles
 // blockIdx.x, + gridDim.x, ...: warp 4 loads tile i's dy and input halo into
-// buffer i % nbuf by TMA; warp 5 issues the MMAs; warps 0-3 sum dy for the bias
-// gradient (the CTAs of the first group) and at the end read the TMEM lanes and
-// add them to dW.
+// buffer i % nbuf (up to kWgMaxBufs) by TMA; warp 5 issues the MMAs (the whole
+// warp, one elected lane issuing); warps 0-3 sum dy for the bias gradient (the
+// CTAs of the first group) and at the end read the TMEM lanes: into the
+// scratch rows that k_wgrad_reduce sums over the CTAs, or with FP32 atomics
+// straight into dW when no scratch is given.
 template <int TY>
 __global__ void __launch_bounds__(kWgradThreads) k_conv3_wgrad_tc(
     const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dymap,
