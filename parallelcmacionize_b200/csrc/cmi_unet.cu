@@ -971,16 +971,22 @@ __global__ void __launch_bounds__(kXfThreads, 1) k_conv3_xf(const __grid_constan
                 gy[e + 8] = g1.v[e];
               }
             }
-            __align__(16) bf16 o[16];
+            // leaky ReLU as max(x, slope x): the same for 0 <= slope < 1
+            __align__(16) __nv_bfloat162 o[8];
 #pragma unroll
-            for (int e = 0; e < 16; ++e) {
-              float x = f[e] + sbias[j + e];
-              if (a.act) x = x > 0.f ? x : x * a.slope;
-              if (a.gate) {
-                x = __bfloat162float(__float2bfloat16_rn(x));
-                if (!(gy[e] > 0.f)) x *= a.slope;
+            for (int e = 0; e < 16; e += 2) {
+              float x0 = f[e] + sbias[j + e], x1 = f[e + 1] + sbias[j + e + 1];
+              if (a.act) {
+                x0 = fmaxf(x0, x0 * a.slope);
+                x1 = fmaxf(x1, x1 * a.slope);
               }
-              o[e] = __float2bfloat16_rn(x);
+              if (a.gate) {
+                x0 = __bfloat162float(__float2bfloat16_rn(x0));
+                x1 = __bfloat162float(__float2bfloat16_rn(x1));
+                if (!(gy[e] > 0.f)) x0 *= a.slope;
+                if (!(gy[e + 1] > 0.f)) x1 *= a.slope;
+              }
+              o[e / 2] = __floats2bfloat162_rn(x0, x1);
             }
             uint4 *d4 = reinterpret_cast<uint4 *>(dst);
             d4[0] = reinterpret_cast<const uint4 *>(o)[0];
