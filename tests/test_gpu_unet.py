@@ -228,3 +228,35 @@ def test_training_reduces_loss():
     # FP32 atomics in the weight gradient make runs differ slightly: a threefold
     # drop in 60 steps (typically 14x; at 3e-3 the loss spikes now and then)
     assert np.mean(losses[-5:]) < 0.33 * losses[0], losses[::10]
+
+
+def test_pass_graphs_follow_the_shape():
+    """Each pass is recorded as a CUDA graph on its first call for a (batch,
+    grid) shape and replayed after; a new shape records again.  Forward passes
+    at batch 1, 2, then 1 again (the first sample identical) and at another
+    grid side give the same predictions as a fresh network would, bit for bit
+    (the forward pass has no atomics), and gradients taken after other shapes
+    match the first ones."""
+    rng = np.random.default_rng(21)
+    f1 = torch.from_numpy(rng.normal(size=(1, 32 ** 3, 3)).astype(np.float32)).cuda()
+    f2 = torch.cat([f1, torch.from_numpy(rng.normal(size=(1, 32 ** 3, 3)).astype(np.float32)).cuda()])
+    f64 = torch.from_numpy(rng.normal(size=(1, 64 ** 3, 3)).astype(np.float32)).cuda()
+    t1 = torch.from_numpy(rng.normal(size=(1, 32 ** 3)).astype(np.float32)).cuda()
+    with UNet(seed=3) as fresh:
+        ref1 = fresh.forward(f1, (32, 32, 32)).cpu().numpy()
+        ref64 = fresh.forward(f64, (64, 64, 64)).cpu().numpy()
+    with UNet(seed=3) as n:
+        a = n.forward(f1, (32, 32, 32)).cpu().numpy()
+        b = n.forward(f2, (32, 32, 32)).cpu().numpy()
+        c = n.forward(f64, (64, 64, 64)).cpu().numpy()
+        d = n.forward(f1, (32, 32, 32)).cpu().numpy()
+        loss0, g0 = n.gradients(f1, t1, (32, 32, 32))
+        n.forward(f2, (32, 32, 32))
+        loss1, g1 = n.gradients(f1, t1, (32, 32, 32))
+    np.testing.assert_array_equal(a, ref1)
+    np.testing.assert_array_equal(b[:1], ref1)
+    np.testing.assert_array_equal(c, ref64)
+    np.testing.assert_array_equal(d, ref1)
+    assert loss1 == pytest.approx(loss0, rel=1e-6)
+    # FP32 atomics in the bias and head gradients: same sums in another order
+    np.testing.assert_allclose(g1, g0, rtol=1e-4, atol=1e-7 * np.abs(g0).max())
